@@ -1,0 +1,182 @@
+/*
+ * pigfem_b200.h -- C ABI of the B200 IGFEM assembly/solve path.
+ *
+ * Plain pointers and sizes only; every call returns an int status (0 = ok),
+ * the way the reference's PETSc-touching calls return PetscErrorCode, and
+ * none of them aborts.  A failed call leaves a message retrievable with
+ * pg_last_error().  Streams are passed as opaque handles (cudaStream_t cast to
+ * void*); NULL selects the context's own stream.
+ *
+ * Reference interfaces replaced (PIGFEM 4.6.1, paths relative to PIGFEM4.6.1/):
+ *   Problem::init (IGFEM detection/enrichment, shape cache)  src/Problem.cpp:105-316
+ *   Problem::setup / Solver::setup (DOFs, sparsity)          src/Problem.cpp:319-338, src/Solver.cpp:40-49,365-441
+ *   Assembler::assemble_linear                               src/Assembler.cpp:48-89 (include/Assembler.h:41)
+ *   Assembler::assemble_nonlinear                            src/Assembler.cpp:208-303 (include/Assembler.h:42-44)
+ *   Assembler::assemble_new_load_step                        src/Assembler.cpp:554-663 (include/Assembler.h:51)
+ *   PETScLinearKSPSolver::solve                              src/SolverLinear.cpp:91-162
+ *   SolverNonlinear::solve / nonlinearStep (SNES Newton)     src/SolverNonlinear.cpp:111-397, src/SolverNonlinearSNES.cpp:182-241
+ *   InternalVars::copy_data_in (ISV commit)                  src/InternalVars.cpp:65-85
+ */
+#ifndef PIGFEM_B200_H
+#define PIGFEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define PG_OK 0
+#define PG_ERR_ARG 1          /* invalid argument */
+#define PG_ERR_MESH 2         /* IGFEM preprocessing failed (the reference would err_message + exit) */
+#define PG_ERR_CUDA 3         /* CUDA runtime error */
+#define PG_ERR_NOT_CONVERGED 4/* iteration budget exhausted (Krylov or Newton) */
+#define PG_ERR_BREAKDOWN 5    /* Krylov breakdown (e.g. indefinite operator under CG) */
+#define PG_ERR_STATE 6        /* call out of order (e.g. solve before assemble) */
+#define PG_ERR_LIMIT 7        /* size beyond a documented maximum */
+
+typedef struct pg_mesh pg_mesh;  /* host IGFEM mesh (opaque) */
+typedef struct pg_ctx pg_ctx;    /* device state for one mesh (opaque) */
+
+/* Cohesive laws.  PG_COH_OP: Ortiz-Pandolfi exponential law with linear
+ * unloading and viscous regularisation, params {sigma_c, delta_c, beta,
+ * viscosity} (src/Material_OPCohesive.cpp:38-253, the reference's active law).
+ * PG_COH_BILINEAR: bilinear penalty law, params {sigma_c, G_c, K_p, beta}. */
+#define PG_COH_OP 0
+#define PG_COH_BILINEAR 1
+
+/* RVE description: the inputs the reference's driver builds through
+ * Mesh::generate_mesh(TRI3, ...), Mesh::add_inclusion(Circle_Inclusion),
+ * Mesh::add_material and BoundaryObject::set_dirichlet_bcs_from_nodeset
+ * (Tests/Main.cpp:256, 310-450). */
+typedef struct pg_rve_desc {
+    int32_t nx, ny;                 /* structured TRI3 mesh, 2*nx*ny triangles */
+    double x0, x1, y0, y1;          /* domain */
+    int32_t n_inclusions;
+    const double* inc_cx;           /* n_inclusions each */
+    const double* inc_cy;
+    const double* inc_r;
+    const int32_t* inc_mat;         /* material index of each inclusion */
+    int32_t n_materials;
+    const double* mat_E;            /* linear elastic isotropic (material_lei.cpp:52-97) */
+    const double* mat_nu;
+    int32_t matrix_mat;             /* material of the background */
+    int32_t plane_strain;           /* 1: plane strain (only mode of the configs), 0: plane stress */
+    int32_t cohesive;               /* 1: inclusion interfaces carry cohesive elements */
+    int32_t coh_law;                /* PG_COH_OP or PG_COH_BILINEAR */
+    double coh_params[4];
+    double strain;                  /* prescribed x-displacement of the right edge = (x1-x0)*strain */
+} pg_rve_desc;
+
+typedef struct pg_mesh_info {
+    int32_t n_nodes;                /* regular + enrichment nodes */
+    int32_t n_regular_nodes;
+    int32_t n_enrichment_nodes;
+    int32_t n_elements;
+    int32_t n_cut_elements;
+    int32_t n_cohesive_qp;
+    int32_t n_dof;                  /* 2 * n_nodes */
+    int32_t n_free_dof;
+    int32_t n_blocks;               /* 2x2 blocks in the stiffness pattern (nnz = 4 * n_blocks) */
+    int32_t n_moved_nodes;          /* nodes moved off an inclusion surface */
+} pg_mesh_info;
+
+/* ---- host preprocessing (Problem::init IGFEM steps + Problem::setup DOFs/sparsity) ---- */
+int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out);
+int pg_mesh_info_get(const pg_mesh* m, pg_mesh_info* info);
+/* Copies out host arrays (any pointer may be NULL):
+ *   xy[2*n_nodes] node coordinates (x, y interleaved; regular then enrichment nodes)
+ *   conn[3*n_elements], elem_mat[n_elements], elem_cut[n_elements] (-1 or cut index)
+ *   ref_dof[n_dof]: the reference's global DOF number (free-first, DofObject.cpp:241-386) of
+ *                   this library's DOF 2*node+d
+ *   fixed[n_dof] (1 = Dirichlet), ubar[n_dof] prescribed values at load factor 1 */
+int pg_mesh_export(const pg_mesh* m, double* xy, int32_t* conn, int32_t* elem_mat, int32_t* elem_cut,
+                   int32_t* ref_dof, uint8_t* fixed, double* ubar);
+/* Cut-element description: template id, enrichment node of each slot (12 per element, -1 unused),
+ * child materials (4 per element, -1 unused), first cohesive quadrature point. */
+int pg_mesh_export_cut(const pg_mesh* m, int32_t* cut_elem, int32_t* cut_tmpl, int32_t* cut_enr,
+                       int32_t* cut_child_mat, int32_t* cut_coh_qp0);
+/* 2x2-block CSR pattern: row_ptr[n_nodes+1], col[n_blocks]. */
+int pg_mesh_export_pattern(const pg_mesh* m, int32_t* row_ptr, int32_t* col);
+/* Cut templates: per template 80 int32 (see DESIGN.md table layout); returns count in *n. */
+int pg_template_table(int32_t* out, int32_t* n);
+void pg_mesh_destroy(pg_mesh* m);
+
+/* ---- device context (Solver::setup: matrix/vector preallocation on the GPU) ---- */
+int pg_ctx_create(const pg_mesh* m, int32_t device, pg_ctx** out);
+void pg_ctx_destroy(pg_ctx* c);
+int pg_ctx_sync(pg_ctx* c);
+
+/* Assembler::assemble_linear: K = sum over active elements (uncut: 4-point rule,
+ * cut: sub-element quadrature with enrichment functions) in FP64, written into the
+ * context's 2x2-block CSR (values 4 per block, row-major). */
+int pg_assemble_linear(pg_ctx* c, void* stream);
+/* Same call for callers that hold the inputs and want K on the host: copies node
+ * coordinates xy_host[2*n_nodes] (nullable) host->device, assembles, copies the
+ * 4*n_blocks FP64 values to k_host (nullable).  The drop-in for assemble_linear
+ * filling a host PETSc matrix. */
+int pg_assemble_linear_host(pg_ctx* c, const double* xy_host, double* k_host);
+/* Assembler::assemble_nonlinear: residual vector f_int (want_f) and tangent K (want_K) at
+ * the displacement U_dev[n_dof] (device pointer; NULL: the context's solution), load
+ * step dt, writing trial cohesive state.  The trial state restarts from the committed
+ * state on every call, as InternalVars::copy_data does (Assembler.cpp:235). */
+int pg_assemble_nonlinear(pg_ctx* c, const double* U_dev, double dt, int32_t want_f, int32_t want_K, void* stream);
+/* Assembler::assemble_new_load_step: prescribed values = t_frac * ubar. */
+int pg_new_load_step(pg_ctx* c, double t_frac);
+/* InternalVars::copy_data_in: committed cohesive state <- trial state. */
+int pg_commit_isv(pg_ctx* c);
+
+/* Device pointers to the context's arrays (valid until pg_ctx_destroy). */
+int pg_ctx_device_arrays(pg_ctx* c, double** K, double** U, double** F_int, double** isv_committed,
+                         double** isv_trial);
+
+/* ---- solvers ---- */
+#define PG_KRYLOV_CG 0
+#define PG_KRYLOV_GMRES 1
+#define PG_PREC_JACOBI 0
+#define PG_PREC_BLOCK_JACOBI 1
+#define PG_PREC_NONE 2
+#define PG_PRECISION_FP64 0        /* plain FP64 Krylov */
+#define PG_PRECISION_MIXED 1       /* FP32 SpMV/dot Krylov + FP64 iterative refinement */
+
+typedef struct pg_solver_cfg {
+    int32_t krylov;                 /* PG_KRYLOV_* */
+    int32_t precond;                /* PG_PREC_* */
+    int32_t precision;              /* PG_PRECISION_* */
+    double rtol;                    /* relative residual target of the linear solve (FP64 residual) */
+    int32_t max_iter;               /* Krylov iteration budget (total over refinements) */
+    double inner_rtol;              /* mixed: FP32 inner solve tolerance per refinement */
+    int32_t max_refine;             /* mixed: refinement budget */
+    int32_t gmres_restart;
+    int32_t check_every;            /* host residual check cadence (iterations per captured graph) */
+} pg_solver_cfg;
+
+typedef struct pg_solve_stats {
+    int32_t iterations;             /* Krylov iterations */
+    int32_t refinements;            /* FP64 refinement steps (mixed) */
+    double rel_residual;            /* final FP64 ||r_f|| / ||r_f(0)|| */
+    double seconds;                 /* device time of the solve */
+    int32_t newton_iterations;
+    int32_t status;
+} pg_solve_stats;
+
+void pg_solver_cfg_default(pg_solver_cfg* cfg);
+/* PETScLinearKSPSolver::solve: prescribed U_p = ubar (load factor 1), rhs = -K_fp U_p,
+ * K_ff U_f = rhs, reactions F_p = K_pf U_f + K_pp U_p.  Assembles K first if needed. */
+int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg, pg_solve_stats* stats);
+
+/* ---- host copies (tests, parity, output) ---- */
+int pg_get_matrix(pg_ctx* c, double* vals_host);         /* 4*n_blocks */
+int pg_get_vector(pg_ctx* c, int32_t which, double* out); /* which: 0=U, 1=F_int, 2=reaction/residual work */
+int pg_set_vector(pg_ctx* c, int32_t which, const double* in);
+int pg_get_isv(pg_ctx* c, int32_t committed, double* out);/* n_cohesive_qp delta_max values */
+
+const char* pg_last_error(void);
+const char* pg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIGFEM_B200_H */

@@ -1,0 +1,145 @@
+"""ctypes binding of libpigfem_b200.so (the C ABI in include/pigfem_b200.h).
+
+The library is loaded from the package directory.  There is no CPU fallback:
+if the shared object is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpigfem_b200.so")
+
+PG_OK = 0
+PG_ERR_ARG = 1
+PG_ERR_MESH = 2
+PG_ERR_CUDA = 3
+PG_ERR_NOT_CONVERGED = 4
+PG_ERR_BREAKDOWN = 5
+PG_ERR_STATE = 6
+PG_ERR_LIMIT = 7
+
+PG_COH_OP = 0
+PG_COH_BILINEAR = 1
+PG_KRYLOV_CG = 0
+PG_KRYLOV_GMRES = 1
+PG_PREC_JACOBI = 0
+PG_PREC_BLOCK_JACOBI = 1
+PG_PREC_NONE = 2
+PG_PRECISION_FP64 = 0
+PG_PRECISION_MIXED = 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class RveDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+        ("n_inclusions", C.c_int32),
+        ("inc_cx", _dp), ("inc_cy", _dp), ("inc_r", _dp), ("inc_mat", _ip),
+        ("n_materials", C.c_int32), ("mat_E", _dp), ("mat_nu", _dp),
+        ("matrix_mat", C.c_int32), ("plane_strain", C.c_int32), ("cohesive", C.c_int32),
+        ("coh_law", C.c_int32), ("coh_params", C.c_double * 4), ("strain", C.c_double),
+    ]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "n_nodes", "n_regular_nodes", "n_enrichment_nodes", "n_elements", "n_cut_elements",
+        "n_cohesive_qp", "n_dof", "n_free_dof", "n_blocks", "n_moved_nodes")]
+
+
+class SolverCfg(C.Structure):
+    _fields_ = [
+        ("krylov", C.c_int32), ("precond", C.c_int32), ("precision", C.c_int32),
+        ("rtol", C.c_double), ("max_iter", C.c_int32), ("inner_rtol", C.c_double),
+        ("max_refine", C.c_int32), ("gmres_restart", C.c_int32), ("check_every", C.c_int32),
+    ]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32), ("refinements", C.c_int32), ("rel_residual", C.c_double),
+        ("seconds", C.c_double), ("newton_iterations", C.c_int32), ("status", C.c_int32),
+    ]
+
+
+class PgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[pg status {code}] {msg}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m pigfem_assignment_b200.build` "
+            "(this package has no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    v = C.c_void_p
+    sig = {
+        "pg_mesh_build": ([C.POINTER(RveDesc), C.POINTER(v)], C.c_int),
+        "pg_mesh_info_get": ([v, C.POINTER(MeshInfo)], C.c_int),
+        "pg_mesh_export": ([v, _dp, _ip, _ip, _ip, _ip, _u8p, _dp], C.c_int),
+        "pg_mesh_export_cut": ([v, _ip, _ip, _ip, _ip, _ip], C.c_int),
+        "pg_mesh_export_pattern": ([v, _ip, _ip], C.c_int),
+        "pg_template_table": ([_ip, _ip], C.c_int),
+        "pg_mesh_destroy": ([v], None),
+        "pg_ctx_create": ([v, C.c_int32, C.POINTER(v)], C.c_int),
+        "pg_ctx_destroy": ([v], None),
+        "pg_ctx_sync": ([v], C.c_int),
+        "pg_assemble_linear": ([v, v], C.c_int),
+        "pg_assemble_linear_host": ([v, _dp, _dp], C.c_int),
+        "pg_assemble_nonlinear": ([v, _dp, C.c_double, C.c_int32, C.c_int32, v], C.c_int),
+        "pg_new_load_step": ([v, C.c_double], C.c_int),
+        "pg_commit_isv": ([v], C.c_int),
+        "pg_ctx_device_arrays": ([v, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp),
+                                  C.POINTER(_dp)], C.c_int),
+        "pg_solver_cfg_default": ([C.POINTER(SolverCfg)], None),
+        "pg_solve_linear": ([v, C.POINTER(SolverCfg), C.POINTER(SolveStats)], C.c_int),
+        "pg_get_matrix": ([v, _dp], C.c_int),
+        "pg_get_vector": ([v, C.c_int32, _dp], C.c_int),
+        "pg_set_vector": ([v, C.c_int32, _dp], C.c_int),
+        "pg_get_isv": ([v, C.c_int32, _dp], C.c_int),
+        "pg_last_error": ([], C.c_char_p),
+        "pg_version": ([], C.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+# every extern "C" symbol include/pigfem_b200.h declares
+DECLARED_SYMBOLS = (
+    "pg_mesh_build", "pg_mesh_info_get", "pg_mesh_export", "pg_mesh_export_cut", "pg_mesh_export_pattern",
+    "pg_template_table", "pg_mesh_destroy", "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_sync",
+    "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
+    "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",
+    "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_last_error", "pg_version",
+)
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != PG_OK:
+        msg = lib.pg_last_error()
+        raise PgError(rc, (what + ": " if what else "") + (msg.decode() if msg else ""))
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def u8ptr(a):
+    return a.ctypes.data_as(_u8p)

@@ -1,0 +1,553 @@
+// FP64 element integration and assembly kernels for sm_100a.
+//
+// Reference computation (PIGFEM 4.6.1):
+//   Assembler::assemble_linear / assemble_elem_linear     src/Assembler.cpp:48-185
+//   Assembler::assemble_nonlinear / assemble_elem_nonlinear src/Assembler.cpp:208-528
+//   AssemblerLinearElasticity::KernelLinear               src/AssemblerLinearElasticity.cpp:24-38
+//   AssemblerSmallStrainNonlinearStructural::Kernel*      src/AssemblerSmallStrainNonlinear.cpp:28-91
+//   ProblemUtilities::SmallStrainKFast / Fast / IntForce  src/Utilities.cpp:196-408
+//   ProblemUtilities::cohesiveDeltaFast / KFast / Force   src/Utilities.cpp:465-531
+//   Mesh::store_shape_functions (recomputed, not cached)  src/Mesh.cpp:1443-1605
+//   CohesiveElem::compute_rotation_general                src/CohesiveElem.cpp:207-238
+//   OPCohesiveMaterial::Constitutive                      src/Material_OPCohesive.cpp:38-388
+//
+// Two kernels produce K (2x2-block CSR over nodes, FP64) and f_int:
+//   k_assemble_rows: one thread per node row.  The row's blocks are summed
+//     from the uncut triangles around the node (constant-strain B^T D B,
+//     the 4-point rule's weights sum to 1/2) in a per-CTA shared-memory tile
+//     that mirrors the CTA's contiguous slice of the value array, then leave
+//     with one cp.async.bulk store: each value is written to HBM exactly once,
+//     fully coalesced.  Rows of enrichment nodes are zero-filled here.
+//   k_assemble_cut: one warp per cut element.  Lanes own node-pair blocks of
+//     the (3+n_enr)^2 element matrix, integrate every child (tri3/quad4/
+//     polygon) and cohesive sub-element, and add into the rows with FP64
+//     atomics (a few percent of elements).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "pg_internal.cuh"
+
+namespace pgb {
+
+__constant__ DevTemplate c_tmpl[32];
+__constant__ DevChildQuad c_quad[kNumChildTypes];
+
+void upload_tables() {
+    static bool done_dev[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done_dev[dev]) return;
+    DevTemplate t[32] = {};
+    const int nt = n_cut_templates();
+    for (int i = 0; i < nt; ++i) {
+        const CutTemplate& T = cut_template(i);
+        t[i].n_enr = T.n_enr;
+        t[i].n_child = T.n_child;
+        t[i].n_coh = T.n_coh;
+        for (int c = 0; c < T.n_child; ++c) {
+            t[i].child_n[c] = T.child_n[c];
+            t[i].child_type[c] = T.child_n[c] == 3 ? kChildTri3 : T.child_n[c] == 4 ? kChildQuad4
+                                 : T.child_n[c] == 5 ? kChildPoly5 : kChildPoly6;
+            for (int k = 0; k < T.child_n[c]; ++k) t[i].child_nodes[c][k] = T.child_nodes[c][k];
+        }
+        for (int c = 0; c < T.n_coh; ++c)
+            for (int k = 0; k < 4; ++k) t[i].coh_nodes[c][k] = T.coh_nodes[c][k];
+    }
+    DevChildQuad q[kNumChildTypes] = {};
+    for (int ty = 0; ty < kNumChildTypes; ++ty) {
+        const ChildQuadrature& Q = child_quadrature(ty);
+        q[ty].nq = Q.nq;
+        q[ty].nn = Q.nn;
+        for (int i = 0; i < Q.nq; ++i) q[ty].w[i] = Q.w[i];
+        for (size_t i = 0; i < Q.N.size(); ++i) q[ty].N[i] = Q.N[i];
+        for (size_t i = 0; i < Q.dN.size(); ++i) q[ty].dN[i] = Q.dN[i];
+    }
+    cudaMemcpyToSymbol(c_tmpl, t, sizeof(t));
+    cudaMemcpyToSymbol(c_quad, q, sizeof(q));
+    if (dev >= 0 && dev < 64) done_dev[dev] = true;
+}
+
+// ---------------------------------------------------------------------------
+// Row kernel
+// ---------------------------------------------------------------------------
+constexpr int kRowThreads = 128;
+constexpr int kRowRegCols = 16;           // columns kept in registers for the slot search
+constexpr int kRowTileBlocks = 1536;      // shared tile capacity (48 KB)
+
+struct RowArgs {
+    int n_nodes, n_reg;
+    const int* __restrict__ row_ptr;
+    const int* __restrict__ col;
+    const int* __restrict__ ne_ptr;
+    const int* __restrict__ ne_list;
+    const int4* __restrict__ elem4;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ dmat;
+    double* K;
+    double* f;
+    int want_K, want_f;
+};
+
+__device__ __forceinline__ void bulk_store_smem_to_global(double* gdst, const double* ssrc, unsigned bytes) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst), "r"(saddr), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kRowThreads) k_assemble_rows(RowArgs a) {
+    extern __shared__ __align__(128) double sK[];
+    const int node0 = blockIdx.x * kRowThreads;
+    const int node_end = min(node0 + kRowThreads, a.n_nodes);
+    const int node = node0 + (int)threadIdx.x;
+    const int seg0 = a.row_ptr[node0];
+    const int seg1 = a.row_ptr[node_end];
+    const int nseg = seg1 - seg0;
+    const bool tile = a.want_K && nseg <= kRowTileBlocks;
+    if (tile) {
+        double2* s2 = reinterpret_cast<double2*>(sK);
+        for (int i = threadIdx.x; i < 2 * nseg; i += kRowThreads) s2[i] = make_double2(0.0, 0.0);
+        __syncthreads();
+    }
+    double fx = 0.0, fy = 0.0;
+    if (node < node_end) {
+        const int r0 = a.row_ptr[node];
+        const int r1 = a.row_ptr[node + 1];
+        const int deg = r1 - r0;
+        double* dst = tile ? sK + 4 * (r0 - seg0) : a.K + 4 * (size_t)r0;
+        if (a.want_K && !tile)
+            for (int i = 0; i < 4 * deg; ++i) dst[i] = 0.0;
+        if (node < a.n_reg) {
+            int cols[kRowRegCols];
+#pragma unroll
+            for (int q = 0; q < kRowRegCols; ++q) cols[q] = (q < deg) ? a.col[r0 + q] : -1;
+            const int k0 = a.ne_ptr[node], k1 = a.ne_ptr[node + 1];
+            for (int k = k0; k < k1; ++k) {
+                const int packed = a.ne_list[k];
+                const int e = packed >> 2;
+                const int v = packed & 3;
+                const int4 el = a.elem4[e];
+                const int nid[3] = {el.x, el.y, el.z};
+                const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
+                const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
+                // J = det(dx/dr) of the affine map; grad N_k = (b_k, c_k) / J
+                const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+                const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
+                const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
+                const double d11 = a.dmat[3 * el.w + 0], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
+                // sum_qp J w_qp = J/2; (b/J)(b/J) J/2 = b b * (0.5/J)
+                const double s = 0.5 / J;
+                const double ba = b[v] * s, ca = c[v] * s;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const double bb = b[t], cb = c[t];
+                    const double k00 = ba * d11 * bb + ca * d33 * cb;
+                    const double k01 = ba * d12 * cb + ca * d33 * bb;
+                    const double k10 = ca * d12 * bb + ba * d33 * cb;
+                    const double k11 = ca * d11 * cb + ba * d33 * bb;
+                    const int nt = nid[t];
+                    if (a.want_f) {
+                        const double ux = a.u[2 * nt], uy = a.u[2 * nt + 1];
+                        fx += k00 * ux + k01 * uy;
+                        fy += k10 * ux + k11 * uy;
+                    }
+                    if (a.want_K) {
+                        int sl = -1;
+#pragma unroll
+                        for (int q = 0; q < kRowRegCols; ++q) sl = (cols[q] == nt) ? q : sl;
+                        if (sl < 0)
+                            for (int q = kRowRegCols; q < deg; ++q)
+                                if (a.col[r0 + q] == nt) { sl = q; break; }
+                        double* d = dst + 4 * sl;
+                        d[0] += k00;
+                        d[1] += k01;
+                        d[2] += k10;
+                        d[3] += k11;
+                    }
+                }
+            }
+        }
+        if (a.want_f) {
+            a.f[2 * node] = fx;
+            a.f[2 * node + 1] = fy;
+        }
+    }
+    if (tile) {
+        // make the generic-proxy shared writes visible to the async (bulk copy) proxy
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) bulk_store_smem_to_global(a.K + 4 * (size_t)seg0, sK, (unsigned)nseg * 32u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cohesive laws (FP64)
+// ---------------------------------------------------------------------------
+// delta = {tangential, normal} opening in the element's (t, n) frame; may be
+// modified by the tiny-opening guard of OPCohesiveNUMaterial::getDeltaEff
+// (Material_OPCohesiveNU.cpp:45-63).
+__device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, double delta[2], double t[2],
+                             double D[2][2], double& dmax_trial) {
+    const double beta2 = (L.law == PG_COH_OP) ? L.p[2] * L.p[2] : L.p[3] * L.p[3];
+    double d0 = delta[0], d1 = delta[1];
+    if (d0 * d0 + d1 * d1 < 1e-40) { d0 = 1e-20; d1 = 1e-20; }
+    delta[0] = d0;
+    delta[1] = d1;
+    if (L.law == PG_COH_OP) {
+        const double sc = L.p[0], dc = L.p[1], visc = L.p[3];
+        const double de = sqrt(d1 * d1 + beta2 * (d0 * d0));
+        double T, dT;
+        dmax_trial = dmax_c;
+        if (de >= dmax_c || de < 0.0) {
+            const double ex = exp(1.0 - de / dc);
+            T = sc * (de / dc) * ex + visc / sc * (de - dmax_c) / dt / dc;
+            dT = (sc / dc) * (1.0 - de / dc) * ex + visc / sc / dt / dc;
+            dmax_trial = de;
+        } else {
+            const double Tm = sc * (dmax_c / dc) * exp(1.0 - dmax_c / dc);
+            T = Tm * (de / dmax_c);
+            dT = Tm / dmax_c;
+        }
+        const double br0 = beta2 * d0;
+        const double br1 = beta2 * d1 + (1.0 - beta2) * d1;
+        const double s = T / de;
+        t[0] = s * br0;
+        t[1] = s * br1;
+        const double dd0 = beta2 * d0 / de, dd1 = d1 / de;
+        const double aa = dT * de - T;
+        const double de2 = de * de;
+        D[0][0] = br0 * aa * (dd0 / de2) + s * beta2;
+        D[0][1] = br0 * aa * (dd1 / de2);
+        D[1][0] = br1 * aa * (dd0 / de2);
+        D[1][1] = br1 * aa * (dd1 / de2) + s * (beta2 + (1.0 - beta2));
+        return;
+    }
+    // bilinear penalty law with a compression penalty on the normal opening
+    const double sc = L.p[0], Gc = L.p[1], Kp = L.p[2];
+    const double dlt0 = sc / Kp, dltf = 2.0 * Gc / sc;
+    const double dn = d1 > 0.0 ? d1 : 0.0;
+    const double de = sqrt(dn * dn + beta2 * (d0 * d0)) + 1e-300;
+    auto env = [&](double dd, double& T, double& dT) {
+        if (dd <= dlt0) { T = Kp * dd; dT = Kp; }
+        else if (dd < dltf) { T = sc * (dltf - dd) / (dltf - dlt0); dT = -sc / (dltf - dlt0); }
+        else { T = 0.0; dT = 0.0; }
+    };
+    double T, dT;
+    dmax_trial = dmax_c;
+    if (de >= dmax_c) {
+        env(de, T, dT);
+        dmax_trial = de;
+    } else {
+        double Tm, dTm;
+        env(dmax_c, Tm, dTm);
+        T = Tm * (de / dmax_c);
+        dT = Tm / dmax_c;
+    }
+    const double s = T / de;
+    const double aa = dT * de - T;
+    const double de2 = de * de;
+    const double br0 = beta2 * d0, br1 = dn;
+    const double dd0 = beta2 * d0 / de, dd1 = dn / de;
+    t[0] = s * br0;
+    D[0][0] = br0 * aa * (dd0 / de2) + s * beta2;
+    if (d1 >= 0.0) {
+        t[1] = s * br1;
+        D[0][1] = br0 * aa * (dd1 / de2);
+        D[1][0] = br1 * aa * (dd0 / de2);
+        D[1][1] = br1 * aa * (dd1 / de2) + s;
+    } else {
+        t[1] = Kp * d1;
+        D[0][1] = 0.0;
+        D[1][0] = 0.0;
+        D[1][1] = Kp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cut-element kernel
+// ---------------------------------------------------------------------------
+constexpr int kCutWarps = 4;
+constexpr int kCutPairsPerLane = 8;       // (3 + kMaxEnr)^2 = 225 <= 8 * 32
+
+struct CutArgs {
+    int n_cut;
+    const int* __restrict__ cut_elem;
+    const int* __restrict__ cut_tmpl;
+    const int* __restrict__ cut_enr;
+    const int* __restrict__ cut_child_mat;
+    const int* __restrict__ cut_coh_qp0;
+    const int* __restrict__ cut_slot_ptr;
+    const int* __restrict__ cut_slot;
+    const int4* __restrict__ elem4;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ dmat;
+    const double* __restrict__ isv_c;
+    double* isv_t;
+    DevCohLaw coh;
+    double dt;
+    double* K;
+    double* f;
+    int want_K, want_f;
+};
+
+__global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
+    __shared__ double sX[kCutWarps][kMaxElemNodes], sY[kCutWarps][kMaxElemNodes];
+    __shared__ double sU[kCutWarps][2 * kMaxElemNodes];
+    __shared__ double sGx[kCutWarps][kMaxElemNodes], sGy[kCutWarps][kMaxElemNodes];
+    __shared__ int sL[kCutWarps][kMaxElemNodes];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int ci = blockIdx.x * kCutWarps + w;
+    if (ci >= a.n_cut) return;
+    const DevTemplate& T = c_tmpl[a.cut_tmpl[ci]];
+    const int nl = 3 + T.n_enr;
+    const int e = a.cut_elem[ci];
+    const int4 el = a.elem4[e];
+    if (lane < nl) {
+        const int node = lane < 3 ? (lane == 0 ? el.x : (lane == 1 ? el.y : el.z)) : a.cut_enr[ci * kMaxEnr + lane - 3];
+        sL[w][lane] = node;
+        sX[w][lane] = a.x[node];
+        sY[w][lane] = a.y[node];
+        if (a.want_f || T.n_coh > 0) {
+            sU[w][2 * lane] = a.u[2 * node];
+            sU[w][2 * lane + 1] = a.u[2 * node + 1];
+        }
+    }
+    __syncwarp();
+    // parent (Tri3) gradients are constant over the element
+    const double PX0 = sX[w][0], PX1 = sX[w][1], PX2 = sX[w][2];
+    const double PY0 = sY[w][0], PY1 = sY[w][1], PY2 = sY[w][2];
+    const double PJ = (PX1 - PX0) * (PY2 - PY0) - (PX2 - PX0) * (PY1 - PY0);
+    const double pbx[3] = {(PY1 - PY2) / PJ, (PY2 - PY0) / PJ, (PY0 - PY1) / PJ};
+    const double pby[3] = {(PX2 - PX1) / PJ, (PX0 - PX2) / PJ, (PX1 - PX0) / PJ};
+
+    double acc[kCutPairsPerLane][4];
+#pragma unroll
+    for (int k = 0; k < kCutPairsPerLane; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
+    const int npairs = nl * nl;
+
+    for (int ch = 0; ch < T.n_child; ++ch) {
+        const int nc = T.child_n[ch];
+        const DevChildQuad& Q = c_quad[T.child_type[ch]];
+        const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
+        const double d11 = a.dmat[3 * mat], d12 = a.dmat[3 * mat + 1], d33 = a.dmat[3 * mat + 2];
+        for (int q = 0; q < Q.nq; ++q) {
+            double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+            for (int k = 0; k < nc; ++k) {
+                const int ln = T.child_nodes[ch][k];
+                const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+                J00 += dr * sX[w][ln];
+                J01 += dr * sY[w][ln];
+                J10 += ds * sX[w][ln];
+                J11 += ds * sY[w][ln];
+            }
+            const double det = J00 * J11 - J01 * J10;
+            const double wgt = det * Q.w[q];
+            // gradients of the element's local functions at this point
+            if (lane < nl) {
+                double gx = 0.0, gy = 0.0;
+                if (lane < 3) {
+                    gx = pbx[lane];
+                    gy = pby[lane];
+                } else {
+                    for (int k = 0; k < nc; ++k)
+                        if (T.child_nodes[ch][k] == lane) {
+                            const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+                            gx = (J11 * dr - J01 * ds) / det;
+                            gy = (-J10 * dr + J00 * ds) / det;
+                        }
+                }
+                sGx[w][lane] = gx;
+                sGy[w][lane] = gy;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < kCutPairsPerLane; ++k) {
+                const int p = lane + 32 * k;
+                if (p < npairs) {
+                    const int ia = p / nl, ib = p - ia * nl;
+                    const double ba = sGx[w][ia] * wgt, ca = sGy[w][ia] * wgt;
+                    const double bb = sGx[w][ib], cb = sGy[w][ib];
+                    acc[k][0] += ba * d11 * bb + ca * d33 * cb;
+                    acc[k][1] += ba * d12 * cb + ca * d33 * bb;
+                    acc[k][2] += ca * d12 * bb + ba * d33 * cb;
+                    acc[k][3] += ca * d11 * cb + ba * d33 * bb;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    // bulk internal force f_a = sum_b K_ab u_b
+    if (a.want_f) {
+#pragma unroll
+        for (int k = 0; k < kCutPairsPerLane; ++k) {
+            const int p = lane + 32 * k;
+            if (p < npairs) {
+                const int ia = p / nl, ib = p - ia * nl;
+                const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
+                const double fx = acc[k][0] * ux + acc[k][1] * uy;
+                const double fy = acc[k][2] * ux + acc[k][3] * uy;
+                atomicAdd(&a.f[2 * sL[w][ia]], fx);
+                atomicAdd(&a.f[2 * sL[w][ia] + 1], fy);
+            }
+        }
+    }
+    // cohesive sub-elements: two Gauss points each (CohEdge2, w = 1)
+    for (int ce = 0; ce < T.n_coh; ++ce) {
+        const int c0 = T.coh_nodes[ce][0], c1 = T.coh_nodes[ce][1], c2 = T.coh_nodes[ce][2], c3 = T.coh_nodes[ce][3];
+        const double jx = 0.5 * (sX[w][c1] - sX[w][c0]);
+        const double jy = 0.5 * (sY[w][c1] - sY[w][c0]);
+        const double mag = sqrt(jx * jx + jy * jy);
+        const double nx = -jy, ny = jx;
+        const double dA = sqrt(nx * nx + ny * ny);
+        const double R[2][2] = {{jx / mag, jy / mag}, {nx / dA, ny / dA}};
+        for (int q = 0; q < 2; ++q) {
+            const double xi = q == 0 ? -0.57735026918962576450914878050196 : 0.57735026918962576450914878050196;
+            const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+            double dg[2];
+            for (int d = 0; d < 2; ++d)
+                dg[d] = N0 * (sU[w][2 * c2 + d] - sU[w][2 * c0 + d]) + N1 * (sU[w][2 * c3 + d] - sU[w][2 * c1 + d]);
+            double dl[2] = {R[0][0] * dg[0] + R[0][1] * dg[1], R[1][0] * dg[0] + R[1][1] * dg[1]};
+            const int qp = a.cut_coh_qp0[ci] + 2 * ce + q;
+            const double dmax_c = a.isv_c[qp];
+            double tr[2], Dc[2][2], dmax_t;
+            cohesive_law(a.coh, a.dt, dmax_c, dl, tr, Dc, dmax_t);
+            if (lane == 0) a.isv_t[qp] = dmax_t;
+            // R^T D R and R^T t
+            double RDR[2][2];
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j) {
+                    double s = 0.0;
+                    for (int k1 = 0; k1 < 2; ++k1)
+                        for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
+                    RDR[i][j] = s;
+                }
+            const double tR[2] = {R[0][0] * tr[0] + R[1][0] * tr[1], R[0][1] * tr[0] + R[1][1] * tr[1]};
+            const double wgt = dA * 1.0;
+            const int cn[4] = {c0, c1, c2, c3};
+            const double Nn[2] = {N0, N1};
+            if (a.want_K) {
+#pragma unroll
+                for (int k = 0; k < kCutPairsPerLane; ++k) {
+                    const int p = lane + 32 * k;
+                    if (p < npairs) {
+                        const int ia = p / nl, ib = p - ia * nl;
+                        int i = -1, j = -1;
+                        for (int m = 0; m < 4; ++m) {
+                            if (cn[m] == ia) i = m;
+                            if (cn[m] == ib) j = m;
+                        }
+                        if (i >= 0 && j >= 0) {
+                            const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
+                            const double v = wgt * sgn * Nn[i & 1] * Nn[j & 1];
+                            acc[k][0] += v * RDR[0][0];
+                            acc[k][1] += v * RDR[0][1];
+                            acc[k][2] += v * RDR[1][0];
+                            acc[k][3] += v * RDR[1][1];
+                        }
+                    }
+                }
+            }
+            if (a.want_f && lane < 4) {
+                const double sgn = lane < 2 ? -1.0 : 1.0;
+                const double nn = Nn[lane & 1];
+                const int node = sL[w][cn[lane]];
+                atomicAdd(&a.f[2 * node], wgt * sgn * nn * tR[0]);
+                atomicAdd(&a.f[2 * node + 1], wgt * sgn * nn * tR[1]);
+            }
+        }
+    }
+    if (a.want_K) {
+        const int* slots = a.cut_slot + a.cut_slot_ptr[ci];
+#pragma unroll
+        for (int k = 0; k < kCutPairsPerLane; ++k) {
+            const int p = lane + 32 * k;
+            if (p < npairs) {
+                double* d = a.K + 4 * (size_t)slots[p];
+                atomicAdd(d + 0, acc[k][0]);
+                atomicAdd(d + 1, acc[k][1]);
+                atomicAdd(d + 2, acc[k][2]);
+                atomicAdd(d + 3, acc[k][3]);
+            }
+        }
+    }
+}
+
+__global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (; i < n / 2; i += stride) {
+        const double2 v = reinterpret_cast<const double2*>(a)[i];
+        reinterpret_cast<float2*>(b)[i] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
+    if (want_K && c.n_blocks > 0) {
+        // nothing to clear: the row kernel writes every value of K
+    }
+    RowArgs ra;
+    ra.n_nodes = c.n_nodes;
+    ra.n_reg = c.n_reg;
+    ra.row_ptr = c.row_ptr;
+    ra.col = c.col;
+    ra.ne_ptr = c.ne_ptr;
+    ra.ne_list = c.ne_list;
+    ra.elem4 = c.elem4;
+    ra.x = c.x;
+    ra.y = c.y;
+    ra.u = U;
+    ra.dmat = c.dmat;
+    ra.K = c.K;
+    ra.f = c.F;
+    ra.want_K = want_K;
+    ra.want_f = want_f;
+    const int rblocks = (c.n_nodes + kRowThreads - 1) / kRowThreads;
+    const size_t smem = want_K ? (size_t)kRowTileBlocks * 32 : 0;
+    if (rblocks > 0) k_assemble_rows<<<rblocks, kRowThreads, smem, s>>>(ra);
+    PG_CUDA(cudaGetLastError());
+    if (c.n_cut > 0) {
+        CutArgs ca;
+        ca.n_cut = c.n_cut;
+        ca.cut_elem = c.cut_elem;
+        ca.cut_tmpl = c.cut_tmpl;
+        ca.cut_enr = c.cut_enr;
+        ca.cut_child_mat = c.cut_child_mat;
+        ca.cut_coh_qp0 = c.cut_coh_qp0;
+        ca.cut_slot_ptr = c.cut_slot_ptr;
+        ca.cut_slot = c.cut_slot;
+        ca.elem4 = c.elem4;
+        ca.x = c.x;
+        ca.y = c.y;
+        ca.u = U;
+        ca.dmat = c.dmat;
+        ca.isv_c = c.isv_c;
+        ca.isv_t = c.isv_t;
+        ca.coh = c.coh;
+        ca.dt = dt;
+        ca.K = c.K;
+        ca.f = c.F;
+        ca.want_K = want_K;
+        ca.want_f = want_f;
+        const int cblocks = (c.n_cut + kCutWarps - 1) / kCutWarps;
+        k_assemble_cut<<<cblocks, 32 * kCutWarps, 0, s>>>(ca);
+        PG_CUDA(cudaGetLastError());
+    }
+    return PG_OK;
+}
+
+int launch_to_fp32(Ctx& c, cudaStream_t s) {
+    const size_t n = 4 * (size_t)c.n_blocks;
+    k_to_fp32<<<148 * 8, 256, 0, s>>>(c.K, c.Kf, n);
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+}  // namespace pgb

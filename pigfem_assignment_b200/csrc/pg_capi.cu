@@ -1,0 +1,476 @@
+// extern "C" entry points of libpigfem_b200 (declared in include/pigfem_b200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pg_internal.cuh"
+#include "pg_solve_kernels.cuh"
+
+namespace pgb {
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename T>
+int dev_upload(T** dst, const std::vector<T>& src) {
+    *dst = nullptr;
+    if (src.empty()) return PG_OK;
+    PG_CUDA(cudaMalloc((void**)dst, src.size() * sizeof(T)));
+    PG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PG_OK;
+}
+
+template <typename T>
+int dev_alloc(T** dst, size_t n) {
+    *dst = nullptr;
+    if (n == 0) n = 1;
+    PG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+    PG_CUDA(cudaMemset(*dst, 0, n * sizeof(T)));
+    return PG_OK;
+}
+
+void free_ctx(Ctx& c) {
+    void* ptrs[] = {c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.dmat, c.cut_elem, c.cut_tmpl,
+                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
+                    c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
+                    c.minvf, c.scal, c.iflags};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.h_scal) cudaFreeHost(c.h_scal);
+    if (c.h_iflags) cudaFreeHost(c.h_iflags);
+    if (c.ev0) cudaEventDestroy(c.ev0);
+    if (c.ev1) cudaEventDestroy(c.ev1);
+    if (c.stream) cudaStreamDestroy(c.stream);
+}
+
+// D = E/((1+nu)(1-2nu)) [[1-nu, nu, 0], [nu, 1-nu, 0], [0, 0, (1-2nu)/2]]
+// (material_lei.cpp:62-77; plane stress :78-84)
+void dmat_coeffs(const Material& m, bool plane_strain, double out[3]) {
+    if (plane_strain) {
+        const double coef = m.E / ((1.0 + m.nu) * (1.0 - 2.0 * m.nu));
+        out[0] = coef * (1.0 - m.nu);
+        out[1] = coef * (m.nu);
+        out[2] = coef * (1.0 - 2.0 * m.nu) / 2.0;
+    } else {
+        const double coef = m.E / (1.0 - m.nu * m.nu);
+        out[0] = coef;
+        out[1] = coef * (m.nu);
+        out[2] = coef * (1.0 - m.nu) / 2.0;
+    }
+}
+
+cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
+
+}  // namespace
+
+void set_error(const std::string& s) { g_last_error = s; }
+
+int cuda_fail(cudaError_t e, const char* where) {
+    g_last_error = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+    return PG_ERR_CUDA;
+}
+
+int ctx_create(const HostMesh& hm, int device, Ctx& c) {
+    c.device = device;
+    PG_CUDA(cudaSetDevice(device));
+    upload_tables();
+    PG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    PG_CUDA(cudaEventCreate(&c.ev0));
+    PG_CUDA(cudaEventCreate(&c.ev1));
+    c.hm = hm;
+    c.n_nodes = hm.n_nodes();
+    c.n_reg = hm.n_reg;
+    c.n_elem = hm.n_elem;
+    c.n_cut = hm.n_cut;
+    c.n_blocks = hm.n_blocks();
+    c.n_dof = hm.n_dof();
+    c.n_coh_qp = hm.n_coh_qp;
+    c.coh.law = hm.spec.coh.law;
+    for (int k = 0; k < 4; ++k) c.coh.p[k] = hm.spec.coh.p[k];
+
+    int rc;
+    if ((rc = dev_upload(&c.x, hm.x))) return rc;
+    if ((rc = dev_upload(&c.y, hm.y))) return rc;
+    std::vector<int4> e4(hm.n_elem);
+    for (int e = 0; e < hm.n_elem; ++e)
+        e4[e] = make_int4(hm.conn[3 * e], hm.conn[3 * e + 1], hm.conn[3 * e + 2], hm.elem_mat[e]);
+    if ((rc = dev_upload(&c.elem4, e4))) return rc;
+    if ((rc = dev_upload(&c.row_ptr, hm.row_ptr))) return rc;
+    if ((rc = dev_upload(&c.col, hm.col))) return rc;
+    if ((rc = dev_upload(&c.diag, hm.diag_slot))) return rc;
+    if ((rc = dev_upload(&c.ne_ptr, hm.ne_ptr))) return rc;
+    if ((rc = dev_upload(&c.ne_list, hm.ne_list))) return rc;
+    std::vector<double> dm(3 * hm.spec.materials.size());
+    for (size_t m = 0; m < hm.spec.materials.size(); ++m) dmat_coeffs(hm.spec.materials[m], hm.spec.plane_strain, &dm[3 * m]);
+    if ((rc = dev_upload(&c.dmat, dm))) return rc;
+    if (hm.n_cut > 0) {
+        if ((rc = dev_upload(&c.cut_elem, hm.cut_elem))) return rc;
+        if ((rc = dev_upload(&c.cut_tmpl, hm.cut_tmpl))) return rc;
+        if ((rc = dev_upload(&c.cut_enr, hm.cut_enr))) return rc;
+        if ((rc = dev_upload(&c.cut_child_mat, hm.cut_child_mat))) return rc;
+        if ((rc = dev_upload(&c.cut_coh_qp0, hm.cut_coh_qp0))) return rc;
+        // compact per-element slot tables: (3 + n_enr)^2 entries each
+        std::vector<int> sp(hm.n_cut + 1, 0), sl;
+        constexpr int S = kMaxElemNodes;
+        for (int ci = 0; ci < hm.n_cut; ++ci) {
+            const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
+            for (int a = 0; a < nl; ++a)
+                for (int b = 0; b < nl; ++b) sl.push_back(hm.cut_slot[(size_t)ci * S * S + a * S + b]);
+            sp[ci + 1] = (int)sl.size();
+        }
+        if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
+        if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
+    }
+    const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
+    if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;
+    if ((rc = dev_alloc(&c.Kf, 4 * nb))) return rc;
+    if ((rc = dev_upload(&c.fixed, hm.fixed))) return rc;
+    if ((rc = dev_upload(&c.ubar, hm.ubar))) return rc;
+    if ((rc = dev_alloc(&c.U, nd))) return rc;
+    if ((rc = dev_alloc(&c.F, nd))) return rc;
+    if ((rc = dev_alloc(&c.isv_c, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
+    if ((rc = dev_alloc(&c.isv_t, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
+    for (double** v : {&c.r, &c.z, &c.p, &c.q, &c.dx})
+        if ((rc = dev_alloc(v, nd))) return rc;
+    if ((rc = dev_alloc(&c.minv, 4 * nn))) return rc;
+    for (float** v : {&c.rf, &c.zf, &c.pf, &c.qf, &c.xf})
+        if ((rc = dev_alloc(v, nd))) return rc;
+    if ((rc = dev_alloc(&c.minvf, 4 * nn))) return rc;
+    if ((rc = dev_alloc(&c.scal, 64))) return rc;
+    if ((rc = dev_alloc(&c.iflags, 64))) return rc;
+    PG_CUDA(cudaMallocHost((void**)&c.h_scal, 64 * sizeof(double)));
+    PG_CUDA(cudaMallocHost((void**)&c.h_iflags, 64 * sizeof(int)));
+    // prescribed values at load factor 1
+    set_prescribed(c, 1.0, c.stream);
+    PG_CUDA(cudaStreamSynchronize(c.stream));
+    return PG_OK;
+}
+
+}  // namespace pgb
+
+namespace pgb {
+const char* last_error_cstr() { return g_last_error.c_str(); }
+}  // namespace pgb
+
+using namespace pgb;
+
+#define PG_GUARD_CTX(c)                                   \
+    do {                                                  \
+        if (!(c)) { set_error("null context"); return PG_ERR_ARG; } \
+        cudaSetDevice((c)->c.device);                     \
+    } while (0)
+
+extern "C" {
+
+const char* pg_last_error(void) { return last_error_cstr(); }
+const char* pg_version(void) { return "pigfem_b200 0.1 (sm_100a)"; }
+
+int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
+    if (!rve || !out) { set_error("pg_mesh_build: null argument"); return PG_ERR_ARG; }
+    *out = nullptr;
+    RveSpec spec;
+    spec.nx = rve->nx;
+    spec.ny = rve->ny;
+    spec.x0 = rve->x0;
+    spec.x1 = rve->x1;
+    spec.y0 = rve->y0;
+    spec.y1 = rve->y1;
+    if (rve->n_materials <= 0 || !rve->mat_E || !rve->mat_nu) { set_error("pg_mesh_build: no materials"); return PG_ERR_ARG; }
+    for (int m = 0; m < rve->n_materials; ++m) spec.materials.push_back({rve->mat_E[m], rve->mat_nu[m]});
+    spec.matrix_mat = rve->matrix_mat;
+    if (rve->n_inclusions < 0 || (rve->n_inclusions > 0 && (!rve->inc_cx || !rve->inc_cy || !rve->inc_r || !rve->inc_mat))) {
+        set_error("pg_mesh_build: inclusion arrays missing");
+        return PG_ERR_ARG;
+    }
+    for (int i = 0; i < rve->n_inclusions; ++i)
+        spec.inclusions.push_back({rve->inc_cx[i], rve->inc_cy[i], rve->inc_r[i], rve->inc_mat[i]});
+    spec.plane_strain = rve->plane_strain != 0;
+    spec.cohesive = rve->cohesive != 0;
+    spec.coh.law = rve->coh_law;
+    for (int k = 0; k < 4; ++k) spec.coh.p[k] = rve->coh_params[k];
+    if (spec.cohesive && spec.coh.law != PG_COH_OP && spec.coh.law != PG_COH_BILINEAR) {
+        set_error("pg_mesh_build: unknown cohesive law");
+        return PG_ERR_ARG;
+    }
+    spec.strain = rve->strain;
+    pg_mesh* m = new (std::nothrow) pg_mesh;
+    if (!m) { set_error("pg_mesh_build: out of host memory"); return PG_ERR_ARG; }
+    std::string err;
+    try {
+        err = build_mesh(spec, m->m);
+    } catch (const std::exception& ex) {
+        err = std::string("host exception: ") + ex.what();
+    }
+    if (!err.empty()) {
+        delete m;
+        set_error("pg_mesh_build: " + err);
+        return PG_ERR_MESH;
+    }
+    *out = m;
+    return PG_OK;
+}
+
+int pg_mesh_info_get(const pg_mesh* mm, pg_mesh_info* info) {
+    if (!mm || !info) { set_error("pg_mesh_info_get: null argument"); return PG_ERR_ARG; }
+    const HostMesh& m = mm->m;
+    info->n_nodes = m.n_nodes();
+    info->n_regular_nodes = m.n_reg;
+    info->n_enrichment_nodes = m.n_enr;
+    info->n_elements = m.n_elem;
+    info->n_cut_elements = m.n_cut;
+    info->n_cohesive_qp = m.n_coh_qp;
+    info->n_dof = m.n_dof();
+    info->n_free_dof = m.n_free;
+    info->n_blocks = m.n_blocks();
+    info->n_moved_nodes = m.n_moved;
+    return PG_OK;
+}
+
+int pg_mesh_export(const pg_mesh* mm, double* xy, int32_t* conn, int32_t* elem_mat, int32_t* elem_cut, int32_t* ref_dof,
+                   uint8_t* fixed, double* ubar) {
+    if (!mm) { set_error("pg_mesh_export: null mesh"); return PG_ERR_ARG; }
+    const HostMesh& m = mm->m;
+    if (xy)
+        for (int n = 0; n < m.n_nodes(); ++n) { xy[2 * n] = m.x[n]; xy[2 * n + 1] = m.y[n]; }
+    if (conn) std::memcpy(conn, m.conn.data(), m.conn.size() * sizeof(int));
+    if (elem_mat) std::memcpy(elem_mat, m.elem_mat.data(), m.elem_mat.size() * sizeof(int));
+    if (elem_cut) std::memcpy(elem_cut, m.elem_cut.data(), m.elem_cut.size() * sizeof(int));
+    if (ref_dof) std::memcpy(ref_dof, m.ref_dof.data(), m.ref_dof.size() * sizeof(int));
+    if (fixed) std::memcpy(fixed, m.fixed.data(), m.fixed.size());
+    if (ubar) std::memcpy(ubar, m.ubar.data(), m.ubar.size() * sizeof(double));
+    return PG_OK;
+}
+
+int pg_mesh_export_cut(const pg_mesh* mm, int32_t* cut_elem, int32_t* cut_tmpl, int32_t* cut_enr, int32_t* cut_child_mat,
+                       int32_t* cut_coh_qp0) {
+    if (!mm) { set_error("pg_mesh_export_cut: null mesh"); return PG_ERR_ARG; }
+    const HostMesh& m = mm->m;
+    if (cut_elem && m.n_cut) std::memcpy(cut_elem, m.cut_elem.data(), m.n_cut * sizeof(int));
+    if (cut_tmpl && m.n_cut) std::memcpy(cut_tmpl, m.cut_tmpl.data(), m.n_cut * sizeof(int));
+    if (cut_enr && m.n_cut) std::memcpy(cut_enr, m.cut_enr.data(), m.cut_enr.size() * sizeof(int));
+    if (cut_child_mat && m.n_cut) std::memcpy(cut_child_mat, m.cut_child_mat.data(), m.cut_child_mat.size() * sizeof(int));
+    if (cut_coh_qp0 && m.n_cut) std::memcpy(cut_coh_qp0, m.cut_coh_qp0.data(), m.n_cut * sizeof(int));
+    return PG_OK;
+}
+
+int pg_mesh_export_pattern(const pg_mesh* mm, int32_t* row_ptr, int32_t* col) {
+    if (!mm) { set_error("pg_mesh_export_pattern: null mesh"); return PG_ERR_ARG; }
+    const HostMesh& m = mm->m;
+    if (row_ptr) std::memcpy(row_ptr, m.row_ptr.data(), m.row_ptr.size() * sizeof(int));
+    if (col) std::memcpy(col, m.col.data(), m.col.size() * sizeof(int));
+    return PG_OK;
+}
+
+// 80 int32 per template: n_cut_edges, n_enr, n_child, n_coh, cut_edge[6],
+// enr_inc_node[6], child_n[4], child_mat_node[4], child_nodes[4][6], coh_nodes[3][4],
+// then padding to 80.
+int pg_template_table(int32_t* out, int32_t* n) {
+    const int nt = n_cut_templates();
+    if (n) *n = nt;
+    if (!out) return PG_OK;
+    for (int t = 0; t < nt; ++t) {
+        const CutTemplate& T = cut_template(t);
+        int32_t* o = out + 80 * t;
+        std::memset(o, 0xff, 80 * sizeof(int32_t));
+        o[0] = T.n_cut_edges; o[1] = T.n_enr; o[2] = T.n_child; o[3] = T.n_coh;
+        for (int i = 0; i < 6; ++i) { o[4 + i] = i < T.n_cut_edges ? T.cut_edge[i] : -1; o[10 + i] = i < T.n_cut_edges ? T.enr_inc_node[i] : -1; }
+        for (int c = 0; c < 4; ++c) {
+            o[16 + c] = c < T.n_child ? T.child_n[c] : 0;
+            o[20 + c] = c < T.n_child ? T.child_mat_node[c] : -2;
+            for (int k = 0; k < 6; ++k) o[24 + 6 * c + k] = (c < T.n_child && k < T.child_n[c]) ? T.child_nodes[c][k] : -1;
+        }
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 4; ++k) o[48 + 4 * c + k] = c < T.n_coh ? T.coh_nodes[c][k] : -1;
+    }
+    return PG_OK;
+}
+
+void pg_mesh_destroy(pg_mesh* m) { delete m; }
+
+int pg_ctx_create(const pg_mesh* m, int32_t device, pg_ctx** out) {
+    if (!m || !out) { set_error("pg_ctx_create: null argument"); return PG_ERR_ARG; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("pg_ctx_create: no CUDA device (this library has no CPU fallback)");
+        return PG_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) { set_error("pg_ctx_create: invalid device"); return PG_ERR_ARG; }
+    pg_ctx* c = new (std::nothrow) pg_ctx;
+    if (!c) { set_error("pg_ctx_create: out of host memory"); return PG_ERR_ARG; }
+    const int rc = ctx_create(m->m, device, c->c);
+    if (rc != PG_OK) {
+        free_ctx(c->c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return PG_OK;
+}
+
+void pg_ctx_destroy(pg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->c.device);
+    free_ctx(c->c);
+    delete c;
+}
+
+int pg_ctx_sync(pg_ctx* c) {
+    PG_GUARD_CTX(c);
+    PG_CUDA(cudaStreamSynchronize(c->c.stream));
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+int pg_assemble_linear(pg_ctx* c, void* stream) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    const int rc = launch_assemble(x, x.U, 0.0, false, true, pick(x, stream));
+    if (rc == PG_OK) x.assembled = true;
+    return rc;
+}
+
+int pg_assemble_linear_host(pg_ctx* c, const double* xy_host, double* k_host) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    cudaStream_t s = x.stream;
+    if (xy_host) {
+        // de-interleave on the device from a staging copy in the F work vector
+        PG_CUDA(cudaMemcpyAsync(x.F, xy_host, 2 * (size_t)x.n_nodes * sizeof(double), cudaMemcpyHostToDevice, s));
+        PG_CUDA(cudaMemcpy2DAsync(x.x, sizeof(double), x.F, 2 * sizeof(double), sizeof(double), x.n_nodes,
+                                  cudaMemcpyDeviceToDevice, s));
+        PG_CUDA(cudaMemcpy2DAsync(x.y, sizeof(double), x.F + 1, 2 * sizeof(double), sizeof(double), x.n_nodes,
+                                  cudaMemcpyDeviceToDevice, s));
+    }
+    int rc = launch_assemble(x, x.U, 0.0, false, true, s);
+    if (rc != PG_OK) return rc;
+    x.assembled = true;
+    if (k_host) PG_CUDA(cudaMemcpyAsync(k_host, x.K, 4 * (size_t)x.n_blocks * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    return PG_OK;
+}
+
+int pg_assemble_nonlinear(pg_ctx* c, const double* U_dev, double dt, int32_t want_f, int32_t want_K, void* stream) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!want_f && !want_K) return PG_OK;
+    cudaStream_t s = pick(x, stream);
+    const double* U = U_dev ? U_dev : x.U;
+    if (want_f) PG_CUDA(cudaMemsetAsync(x.F, 0, (size_t)x.n_dof * sizeof(double), s));
+    const int rc = launch_assemble(x, U, dt, want_f != 0, want_K != 0, s);
+    if (rc == PG_OK && want_K) x.assembled = true;
+    return rc;
+}
+
+int pg_new_load_step(pg_ctx* c, double t_frac) {
+    PG_GUARD_CTX(c);
+    c->c.t_frac = t_frac;
+    set_prescribed(c->c, t_frac, c->c.stream);
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+int pg_commit_isv(pg_ctx* c) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (x.n_coh_qp > 0)
+        PG_CUDA(cudaMemcpyAsync(x.isv_c, x.isv_t, (size_t)x.n_coh_qp * sizeof(double), cudaMemcpyDeviceToDevice, x.stream));
+    return PG_OK;
+}
+
+int pg_ctx_device_arrays(pg_ctx* c, double** K, double** U, double** F_int, double** isv_committed, double** isv_trial) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (K) *K = x.K;
+    if (U) *U = x.U;
+    if (F_int) *F_int = x.F;
+    if (isv_committed) *isv_committed = x.isv_c;
+    if (isv_trial) *isv_trial = x.isv_t;
+    return PG_OK;
+}
+
+void pg_solver_cfg_default(pg_solver_cfg* cfg) {
+    if (!cfg) return;
+    cfg->krylov = PG_KRYLOV_CG;
+    cfg->precond = PG_PREC_BLOCK_JACOBI;
+    cfg->precision = PG_PRECISION_FP64;
+    cfg->rtol = 1e-8;
+    cfg->max_iter = 200000;
+    cfg->inner_rtol = 1e-4;
+    cfg->max_refine = 50;
+    cfg->gmres_restart = 60;
+    cfg->check_every = 64;
+}
+
+int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg_in, pg_solve_stats* stats) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    pg_solver_cfg cfg;
+    if (cfg_in) cfg = *cfg_in;
+    else pg_solver_cfg_default(&cfg);
+    pg_solve_stats st{};
+    cudaStream_t s = x.stream;
+    set_prescribed(x, 1.0, s);
+    if (!x.assembled) {
+        const int rc = launch_assemble(x, x.U, 0.0, false, true, s);
+        if (rc != PG_OK) return rc;
+        x.assembled = true;
+    }
+    const int rc = solve_linear_system(x, cfg, st, s);
+    if (stats) *stats = st;
+    if (rc != PG_OK) return rc;
+    if (st.status != PG_OK) {
+        set_error(st.status == PG_ERR_BREAKDOWN ? "pg_solve_linear: Krylov breakdown"
+                                                : "pg_solve_linear: iteration budget exhausted before the tolerance");
+        return st.status;
+    }
+    return PG_OK;
+}
+
+int pg_get_matrix(pg_ctx* c, double* vals_host) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!vals_host) { set_error("pg_get_matrix: null output"); return PG_ERR_ARG; }
+    PG_CUDA(cudaStreamSynchronize(x.stream));
+    PG_CUDA(cudaMemcpy(vals_host, x.K, 4 * (size_t)x.n_blocks * sizeof(double), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+int pg_get_vector(pg_ctx* c, int32_t which, double* out) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!out) { set_error("pg_get_vector: null output"); return PG_ERR_ARG; }
+    const double* src = which == 0 ? x.U : which == 1 ? x.F : which == 2 ? x.r : nullptr;
+    if (!src) { set_error("pg_get_vector: unknown vector"); return PG_ERR_ARG; }
+    PG_CUDA(cudaStreamSynchronize(x.stream));
+    PG_CUDA(cudaMemcpy(out, src, (size_t)x.n_dof * sizeof(double), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+int pg_set_vector(pg_ctx* c, int32_t which, const double* in) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!in) { set_error("pg_set_vector: null input"); return PG_ERR_ARG; }
+    double* dst = which == 0 ? x.U : which == 1 ? x.F : nullptr;
+    if (!dst) { set_error("pg_set_vector: unknown vector"); return PG_ERR_ARG; }
+    PG_CUDA(cudaStreamSynchronize(x.stream));
+    PG_CUDA(cudaMemcpy(dst, in, (size_t)x.n_dof * sizeof(double), cudaMemcpyHostToDevice));
+    return PG_OK;
+}
+
+int pg_get_isv(pg_ctx* c, int32_t committed, double* out) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!out) { set_error("pg_get_isv: null output"); return PG_ERR_ARG; }
+    if (x.n_coh_qp == 0) return PG_OK;
+    PG_CUDA(cudaStreamSynchronize(x.stream));
+    PG_CUDA(cudaMemcpy(out, committed ? x.isv_c : x.isv_t, (size_t)x.n_coh_qp * sizeof(double), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Internal device-side state of the B200 IGFEM path (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "igfem_host.h"
+#include "pigfem_b200.h"
+
+struct pg_mesh {
+    pgb::HostMesh m;
+};
+
+namespace pgb {
+
+// Cohesive law parameters on the device.
+struct DevCohLaw {
+    int law;          // PG_COH_OP / PG_COH_BILINEAR
+    double p[4];
+};
+
+// Template table entry as the cut-element kernel reads it (constant memory).
+struct DevTemplate {
+    int n_enr, n_child, n_coh, pad;
+    int child_n[kMaxChildren];
+    int child_type[kMaxChildren];
+    int child_nodes[kMaxChildren][kMaxChildNodes];
+    int coh_nodes[kMaxCoh][4];
+};
+
+constexpr int kMaxChildQ = 24;
+struct DevChildQuad {
+    int nq, nn, pad0, pad1;
+    double w[kMaxChildQ];
+    double N[kMaxChildQ * kMaxChildNodes];
+    double dN[kMaxChildQ * kMaxChildNodes * 2];
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    HostMesh hm;                       // host copy (sizes, maps, export)
+    int n_nodes = 0, n_reg = 0, n_elem = 0, n_cut = 0, n_blocks = 0, n_dof = 0, n_coh_qp = 0;
+    DevCohLaw coh{};
+    // mesh
+    double* x = nullptr;
+    double* y = nullptr;
+    int4* elem4 = nullptr;             // n0, n1, n2, material
+    int* row_ptr = nullptr;
+    int* col = nullptr;
+    int* diag = nullptr;
+    int* ne_ptr = nullptr;
+    int* ne_list = nullptr;
+    double* dmat = nullptr;            // 3 per material: D11, D12, D33
+    // cut elements
+    int* cut_elem = nullptr;
+    int* cut_tmpl = nullptr;
+    int* cut_enr = nullptr;
+    int* cut_child_mat = nullptr;
+    int* cut_coh_qp0 = nullptr;
+    int* cut_slot_ptr = nullptr;
+    int* cut_slot = nullptr;
+    // system
+    double* K = nullptr;               // 4 * n_blocks
+    float* Kf = nullptr;               // FP32 copy for mixed precision
+    uint8_t* fixed = nullptr;          // n_dof
+    double* ubar = nullptr;            // n_dof
+    double* U = nullptr;               // n_dof (full vector incl. prescribed)
+    double* F = nullptr;               // n_dof internal force / work
+    double* isv_c = nullptr;           // committed delta_max
+    double* isv_t = nullptr;           // trial delta_max
+    // solver work (FP64)
+    double* r = nullptr;
+    double* z = nullptr;
+    double* p = nullptr;
+    double* q = nullptr;
+    double* dx = nullptr;
+    double* minv = nullptr;            // 4 per node: inverse of the (masked) diagonal 2x2 block or Jacobi
+    // solver work (FP32)
+    float* rf = nullptr;
+    float* zf = nullptr;
+    float* pf = nullptr;
+    float* qf = nullptr;
+    float* xf = nullptr;
+    float* minvf = nullptr;
+    double* scal = nullptr;            // device scalars
+    int* iflags = nullptr;             // device flags
+    double* h_scal = nullptr;          // pinned host mirror
+    int* h_iflags = nullptr;
+    bool assembled = false;
+    double t_frac = 1.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_assemble_ms = 0.0;
+};
+
+// error plumbing
+void set_error(const std::string& s);
+int cuda_fail(cudaError_t e, const char* where);
+
+// assembly entry points (pg_assemble.cu)
+void upload_tables();
+int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s);
+int launch_to_fp32(Ctx& c, cudaStream_t s);
+
+// solver entry points (pg_solve.cu)
+int solve_linear_system(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
+
+}  // namespace pgb
+
+struct pg_ctx {
+    pgb::Ctx c;
+};
+
+#define PG_CUDA(call)                                                      \
+    do {                                                                   \
+        cudaError_t _e = (call);                                           \
+        if (_e != cudaSuccess) return ::pgb::cuda_fail(_e, #call);         \
+    } while (0)

@@ -1,0 +1,251 @@
+// Vector/SpMV kernels of the Krylov solves (see pg_solve.cu for the scalar
+// bookkeeping they implement).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "pg_internal.cuh"
+
+namespace pgb {
+
+constexpr int kThreads = 256;
+
+enum : int {
+    S_PQ0 = 0, S_RZ0 = 2, S_RR0 = 4, S_TOL2 = 6, S_AUX = 8, S_NSCAL = 16
+};
+enum : int { F_DONE = 0, F_BREAKDOWN = 1, F_ITERS = 2, F_NFLAGS = 8 };
+
+__device__ __forceinline__ double block_sum(double d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = d;
+    __syncthreads();
+    d = 0.0;
+    if (wid == 0) {
+        d = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    }
+    return d;  // valid in thread 0
+}
+
+// y_i = sum_j K_ij x_j over 2x2 blocks (FP64 accumulation), masked rows zeroed
+template <typename MT, typename VT>
+__device__ __forceinline__ void bsr_row(int i, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                                        const MT* __restrict__ K, const VT* __restrict__ x, double& y0, double& y1) {
+    const int r0 = row_ptr[i], r1 = row_ptr[i + 1];
+    y0 = 0.0;
+    y1 = 0.0;
+    for (int k = r0; k < r1; ++k) {
+        const int j = col[k];
+        const MT* b = K + 4 * (size_t)k;
+        const double x0 = (double)x[2 * j], x1 = (double)x[2 * j + 1];
+        y0 += (double)b[0] * x0 + (double)b[1] * x1;
+        y1 += (double)b[2] * x0 + (double)b[3] * x1;
+    }
+}
+
+template <typename MT, typename VT>
+__global__ void __launch_bounds__(kThreads) k_spmv_plain(int n, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                                                          const MT* __restrict__ K, const VT* __restrict__ x,
+                                                          const uint8_t* __restrict__ fixed, VT* __restrict__ y) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    double y0, y1;
+    bsr_row<MT, VT>(i, row_ptr, col, K, x, y0, y1);
+    y[2 * i] = fixed[2 * i] ? (VT)0 : (VT)y0;
+    y[2 * i + 1] = fixed[2 * i + 1] ? (VT)0 : (VT)y1;
+}
+
+template <typename MT, typename VT>
+__global__ void __launch_bounds__(kThreads) k_spmv_cg(int n, int P, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                                                       const MT* __restrict__ K, const VT* __restrict__ p,
+                                                       const uint8_t* __restrict__ fixed, VT* __restrict__ q, double* scal,
+                                                       const int* flags) {
+    if (flags[F_DONE]) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scal[S_RZ0 + P] = 0.0;
+        scal[S_RR0 + P] = 0.0;
+    }
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    double part = 0.0;
+    if (i < n) {
+        double y0, y1;
+        bsr_row<MT, VT>(i, row_ptr, col, K, p, y0, y1);
+        const VT q0 = fixed[2 * i] ? (VT)0 : (VT)y0;
+        const VT q1 = fixed[2 * i + 1] ? (VT)0 : (VT)y1;
+        q[2 * i] = q0;
+        q[2 * i + 1] = q1;
+        part = (double)p[2 * i] * (double)q0 + (double)p[2 * i + 1] * (double)q1;
+    }
+    const double s = block_sum(part);
+    if (threadIdx.x == 0) atomicAdd(&scal[S_PQ0 + P], s);
+}
+
+template <typename VT>
+__global__ void k_neg(int nd, VT* r) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) r[i] = -r[i];
+}
+
+template <typename VT, typename PT>
+__device__ __forceinline__ void apply_prec(const PT* __restrict__ minv, int node, double r0, double r1, double& z0, double& z1) {
+    const PT* m = minv + 4 * (size_t)node;
+    z0 = (double)m[0] * r0 + (double)m[1] * r1;
+    z1 = (double)m[2] * r0 + (double)m[3] * r1;
+}
+
+template <typename VT, typename PT>
+__global__ void __launch_bounds__(kThreads) k_cg_init(int n, const VT* __restrict__ r, VT* __restrict__ z, VT* __restrict__ p,
+                                                       const PT* __restrict__ minv, double* scal) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    double prz = 0.0, prr = 0.0;
+    if (i < n) {
+        const double r0 = (double)r[2 * i], r1 = (double)r[2 * i + 1];
+        double z0, z1;
+        apply_prec<VT, PT>(minv, i, r0, r1, z0, z1);
+        z[2 * i] = (VT)z0;
+        z[2 * i + 1] = (VT)z1;
+        p[2 * i] = (VT)z0;
+        p[2 * i + 1] = (VT)z1;
+        prz = r0 * z0 + r1 * z1;
+        prr = r0 * r0 + r1 * r1;
+    }
+    const double a = block_sum(prz);
+    const double b = block_sum(prr);
+    if (threadIdx.x == 0) {
+        atomicAdd(&scal[S_RZ0 + 1], a);
+        atomicAdd(&scal[S_RR0 + 1], b);
+    }
+}
+
+template <typename VT, typename PT>
+__global__ void __launch_bounds__(kThreads) k_cg_update(int n, int P, VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ z,
+                                                         const VT* __restrict__ p, const VT* __restrict__ q,
+                                                         const PT* __restrict__ minv, double* scal, int* flags) {
+    if (flags[F_DONE]) return;
+    const int Q = 1 - P;
+    const double pq = scal[S_PQ0 + P];
+    if (!(pq > 0.0)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            flags[F_BREAKDOWN] = 1;
+            flags[F_DONE] = 1;
+        }
+        return;
+    }
+    const double alpha = scal[S_RZ0 + Q] / pq;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    double prz = 0.0, prr = 0.0;
+    if (i < n) {
+        const double r0 = (double)r[2 * i] - alpha * (double)q[2 * i];
+        const double r1 = (double)r[2 * i + 1] - alpha * (double)q[2 * i + 1];
+        x[2 * i] = (VT)((double)x[2 * i] + alpha * (double)p[2 * i]);
+        x[2 * i + 1] = (VT)((double)x[2 * i + 1] + alpha * (double)p[2 * i + 1]);
+        r[2 * i] = (VT)r0;
+        r[2 * i + 1] = (VT)r1;
+        double z0, z1;
+        apply_prec<VT, PT>(minv, i, r0, r1, z0, z1);
+        z[2 * i] = (VT)z0;
+        z[2 * i + 1] = (VT)z1;
+        prz = r0 * z0 + r1 * z1;
+        prr = r0 * r0 + r1 * r1;
+    }
+    const double a = block_sum(prz);
+    const double b = block_sum(prr);
+    if (threadIdx.x == 0) {
+        atomicAdd(&scal[S_RZ0 + P], a);
+        atomicAdd(&scal[S_RR0 + P], b);
+        if (blockIdx.x == 0) {
+            scal[S_PQ0 + Q] = 0.0;
+            flags[F_ITERS] += 1;
+        }
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kThreads) k_cg_pupdate(int n, int P, const VT* __restrict__ z, VT* __restrict__ p,
+                                                          double* scal, int* flags) {
+    if (flags[F_DONE]) return;
+    const int Q = 1 - P;
+    const double rz = scal[S_RZ0 + P];
+    const double rz_old = scal[S_RZ0 + Q];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && scal[S_RR0 + P] <= scal[S_TOL2]) flags[F_DONE] = 1;
+    const double beta = rz / rz_old;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) {
+        p[2 * i] = (VT)((double)z[2 * i] + beta * (double)p[2 * i]);
+        p[2 * i + 1] = (VT)((double)z[2 * i + 1] + beta * (double)p[2 * i + 1]);
+    }
+}
+
+// Per-node preconditioner: inverse of the masked 2x2 diagonal block (block
+// Jacobi), inverse diagonal (Jacobi) or the free-DOF identity.
+template <typename PT>
+__global__ void k_prec_setup(int n, const int* __restrict__ diag, const double* __restrict__ K,
+                             const uint8_t* __restrict__ fixed, int block, int ident, PT* minv) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const double* b = K + 4 * (size_t)diag[i];
+    const bool f0 = fixed[2 * i], f1 = fixed[2 * i + 1];
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ident) {
+        m[0] = f0 ? 0.0 : 1.0;
+        m[3] = f1 ? 0.0 : 1.0;
+    } else if (block && !f0 && !f1) {
+        const double det = b[0] * b[3] - b[1] * b[2];
+        m[0] = b[3] / det;
+        m[1] = -b[1] / det;
+        m[2] = -b[2] / det;
+        m[3] = b[0] / det;
+    } else {
+        m[0] = f0 ? 0.0 : 1.0 / b[0];
+        m[3] = f1 ? 0.0 : 1.0 / b[3];
+    }
+    for (int k = 0; k < 4; ++k) minv[4 * (size_t)i + k] = (PT)m[k];
+}
+
+template <typename VT>
+__global__ void k_fill(int n, VT* v, VT a) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) v[i] = a;
+}
+
+template <typename VT>
+__global__ void k_axpy_free(int nd, const uint8_t* __restrict__ fixed, double* U, const VT* __restrict__ e, double s) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd && !fixed[i]) U[i] += s * (double)e[i];
+}
+
+__global__ inline void k_axpy_free_f(int nd, const uint8_t* __restrict__ fixed, double* U, const float* __restrict__ e,
+                                     double s) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd && !fixed[i]) U[i] += s * (double)e[i];
+}
+
+__global__ inline void k_to_float_scaled(int nd, const double* __restrict__ a, float* b, double s) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) b[i] = (float)(a[i] * s);
+}
+
+__global__ inline void k_dot_self(int nd, const double* __restrict__ a, double* out) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const double v = (i < nd) ? a[i] * a[i] : 0.0;
+    const double s = block_sum(v);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+__global__ inline void k_apply_dirichlet(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ ubar,
+                                         double tf, double* U) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd && fixed[i]) U[i] = tf * ubar[i];
+}
+
+void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
+
+}  // namespace pgb

@@ -1,0 +1,338 @@
+"""Benchmark: elements assembled/s of the FP64 IGFEM stiffness assembly, plus the
+linear load-step time at 1e-8 relative residual (plain FP64 PCG vs FP32-Krylov
+with FP64 refinement), on configuration 1: a 512x512 structured TRI3 mesh
+(524,288 elements) cut by 100 seeded random-sequential-addition circles
+(r ~ U[0.02, 0.04], gap >= 0.005), matrix 3.0 GPa / 0.35, inclusions 70 GPa / 0.2,
+1% uniaxial strain.  Synthetic inputs of the stated shapes (seed 1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one full assembly pass (node-row kernel + cut-element kernel) of K.
+Timing: CUDA events on the assembly stream around each step; the L2 (126 MB)
+is flushed by writing a 512 MB buffer between steps; max over ranks.  For N > 1
+every rank assembles its own replica of the RVE (replicas only: a single RVE
+does not shard without a halo exchange), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "elements assembled/s"
+UNIT = "elements/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-load-step", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def workload_config(rve, info):
+    return {
+        "workload": "config1: 512x512 TRI3 RVE (524,288 elements), 100 RSA circles r~U[0.02,0.04] gap>=0.005 seed 1, "
+                    "E 3.0/70 GPa, nu 0.35/0.2, plane strain, 1% uniaxial strain; FP64 stiffness assembly",
+        "elements": info["n_elements"],
+        "cut_elements": info["n_cut_elements"],
+        "nodes": info["n_nodes"],
+        "dof": info["n_dof"],
+        "free_dof": info["n_free_dof"],
+        "nnz": 4 * info["n_blocks"],
+        "l2": "flushed between steps (512 MB write)",
+        "parallelism": "replicas",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([v.strip() for v in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference itself (oracle/_ref) or, if it was not built,
+# the C oracle port.  Bounded sample: one process, a few assembly passes.
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(rve, repeats: int, procs: int = 1):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+    cfg = dict(nx=rve.nx, ny=rve.ny, E_matrix=rve.materials[0][0], nu_matrix=rve.materials[0][1], strain=rve.strain,
+               problem="linear", assemble_repeats=repeats,
+               inclusions=[(c[0], c[1], c[2], rve.materials[c[3]][0], rve.materials[c[3]][1]) for c in rve.inclusions])
+    if refio.driver_available():
+        if procs == 1:
+            r = refio.run(cfg, timeout=1800)
+            return {"kind": "reference", "each": list(r["time.assemble_each"]), "n": int(r["mesh.n_elem_active"][0]),
+                    "cores": 1}
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(procs) as ex:
+            rs = list(ex.map(lambda _: refio.run(cfg, timeout=1800), range(procs)))
+        return {"kind": "reference", "each_per_proc": [list(r["time.assemble_each"]) for r in rs],
+                "n": int(rs[0]["mesh.n_elem_active"][0]), "cores": procs}
+    # port: the C oracle's assembly of the same enriched mesh, one thread
+    import oracle
+    import pigfem_assignment_b200.problem as pb
+    m = pb.Mesh(rve)
+    om = oracle.from_product(m.export(), pb.template_table(), rve)
+    om.pattern()
+    each = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        om.assemble()
+        each.append(time.perf_counter() - t0)
+    return {"kind": "port", "each": each, "n": m.info["n_elements"], "cores": 1}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    from pigfem_assignment_b200.rve import config1
+    if rank != 0:
+        return
+    rve = config1()
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    res = cpu_reference_sample(rve, args.warmup + args.steps, procs)
+    if "each_per_proc" in res:
+        times = [sum(e[args.warmup:]) for e in res["each_per_proc"]]
+        total_elems = res["n"] * args.steps * procs
+        t = max(times)
+    else:
+        t = sum(res["each"][args.warmup:])
+        total_elems = res["n"] * args.steps * res["cores"]
+    value = total_elems / t
+    sample = (f"{res['cores']} independent single-rank processes, each assembling config1 "
+              f"({res['n']} elements) {args.steps} timed + {args.warmup} warm-up times")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "config1 (see b200 arm), reference Assembler::assemble_linear + shim MatSetValue",
+                   "parallelism": "independent processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"], "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200_arm(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import pigfem_assignment_b200.problem as pb
+    from pigfem_assignment_b200 import _lib
+    from pigfem_assignment_b200.rve import config1
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    rve = config1()
+    mesh = pb.Mesh(rve)
+    info = mesh.info
+    ctx = pb.DeviceContext(mesh, device=local)
+    asm = pb.Assembler(ctx)
+    flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 512 MB
+
+    def assemble_timed():
+        _lib.check(_lib.lib.pg_assembly_timing(ctx.handle, 1, None, None))
+        asm.assemble_linear()
+        a, b = C.c_float(), C.c_float()
+        _lib.check(_lib.lib.pg_assembly_timing(ctx.handle, 1, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        assemble_timed()
+    ctx.sync()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    rows_ms, cut_ms = [], []
+    for _ in range(args.steps):
+        flush.fill_(float(len(rows_ms)))
+        torch.cuda.synchronize()
+        a, b = assemble_timed()
+        rows_ms.append(a)
+        cut_ms.append(b)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a + b for a, b in zip(rows_ms, cut_ms)]
+    t_local = sum(step_ms) / 1e3
+    if dist:
+        tt = torch.tensor([t_local], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    else:
+        t_max = t_local
+    n_e = info["n_elements"]
+    value = n_e * args.steps * world / t_max
+
+    # ---- roofline of the dominant kernel (node rows) ----
+    n_blocks, n_nodes, n_cut = info["n_blocks"], info["n_nodes"], info["n_cut_elements"]
+    n_uncut = n_e - n_cut
+    rows_bytes = 32 * n_blocks + 13 * n_uncut + 16 * n_nodes
+    pass_bytes = rows_bytes + 64 * n_cut + 16 * info["n_enrichment_nodes"]
+    peak, peak_kind = measured_peak_hbm()
+    avg_rows = statistics.mean(rows_ms) / 1e3
+    achieved = rows_bytes / avg_rows / 1e9
+    share = sum(rows_ms) / sum(step_ms)
+
+    # ---- end to end through the host-buffer entry point ----
+    xy = torch.from_numpy(np.ascontiguousarray(mesh.export()["xy"].reshape(-1))).pin_memory()
+    kh = torch.empty(4 * n_blocks, dtype=torch.float64).pin_memory()
+    xy_p = C.cast(C.c_void_p(xy.data_ptr()), _lib._dp)
+    kh_p = C.cast(C.c_void_p(kh.data_ptr()), _lib._dp)
+    for _ in range(2):
+        _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, xy_p, kh_p))
+    e2e_ms = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(2.0)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, xy_p, kh_p))
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_value = n_e * world / (statistics.median(e2e_ms) / 1e3)
+
+    # ---- load-step time at 1e-8 relative residual: plain FP64 vs mixed ----
+    load = None
+    if not args.no_load_step:
+        load = {}
+        for name, prec in (("plain_fp64", _lib.PG_PRECISION_FP64), ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED)):
+            solver = pb.Solver(ctx)
+            solver.configure(precision=prec, precond=_lib.PG_PREC_BLOCK_JACOBI, rtol=1e-8, inner_rtol=1e-3,
+                             check_every=64)
+            ctx.set_vector(0, np.zeros(info["n_dof"]))
+            torch.cuda.synchronize()
+            a, b = assemble_timed()
+            st = solver.solve_linear()
+            load[name] = {"ms": a + b + 1e3 * st.seconds, "assemble_ms": a + b, "solve_ms": 1e3 * st.seconds,
+                          "krylov_iterations": st.iterations, "refinements": st.refinements,
+                          "rel_residual": st.rel_residual}
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            res = cpu_reference_sample(rve, 3, 1)
+            t = sum(res["each"])
+            cpu = {"value": res["n"] * len(res["each"]) / t, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                   "sample": f"config1 assembled {len(res['each'])} times by one single-threaded process "
+                             f"({'the reference built from its sources with the PETSc/MPI shim' if res['kind'] == 'reference' else 'the C oracle port'})"}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(rve, info),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_assemble_rows",
+                         "peak_kind": peak_kind, "bytes_per_launch": rows_bytes, "kernel_share": share,
+                         "pass_bytes": pass_bytes,
+                         "pass_achieved": pass_bytes / (statistics.mean(step_ms) / 1e3) / 1e9},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n_nodes,
+                    "d2h_bytes_per_step": 32 * n_blocks},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+            "load_step": load,
+            "kernel_ms": {"rows_median": statistics.median(rows_ms), "cut_median": statistics.median(cut_ms)},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -99,7 +99,9 @@ int pg_mesh_export_cut(const pg_mesh* m, int32_t* cut_elem, int32_t* cut_tmpl, i
                        int32_t* cut_child_mat, int32_t* cut_coh_qp0);
 /* 2x2-block CSR pattern: row_ptr[n_nodes+1], col[n_blocks]. */
 int pg_mesh_export_pattern(const pg_mesh* m, int32_t* row_ptr, int32_t* col);
-/* Cut templates: per template 80 int32 (see DESIGN.md table layout); returns count in *n. */
+/* Cut templates: 80 int32 per template -- n_cut_edges, n_enr, n_child, n_coh,
+ * cut_edge[6], enr_inc_node[6], child_n[4], child_mat_node[4], child_nodes[4][6],
+ * coh_nodes[3][4], padding; returns the count in *n. */
 int pg_template_table(int32_t* out, int32_t* n);
 void pg_mesh_destroy(pg_mesh* m);
 
@@ -171,6 +173,11 @@ int pg_get_matrix(pg_ctx* c, double* vals_host);         /* 4*n_blocks */
 int pg_get_vector(pg_ctx* c, int32_t which, double* out); /* which: 0=U, 1=F_int, 2=reaction/residual work */
 int pg_set_vector(pg_ctx* c, int32_t which, const double* in);
 int pg_get_isv(pg_ctx* c, int32_t committed, double* out);/* n_cohesive_qp delta_max values */
+int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
+/* Device time of the last assembly's two kernels (node rows, cut elements), from CUDA
+ * events recorded on the assembly stream while timing is enabled; pass NULLs to only
+ * switch timing on/off. */
+int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
 const char* pg_last_error(void);
 const char* pg_version(void);

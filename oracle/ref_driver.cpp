@@ -257,14 +257,18 @@ int main(int argc, char** argv) {
     if (cfg.assemble_repeats > 0 && !cohesive) {
         problem->setup();
         Assembler* assem = problem->get_assembler();
+        std::vector<double> each;
         for (int r = 0; r < cfg.assemble_repeats; ++r) {
             MatZeroEntries(solver->_K.ff); MatZeroEntries(solver->_K.fp);
             MatZeroEntries(solver->_K.pf); MatZeroEntries(solver->_K.pp);
             const double t0 = now_s();
             assem->assemble_linear(solver->_K);
-            t_asm_rep += now_s() - t0;
+            each.push_back(now_s() - t0);
+            t_asm_rep += each.back();
         }
         o.d1("time.assemble_repeat_total", t_asm_rep);
+        o.d("time.assemble_each", each);
+        o.d1("time.init", t_init);
         o.i1("time.assemble_repeats", cfg.assemble_repeats);
         o.i1("mesh.n_elem_active", (int32_t)mesh.n_local_active_elem());
         fclose(fp);

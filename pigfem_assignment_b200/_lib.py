@@ -105,6 +105,8 @@ def _load() -> C.CDLL:
         "pg_get_vector": ([v, C.c_int32, _dp], C.c_int),
         "pg_set_vector": ([v, C.c_int32, _dp], C.c_int),
         "pg_get_isv": ([v, C.c_int32, _dp], C.c_int),
+        "pg_set_isv": ([v, C.c_int32, _dp], C.c_int),
+        "pg_assembly_timing": ([v, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
         "pg_last_error": ([], C.c_char_p),
         "pg_version": ([], C.c_char_p),
     }
@@ -123,7 +125,7 @@ DECLARED_SYMBOLS = (
     "pg_template_table", "pg_mesh_destroy", "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_sync",
     "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
     "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",
-    "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_last_error", "pg_version",
+    "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_last_error", "pg_version",
 )
 
 

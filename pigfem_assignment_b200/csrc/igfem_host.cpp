@@ -424,8 +424,17 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
                 err << "no valid intersection between nodes " << a << " and " << b;
                 return err.str();
             }
-            const double ex = m.x[a] + alpha * (m.x[b] - m.x[a]);
-            const double ey = m.y[a] + alpha * (m.y[b] - m.y[a]);
+            double ex = m.x[a] + alpha * (m.x[b] - m.x[a]);
+            double ey = m.y[a] + alpha * (m.y[b] - m.y[a]);
+            // An interface that passes through a mesh node to within rounding
+            // (a node the moving rule misses because its bounding-box test
+            // rounds it out, Mesh.cpp:2850) puts the intersection on the node:
+            // the child element collapses and its zero-weight points are
+            // skipped, as the reference's iterative root lands there too.
+            const double tol = 8.0 * std::numeric_limits<double>::epsilon() *
+                               (std::fabs(m.x[b] - m.x[a]) + std::fabs(m.y[b] - m.y[a]) + std::fabs(m.x[b]) + std::fabs(m.y[b]));
+            for (int end : {a, b})
+                if (std::fabs(ex - m.x[end]) + std::fabs(ey - m.y[end]) <= tol) { ex = m.x[end]; ey = m.y[end]; }
             for (int copy = 0; copy < (spec.cohesive ? 2 : 1); ++copy) {
                 const int idx = k + copy * m.n_enr_initial;
                 m.x[m.n_reg + idx] = ex;

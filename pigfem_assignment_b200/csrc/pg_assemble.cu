@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(kRowThreads) k_assemble_rows(RowArgs a) {
                         if (sl < 0)
                             for (int q = kRowRegCols; q < deg; ++q)
                                 if (a.col[r0 + q] == nt) { sl = q; break; }
+                        if (sl < 0) continue;  // not in the pattern: cannot happen for a pattern built from these elements
                         double* d = dst + 4 * sl;
                         d[0] += k00;
                         d[1] += k01;
@@ -350,6 +351,9 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
             }
             const double det = J00 * J11 - J01 * J10;
             const double wgt = det * Q.w[q];
+            // a zero weight (collapsed child) contributes nothing: the reference's
+            // K_el.AXPY is cblas_daxpy, which returns at once for alpha == 0
+            if (wgt == 0.0) continue;
             // gradients of the element's local functions at this point
             if (lane < nl) {
                 double gx = 0.0, gy = 0.0;
@@ -431,6 +435,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
                 }
             const double tR[2] = {R[0][0] * tr[0] + R[1][0] * tr[1], R[0][1] * tr[0] + R[1][1] * tr[1]};
             const double wgt = dA * 1.0;
+            if (wgt == 0.0) continue;
             const int cn[4] = {c0, c1, c2, c3};
             const double Nn[2] = {N0, N1};
             if (a.want_K) {
@@ -469,7 +474,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
 #pragma unroll
         for (int k = 0; k < kCutPairsPerLane; ++k) {
             const int p = lane + 32 * k;
-            if (p < npairs) {
+            if (p < npairs && slots[p] >= 0) {
                 double* d = a.K + 4 * (size_t)slots[p];
                 atomicAdd(d + 0, acc[k][0]);
                 atomicAdd(d + 1, acc[k][1]);
@@ -511,8 +516,10 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.want_f = want_f;
     const int rblocks = (c.n_nodes + kRowThreads - 1) / kRowThreads;
     const size_t smem = want_K ? (size_t)kRowTileBlocks * 32 : 0;
+    if (c.timing) cudaEventRecord(c.ea0, s);
     if (rblocks > 0) k_assemble_rows<<<rblocks, kRowThreads, smem, s>>>(ra);
     PG_CUDA(cudaGetLastError());
+    if (c.timing) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {
         CutArgs ca;
         ca.n_cut = c.n_cut;
@@ -540,6 +547,7 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
         k_assemble_cut<<<cblocks, 32 * kCutWarps, 0, s>>>(ca);
         PG_CUDA(cudaGetLastError());
     }
+    if (c.timing) cudaEventRecord(c.ea2, s);
     return PG_OK;
 }
 

@@ -45,6 +45,8 @@ void free_ctx(Ctx& c) {
     if (c.h_iflags) cudaFreeHost(c.h_iflags);
     if (c.ev0) cudaEventDestroy(c.ev0);
     if (c.ev1) cudaEventDestroy(c.ev1);
+    for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2})
+        if (e) cudaEventDestroy(e);
     if (c.stream) cudaStreamDestroy(c.stream);
 }
 
@@ -82,6 +84,9 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     PG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     PG_CUDA(cudaEventCreate(&c.ev0));
     PG_CUDA(cudaEventCreate(&c.ev1));
+    PG_CUDA(cudaEventCreate(&c.ea0));
+    PG_CUDA(cudaEventCreate(&c.ea1));
+    PG_CUDA(cudaEventCreate(&c.ea2));
     c.hm = hm;
     c.n_nodes = hm.n_nodes();
     c.n_reg = hm.n_reg;
@@ -470,6 +475,32 @@ int pg_get_isv(pg_ctx* c, int32_t committed, double* out) {
     if (x.n_coh_qp == 0) return PG_OK;
     PG_CUDA(cudaStreamSynchronize(x.stream));
     PG_CUDA(cudaMemcpy(out, committed ? x.isv_c : x.isv_t, (size_t)x.n_coh_qp * sizeof(double), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (ms_rows || ms_cut) {
+        if (!x.timing) { set_error("pg_assembly_timing: timing was not enabled"); return PG_ERR_STATE; }
+        PG_CUDA(cudaEventSynchronize(x.ea2));
+        float a = 0.f, b = 0.f;
+        PG_CUDA(cudaEventElapsedTime(&a, x.ea0, x.ea1));
+        PG_CUDA(cudaEventElapsedTime(&b, x.ea1, x.ea2));
+        if (ms_rows) *ms_rows = a;
+        if (ms_cut) *ms_cut = b;
+    }
+    x.timing = enable != 0;
+    return PG_OK;
+}
+
+int pg_set_isv(pg_ctx* c, int32_t committed, const double* in) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    if (!in) { set_error("pg_set_isv: null input"); return PG_ERR_ARG; }
+    if (x.n_coh_qp == 0) return PG_OK;
+    PG_CUDA(cudaStreamSynchronize(x.stream));
+    PG_CUDA(cudaMemcpy(committed ? x.isv_c : x.isv_t, in, (size_t)x.n_coh_qp * sizeof(double), cudaMemcpyHostToDevice));
     return PG_OK;
 }
 

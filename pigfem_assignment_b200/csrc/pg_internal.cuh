@@ -93,7 +93,9 @@ struct Ctx {
     bool assembled = false;
     double t_frac = 1.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double last_assemble_ms = 0.0;
+    // events bracketing the two assembly kernels of the last assembly (rows, cut)
+    cudaEvent_t ea0 = nullptr, ea1 = nullptr, ea2 = nullptr;
+    bool timing = false;
 };
 
 // error plumbing

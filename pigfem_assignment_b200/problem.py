@@ -146,6 +146,14 @@ class DeviceContext:
         return v[: self.info["n_cohesive_qp"]]
 
 
+def _set_isv(ctx, v, committed=True):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    check(lib.pg_set_isv(ctx.handle, 1 if committed else 0, dptr(v)))
+
+
+DeviceContext.set_isv = _set_isv
+
+
 class Assembler:
     """Assembler surface (include/Assembler.h:41-51)."""
 

@@ -1,0 +1,185 @@
+"""GPU parity: the CUDA path (through the C ABI) against the pinned CPU oracle
+and the reference's golden outputs.
+
+Tolerances (FP64 path, from the targets of this hot path):
+  assembled K: relative Frobenius error <= 1e-12
+  displacement after the linear solve: relative error <= 1e-8
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as sla
+
+import oracle
+import pigfem_assignment_b200.problem as pb
+from helpers import bsr_to_csr, golden, permute_to_ref, ref_full_K, rel_fro, rve_from_golden
+from pigfem_assignment_b200 import _lib
+from pigfem_assignment_b200.rve import RVE, config0, config1, rsa_circles
+
+pytestmark = pytest.mark.gpu
+
+K_TOL = 1e-12
+U_TOL = 1e-8
+
+
+def gpu_K(ctx, export):
+    return bsr_to_csr(export["row_ptr"], export["col"], ctx.matrix_values())
+
+
+def multi_cut_rve():
+    """Coarse mesh with close inclusions: exercises the two- and three-region
+    templates (quad and polygon children)."""
+    incs = [(0.30, 0.50, 0.17, 1), (0.66, 0.50, 0.17, 2), (0.50, 0.20, 0.11, 1), (0.49, 0.79, 0.12, 2)]
+    return RVE(nx=12, ny=12, inclusions=incs, materials=[(3000.0, 0.35), (70000.0, 0.2), (20000.0, 0.3)])
+
+
+CASES = {
+    "golden_8x8": lambda: rve_from_golden(golden("linear_8x8.npz")),
+    "config0": config0,
+    "golden_3inc": lambda: rve_from_golden(golden("linear_3inc.npz")),
+    "multi_cut": multi_cut_rve,
+    "rsa_48": lambda: RVE(nx=48, ny=48, inclusions=[(x, y, r, 1) for x, y, r in rsa_circles(7, 12, 0.05, 0.1, 0.01)]),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_gpu_assembled_K_matches_oracle(case):
+    rve = CASES[case]()
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    pb.Assembler(ctx).assemble_linear()
+    Kg = gpu_K(ctx, e)
+    Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()
+    assert rel_fro(Kg, Ko) <= K_TOL
+    ctx.close()
+
+
+def test_multi_cut_case_covers_polygon_templates():
+    m = pb.Mesh(multi_cut_rve())
+    e = m.export()
+    T = pb.template_table()
+    kinds = {int(T[t][2]) for t in e["cut_tmpl"]}  # number of children per template used
+    assert 3 in kinds
+
+
+@pytest.mark.parametrize("name", ["linear_8x8.npz", "linear_cfg0.npz", "linear_3inc.npz"])
+def test_gpu_K_and_solution_match_reference(name):
+    g = golden(name)
+    rve = rve_from_golden(g)
+    prob = pb.ProblemLinearElasticity(rve)
+    prob.init()
+    e = prob.mesh.export()
+    prob.get_solver().configure(rtol=1e-13)
+    st = prob.solve_problem()
+    assert st.status == 0
+    Kg = gpu_K(prob.ctx, e)
+    assert rel_fro(permute_to_ref(Kg, e["ref_dof"]), ref_full_K(g)) <= K_TOL
+    u = prob.get_solution()
+    n = u.size
+    ur = np.empty(n)
+    ur[e["ref_dof"]] = u
+    uref = np.concatenate([g["U.f"], g["U.p"]])
+    assert np.linalg.norm(ur - uref) / np.linalg.norm(uref) <= U_TOL
+    prob.ctx.close()
+
+
+@pytest.mark.parametrize("precision", [_lib.PG_PRECISION_FP64, _lib.PG_PRECISION_MIXED])
+@pytest.mark.parametrize("precond", [_lib.PG_PREC_JACOBI, _lib.PG_PREC_BLOCK_JACOBI])
+def test_gpu_linear_solve_matches_direct_solve(precision, precond):
+    rve = config0()
+    prob = pb.ProblemLinearElasticity(rve)
+    prob.init()
+    e = prob.mesh.export()
+    prob.get_solver().configure(precision=precision, precond=precond, rtol=1e-13, inner_rtol=1e-4)
+    st = prob.solve_problem()
+    assert st.status == 0 and st.rel_residual <= 1e-13
+    if precision == _lib.PG_PRECISION_MIXED:
+        assert st.refinements >= 1
+    Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()
+    uo = oracle.solve_linear(Ko, e["fixed"], e["ubar"])
+    u = prob.get_solution()
+    assert np.linalg.norm(u - uo) / np.linalg.norm(uo) <= U_TOL
+    prob.ctx.close()
+
+
+def test_gpu_cohesive_residual_and_state_match_reference():
+    """Internal force and trial delta_max at the reference's converged states
+    of four load steps (Ortiz-Pandolfi law, viscosity, history)."""
+    g = golden("cohesive_16x16.npz")
+    rve = rve_from_golden(g, cohesive=True)
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    asm = pb.Assembler(ctx)
+    ref = e["ref_dof"]
+    dt = float(g["cfg.dt"][0])
+    isv_c = np.zeros(m.info["n_cohesive_qp"])
+    om = oracle.from_product(e, pb.template_table(), rve)
+    for k in range(1, int(g["cfg.nsteps"][0]) + 1):
+        U = np.concatenate([g[f"step{k}.U.f"], g[f"step{k}.U.p"]])[ref]
+        ctx.set_vector(0, U)
+        ctx.set_isv(isv_c, committed=True)
+        asm.assemble_nonlinear(dt, True, True)
+        f = ctx.vector(1)
+        fref = np.concatenate([g[f"step{k}.Pint.f"], g[f"step{k}.Pint.p"]])[ref]
+        assert np.linalg.norm(f - fref) / np.linalg.norm(fref) <= 1e-11
+        np.testing.assert_allclose(ctx.isv(committed=False), g[f"step{k}.isv.delta_max"], rtol=1e-12, atol=0)
+        # tangent against the oracle at the same state
+        Ko, fo, _ = om.assemble(u=U, dt=dt, isv_c=isv_c, want_K=True, want_f=True)
+        assert rel_fro(gpu_K(ctx, e), Ko) <= K_TOL
+        isv_c = g[f"step{k}.isv.delta_max"]
+    ctx.close()
+
+
+def test_gpu_bilinear_cohesive_matches_oracle():
+    rve = RVE(nx=20, ny=20, inclusions=[(0.45, 0.5, 0.27, 1)], cohesive=True, coh_law=1,
+              coh_params=(30.0, 0.01, 1.0e6, 1.0), strain=0.02)
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    rng = np.random.default_rng(3)
+    U = 1e-4 * rng.standard_normal(m.info["n_dof"])
+    isv_c = np.abs(2e-5 * rng.standard_normal(m.info["n_cohesive_qp"]))
+    ctx.set_vector(0, U)
+    ctx.set_isv(isv_c, committed=True)
+    pb.Assembler(ctx).assemble_nonlinear(0.02, True, True)
+    Ko, fo, io = oracle.from_product(e, pb.template_table(), rve).assemble(u=U, dt=0.02, isv_c=isv_c, want_K=True,
+                                                                           want_f=True)
+    assert rel_fro(gpu_K(ctx, e), Ko) <= K_TOL
+    assert np.linalg.norm(ctx.vector(1) - fo) / np.linalg.norm(fo) <= 1e-12
+    np.testing.assert_allclose(ctx.isv(committed=False), io, rtol=1e-13, atol=0)
+    ctx.close()
+
+
+def test_gpu_host_buffer_entry_point():
+    rve = config0()
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    xy = np.ascontiguousarray(e["xy"].reshape(-1))
+    kh = np.zeros(4 * m.info["n_blocks"])
+    _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, _lib.dptr(xy), _lib.dptr(kh)))
+    Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()
+    assert rel_fro(bsr_to_csr(e["row_ptr"], e["col"], kh), Ko) <= K_TOL
+    ctx.close()
+
+
+@pytest.mark.slow
+def test_gpu_config1_full_size_K_and_properties():
+    """Full-size configuration 1 (524,288 elements): GPU K against the oracle,
+    plus size-independent properties (symmetry, rigid-body null space)."""
+    rve = config1()
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    pb.Assembler(ctx).assemble_linear()
+    Kg = gpu_K(ctx, e)
+    Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()
+    assert rel_fro(Kg, Ko) <= K_TOL
+    assert rel_fro(Kg.T.tocsr(), Kg) <= 1e-14
+    # translations are in the null space of K (enrichment DOFs move with zero)
+    n_reg = e["n_regular_nodes"]
+    t = np.zeros(Kg.shape[0])
+    t[0:2 * n_reg:2] = 1.0
+    assert np.abs(Kg @ t).max() <= 1e-9 * np.abs(Kg.data).max()
+    ctx.close()

@@ -168,6 +168,43 @@ void pg_solver_cfg_default(pg_solver_cfg* cfg);
  * K_ff U_f = rhs, reactions F_p = K_pf U_f + K_pp U_p.  Assembles K first if needed. */
 int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg, pg_solve_stats* stats);
 
+/* ---- nonlinear load stepping (cohesive RVEs) ---- */
+#define PG_PREDICT_ZEROTH 0   /* keep the last converged free DOFs (the reference, SolverNonlinear.cpp:254-267) */
+#define PG_PREDICT_LINEAR 1   /* extrapolate linearly in the load factor */
+#define PG_PREDICT_GIVEN 2    /* the caller set U before the step (e.g. a learned warm start) */
+
+typedef struct pg_newton_cfg {
+    int32_t n_steps;                /* equal load steps to T_final */
+    double T_final;
+    double rtol, atol, stol;        /* SNES defaults: 1e-8, 1e-50, 1e-8 */
+    int32_t max_it;                 /* Newton iterations per step (SNES default 50) */
+    int32_t precision;              /* linear solves: PG_PRECISION_FP64 or PG_PRECISION_MIXED */
+    int32_t precond;
+    double lin_rtol;                /* floor of the Krylov forcing term */
+    double inner_rtol;              /* mixed: FP32 inner tolerance */
+    int32_t lin_max_iter;
+    int32_t max_repeat;             /* load-step repeats with dt *= 0.25 (reference: 20) */
+    int32_t predictor;              /* PG_PREDICT_* */
+} pg_newton_cfg;
+
+typedef struct pg_step_stats {
+    double t_frac, dt;
+    int32_t newton_its, krylov_its, gmres_fallbacks, repeats;
+    double res0, res;               /* FP64 ||r|| of the predictor and at the end */
+    int32_t reason;                 /* SNES-style: 2 abs, 3 rel, 4 step; <0 diverged */
+    double seconds;                 /* device time of the step */
+} pg_step_stats;
+
+void pg_newton_cfg_default(pg_newton_cfg* cfg);
+/* SolverNonlinearSNES::nonlinearStep for one load step at load factor t_frac with
+ * step dt (viscous regularisation); the trial cohesive state is left for pg_commit_isv. */
+int pg_newton_load_step(pg_ctx* c, double t_frac, double dt, const pg_newton_cfg* cfg, pg_step_stats* stats);
+/* SolverNonlinear::solve: equal load steps with the reference's step cutting on failure;
+ * commits the cohesive state after every converged step.  Writes up to max_records
+ * step records. */
+int pg_solve_nonlinear(pg_ctx* c, const pg_newton_cfg* cfg, pg_step_stats* per_step, int32_t max_records,
+                       int32_t* n_records);
+
 /* ---- host copies (tests, parity, output) ---- */
 int pg_get_matrix(pg_ctx* c, double* vals_host);         /* 4*n_blocks */
 int pg_get_vector(pg_ctx* c, int32_t which, double* out); /* which: 0=U, 1=F_int, 2=reaction/residual work */

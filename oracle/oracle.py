@@ -263,3 +263,35 @@ def cohesive_law(law, params, dt, dmax, delta):
     dm = C.c_double()
     lib().orc_cohesive_law(int(law), _d(p), float(dt), float(dmax), _d(d), _d(t), _d(Dc), C.byref(dm))
     return t, Dc.reshape(2, 2), dm.value
+
+
+def newton_load_step(om: "OracleMesh", U, fixed, ubar, t_frac, dt, isv_c, rtol=1e-8, max_it=50):
+    """The reference's SNES Newton step restated on the CPU (direct solves,
+    backtracking on 0.5||r||^2 with sufficient decrease 1e-4).  Returns
+    (U, isv_trial, iterations, ||r0||, ||r||)."""
+    import scipy.sparse.linalg as sla
+    fixed = np.asarray(fixed, bool)
+    free = ~fixed
+    U = np.array(U, dtype=np.float64)
+    U[fixed] = t_frac * np.asarray(ubar)[fixed]
+    _, f, isv_t = om.assemble(u=U, dt=dt, isv_c=isv_c, want_K=False, want_f=True)
+    r = f.copy(); r[fixed] = 0.0
+    r0 = np.linalg.norm(r)
+    rn = r0
+    it = 0
+    while it < max_it and rn > rtol * r0:
+        K, _, _ = om.assemble(u=U, dt=dt, isv_c=isv_c, want_K=True, want_f=False)
+        d = np.zeros_like(U)
+        d[free] = sla.spsolve(K[free][:, free].tocsc(), -r[free])
+        lam = 1.0
+        for _ in range(12):
+            Ut = U + lam * d
+            _, ft, it_t = om.assemble(u=Ut, dt=dt, isv_c=isv_c, want_K=False, want_f=True)
+            rt = ft.copy(); rt[fixed] = 0.0
+            if np.linalg.norm(rt) ** 2 <= (1 - 2e-4 * lam) * rn ** 2:
+                break
+            lam *= 0.5
+        U, r, isv_t = Ut, rt, it_t
+        rn = np.linalg.norm(r)
+        it += 1
+    return U, isv_t, it, r0, rn

@@ -68,6 +68,28 @@ class SolveStats(C.Structure):
     ]
 
 
+PG_PREDICT_ZEROTH = 0
+PG_PREDICT_LINEAR = 1
+PG_PREDICT_GIVEN = 2
+
+
+class NewtonCfg(C.Structure):
+    _fields_ = [
+        ("n_steps", C.c_int32), ("T_final", C.c_double), ("rtol", C.c_double), ("atol", C.c_double),
+        ("stol", C.c_double), ("max_it", C.c_int32), ("precision", C.c_int32), ("precond", C.c_int32),
+        ("lin_rtol", C.c_double), ("inner_rtol", C.c_double), ("lin_max_iter", C.c_int32),
+        ("max_repeat", C.c_int32), ("predictor", C.c_int32),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("t_frac", C.c_double), ("dt", C.c_double), ("newton_its", C.c_int32), ("krylov_its", C.c_int32),
+        ("gmres_fallbacks", C.c_int32), ("repeats", C.c_int32), ("res0", C.c_double), ("res", C.c_double),
+        ("reason", C.c_int32), ("seconds", C.c_double),
+    ]
+
+
 class PgError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[pg status {code}] {msg}")
@@ -107,6 +129,10 @@ def _load() -> C.CDLL:
         "pg_get_isv": ([v, C.c_int32, _dp], C.c_int),
         "pg_set_isv": ([v, C.c_int32, _dp], C.c_int),
         "pg_assembly_timing": ([v, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+        "pg_newton_cfg_default": ([C.POINTER(NewtonCfg)], None),
+        "pg_newton_load_step": ([v, C.c_double, C.c_double, C.POINTER(NewtonCfg), C.POINTER(StepStats)], C.c_int),
+        "pg_solve_nonlinear": ([v, C.POINTER(NewtonCfg), C.POINTER(StepStats), C.c_int32, C.POINTER(C.c_int32)],
+                               C.c_int),
         "pg_last_error": ([], C.c_char_p),
         "pg_version": ([], C.c_char_p),
     }
@@ -125,7 +151,8 @@ DECLARED_SYMBOLS = (
     "pg_template_table", "pg_mesh_destroy", "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_sync",
     "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
     "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",
-    "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_last_error", "pg_version",
+    "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
+    "pg_solve_nonlinear", "pg_last_error", "pg_version",
 )
 
 

@@ -86,6 +86,14 @@ struct Ctx {
     float* qf = nullptr;
     float* xf = nullptr;
     float* minvf = nullptr;
+    double* b = nullptr;               // right-hand side of the current Krylov solve
+    double* res = nullptr;             // Newton residual
+    double* Ut = nullptr;              // Newton trial displacement
+    double* Uprev = nullptr;           // last converged displacement
+    double* Uold = nullptr;            // the one before (linear extrapolation predictor)
+    double* V = nullptr;               // GMRES basis, (gm + 1) * n_dof, allocated on first use
+    int gm = 0;
+    double* hbuf = nullptr;            // GMRES multi-dot results (64)
     double* scal = nullptr;            // device scalars
     int* iflags = nullptr;             // device flags
     double* h_scal = nullptr;          // pinned host mirror
@@ -109,6 +117,14 @@ int launch_to_fp32(Ctx& c, cudaStream_t s);
 
 // solver entry points (pg_solve.cu)
 int solve_linear_system(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
+// mask(K) x = b for x (x starts at 0); b = c.b (masked); result in c.dx
+int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
+// ||v||^2 of a device vector (synchronises)
+double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s);
+void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
+
+// Newton (pg_newton.cu)
+int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s);
 
 }  // namespace pgb
 

@@ -246,6 +246,89 @@ __global__ inline void k_apply_dirichlet(int nd, const uint8_t* __restrict__ fix
     if (i < nd && fixed[i]) U[i] = tf * ubar[i];
 }
 
-void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
+// out = mask(b) - out  (b may be null: zero)
+__global__ inline void k_rhs_minus(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ b, double* out) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) out[i] = fixed[i] ? 0.0 : ((b ? b[i] : 0.0) - out[i]);
+}
+
+template <typename VT>
+__global__ void k_copy(int n, const VT* __restrict__ a, VT* __restrict__ b) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+__global__ inline void k_scale_copy(int n, const double* __restrict__ a, double* __restrict__ b, double s) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) b[i] = s * a[i];
+}
+
+__global__ inline void k_scale_inplace(int n, double* a, double s) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) a[i] *= s;
+}
+
+// z = M^-1 v per node (2x2 blocks)
+__global__ inline void k_apply_prec_vec(int n, const double* __restrict__ minv, const double* __restrict__ v,
+                                        double* __restrict__ z) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const double* m = minv + 4 * (size_t)i;
+    const double v0 = v[2 * i], v1 = v[2 * i + 1];
+    z[2 * i] = m[0] * v0 + m[1] * v1;
+    z[2 * i + 1] = m[2] * v0 + m[3] * v1;
+}
+
+// out[j] += V_j . w for j < k (V: k vectors of length nd, contiguous)
+__global__ inline void k_multidot(int nd, int k, const double* __restrict__ V, const double* __restrict__ w,
+                                  double* out) {
+    for (int j = 0; j < k; ++j) {
+        const double* vj = V + (size_t)j * nd;
+        double part = 0.0;
+        for (int i = blockIdx.x * kThreads + threadIdx.x; i < nd; i += gridDim.x * kThreads) part += vj[i] * w[i];
+        const double s = block_sum(part);
+        if (threadIdx.x == 0) atomicAdd(&out[j], s);
+    }
+}
+
+// w -= sum_j h_j V_j
+__global__ inline void k_multi_axpy(int nd, int k, const double* __restrict__ V, const double* __restrict__ h,
+                                    double* w) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= nd) return;
+    double acc = w[i];
+    for (int j = 0; j < k; ++j) acc -= h[j] * V[(size_t)j * nd + i];
+    w[i] = acc;
+}
+
+// q += sum_j y_j V_j
+__global__ inline void k_multi_axpy_add(int nd, int k, const double* __restrict__ V, const double* __restrict__ y,
+                                        double* q) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= nd) return;
+    double acc = q[i];
+    for (int j = 0; j < k; ++j) acc += y[j] * V[(size_t)j * nd + i];
+    q[i] = acc;
+}
+
+// out = mask(a)
+__global__ inline void k_mask_copy(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ a, double* out) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) out[i] = fixed[i] ? 0.0 : a[i];
+}
+
+// out = U + s d on free DOFs, U on prescribed DOFs
+__global__ inline void k_axpy_to(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ U,
+                                 const double* __restrict__ d, double s, double* out) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) out[i] = fixed[i] ? U[i] : U[i] + s * d[i];
+}
+
+// U += ratio (U - Uold) on free DOFs (linear extrapolation in load)
+__global__ inline void k_extrapolate(int nd, const uint8_t* __restrict__ fixed, double* U, const double* __restrict__ Uold,
+                                     double ratio) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd && !fixed[i]) U[i] += ratio * (U[i] - Uold[i]);
+}
 
 }  // namespace pgb

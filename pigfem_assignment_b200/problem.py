@@ -234,3 +234,53 @@ class ProblemLinearElasticity:
 
     def get_solution(self) -> np.ndarray:
         return self.ctx.vector(0)
+
+
+class ProblemNonlinearStructural:
+    """Problem::init / solve_problem for cohesive RVEs: load stepping with
+    Newton (SolverNonlinear::solve, src/SolverNonlinear.cpp:111-397)."""
+
+    def __init__(self, rve: RVE, device: int = 0):
+        self.rve = rve
+        self.device = device
+        self.mesh: Optional[Mesh] = None
+        self.ctx: Optional[DeviceContext] = None
+        self.cfg = _lib.NewtonCfg()
+        lib.pg_newton_cfg_default(C.byref(self.cfg))
+
+    def init(self) -> None:
+        self.mesh = Mesh(self.rve)
+        self.ctx = DeviceContext(self.mesh, self.device)
+        self.assembler = Assembler(self.ctx)
+        self.solver = Solver(self.ctx)
+
+    def get_solver(self) -> Solver:
+        return self.solver
+
+    def get_assembler(self) -> Assembler:
+        return self.assembler
+
+    def configure(self, **kw) -> None:
+        for k, v in kw.items():
+            if not hasattr(self.cfg, k):
+                raise KeyError(k)
+            setattr(self.cfg, k, v)
+
+    def solve_problem(self, max_records: int = 4096):
+        recs = (_lib.StepStats * max_records)()
+        n = C.c_int32()
+        check(lib.pg_solve_nonlinear(self.ctx.handle, C.byref(self.cfg), recs, max_records, C.byref(n)),
+              "pg_solve_nonlinear")
+        return [recs[i] for i in range(min(n.value, max_records))]
+
+    def load_step(self, t_frac: float, dt: float) -> _lib.StepStats:
+        st = _lib.StepStats()
+        check(lib.pg_newton_load_step(self.ctx.handle, t_frac, dt, C.byref(self.cfg), C.byref(st)),
+              "pg_newton_load_step")
+        return st
+
+    def commit(self) -> None:
+        check(lib.pg_commit_isv(self.ctx.handle))
+
+    def get_solution(self) -> np.ndarray:
+        return self.ctx.vector(0)

@@ -266,7 +266,6 @@ def run_b200_arm(args):
     for _ in range(max(3, args.steps // 2)):
         flush.fill_(2.0)
         torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, xy_p, kh_p))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
@@ -283,8 +282,13 @@ def run_b200_arm(args):
             ctx.set_vector(0, np.zeros(info["n_dof"]))
             torch.cuda.synchronize()
             a, b = assemble_timed()
-            st = solver.solve_linear()
-            load[name] = {"ms": a + b + 1e3 * st.seconds, "assemble_ms": a + b, "solve_ms": 1e3 * st.seconds,
+            try:
+                st = solver.solve_linear()
+                status = "ok"
+            except _lib.PgError as ex:
+                st = solver.stats
+                status = str(ex)
+            load[name] = {"status": status, "ms": a + b + 1e3 * st.seconds, "assemble_ms": a + b, "solve_ms": 1e3 * st.seconds,
                           "krylov_iterations": st.iterations, "refinements": st.refinements,
                           "rel_residual": st.rel_residual}
 

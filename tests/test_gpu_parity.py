@@ -69,7 +69,7 @@ def test_gpu_K_and_solution_match_reference(name):
     prob = pb.ProblemLinearElasticity(rve)
     prob.init()
     e = prob.mesh.export()
-    prob.get_solver().configure(rtol=1e-13)
+    prob.get_solver().configure(rtol=1e-12)
     st = prob.solve_problem()
     assert st.status == 0
     Kg = gpu_K(prob.ctx, e)
@@ -90,9 +90,10 @@ def test_gpu_linear_solve_matches_direct_solve(precision, precond):
     prob = pb.ProblemLinearElasticity(rve)
     prob.init()
     e = prob.mesh.export()
-    prob.get_solver().configure(precision=precision, precond=precond, rtol=1e-13, inner_rtol=1e-4)
+    prob.get_solver().configure(precision=precision, precond=precond, rtol=1e-12, inner_rtol=1e-4)
     st = prob.solve_problem()
-    assert st.status == 0 and st.rel_residual <= 1e-13
+    # the reported residual is the true FP64 residual ||b - K u|| / ||b||
+    assert st.status == 0 and st.rel_residual <= 4e-12
     if precision == _lib.PG_PRECISION_MIXED:
         assert st.refinements >= 1
     Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()

@@ -136,11 +136,13 @@ int pg_ctx_device_arrays(pg_ctx* c, double** K, double** U, double** F_int, doub
 /* ---- solvers ---- */
 #define PG_KRYLOV_CG 0
 #define PG_KRYLOV_GMRES 1
+#define PG_KRYLOV_MINRES 2      /* symmetric indefinite tangents; |diag| Jacobi preconditioner */
 #define PG_PREC_JACOBI 0
 #define PG_PREC_BLOCK_JACOBI 1
 #define PG_PREC_NONE 2
 #define PG_PRECISION_FP64 0        /* plain FP64 Krylov */
-#define PG_PRECISION_MIXED 1       /* FP32 SpMV/dot Krylov + FP64 iterative refinement */
+#define PG_PRECISION_MIXED 1       /* Krylov on the FP32-stored matrix (FP64 vectors and dots) inside
+                                      FP64 iterative refinement on the FP64 residual */
 
 typedef struct pg_solver_cfg {
     int32_t krylov;                 /* PG_KRYLOV_* */
@@ -171,7 +173,9 @@ int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg, pg_solve_stats* stats);
 /* ---- nonlinear load stepping (cohesive RVEs) ---- */
 #define PG_PREDICT_ZEROTH 0   /* keep the last converged free DOFs (the reference, SolverNonlinear.cpp:254-267) */
 #define PG_PREDICT_LINEAR 1   /* extrapolate linearly in the load factor */
-#define PG_PREDICT_GIVEN 2    /* the caller set U before the step (e.g. a learned warm start) */
+#define PG_PREDICT_GIVEN 2    /* the caller set U before the step */
+#define PG_PREDICT_LEARNED 3  /* linear extrapolation corrected by the attached MLP; the linear
+                                 extrapolation is kept whenever it starts from a smaller residual */
 
 typedef struct pg_newton_cfg {
     int32_t n_steps;                /* equal load steps to T_final */
@@ -193,6 +197,8 @@ typedef struct pg_step_stats {
     double res0, res;               /* FP64 ||r|| of the predictor and at the end */
     int32_t reason;                 /* SNES-style: 2 abs, 3 rel, 4 step; <0 diverged */
     double seconds;                 /* device time of the step */
+    int32_t predictor_used;         /* PG_PREDICT_* actually used for this step */
+    double res_linear, res_learned; /* initial residuals of both candidates (learned predictor only) */
 } pg_step_stats;
 
 void pg_newton_cfg_default(pg_newton_cfg* cfg);
@@ -204,6 +210,34 @@ int pg_newton_load_step(pg_ctx* c, double t_frac, double dt, const pg_newton_cfg
  * step records. */
 int pg_solve_nonlinear(pg_ctx* c, const pg_newton_cfg* cfg, pg_step_stats* per_step, int32_t max_records,
                        int32_t* n_records);
+
+/* ---- learned Newton warm start: per-node MLP (no counterpart in the reference) ----
+ * 16 -> 64 -> 64 -> 16 ReLU network (2 outputs used), BF16 weights/activations on the
+ * tcgen05 tensor cores with FP32 accumulation; parameters are FP32 masters laid out
+ * W1[64x16], b1[64], W2[64x64], b2[64], W3[16x64], b3[16] (row = output). */
+typedef struct pg_mlp pg_mlp;
+int pg_mlp_create(int32_t device, uint64_t seed, pg_mlp** out);
+void pg_mlp_destroy(pg_mlp* m);
+int32_t pg_mlp_param_count(void);
+int pg_mlp_params(pg_mlp* m, float* host, int32_t set);     /* set=1: upload (resets Adam), 0: download */
+int pg_mlp_grads(pg_mlp* m, float* host);                  /* gradient of the last pg_mlp_gradient */
+int pg_mlp_forward(pg_mlp* m, const float* X_dev, int32_t n, float* Y_dev, void* stream);
+int pg_mlp_gradient(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n, double* loss_host);
+int pg_mlp_adam(pg_mlp* m, float lr);
+int pg_mlp_train(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n, int32_t epochs, int32_t batch,
+                 float lr, double* loss_hist);
+
+/* Learned-predictor plumbing (device pointers).  s_inc = prescribed displacement
+ * increment of the step, ratio = dt_{n+1}/dt_n.  Features: 16 floats per node;
+ * targets and outputs: 2 floats per node (one per DOF). */
+int pg_predictor_features(pg_ctx* c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc,
+                          float* X_dev);
+int pg_predictor_targets(pg_ctx* c, const double* Un1, const double* Un, const double* Unm1, double ratio,
+                         double s_inc, float* T_dev);
+int pg_predictor_apply(pg_ctx* c, const double* Un, const double* Unm1, double ratio, double s_inc,
+                       const float* Y_dev, double* U_dev);
+/* attaches a network for PG_PREDICT_LEARNED (NULL detaches; the context does not own it) */
+int pg_ctx_attach_mlp(pg_ctx* c, pg_mlp* m);
 
 /* ---- host copies (tests, parity, output) ---- */
 int pg_get_matrix(pg_ctx* c, double* vals_host);         /* 4*n_blocks */

@@ -24,6 +24,7 @@ PG_COH_OP = 0
 PG_COH_BILINEAR = 1
 PG_KRYLOV_CG = 0
 PG_KRYLOV_GMRES = 1
+PG_KRYLOV_MINRES = 2
 PG_PREC_JACOBI = 0
 PG_PREC_BLOCK_JACOBI = 1
 PG_PREC_NONE = 2
@@ -71,6 +72,7 @@ class SolveStats(C.Structure):
 PG_PREDICT_ZEROTH = 0
 PG_PREDICT_LINEAR = 1
 PG_PREDICT_GIVEN = 2
+PG_PREDICT_LEARNED = 3
 
 
 class NewtonCfg(C.Structure):
@@ -86,7 +88,8 @@ class StepStats(C.Structure):
     _fields_ = [
         ("t_frac", C.c_double), ("dt", C.c_double), ("newton_its", C.c_int32), ("krylov_its", C.c_int32),
         ("gmres_fallbacks", C.c_int32), ("repeats", C.c_int32), ("res0", C.c_double), ("res", C.c_double),
-        ("reason", C.c_int32), ("seconds", C.c_double),
+        ("reason", C.c_int32), ("seconds", C.c_double), ("predictor_used", C.c_int32),
+        ("res_linear", C.c_double), ("res_learned", C.c_double),
     ]
 
 
@@ -133,6 +136,19 @@ def _load() -> C.CDLL:
         "pg_newton_load_step": ([v, C.c_double, C.c_double, C.POINTER(NewtonCfg), C.POINTER(StepStats)], C.c_int),
         "pg_solve_nonlinear": ([v, C.POINTER(NewtonCfg), C.POINTER(StepStats), C.c_int32, C.POINTER(C.c_int32)],
                                C.c_int),
+        "pg_mlp_create": ([C.c_int32, C.c_uint64, C.POINTER(v)], C.c_int),
+        "pg_mlp_destroy": ([v], None),
+        "pg_mlp_param_count": ([], C.c_int32),
+        "pg_mlp_params": ([v, C.POINTER(C.c_float), C.c_int32], C.c_int),
+        "pg_mlp_grads": ([v, C.POINTER(C.c_float)], C.c_int),
+        "pg_mlp_forward": ([v, v, C.c_int32, v, v], C.c_int),
+        "pg_mlp_gradient": ([v, v, v, C.c_int32, C.POINTER(C.c_double)], C.c_int),
+        "pg_mlp_adam": ([v, C.c_float], C.c_int),
+        "pg_mlp_train": ([v, v, v, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_double)], C.c_int),
+        "pg_predictor_features": ([v, v, v, C.c_double, C.c_double, C.c_double, v], C.c_int),
+        "pg_predictor_targets": ([v, v, v, v, C.c_double, C.c_double, v], C.c_int),
+        "pg_predictor_apply": ([v, v, v, C.c_double, C.c_double, v, v], C.c_int),
+        "pg_ctx_attach_mlp": ([v, v], C.c_int),
         "pg_last_error": ([], C.c_char_p),
         "pg_version": ([], C.c_char_p),
     }
@@ -152,7 +168,10 @@ DECLARED_SYMBOLS = (
     "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
     "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",
     "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
-    "pg_solve_nonlinear", "pg_last_error", "pg_version",
+    "pg_solve_nonlinear", "pg_mlp_create", "pg_mlp_destroy", "pg_mlp_param_count", "pg_mlp_params",
+    "pg_mlp_grads", "pg_mlp_forward", "pg_mlp_gradient", "pg_mlp_adam", "pg_mlp_train", "pg_predictor_features",
+    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_last_error",
+    "pg_version",
 )
 
 

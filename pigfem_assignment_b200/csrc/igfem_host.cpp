@@ -524,12 +524,13 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
         return (it != e && *it == c) ? (int)(it - m.col.data()) : -1;
     };
 
-    // per regular node: adjacent uncut elements with the node's local vertex
-    m.ne_ptr.assign(m.n_reg + 1, 0);
+    // per node: adjacent uncut elements with the node's local vertex (empty
+    // for enrichment nodes, whose rows only the cut-element kernel fills)
+    m.ne_ptr.assign(nn + 1, 0);
     for (int e = 0; e < m.n_elem; ++e)
         if (m.elem_cut[e] < 0)
             for (int v = 0; v < 3; ++v) m.ne_ptr[m.conn[3 * e + v] + 1]++;
-    for (int n = 0; n < m.n_reg; ++n) m.ne_ptr[n + 1] += m.ne_ptr[n];
+    for (int n = 0; n < nn; ++n) m.ne_ptr[n + 1] += m.ne_ptr[n];
     m.ne_list.resize(m.ne_ptr.back());
     {
         std::vector<int> fill(m.ne_ptr.begin(), m.ne_ptr.end() - 1);

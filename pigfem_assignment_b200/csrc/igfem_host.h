@@ -106,7 +106,7 @@ struct HostMesh {
     int n_free = 0;
     // 2x2-block CSR pattern over all nodes
     std::vector<int> row_ptr, col, diag_slot;
-    // per regular node: adjacent uncut elements, packed (elem << 2) | local vertex
+    // per node: adjacent uncut elements, packed (elem << 2) | local vertex
     std::vector<int> ne_ptr, ne_list;
     // per cut element: block slots for every (local a, local b), (3+kMaxEnr)^2 entries, -1 unused
     std::vector<int> cut_slot;

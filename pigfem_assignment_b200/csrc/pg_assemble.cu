@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kRowThreads) k_assemble_rows(RowArgs a) {
         double* dst = tile ? sK + 4 * (r0 - seg0) : a.K + 4 * (size_t)r0;
         if (a.want_K && !tile)
             for (int i = 0; i < 4 * deg; ++i) dst[i] = 0.0;
-        if (node < a.n_reg) {
+        {
             int cols[kRowRegCols];
 #pragma unroll
             for (int q = 0; q < kRowRegCols; ++q) cols[q] = (q < deg) ? a.col[r0 + q] : -1;
@@ -184,6 +184,144 @@ __global__ void __launch_bounds__(kRowThreads) k_assemble_rows(RowArgs a) {
         __syncthreads();
         if (threadIdx.x == 0) bulk_store_smem_to_global(a.K + 4 * (size_t)seg0, sK, (unsigned)nseg * 32u);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled row kernel: a CTA of 256 threads owns 128 consecutive node rows.  The
+// rows' column indices and pointers are staged in shared memory, every
+// (node, adjacent uncut element) entry of the CTA's slice of ne_list is one
+// thread's work item (independent loads, no per-row serial chain), its three
+// 2x2 blocks go into the shared tile with FP64 shared atomics, and the tile
+// leaves with one bulk async store.  A CTA whose slice does not fit the tile
+// runs the per-row code path below instead.
+// ---------------------------------------------------------------------------
+constexpr int kTileNodes = 128;
+constexpr int kTileThreads = 256;
+constexpr int kTileCap = 1152;  // blocks per tile (36 KB of values)
+
+__global__ void __launch_bounds__(kTileThreads) k_assemble_tile(RowArgs a) {
+    extern __shared__ __align__(128) double sK[];
+    int* scol = reinterpret_cast<int*>(sK + 4 * kTileCap);
+    __shared__ int srp[kTileNodes + 1];
+    __shared__ int sne[kTileNodes + 1];
+    __shared__ double sF[2 * kTileNodes];
+    const int node0 = blockIdx.x * kTileNodes;
+    const int node_end = min(node0 + kTileNodes, a.n_nodes);
+    const int nn = node_end - node0;
+    const int seg0 = a.row_ptr[node0];
+    const int nseg = a.row_ptr[node_end] - seg0;
+    if (nseg > kTileCap) {
+        // per-row path for an oversized slice (rows near many enrichment nodes)
+        const int node = node0 + (int)threadIdx.x;
+        if (threadIdx.x >= kTileNodes || node >= node_end) return;
+        const int r0 = a.row_ptr[node], r1 = a.row_ptr[node + 1];
+        double* dst = a.K + 4 * (size_t)r0;
+        if (a.want_K)
+            for (int i = 0; i < 4 * (r1 - r0); ++i) dst[i] = 0.0;
+        double fx = 0.0, fy = 0.0;
+        for (int k = a.ne_ptr[node]; k < a.ne_ptr[node + 1]; ++k) {
+            const int e = a.ne_list[k] >> 2, v = a.ne_list[k] & 3;
+            const int4 el = a.elem4[e];
+            const int nid[3] = {el.x, el.y, el.z};
+            const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
+            const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
+            const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+            const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
+            const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
+            const double d11 = a.dmat[3 * el.w], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
+            const double s = 0.5 / J;
+            const double ba = (v == 0 ? b[0] : v == 1 ? b[1] : b[2]) * s;
+            const double ca = (v == 0 ? c[0] : v == 1 ? c[1] : c[2]) * s;
+            for (int t = 0; t < 3; ++t) {
+                const double bb = b[t], cb = c[t];
+                const double k00 = ba * d11 * bb + ca * d33 * cb, k01 = ba * d12 * cb + ca * d33 * bb;
+                const double k10 = ca * d12 * bb + ba * d33 * cb, k11 = ca * d11 * cb + ba * d33 * bb;
+                const int nt = nid[t];
+                if (a.want_f) {
+                    fx += k00 * a.u[2 * nt] + k01 * a.u[2 * nt + 1];
+                    fy += k10 * a.u[2 * nt] + k11 * a.u[2 * nt + 1];
+                }
+                if (a.want_K)
+                    for (int q = r0; q < r1; ++q)
+                        if (a.col[q] == nt) {
+                            double* d = a.K + 4 * (size_t)q;
+                            d[0] += k00; d[1] += k01; d[2] += k10; d[3] += k11;
+                            break;
+                        }
+            }
+        }
+        if (a.want_f) { a.f[2 * node] = fx; a.f[2 * node + 1] = fy; }
+        return;
+    }
+    // stage the slice: row pointers, adjacency pointers, columns; zero the tile
+    for (int i = threadIdx.x; i <= nn; i += kTileThreads) {
+        srp[i] = a.row_ptr[node0 + i] - seg0;
+        sne[i] = a.ne_ptr[node0 + i];
+    }
+    if (a.want_K) {
+        double2* s2 = reinterpret_cast<double2*>(sK);
+        for (int i = threadIdx.x; i < 2 * nseg; i += kTileThreads) s2[i] = make_double2(0.0, 0.0);
+        for (int i = threadIdx.x; i < nseg; i += kTileThreads) scol[i] = a.col[seg0 + i];
+    }
+    for (int i = threadIdx.x; i < 2 * kTileNodes; i += kTileThreads) sF[i] = 0.0;
+    __syncthreads();
+    const int k_begin = sne[0], k_end = sne[nn];
+    for (int k = k_begin + (int)threadIdx.x; k < k_end; k += kTileThreads) {
+        // owner row: largest li with sne[li] <= k
+        int lo = 0, hi = nn - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sne[mid] <= k) lo = mid; else hi = mid - 1;
+        }
+        const int li = lo;
+        const int packed = a.ne_list[k];
+        const int e = packed >> 2, v = packed & 3;
+        const int4 el = a.elem4[e];
+        const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
+        const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
+        const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+        const double b0 = Y1 - Y2, b1 = Y2 - Y0, b2 = Y0 - Y1;
+        const double c0 = X2 - X1, c1 = X0 - X2, c2 = X1 - X0;
+        const double d11 = a.dmat[3 * el.w], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
+        const double s = 0.5 / J;
+        const double ba = (v == 0 ? b0 : v == 1 ? b1 : b2) * s;
+        const double ca = (v == 0 ? c0 : v == 1 ? c1 : c2) * s;
+        const int rb = srp[li], re = srp[li + 1];
+        double fx = 0.0, fy = 0.0;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const double bb = t == 0 ? b0 : t == 1 ? b1 : b2;
+            const double cb = t == 0 ? c0 : t == 1 ? c1 : c2;
+            const int nt = t == 0 ? el.x : t == 1 ? el.y : el.z;
+            const double k00 = ba * d11 * bb + ca * d33 * cb, k01 = ba * d12 * cb + ca * d33 * bb;
+            const double k10 = ca * d12 * bb + ba * d33 * cb, k11 = ca * d11 * cb + ba * d33 * bb;
+            if (a.want_f) {
+                const double ux = a.u[2 * nt], uy = a.u[2 * nt + 1];
+                fx += k00 * ux + k01 * uy;
+                fy += k10 * ux + k11 * uy;
+            }
+            if (a.want_K) {
+                int q = rb;
+                while (q < re && scol[q] != nt) ++q;
+                if (q < re) {
+                    double* d = sK + 4 * q;
+                    atomicAdd(d + 0, k00);
+                    atomicAdd(d + 1, k01);
+                    atomicAdd(d + 2, k10);
+                    atomicAdd(d + 3, k11);
+                }
+            }
+        }
+        if (a.want_f) {
+            atomicAdd(&sF[2 * li], fx);
+            atomicAdd(&sF[2 * li + 1], fy);
+        }
+    }
+    if (a.want_K) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (a.want_f)
+        for (int i = threadIdx.x; i < 2 * nn; i += kTileThreads) a.f[2 * (size_t)node0 + i] = sF[i];
+    if (a.want_K && threadIdx.x == 0) bulk_store_smem_to_global(a.K + 4 * (size_t)seg0, sK, (unsigned)nseg * 32u);
 }
 
 // ---------------------------------------------------------------------------
@@ -514,10 +652,10 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.f = c.F;
     ra.want_K = want_K;
     ra.want_f = want_f;
-    const int rblocks = (c.n_nodes + kRowThreads - 1) / kRowThreads;
-    const size_t smem = want_K ? (size_t)kRowTileBlocks * 32 : 0;
+    const int rblocks = (c.n_nodes + kTileNodes - 1) / kTileNodes;
+    const size_t smem = (size_t)kTileCap * 36;  // values (32 B) + column (4 B) per block
     if (c.timing) cudaEventRecord(c.ea0, s);
-    if (rblocks > 0) k_assemble_rows<<<rblocks, kRowThreads, smem, s>>>(ra);
+    if (rblocks > 0) k_assemble_tile<<<rblocks, kTileThreads, smem, s>>>(ra);
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {

@@ -35,7 +35,7 @@ int dev_alloc(T** dst, size_t n) {
 }
 
 void free_ctx(Ctx& c) {
-    void* ptrs[] = {c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.dmat, c.cut_elem, c.cut_tmpl,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.dmat, c.cut_elem, c.cut_tmpl,
                     c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
@@ -140,9 +140,10 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     if ((rc = dev_alloc(&c.F, nd))) return rc;
     if ((rc = dev_alloc(&c.isv_c, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
     if ((rc = dev_alloc(&c.isv_t, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
-    for (double** v : {&c.r, &c.z, &c.p, &c.q, &c.dx, &c.b, &c.res, &c.Ut, &c.Uprev, &c.Uold})
+    for (double** v : {&c.r, &c.z, &c.p, &c.q, &c.dx, &c.b, &c.res, &c.Ut, &c.Uprev, &c.Uold, &c.xi})
         if ((rc = dev_alloc(v, nd))) return rc;
     if ((rc = dev_alloc(&c.minv, 4 * nn))) return rc;
+    if ((rc = dev_alloc(&c.mw, 2 * nd))) return rc;
     for (float** v : {&c.rf, &c.zf, &c.pf, &c.qf, &c.xf})
         if ((rc = dev_alloc(v, nd))) return rc;
     if ((rc = dev_alloc(&c.minvf, 4 * nn))) return rc;

@@ -94,6 +94,14 @@ struct Ctx {
     double* V = nullptr;               // GMRES basis, (gm + 1) * n_dof, allocated on first use
     int gm = 0;
     double* hbuf = nullptr;            // GMRES multi-dot results (64)
+    double* xi = nullptr;              // inner correction of the mixed-precision refinement
+    double* mw = nullptr;              // MINRES direction buffers (2 * n_dof)
+    // learned warm start
+    pg_mlp* mlp = nullptr;             // attached network (not owned)
+    int* nq_ptr = nullptr;             // node -> cohesive quadrature points
+    int* nq_list = nullptr;
+    float* featX = nullptr;            // 16 features per node
+    float* featY = nullptr;            // 2 outputs per node
     double* scal = nullptr;            // device scalars
     int* iflags = nullptr;             // device flags
     double* h_scal = nullptr;          // pinned host mirror
@@ -122,6 +130,14 @@ int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
 // ||v||^2 of a device vector (synchronises)
 double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s);
 void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
+
+// learned predictor (pg_predict.cu)
+int launch_features(Ctx& c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc, float* X,
+                    cudaStream_t s);
+int launch_apply(Ctx& c, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y, double* U,
+                 cudaStream_t s);
+double predictor_app(const Ctx& c);
+double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s);
 
 // Newton (pg_newton.cu)
 int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s);

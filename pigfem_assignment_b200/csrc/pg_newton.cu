@@ -38,6 +38,8 @@ double newton_residual(Ctx& c, const double* U, double dt, cudaStream_t s) {
 
 }  // namespace
 
+double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s) { return newton_residual(c, U, dt, s); }
+
 int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s) {
     const int nd = c.n_dof;
     st = pg_step_stats{};
@@ -73,7 +75,8 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
         if (rc != PG_OK) return rc;
         st.krylov_its += ls.iterations;
         if (ls.status == PG_ERR_BREAKDOWN) {
-            lin.krylov = PG_KRYLOV_GMRES;
+            // indefinite tangent (cohesive softening): symmetric MINRES
+            lin.krylov = PG_KRYLOV_MINRES;
             pg_solve_stats gs{};
             rc = krylov_solve(c, lin, gs, s);
             if (rc != PG_OK) return rc;
@@ -181,9 +184,38 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             }
             ++repeat;
             // U holds the last converged solution here (zeroth-order predictor)
-            if (cfg.predictor == PG_PREDICT_LINEAR && nrec > 0)
+            const double tf = (t + dt) / cfg.T_final;
+            int used = PG_PREDICT_ZEROTH;
+            double res_lin = -1.0, res_mlp = -1.0;
+            if (cfg.predictor == PG_PREDICT_LINEAR && nrec > 0) {
                 k_extrapolate<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.U, c.Uold, dt / dt_prev);
-            const int rc = newton_load_step(c, (t + dt) / cfg.T_final, dt, cfg, st, s);
+                used = PG_PREDICT_LINEAR;
+            } else if (cfg.predictor == PG_PREDICT_LEARNED && nrec > 0 && c.mlp) {
+                const double ratio = dt / dt_prev;
+                const double s_inc = predictor_app(c) * dt / cfg.T_final;
+                // candidate 1: linear extrapolation (into Ut)
+                cudaMemcpyAsync(c.Ut, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
+                launch_apply(c, c.Uprev, c.Uold, ratio, s_inc, nullptr, c.Ut, s);
+                k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.Ut);
+                res_lin = std::sqrt(predictor_residual(c, c.Ut, dt, s));
+                // candidate 2: learned correction (into U)
+                int rc = launch_features(c, c.Uprev, c.Uold, tf, ratio, s_inc, c.featX, s);
+                if (rc) return rc;
+                rc = pg_mlp_forward(c.mlp, c.featX, c.n_nodes, c.featY, s);
+                if (rc) return rc;
+                launch_apply(c, c.Uprev, c.Uold, ratio, s_inc, c.featY, c.U, s);
+                k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
+                res_mlp = std::sqrt(predictor_residual(c, c.U, dt, s));
+                used = PG_PREDICT_LEARNED;
+                if (!(res_mlp <= res_lin)) {
+                    cudaMemcpyAsync(c.U, c.Ut, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
+                    used = PG_PREDICT_LINEAR;
+                }
+            }
+            const int rc = newton_load_step(c, tf, dt, cfg, st, s);
+            st.predictor_used = used;
+            st.res_linear = res_lin;
+            st.res_learned = res_mlp;
             if (rc != PG_OK) return rc;
             converged = st.reason > 0;
             if (!converged) {

@@ -311,6 +311,131 @@ __global__ inline void k_multi_axpy_add(int nd, int k, const double* __restrict_
     q[i] = acc;
 }
 
+// ---------------- MINRES (symmetric indefinite, SPD preconditioner) ----------------
+// Scalar slots (device), updated by one thread per iteration.
+enum : int {
+    M_BETA = 16, M_OLDB, M_ALFA, M_BB, M_DBAR, M_EPSLN, M_PHIBAR, M_CS, M_SN, M_PHI, M_DELTA, M_OLDEPS, M_DENOM,
+    M_BETA1, M_TOL, M_ITER, M_NSCAL
+};
+
+// v = y / beta
+__global__ inline void k_mr_v(int nd, const double* __restrict__ y, double* __restrict__ v, const double* scal,
+                              const int* flags) {
+    if (flags[F_DONE]) return;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < nd) v[i] = y[i] / scal[M_BETA];
+}
+
+// y = mask(K v) - (beta/oldb) r1 ; alfa += v.y
+template <typename MT>
+__global__ void __launch_bounds__(kThreads) k_mr_av(int n, const int* __restrict__ row_ptr, const int* __restrict__ col,
+                                                    const MT* __restrict__ K, const double* __restrict__ v,
+                                                    const uint8_t* __restrict__ fixed, const double* __restrict__ r1,
+                                                    double* __restrict__ y, double* scal, const int* flags) {
+    if (flags[F_DONE]) return;
+    const double c = scal[M_OLDB] > 0.0 ? scal[M_BETA] / scal[M_OLDB] : 0.0;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    double part = 0.0;
+    if (i < n) {
+        double y0, y1;
+        bsr_row<MT, double>(i, row_ptr, col, K, v, y0, y1);
+        y0 = fixed[2 * i] ? 0.0 : y0 - c * r1[2 * i];
+        y1 = fixed[2 * i + 1] ? 0.0 : y1 - c * r1[2 * i + 1];
+        y[2 * i] = y0;
+        y[2 * i + 1] = y1;
+        part = v[2 * i] * y0 + v[2 * i + 1] * y1;
+    }
+    const double s = block_sum(part);
+    if (threadIdx.x == 0) atomicAdd(&scal[M_ALFA], s);
+}
+
+// y -= (alfa/beta) r2; r2new = y (written over r1); z = M^-1 r2new (into y); bb += r2new.z
+__global__ inline void __launch_bounds__(kThreads) k_mr_2(int n, double* __restrict__ y, const double* __restrict__ r2,
+                                                           double* __restrict__ r1_to_r2new,
+                                                           const double* __restrict__ minv, double* scal, const int* flags) {
+    if (flags[F_DONE]) return;
+    const double c = scal[M_ALFA] / scal[M_BETA];
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    double part = 0.0;
+    if (i < n) {
+        const double a0 = y[2 * i] - c * r2[2 * i], a1 = y[2 * i + 1] - c * r2[2 * i + 1];
+        r1_to_r2new[2 * i] = a0;
+        r1_to_r2new[2 * i + 1] = a1;
+        const double* m = minv + 4 * (size_t)i;
+        const double z0 = m[0] * a0 + m[1] * a1, z1 = m[2] * a0 + m[3] * a1;
+        y[2 * i] = z0;
+        y[2 * i + 1] = z1;
+        part = a0 * z0 + a1 * z1;
+    }
+    const double s = block_sum(part);
+    if (threadIdx.x == 0) atomicAdd(&scal[M_BB], s);
+}
+
+// Lanczos / Givens scalar recurrences of MINRES (Paige & Saunders 1975)
+__global__ inline void k_mr_scalars(double* sc, int* flags) {
+    if (flags[F_DONE]) return;
+    const double alfa = sc[M_ALFA];
+    const double beta_new = sqrt(fmax(sc[M_BB], 0.0));
+    sc[M_OLDB] = sc[M_BETA];
+    const double oldeps = sc[M_EPSLN];
+    const double delta = sc[M_CS] * sc[M_DBAR] + sc[M_SN] * alfa;
+    const double gbar = sc[M_SN] * sc[M_DBAR] - sc[M_CS] * alfa;
+    sc[M_EPSLN] = sc[M_SN] * beta_new;
+    sc[M_DBAR] = -sc[M_CS] * beta_new;
+    const double gamma = fmax(sqrt(gbar * gbar + beta_new * beta_new), 1e-300);
+    sc[M_CS] = gbar / gamma;
+    sc[M_SN] = beta_new / gamma;
+    sc[M_PHI] = sc[M_CS] * sc[M_PHIBAR];
+    sc[M_PHIBAR] = sc[M_SN] * sc[M_PHIBAR];
+    sc[M_DELTA] = delta;
+    sc[M_OLDEPS] = oldeps;
+    sc[M_DENOM] = 1.0 / gamma;
+    sc[M_BETA] = beta_new;
+    sc[M_ALFA] = 0.0;
+    sc[M_BB] = 0.0;
+    flags[F_ITERS] += 1;
+    if (sc[M_PHIBAR] <= sc[M_TOL] * sc[M_BETA1] || beta_new == 0.0) flags[F_DONE] = 1;
+}
+
+// w_new = (v - oldeps w_{k-2} - delta w_{k-1}) / gamma, written over w_{k-2}; x += phi w_new
+__global__ inline void k_mr_w(int nd, const double* __restrict__ v, double* __restrict__ wkm2,
+                              const double* __restrict__ wkm1, double* __restrict__ x, const double* scal,
+                              const int* flags) {
+    // runs after k_mr_scalars of the same iteration: F_DONE may already be set by it,
+    // the update of this iteration still has to be applied
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= nd) return;
+    if (flags[F_DONE] > 1) return;
+    const double w = (v[i] - scal[M_OLDEPS] * wkm2[i] - scal[M_DELTA] * wkm1[i]) * scal[M_DENOM];
+    wkm2[i] = w;
+    x[i] += scal[M_PHI] * w;
+}
+
+// after an iteration's w-update, a DONE flag raised by this iteration's scalars becomes final
+__global__ inline void k_mr_seal(int* flags) {
+    if (flags[F_DONE] == 1) flags[F_DONE] = 2;
+}
+
+// z = M^-1 r with |diag| Jacobi (SPD preconditioner for MINRES)
+__global__ inline void k_prec_absjacobi(int n, const int* __restrict__ diag, const double* __restrict__ K,
+                                        const uint8_t* __restrict__ fixed, double* minv) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const double* b = K + 4 * (size_t)diag[i];
+    double* m = minv + 4 * (size_t)i;
+    m[0] = fixed[2 * i] ? 0.0 : 1.0 / fabs(b[0]);
+    m[1] = 0.0;
+    m[2] = 0.0;
+    m[3] = fixed[2 * i + 1] ? 0.0 : 1.0 / fabs(b[3]);
+}
+
+__global__ inline void k_dot2(int nd, const double* __restrict__ a, const double* __restrict__ b, double* out) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const double v = (i < nd) ? a[i] * b[i] : 0.0;
+    const double s = block_sum(v);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
 // out = mask(a)
 __global__ inline void k_mask_copy(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ a, double* out) {
     const int i = blockIdx.x * kThreads + threadIdx.x;

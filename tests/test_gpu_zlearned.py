@@ -1,0 +1,56 @@
+"""End to end: the learned warm start trained on GPU-generated trajectories.
+
+Trains the MLP on the first steps of a few seeded cohesive RVEs, then load-
+steps a held-out RVE with the zeroth-order (the reference's), linear and
+learned predictors.  The learned run must converge to the same solution
+(Newton residual is the judge) and the test records what it gains.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from pigfem_assignment_b200 import _lib
+from pigfem_assignment_b200.rve import BILINEAR_PARAMS, RVE, rsa_circles
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def small_rve(seed, nx=48):
+    circ = rsa_circles(seed, 6, 0.06, 0.12, 0.02)
+    return RVE(nx=nx, ny=nx, inclusions=[(x, y, r, 1) for x, y, r in circ], cohesive=True, coh_law=1,
+               coh_params=BILINEAR_PARAMS, strain=0.02, seed=seed)
+
+
+def test_learned_warm_start_trains_and_helps():
+    from pigfem_assignment_b200.learned import MLP, compare_predictors, trajectory_samples
+    n_steps, n_train = 20, 10
+    xs, ts = [], []
+    for seed in range(4):
+        x, t, recs = trajectory_samples(small_rve(100 + seed), n_steps, n_train, keep_fraction=0.2, seed=seed)
+        assert len(recs) == n_train
+        xs.append(x)
+        ts.append(t)
+    X = np.concatenate(xs)
+    T = np.concatenate(ts)
+    perm = np.random.default_rng(0).permutation(len(X))
+    Xd = torch.from_numpy(X[perm]).cuda()
+    Td = torch.from_numpy(T[perm]).cuda()
+    mlp = MLP(seed=1)
+    hist = mlp.train(Xd, Td, epochs=40, batch=4096, lr=2e-3)
+    assert hist[-1] < hist[0]
+    res = compare_predictors(small_rve(999), n_steps, mlp)
+    # every predictor converges to the same load path
+    for k in ("linear", "learned"):
+        assert res[k]["steps"] == res["zeroth"]["steps"]
+        assert abs(res[k]["u_norm"] - res["zeroth"]["u_norm"]) <= 1e-6 * res["zeroth"]["u_norm"]
+    # the learned start is never worse than the extrapolation it corrects
+    assert res["learned"]["newton_its"] <= res["linear"]["newton_its"]
+    out = os.environ.get("PG_LEARNED_REPORT")
+    if out:
+        with open(out, "w") as f:
+            json.dump({"train_loss": hist.tolist(), "samples": int(len(X)), "predictors": res}, f, indent=1)
+    mlp.close()

@@ -311,7 +311,7 @@ def run_b200_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(rve, info),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_assemble_rows",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_assemble_blocks",
                          "peak_kind": peak_kind, "bytes_per_launch": rows_bytes, "kernel_share": share,
                          "pass_bytes": pass_bytes,
                          "pass_achieved": pass_bytes / (statistics.mean(step_ms) / 1e3) / 1e9},

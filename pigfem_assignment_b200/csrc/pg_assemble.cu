@@ -12,12 +12,11 @@
 //   OPCohesiveMaterial::Constitutive                      src/Material_OPCohesive.cpp:38-388
 //
 // Two kernels produce K (2x2-block CSR over nodes, FP64) and f_int:
-//   k_assemble_rows: one thread per node row.  The row's blocks are summed
-//     from the uncut triangles around the node (constant-strain B^T D B,
-//     the 4-point rule's weights sum to 1/2) in a per-CTA shared-memory tile
-//     that mirrors the CTA's contiguous slice of the value array, then leave
-//     with one cp.async.bulk store: each value is written to HBM exactly once,
-//     fully coalesced.  Rows of enrichment nodes are zero-filled here.
+//   k_assemble_blocks: one thread per 2x2 block of K.  The block (i, j) is
+//     summed from the uncut triangles around node i that contain node j
+//     (constant-strain B^T D B; the 4-point rule's weights sum to 1/2) and
+//     stored once with coalesced 16-byte stores: no atomics, no prior clear.
+//     Blocks of enrichment rows and columns are written as zeros here.
 //   k_assemble_cut: one warp per cut element.  Lanes own node-pair blocks of
 //     the (3+n_enr)^2 element matrix, integrate every child (tri3/quad4/
 //     polygon) and cohesive sub-element, and add into the rows with FP64
@@ -70,14 +69,15 @@ void upload_tables() {
 }
 
 // ---------------------------------------------------------------------------
-// Row kernel
+// Uncut triangles: gather assembly, one thread per 2x2 block of K
 // ---------------------------------------------------------------------------
-constexpr int kRowThreads = 128;
-constexpr int kRowRegCols = 16;           // columns kept in registers for the slot search
-constexpr int kRowTileBlocks = 1536;      // shared tile capacity (48 KB)
+constexpr int kTileNodes = 128;           // node rows per CTA
+constexpr int kTileThreads = 256;
+constexpr int kTileCap = 1536;            // blocks of a tile that fit the f_int staging buffer (48 KB)
 
 struct RowArgs {
-    int n_nodes, n_reg;
+    int n_nodes;
+    int n_reg;
     const int* __restrict__ row_ptr;
     const int* __restrict__ col;
     const int* __restrict__ ne_ptr;
@@ -92,236 +92,123 @@ struct RowArgs {
     int want_K, want_f;
 };
 
-__device__ __forceinline__ void bulk_store_smem_to_global(double* gdst, const double* ssrc, unsigned bytes) {
-    const unsigned saddr = (unsigned)__cvta_generic_to_shared(ssrc);
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst), "r"(saddr), "r"(bytes)
-                 : "memory");
-    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+// Block (v, t) of the constant-strain triangle e: B_v^T D B_t times the area
+// (the reference's 4-point rule integrates the constant integrand exactly:
+// its weights sum to 1/2, so K_e = J/2 * B^T D B with B = grad N / 1).
+// Adds into k[4] when node j is a vertex of e.
+__device__ __forceinline__ void cst_block_add(const RowArgs& a, int packed, int j, double k[4]) {
+    const int e = packed >> 2, v = packed & 3;
+    const int4 el = __ldg(&a.elem4[e]);
+    const int t = el.x == j ? 0 : el.y == j ? 1 : el.z == j ? 2 : -1;
+    if (t < 0) return;
+    const double X0 = __ldg(&a.x[el.x]), X1 = __ldg(&a.x[el.y]), X2 = __ldg(&a.x[el.z]);
+    const double Y0 = __ldg(&a.y[el.x]), Y1 = __ldg(&a.y[el.y]), Y2 = __ldg(&a.y[el.z]);
+    const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+    const double b0 = Y1 - Y2, b1 = Y2 - Y0, b2 = Y0 - Y1;
+    const double c0 = X2 - X1, c1 = X0 - X2, c2 = X1 - X0;
+    const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]), d33 = __ldg(&a.dmat[3 * el.w + 2]);
+    const double s = 0.5 / J;
+    const double ba = (v == 0 ? b0 : v == 1 ? b1 : b2) * s;
+    const double ca = (v == 0 ? c0 : v == 1 ? c1 : c2) * s;
+    const double bb = t == 0 ? b0 : t == 1 ? b1 : b2;
+    const double cb = t == 0 ? c0 : t == 1 ? c1 : c2;
+    k[0] += ba * d11 * bb + ca * d33 * cb;
+    k[1] += ba * d12 * cb + ca * d33 * bb;
+    k[2] += ca * d12 * bb + ba * d33 * cb;
+    k[3] += ca * d11 * cb + ba * d33 * bb;
 }
 
-__global__ void __launch_bounds__(kRowThreads) k_assemble_rows(RowArgs a) {
-    extern __shared__ __align__(128) double sK[];
-    const int node0 = blockIdx.x * kRowThreads;
-    const int node_end = min(node0 + kRowThreads, a.n_nodes);
-    const int node = node0 + (int)threadIdx.x;
-    const int seg0 = a.row_ptr[node0];
-    const int seg1 = a.row_ptr[node_end];
-    const int nseg = seg1 - seg0;
-    const bool tile = a.want_K && nseg <= kRowTileBlocks;
-    if (tile) {
-        double2* s2 = reinterpret_cast<double2*>(sK);
-        for (int i = threadIdx.x; i < 2 * nseg; i += kRowThreads) s2[i] = make_double2(0.0, 0.0);
-        __syncthreads();
-    }
-    double fx = 0.0, fy = 0.0;
-    if (node < node_end) {
-        const int r0 = a.row_ptr[node];
-        const int r1 = a.row_ptr[node + 1];
-        const int deg = r1 - r0;
-        double* dst = tile ? sK + 4 * (r0 - seg0) : a.K + 4 * (size_t)r0;
-        if (a.want_K && !tile)
-            for (int i = 0; i < 4 * deg; ++i) dst[i] = 0.0;
-        {
-            int cols[kRowRegCols];
+// f_int contribution of the uncut triangle `packed` to its vertex v:
+// sum_t K_e(v, t) u_t.
+__device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, double& fx, double& fy) {
+    const int e = packed >> 2, v = packed & 3;
+    const int4 el = __ldg(&a.elem4[e]);
+    const double X0 = __ldg(&a.x[el.x]), X1 = __ldg(&a.x[el.y]), X2 = __ldg(&a.x[el.z]);
+    const double Y0 = __ldg(&a.y[el.x]), Y1 = __ldg(&a.y[el.y]), Y2 = __ldg(&a.y[el.z]);
+    const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+    const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
+    const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
+    const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]), d33 = __ldg(&a.dmat[3 * el.w + 2]);
+    const double s = 0.5 / J;
+    const double ba = (v == 0 ? b[0] : v == 1 ? b[1] : b[2]) * s;
+    const double ca = (v == 0 ? c[0] : v == 1 ? c[1] : c[2]) * s;
+    const int nid[3] = {el.x, el.y, el.z};
 #pragma unroll
-            for (int q = 0; q < kRowRegCols; ++q) cols[q] = (q < deg) ? a.col[r0 + q] : -1;
-            const int k0 = a.ne_ptr[node], k1 = a.ne_ptr[node + 1];
-            for (int k = k0; k < k1; ++k) {
-                const int packed = a.ne_list[k];
-                const int e = packed >> 2;
-                const int v = packed & 3;
-                const int4 el = a.elem4[e];
-                const int nid[3] = {el.x, el.y, el.z};
-                const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
-                const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
-                // J = det(dx/dr) of the affine map; grad N_k = (b_k, c_k) / J
-                const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
-                const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
-                const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
-                const double d11 = a.dmat[3 * el.w + 0], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
-                // sum_qp J w_qp = J/2; (b/J)(b/J) J/2 = b b * (0.5/J)
-                const double s = 0.5 / J;
-                const double ba = b[v] * s, ca = c[v] * s;
-#pragma unroll
-                for (int t = 0; t < 3; ++t) {
-                    const double bb = b[t], cb = c[t];
-                    const double k00 = ba * d11 * bb + ca * d33 * cb;
-                    const double k01 = ba * d12 * cb + ca * d33 * bb;
-                    const double k10 = ca * d12 * bb + ba * d33 * cb;
-                    const double k11 = ca * d11 * cb + ba * d33 * bb;
-                    const int nt = nid[t];
-                    if (a.want_f) {
-                        const double ux = a.u[2 * nt], uy = a.u[2 * nt + 1];
-                        fx += k00 * ux + k01 * uy;
-                        fy += k10 * ux + k11 * uy;
-                    }
-                    if (a.want_K) {
-                        int sl = -1;
-#pragma unroll
-                        for (int q = 0; q < kRowRegCols; ++q) sl = (cols[q] == nt) ? q : sl;
-                        if (sl < 0)
-                            for (int q = kRowRegCols; q < deg; ++q)
-                                if (a.col[r0 + q] == nt) { sl = q; break; }
-                        if (sl < 0) continue;  // not in the pattern: cannot happen for a pattern built from these elements
-                        double* d = dst + 4 * sl;
-                        d[0] += k00;
-                        d[1] += k01;
-                        d[2] += k10;
-                        d[3] += k11;
-                    }
-                }
-            }
-        }
-        if (a.want_f) {
-            a.f[2 * node] = fx;
-            a.f[2 * node + 1] = fy;
-        }
-    }
-    if (tile) {
-        // make the generic-proxy shared writes visible to the async (bulk copy) proxy
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) bulk_store_smem_to_global(a.K + 4 * (size_t)seg0, sK, (unsigned)nseg * 32u);
+    for (int t = 0; t < 3; ++t) {
+        const double bb = b[t], cb = c[t];
+        const double ux = a.u[2 * nid[t]], uy = a.u[2 * nid[t] + 1];
+        fx += (ba * d11 * bb + ca * d33 * cb) * ux + (ba * d12 * cb + ca * d33 * bb) * uy;
+        fy += (ca * d12 * bb + ba * d33 * cb) * ux + (ca * d11 * cb + ba * d33 * bb) * uy;
     }
 }
 
-// ---------------------------------------------------------------------------
-// Tiled row kernel: a CTA of 256 threads owns 128 consecutive node rows.  The
-// rows' column indices and pointers are staged in shared memory, every
-// (node, adjacent uncut element) entry of the CTA's slice of ne_list is one
-// thread's work item (independent loads, no per-row serial chain), its three
-// 2x2 blocks go into the shared tile with FP64 shared atomics, and the tile
-// leaves with one bulk async store.  A CTA whose slice does not fit the tile
-// runs the per-row code path below instead.
-// ---------------------------------------------------------------------------
-constexpr int kTileNodes = 128;
-constexpr int kTileThreads = 256;
-constexpr int kTileCap = 1152;  // blocks per tile (36 KB of values)
-
-__global__ void __launch_bounds__(kTileThreads) k_assemble_tile(RowArgs a) {
-    extern __shared__ __align__(128) double sK[];
-    int* scol = reinterpret_cast<int*>(sK + 4 * kTileCap);
+// A CTA owns the 2x2-block CSR slice of kTileNodes consecutive node rows.
+// Each thread takes blocks (i, j) of the slice, sums the contributions of
+// the uncut triangles around node i that also contain node j, and stores
+// the block with coalesced 16-byte stores: every value of K is written
+// once, without atomics and without a prior clear (blocks that couple to
+// enrichment nodes, and the rows of enrichment nodes, are written as zeros
+// and completed by the cut-element kernel).  With WANT_F the blocks are
+// also staged in shared memory and each row's f_int = sum_j K_ij u_j is
+// formed from them; in a slice larger than the staging buffer each row's
+// thread sums f_int over its triangles directly.
+template <bool WANT_F>
+__global__ void __launch_bounds__(kTileThreads) k_assemble_blocks(RowArgs a) {
+    extern __shared__ __align__(16) double sK[];
     __shared__ int srp[kTileNodes + 1];
     __shared__ int sne[kTileNodes + 1];
-    __shared__ double sF[2 * kTileNodes];
     const int node0 = blockIdx.x * kTileNodes;
     const int node_end = min(node0 + kTileNodes, a.n_nodes);
     const int nn = node_end - node0;
-    const int seg0 = a.row_ptr[node0];
-    const int nseg = a.row_ptr[node_end] - seg0;
-    if (nseg > kTileCap) {
-        // per-row path for an oversized slice (rows near many enrichment nodes)
-        const int node = node0 + (int)threadIdx.x;
-        if (threadIdx.x >= kTileNodes || node >= node_end) return;
-        const int r0 = a.row_ptr[node], r1 = a.row_ptr[node + 1];
-        double* dst = a.K + 4 * (size_t)r0;
-        if (a.want_K)
-            for (int i = 0; i < 4 * (r1 - r0); ++i) dst[i] = 0.0;
-        double fx = 0.0, fy = 0.0;
-        for (int k = a.ne_ptr[node]; k < a.ne_ptr[node + 1]; ++k) {
-            const int e = a.ne_list[k] >> 2, v = a.ne_list[k] & 3;
-            const int4 el = a.elem4[e];
-            const int nid[3] = {el.x, el.y, el.z};
-            const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
-            const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
-            const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
-            const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
-            const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
-            const double d11 = a.dmat[3 * el.w], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
-            const double s = 0.5 / J;
-            const double ba = (v == 0 ? b[0] : v == 1 ? b[1] : b[2]) * s;
-            const double ca = (v == 0 ? c[0] : v == 1 ? c[1] : c[2]) * s;
-            for (int t = 0; t < 3; ++t) {
-                const double bb = b[t], cb = c[t];
-                const double k00 = ba * d11 * bb + ca * d33 * cb, k01 = ba * d12 * cb + ca * d33 * bb;
-                const double k10 = ca * d12 * bb + ba * d33 * cb, k11 = ca * d11 * cb + ba * d33 * bb;
-                const int nt = nid[t];
-                if (a.want_f) {
-                    fx += k00 * a.u[2 * nt] + k01 * a.u[2 * nt + 1];
-                    fy += k10 * a.u[2 * nt] + k11 * a.u[2 * nt + 1];
-                }
-                if (a.want_K)
-                    for (int q = r0; q < r1; ++q)
-                        if (a.col[q] == nt) {
-                            double* d = a.K + 4 * (size_t)q;
-                            d[0] += k00; d[1] += k01; d[2] += k10; d[3] += k11;
-                            break;
-                        }
-            }
-        }
-        if (a.want_f) { a.f[2 * node] = fx; a.f[2 * node + 1] = fy; }
-        return;
-    }
-    // stage the slice: row pointers, adjacency pointers, columns; zero the tile
+    const int seg0 = __ldg(&a.row_ptr[node0]);
     for (int i = threadIdx.x; i <= nn; i += kTileThreads) {
-        srp[i] = a.row_ptr[node0 + i] - seg0;
-        sne[i] = a.ne_ptr[node0 + i];
+        srp[i] = __ldg(&a.row_ptr[node0 + i]) - seg0;
+        sne[i] = __ldg(&a.ne_ptr[node0 + i]);
     }
-    if (a.want_K) {
-        double2* s2 = reinterpret_cast<double2*>(sK);
-        for (int i = threadIdx.x; i < 2 * nseg; i += kTileThreads) s2[i] = make_double2(0.0, 0.0);
-        for (int i = threadIdx.x; i < nseg; i += kTileThreads) scol[i] = a.col[seg0 + i];
-    }
-    for (int i = threadIdx.x; i < 2 * kTileNodes; i += kTileThreads) sF[i] = 0.0;
     __syncthreads();
-    const int k_begin = sne[0], k_end = sne[nn];
-    for (int k = k_begin + (int)threadIdx.x; k < k_end; k += kTileThreads) {
-        // owner row: largest li with sne[li] <= k
+    const int nseg = srp[nn];
+    const bool staged = WANT_F && nseg <= kTileCap;
+    for (int sidx = threadIdx.x; sidx < nseg; sidx += kTileThreads) {
+        // row of this block: the largest li with srp[li] <= sidx
         int lo = 0, hi = nn - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (sne[mid] <= k) lo = mid; else hi = mid - 1;
+            if (srp[mid] <= sidx) lo = mid; else hi = mid - 1;
         }
-        const int li = lo;
-        const int packed = a.ne_list[k];
-        const int e = packed >> 2, v = packed & 3;
-        const int4 el = a.elem4[e];
-        const double X0 = a.x[el.x], X1 = a.x[el.y], X2 = a.x[el.z];
-        const double Y0 = a.y[el.x], Y1 = a.y[el.y], Y2 = a.y[el.z];
-        const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
-        const double b0 = Y1 - Y2, b1 = Y2 - Y0, b2 = Y0 - Y1;
-        const double c0 = X2 - X1, c1 = X0 - X2, c2 = X1 - X0;
-        const double d11 = a.dmat[3 * el.w], d12 = a.dmat[3 * el.w + 1], d33 = a.dmat[3 * el.w + 2];
-        const double s = 0.5 / J;
-        const double ba = (v == 0 ? b0 : v == 1 ? b1 : b2) * s;
-        const double ca = (v == 0 ? c0 : v == 1 ? c1 : c2) * s;
-        const int rb = srp[li], re = srp[li + 1];
-        double fx = 0.0, fy = 0.0;
-#pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const double bb = t == 0 ? b0 : t == 1 ? b1 : b2;
-            const double cb = t == 0 ? c0 : t == 1 ? c1 : c2;
-            const int nt = t == 0 ? el.x : t == 1 ? el.y : el.z;
-            const double k00 = ba * d11 * bb + ca * d33 * cb, k01 = ba * d12 * cb + ca * d33 * bb;
-            const double k10 = ca * d12 * bb + ba * d33 * cb, k11 = ca * d11 * cb + ba * d33 * bb;
-            if (a.want_f) {
-                const double ux = a.u[2 * nt], uy = a.u[2 * nt + 1];
-                fx += k00 * ux + k01 * uy;
-                fy += k10 * ux + k11 * uy;
-            }
-            if (a.want_K) {
-                int q = rb;
-                while (q < re && scol[q] != nt) ++q;
-                if (q < re) {
-                    double* d = sK + 4 * q;
-                    atomicAdd(d + 0, k00);
-                    atomicAdd(d + 1, k01);
-                    atomicAdd(d + 2, k10);
-                    atomicAdd(d + 3, k11);
-                }
-            }
+        const int j = __ldg(&a.col[seg0 + sidx]);
+        double k[4] = {0.0, 0.0, 0.0, 0.0};
+        const int k1 = sne[lo + 1];
+        for (int kk = sne[lo]; kk < k1; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
+        if (a.want_K) {
+            double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + sidx));
+            dst[0] = make_double2(k[0], k[1]);
+            dst[1] = make_double2(k[2], k[3]);
         }
-        if (a.want_f) {
-            atomicAdd(&sF[2 * li], fx);
-            atomicAdd(&sF[2 * li + 1], fy);
+        if (staged) {
+            double2* sd = reinterpret_cast<double2*>(sK + 4 * sidx);
+            sd[0] = make_double2(k[0], k[1]);
+            sd[1] = make_double2(k[2], k[3]);
         }
     }
-    if (a.want_K) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    if (!WANT_F) return;
     __syncthreads();
-    if (a.want_f)
-        for (int i = threadIdx.x; i < 2 * nn; i += kTileThreads) a.f[2 * (size_t)node0 + i] = sF[i];
-    if (a.want_K && threadIdx.x == 0) bulk_store_smem_to_global(a.K + 4 * (size_t)seg0, sK, (unsigned)nseg * 32u);
+    if (threadIdx.x < nn) {
+        // the cut-element kernel adds its own f_int contributions afterwards
+        const int li = threadIdx.x;
+        double fx = 0.0, fy = 0.0;
+        if (staged) {
+            for (int q = srp[li]; q < srp[li + 1]; ++q) {
+                const int j = __ldg(&a.col[seg0 + q]);
+                const double ux = a.u[2 * j], uy = a.u[2 * j + 1];
+                fx += sK[4 * q] * ux + sK[4 * q + 1] * uy;
+                fy += sK[4 * q + 2] * ux + sK[4 * q + 3] * uy;
+            }
+        } else {
+            for (int kk = sne[li]; kk < sne[li + 1]; ++kk) cst_force_add(a, __ldg(&a.ne_list[kk]), fx, fy);
+        }
+        a.f[2 * (node0 + li)] = fx;
+        a.f[2 * (node0 + li) + 1] = fy;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -436,11 +323,19 @@ struct CutArgs {
     int want_K, want_f;
 };
 
+// Per-warp shared tables: one row per quadrature point of the current chunk
+// holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
+// row per cohesive point holding {wgt, N0, N1, (R^T D R) 4, (R^T t) 2}.
+constexpr int kQpChunk = 32;
+constexpr int kQRow = 4 + 2 * kMaxElemNodes;
+constexpr int kCRow = 10;
+
 __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
     __shared__ double sX[kCutWarps][kMaxElemNodes], sY[kCutWarps][kMaxElemNodes];
     __shared__ double sU[kCutWarps][2 * kMaxElemNodes];
-    __shared__ double sGx[kCutWarps][kMaxElemNodes], sGy[kCutWarps][kMaxElemNodes];
     __shared__ int sL[kCutWarps][kMaxElemNodes];
+    __shared__ double sQ[kCutWarps][kQpChunk][kQRow];
+    __shared__ double sC[kCutWarps][2 * kMaxCoh][kCRow];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int ci = blockIdx.x * kCutWarps + w;
@@ -467,17 +362,33 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
     const double pbx[3] = {(PY1 - PY2) / PJ, (PY2 - PY0) / PJ, (PY0 - PY1) / PJ};
     const double pby[3] = {(PX2 - PX1) / PJ, (PX0 - PX2) / PJ, (PX1 - PX0) / PJ};
 
+    int nq_total = 0;
+    for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
+
     double acc[kCutPairsPerLane][4];
 #pragma unroll
     for (int k = 0; k < kCutPairsPerLane; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
     const int npairs = nl * nl;
+    int pa[kCutPairsPerLane], pb[kCutPairsPerLane];
+#pragma unroll
+    for (int k = 0; k < kCutPairsPerLane; ++k) {
+        const int p = lane + 32 * k;
+        pa[k] = p / nl;
+        pb[k] = p - pa[k] * nl;
+    }
 
-    for (int ch = 0; ch < T.n_child; ++ch) {
-        const int nc = T.child_n[ch];
-        const DevChildQuad& Q = c_quad[T.child_type[ch]];
-        const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
-        const double d11 = a.dmat[3 * mat], d12 = a.dmat[3 * mat + 1], d33 = a.dmat[3 * mat + 2];
-        for (int q = 0; q < Q.nq; ++q) {
+    for (int qbase = 0; qbase < nq_total; qbase += kQpChunk) {
+        // geometry of one quadrature point per lane, all points in parallel
+        const int l = qbase + lane;
+        if (l < nq_total) {
+            int ch = 0, q = l;
+            while (q >= c_quad[T.child_type[ch]].nq) {
+                q -= c_quad[T.child_type[ch]].nq;
+                ++ch;
+            }
+            const int nc = T.child_n[ch];
+            const DevChildQuad& Q = c_quad[T.child_type[ch]];
+            const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
             double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
             for (int k = 0; k < nc; ++k) {
                 const int ln = T.child_nodes[ch][k];
@@ -489,50 +400,59 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
             }
             const double det = J00 * J11 - J01 * J10;
             const double wgt = det * Q.w[q];
+            double* row = sQ[w][lane];
             // a zero weight (collapsed child) contributes nothing: the reference's
-            // K_el.AXPY is cblas_daxpy, which returns at once for alpha == 0
-            if (wgt == 0.0) continue;
-            // gradients of the element's local functions at this point
-            if (lane < nl) {
-                double gx = 0.0, gy = 0.0;
-                if (lane < 3) {
-                    gx = pbx[lane];
-                    gy = pby[lane];
-                } else {
-                    for (int k = 0; k < nc; ++k)
-                        if (T.child_nodes[ch][k] == lane) {
-                            const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
-                            gx = (J11 * dr - J01 * ds) / det;
-                            gy = (-J10 * dr + J00 * ds) / det;
-                        }
-                }
-                sGx[w][lane] = gx;
-                sGy[w][lane] = gy;
+            // K_el.AXPY is cblas_daxpy, which returns at once for alpha == 0;
+            // the row is zeroed so that no 0/0 gradient enters the sums
+            const bool live = wgt != 0.0;
+            row[0] = live ? wgt : 0.0;
+            row[1] = a.dmat[3 * mat];
+            row[2] = a.dmat[3 * mat + 1];
+            row[3] = a.dmat[3 * mat + 2];
+            for (int j = 0; j < 3; ++j) {
+                row[4 + 2 * j] = pbx[j];
+                row[5 + 2 * j] = pby[j];
             }
-            __syncwarp();
+            for (int j = 3; j < nl; ++j) {
+                row[4 + 2 * j] = 0.0;
+                row[5 + 2 * j] = 0.0;
+            }
+            if (live)
+                for (int k = 0; k < nc; ++k) {
+                    const int ln = T.child_nodes[ch][k];
+                    if (ln >= 3) {
+                        const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+                        row[4 + 2 * ln] = (J11 * dr - J01 * ds) / det;
+                        row[5 + 2 * ln] = (-J10 * dr + J00 * ds) / det;
+                    }
+                }
+        }
+        __syncwarp();
+        // each lane integrates its node-pair blocks over the chunk's points
+        const int nqc = min(kQpChunk, nq_total - qbase);
+        for (int q = 0; q < nqc; ++q) {
+            const double* row = sQ[w][q];
+            const double wgt = row[0], d11 = row[1], d12 = row[2], d33 = row[3];
 #pragma unroll
             for (int k = 0; k < kCutPairsPerLane; ++k) {
-                const int p = lane + 32 * k;
-                if (p < npairs) {
-                    const int ia = p / nl, ib = p - ia * nl;
-                    const double ba = sGx[w][ia] * wgt, ca = sGy[w][ia] * wgt;
-                    const double bb = sGx[w][ib], cb = sGy[w][ib];
+                if (lane + 32 * k < npairs) {
+                    const double ba = row[4 + 2 * pa[k]] * wgt, ca = row[5 + 2 * pa[k]] * wgt;
+                    const double bb = row[4 + 2 * pb[k]], cb = row[5 + 2 * pb[k]];
                     acc[k][0] += ba * d11 * bb + ca * d33 * cb;
                     acc[k][1] += ba * d12 * cb + ca * d33 * bb;
                     acc[k][2] += ca * d12 * bb + ba * d33 * cb;
                     acc[k][3] += ca * d11 * cb + ba * d33 * bb;
                 }
             }
-            __syncwarp();
         }
+        __syncwarp();
     }
     // bulk internal force f_a = sum_b K_ab u_b
     if (a.want_f) {
 #pragma unroll
         for (int k = 0; k < kCutPairsPerLane; ++k) {
-            const int p = lane + 32 * k;
-            if (p < npairs) {
-                const int ia = p / nl, ib = p - ia * nl;
+            if (lane + 32 * k < npairs) {
+                const int ia = pa[k], ib = pb[k];
                 const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
                 const double fx = acc[k][0] * ux + acc[k][1] * uy;
                 const double fy = acc[k][2] * ux + acc[k][3] * uy;
@@ -541,8 +461,10 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
             }
         }
     }
-    // cohesive sub-elements: two Gauss points each (CohEdge2, w = 1)
-    for (int ce = 0; ce < T.n_coh; ++ce) {
+    if (T.n_coh == 0) goto scatter;
+    // cohesive sub-elements: two Gauss points each (CohEdge2, w = 1), one lane per point
+    if (lane < 2 * T.n_coh) {
+        const int ce = lane >> 1, q = lane & 1;
         const int c0 = T.coh_nodes[ce][0], c1 = T.coh_nodes[ce][1], c2 = T.coh_nodes[ce][2], c3 = T.coh_nodes[ce][3];
         const double jx = 0.5 * (sX[w][c1] - sX[w][c0]);
         const double jy = 0.5 * (sY[w][c1] - sY[w][c0]);
@@ -550,63 +472,74 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         const double nx = -jy, ny = jx;
         const double dA = sqrt(nx * nx + ny * ny);
         const double R[2][2] = {{jx / mag, jy / mag}, {nx / dA, ny / dA}};
-        for (int q = 0; q < 2; ++q) {
-            const double xi = q == 0 ? -0.57735026918962576450914878050196 : 0.57735026918962576450914878050196;
-            const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
-            double dg[2];
-            for (int d = 0; d < 2; ++d)
-                dg[d] = N0 * (sU[w][2 * c2 + d] - sU[w][2 * c0 + d]) + N1 * (sU[w][2 * c3 + d] - sU[w][2 * c1 + d]);
-            double dl[2] = {R[0][0] * dg[0] + R[0][1] * dg[1], R[1][0] * dg[0] + R[1][1] * dg[1]};
-            const int qp = a.cut_coh_qp0[ci] + 2 * ce + q;
-            const double dmax_c = a.isv_c[qp];
-            double tr[2], Dc[2][2], dmax_t;
-            cohesive_law(a.coh, a.dt, dmax_c, dl, tr, Dc, dmax_t);
-            if (lane == 0) a.isv_t[qp] = dmax_t;
-            // R^T D R and R^T t
-            double RDR[2][2];
-            for (int i = 0; i < 2; ++i)
-                for (int j = 0; j < 2; ++j) {
-                    double s = 0.0;
-                    for (int k1 = 0; k1 < 2; ++k1)
-                        for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
-                    RDR[i][j] = s;
-                }
-            const double tR[2] = {R[0][0] * tr[0] + R[1][0] * tr[1], R[0][1] * tr[0] + R[1][1] * tr[1]};
-            const double wgt = dA * 1.0;
-            if (wgt == 0.0) continue;
+        const double xi = q == 0 ? -0.57735026918962576450914878050196 : 0.57735026918962576450914878050196;
+        const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+        double dg[2];
+        for (int d = 0; d < 2; ++d)
+            dg[d] = N0 * (sU[w][2 * c2 + d] - sU[w][2 * c0 + d]) + N1 * (sU[w][2 * c3 + d] - sU[w][2 * c1 + d]);
+        double dl[2] = {R[0][0] * dg[0] + R[0][1] * dg[1], R[1][0] * dg[0] + R[1][1] * dg[1]};
+        const int qp = a.cut_coh_qp0[ci] + lane;
+        const double dmax_c = a.isv_c[qp];
+        double tr[2], Dc[2][2], dmax_t;
+        cohesive_law(a.coh, a.dt, dmax_c, dl, tr, Dc, dmax_t);
+        a.isv_t[qp] = dmax_t;
+        double* row = sC[w][lane];
+        row[0] = dA * 1.0;
+        row[1] = N0;
+        row[2] = N1;
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j) {
+                double s = 0.0;
+                for (int k1 = 0; k1 < 2; ++k1)
+                    for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
+                row[3 + 2 * i + j] = s;
+            }
+        const double tR0 = R[0][0] * tr[0] + R[1][0] * tr[1];
+        const double tR1 = R[0][1] * tr[0] + R[1][1] * tr[1];
+        row[7] = tR0;
+        row[8] = tR1;
+        const double wgt = row[0];
+        if (a.want_f && wgt != 0.0) {
             const int cn[4] = {c0, c1, c2, c3};
             const double Nn[2] = {N0, N1};
-            if (a.want_K) {
+            for (int m = 0; m < 4; ++m) {
+                const double sgn = m < 2 ? -1.0 : 1.0;
+                const int node = sL[w][cn[m]];
+                atomicAdd(&a.f[2 * node], wgt * sgn * Nn[m & 1] * tR0);
+                atomicAdd(&a.f[2 * node + 1], wgt * sgn * Nn[m & 1] * tR1);
+            }
+        }
+    }
+    __syncwarp();
+    if (a.want_K) {
+        for (int ce = 0; ce < T.n_coh; ++ce) {
+            const int cn[4] = {T.coh_nodes[ce][0], T.coh_nodes[ce][1], T.coh_nodes[ce][2], T.coh_nodes[ce][3]};
 #pragma unroll
-                for (int k = 0; k < kCutPairsPerLane; ++k) {
-                    const int p = lane + 32 * k;
-                    if (p < npairs) {
-                        const int ia = p / nl, ib = p - ia * nl;
-                        int i = -1, j = -1;
-                        for (int m = 0; m < 4; ++m) {
-                            if (cn[m] == ia) i = m;
-                            if (cn[m] == ib) j = m;
-                        }
-                        if (i >= 0 && j >= 0) {
-                            const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
-                            const double v = wgt * sgn * Nn[i & 1] * Nn[j & 1];
-                            acc[k][0] += v * RDR[0][0];
-                            acc[k][1] += v * RDR[0][1];
-                            acc[k][2] += v * RDR[1][0];
-                            acc[k][3] += v * RDR[1][1];
+            for (int k = 0; k < kCutPairsPerLane; ++k) {
+                if (lane + 32 * k < npairs) {
+                    int i = -1, j = -1;
+                    for (int m = 0; m < 4; ++m) {
+                        if (cn[m] == pa[k]) i = m;
+                        if (cn[m] == pb[k]) j = m;
+                    }
+                    if (i >= 0 && j >= 0) {
+                        const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
+                        for (int q = 0; q < 2; ++q) {
+                            const double* row = sC[w][2 * ce + q];
+                            const double wgt = row[0];
+                            if (wgt == 0.0) continue;
+                            const double v = wgt * sgn * row[1 + (i & 1)] * row[1 + (j & 1)];
+                            acc[k][0] += v * row[3];
+                            acc[k][1] += v * row[4];
+                            acc[k][2] += v * row[5];
+                            acc[k][3] += v * row[6];
                         }
                     }
                 }
             }
-            if (a.want_f && lane < 4) {
-                const double sgn = lane < 2 ? -1.0 : 1.0;
-                const double nn = Nn[lane & 1];
-                const int node = sL[w][cn[lane]];
-                atomicAdd(&a.f[2 * node], wgt * sgn * nn * tR[0]);
-                atomicAdd(&a.f[2 * node + 1], wgt * sgn * nn * tR[1]);
-            }
         }
     }
+scatter:
     if (a.want_K) {
         const int* slots = a.cut_slot + a.cut_slot_ptr[ci];
 #pragma unroll
@@ -653,9 +586,13 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.want_K = want_K;
     ra.want_f = want_f;
     const int rblocks = (c.n_nodes + kTileNodes - 1) / kTileNodes;
-    const size_t smem = (size_t)kTileCap * 36;  // values (32 B) + column (4 B) per block
     if (c.timing) cudaEventRecord(c.ea0, s);
-    if (rblocks > 0) k_assemble_tile<<<rblocks, kTileThreads, smem, s>>>(ra);
+    if (rblocks > 0) {
+        if (want_f)
+            k_assemble_blocks<true><<<rblocks, kTileThreads, (size_t)kTileCap * 32, s>>>(ra);
+        else
+            k_assemble_blocks<false><<<rblocks, kTileThreads, 0, s>>>(ra);
+    }
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {

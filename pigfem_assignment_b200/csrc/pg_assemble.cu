@@ -12,11 +12,12 @@
 //   OPCohesiveMaterial::Constitutive                      src/Material_OPCohesive.cpp:38-388
 //
 // Two kernels produce K (2x2-block CSR over nodes, FP64) and f_int:
-//   k_assemble_blocks: one thread per 2x2 block of K.  The block (i, j) is
-//     summed from the uncut triangles around node i that contain node j
-//     (constant-strain B^T D B; the 4-point rule's weights sum to 1/2) and
-//     stored once with coalesced 16-byte stores: no atomics, no prior clear.
-//     Blocks of enrichment rows and columns are written as zeros here.
+//   k_assemble_tri: uncut triangles.  Per CTA slice of node rows, each
+//     triangle's gradients are computed once per adjacent row into shared
+//     memory, then one thread per 2x2 block (i, j) sums the constant-strain
+//     B^T D B of the triangles joining i and j and stores it once with
+//     coalesced 16-byte stores: no atomics, no prior clear.  Blocks of
+//     enrichment rows and columns are written as zeros here.
 //   k_assemble_cut: one warp per cut element.  Lanes own node-pair blocks of
 //     the (3+n_enr)^2 element matrix, integrate every child (tri3/quad4/
 //     polygon) and cohesive sub-element, and add into the rows with FP64
@@ -71,9 +72,9 @@ void upload_tables() {
 // ---------------------------------------------------------------------------
 // Uncut triangles: gather assembly, one thread per 2x2 block of K
 // ---------------------------------------------------------------------------
-constexpr int kTileNodes = 128;           // node rows per CTA
-constexpr int kTileThreads = 256;
-constexpr int kTileCap = 1536;            // blocks of a tile that fit the f_int staging buffer (48 KB)
+constexpr int kTileNodes = 64;            // node rows per CTA
+constexpr int kTileThreads = 128;
+constexpr int kTileEntries = 512;         // staged (node, triangle) entries: 64 nodes x valence <= 8 (40 KB)
 
 struct RowArgs {
     int n_nodes;
@@ -142,19 +143,27 @@ __device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, doub
     }
 }
 
-// A CTA owns the 2x2-block CSR slice of kTileNodes consecutive node rows.
-// Each thread takes blocks (i, j) of the slice, sums the contributions of
-// the uncut triangles around node i that also contain node j, and stores
-// the block with coalesced 16-byte stores: every value of K is written
-// once, without atomics and without a prior clear (blocks that couple to
-// enrichment nodes, and the rows of enrichment nodes, are written as zeros
-// and completed by the cut-element kernel).  With WANT_F the blocks are
-// also staged in shared memory and each row's f_int = sum_j K_ij u_j is
-// formed from them; in a slice larger than the staging buffer each row's
-// thread sums f_int over its triangles directly.
+// A CTA owns the 2x2-block CSR slice of kTileNodes consecutive node rows
+// and works in three phases:
+//   1. one thread per (node, adjacent uncut triangle) entry of the slice
+//      computes the triangle's gradients once (b_t, c_t and the node's own
+//      row scaled by 1/(2J)) into shared memory;
+//   2. one thread per 2x2 block (i, j) of the slice sums, over the staged
+//      entries of row i whose triangle contains node j, the constant-strain
+//      block B_i^T D B_j (the reference's 4-point rule integrates the constant
+//      integrand exactly: its weights sum to 1/2), and stores it once with
+//      coalesced 16-byte stores: no atomics, no prior clear (blocks coupling to
+//      enrichment nodes, and rows of enrichment nodes, are written as zeros
+//      and completed by the cut-element kernel);
+//   3. with WANT_F, one thread per row forms f_int,i = sum_e K_e(i, :) u_e
+//      from the staged entries.
+// A slice with more entries than the staging buffer (never for structured
+// meshes, whose valence is at most 8) evaluates the blocks straight from
+// global memory instead.
 template <bool WANT_F>
-__global__ void __launch_bounds__(kTileThreads) k_assemble_blocks(RowArgs a) {
-    extern __shared__ __align__(16) double sK[];
+__global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
+    __shared__ double sG[kTileEntries][8];   // ba, ca, b0, b1, b2, c0, c1, c2
+    __shared__ int4 sN[kTileEntries];        // the triangle's nodes and material
     __shared__ int srp[kTileNodes + 1];
     __shared__ int sne[kTileNodes + 1];
     const int node0 = blockIdx.x * kTileNodes;
@@ -167,7 +176,29 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_blocks(RowArgs a) {
     }
     __syncthreads();
     const int nseg = srp[nn];
-    const bool staged = WANT_F && nseg <= kTileCap;
+    const int k0 = sne[0];
+    const int nent = sne[nn] - k0;
+    const bool staged = nent <= kTileEntries;
+    if (staged) {
+        for (int k = threadIdx.x; k < nent; k += kTileThreads) {
+            const int packed = __ldg(&a.ne_list[k0 + k]);
+            const int e = packed >> 2, v = packed & 3;
+            const int4 el = __ldg(&a.elem4[e]);
+            const double X0 = __ldg(&a.x[el.x]), X1 = __ldg(&a.x[el.y]), X2 = __ldg(&a.x[el.z]);
+            const double Y0 = __ldg(&a.y[el.x]), Y1 = __ldg(&a.y[el.y]), Y2 = __ldg(&a.y[el.z]);
+            const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+            const double b0 = Y1 - Y2, b1 = Y2 - Y0, b2 = Y0 - Y1;
+            const double c0 = X2 - X1, c1 = X0 - X2, c2 = X1 - X0;
+            const double s = 0.5 / J;
+            double* g = sG[k];
+            g[0] = (v == 0 ? b0 : v == 1 ? b1 : b2) * s;
+            g[1] = (v == 0 ? c0 : v == 1 ? c1 : c2) * s;
+            g[2] = b0; g[3] = b1; g[4] = b2;
+            g[5] = c0; g[6] = c1; g[7] = c2;
+            sN[k] = el;
+        }
+        __syncthreads();
+    }
     for (int sidx = threadIdx.x; sidx < nseg; sidx += kTileThreads) {
         // row of this block: the largest li with srp[li] <= sidx
         int lo = 0, hi = nn - 1;
@@ -177,31 +208,49 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_blocks(RowArgs a) {
         }
         const int j = __ldg(&a.col[seg0 + sidx]);
         double k[4] = {0.0, 0.0, 0.0, 0.0};
-        const int k1 = sne[lo + 1];
-        for (int kk = sne[lo]; kk < k1; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
+        if (staged) {
+            const int kend = sne[lo + 1] - k0;
+            for (int kk = sne[lo] - k0; kk < kend; ++kk) {
+                const int4 el = sN[kk];
+                const int t = el.x == j ? 0 : el.y == j ? 1 : el.z == j ? 2 : -1;
+                if (t < 0) continue;
+                const double* g = sG[kk];
+                const double ba = g[0], ca = g[1], bb = g[2 + t], cb = g[5 + t];
+                const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]);
+                const double d33 = __ldg(&a.dmat[3 * el.w + 2]);
+                k[0] += ba * d11 * bb + ca * d33 * cb;
+                k[1] += ba * d12 * cb + ca * d33 * bb;
+                k[2] += ca * d12 * bb + ba * d33 * cb;
+                k[3] += ca * d11 * cb + ba * d33 * bb;
+            }
+        } else {
+            for (int kk = sne[lo]; kk < sne[lo + 1]; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
+        }
         if (a.want_K) {
             double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + sidx));
             dst[0] = make_double2(k[0], k[1]);
             dst[1] = make_double2(k[2], k[3]);
         }
-        if (staged) {
-            double2* sd = reinterpret_cast<double2*>(sK + 4 * sidx);
-            sd[0] = make_double2(k[0], k[1]);
-            sd[1] = make_double2(k[2], k[3]);
-        }
     }
     if (!WANT_F) return;
-    __syncthreads();
-    if (threadIdx.x < nn) {
-        // the cut-element kernel adds its own f_int contributions afterwards
-        const int li = threadIdx.x;
+    // the cut-element kernel adds its own f_int contributions afterwards
+    for (int li = threadIdx.x; li < nn; li += kTileThreads) {
         double fx = 0.0, fy = 0.0;
         if (staged) {
-            for (int q = srp[li]; q < srp[li + 1]; ++q) {
-                const int j = __ldg(&a.col[seg0 + q]);
-                const double ux = a.u[2 * j], uy = a.u[2 * j + 1];
-                fx += sK[4 * q] * ux + sK[4 * q + 1] * uy;
-                fy += sK[4 * q + 2] * ux + sK[4 * q + 3] * uy;
+            for (int kk = sne[li] - k0; kk < sne[li + 1] - k0; ++kk) {
+                const int4 el = sN[kk];
+                const double* g = sG[kk];
+                const double ba = g[0], ca = g[1];
+                const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]);
+                const double d33 = __ldg(&a.dmat[3 * el.w + 2]);
+                const int nid[3] = {el.x, el.y, el.z};
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const double bb = g[2 + t], cb = g[5 + t];
+                    const double ux = a.u[2 * nid[t]], uy = a.u[2 * nid[t] + 1];
+                    fx += (ba * d11 * bb + ca * d33 * cb) * ux + (ba * d12 * cb + ca * d33 * bb) * uy;
+                    fy += (ca * d12 * bb + ba * d33 * cb) * ux + (ca * d11 * cb + ba * d33 * bb) * uy;
+                }
             }
         } else {
             for (int kk = sne[li]; kk < sne[li + 1]; ++kk) cst_force_add(a, __ldg(&a.ne_list[kk]), fx, fy);
@@ -298,10 +347,9 @@ __device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, doubl
 // Cut-element kernel
 // ---------------------------------------------------------------------------
 constexpr int kCutWarps = 4;
-constexpr int kCutPairsPerLane = 8;       // (3 + kMaxEnr)^2 = 225 <= 8 * 32
-
 struct CutArgs {
-    int n_cut;
+    int n_cut;                      // elements of this launch: order[0 .. n_cut)
+    const int* __restrict__ order;
     const int* __restrict__ cut_elem;
     const int* __restrict__ cut_tmpl;
     const int* __restrict__ cut_enr;
@@ -326,20 +374,24 @@ struct CutArgs {
 // Per-warp shared tables: one row per quadrature point of the current chunk
 // holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
 // row per cohesive point holding {wgt, N0, N1, (R^T D R) 4, (R^T t) 2}.
+// NL is the size class's largest local node count; PPL = ceil(NL^2 / 32)
+// node-pair blocks per lane.
 constexpr int kQpChunk = 32;
-constexpr int kQRow = 4 + 2 * kMaxElemNodes;
 constexpr int kCRow = 10;
 
+template <int NL, int PPL>
 __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
-    __shared__ double sX[kCutWarps][kMaxElemNodes], sY[kCutWarps][kMaxElemNodes];
-    __shared__ double sU[kCutWarps][2 * kMaxElemNodes];
-    __shared__ int sL[kCutWarps][kMaxElemNodes];
+    constexpr int kQRow = 4 + 2 * NL;
+    __shared__ double sX[kCutWarps][NL], sY[kCutWarps][NL];
+    __shared__ double sU[kCutWarps][2 * NL];
+    __shared__ int sL[kCutWarps][NL];
     __shared__ double sQ[kCutWarps][kQpChunk][kQRow];
     __shared__ double sC[kCutWarps][2 * kMaxCoh][kCRow];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int ci = blockIdx.x * kCutWarps + w;
-    if (ci >= a.n_cut) return;
+    const int oi = blockIdx.x * kCutWarps + w;
+    if (oi >= a.n_cut) return;
+    const int ci = a.order[oi];
     const DevTemplate& T = c_tmpl[a.cut_tmpl[ci]];
     const int nl = 3 + T.n_enr;
     const int e = a.cut_elem[ci];
@@ -365,13 +417,13 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
     int nq_total = 0;
     for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
 
-    double acc[kCutPairsPerLane][4];
+    double acc[PPL][4];
 #pragma unroll
-    for (int k = 0; k < kCutPairsPerLane; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
+    for (int k = 0; k < PPL; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
     const int npairs = nl * nl;
-    int pa[kCutPairsPerLane], pb[kCutPairsPerLane];
+    int pa[PPL], pb[PPL];
 #pragma unroll
-    for (int k = 0; k < kCutPairsPerLane; ++k) {
+    for (int k = 0; k < PPL; ++k) {
         const int p = lane + 32 * k;
         pa[k] = p / nl;
         pb[k] = p - pa[k] * nl;
@@ -434,7 +486,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
             const double* row = sQ[w][q];
             const double wgt = row[0], d11 = row[1], d12 = row[2], d33 = row[3];
 #pragma unroll
-            for (int k = 0; k < kCutPairsPerLane; ++k) {
+            for (int k = 0; k < PPL; ++k) {
                 if (lane + 32 * k < npairs) {
                     const double ba = row[4 + 2 * pa[k]] * wgt, ca = row[5 + 2 * pa[k]] * wgt;
                     const double bb = row[4 + 2 * pb[k]], cb = row[5 + 2 * pb[k]];
@@ -450,7 +502,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
     // bulk internal force f_a = sum_b K_ab u_b
     if (a.want_f) {
 #pragma unroll
-        for (int k = 0; k < kCutPairsPerLane; ++k) {
+        for (int k = 0; k < PPL; ++k) {
             if (lane + 32 * k < npairs) {
                 const int ia = pa[k], ib = pb[k];
                 const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
@@ -515,7 +567,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         for (int ce = 0; ce < T.n_coh; ++ce) {
             const int cn[4] = {T.coh_nodes[ce][0], T.coh_nodes[ce][1], T.coh_nodes[ce][2], T.coh_nodes[ce][3]};
 #pragma unroll
-            for (int k = 0; k < kCutPairsPerLane; ++k) {
+            for (int k = 0; k < PPL; ++k) {
                 if (lane + 32 * k < npairs) {
                     int i = -1, j = -1;
                     for (int m = 0; m < 4; ++m) {
@@ -543,7 +595,7 @@ scatter:
     if (a.want_K) {
         const int* slots = a.cut_slot + a.cut_slot_ptr[ci];
 #pragma unroll
-        for (int k = 0; k < kCutPairsPerLane; ++k) {
+        for (int k = 0; k < PPL; ++k) {
             const int p = lane + 32 * k;
             if (p < npairs && slots[p] >= 0) {
                 double* d = a.K + 4 * (size_t)slots[p];
@@ -589,9 +641,9 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     if (c.timing) cudaEventRecord(c.ea0, s);
     if (rblocks > 0) {
         if (want_f)
-            k_assemble_blocks<true><<<rblocks, kTileThreads, (size_t)kTileCap * 32, s>>>(ra);
+            k_assemble_tri<true><<<rblocks, kTileThreads, 0, s>>>(ra);
         else
-            k_assemble_blocks<false><<<rblocks, kTileThreads, 0, s>>>(ra);
+            k_assemble_tri<false><<<rblocks, kTileThreads, 0, s>>>(ra);
     }
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
@@ -618,8 +670,19 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
         ca.f = c.F;
         ca.want_K = want_K;
         ca.want_f = want_f;
-        const int cblocks = (c.n_cut + kCutWarps - 1) / kCutWarps;
-        k_assemble_cut<<<cblocks, 32 * kCutWarps, 0, s>>>(ca);
+        ca.order = c.cut_order;
+        for (int k = 0; k < kCutClasses; ++k) {
+            const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
+            if (n == 0) continue;
+            CutArgs ck = ca;
+            ck.n_cut = n;
+            ck.order = c.cut_order + c.cut_class_off[k];
+            const int cblocks = (n + kCutWarps - 1) / kCutWarps;
+            if (k == 0) k_assemble_cut<5, 1><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
+            else if (k == 1) k_assemble_cut<7, 2><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
+            else if (k == 2) k_assemble_cut<11, 4><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
+            else k_assemble_cut<15, 8><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
+        }
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);

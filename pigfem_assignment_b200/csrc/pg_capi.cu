@@ -36,7 +36,7 @@ int dev_alloc(T** dst, size_t n) {
 
 void free_ctx(Ctx& c) {
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.dmat, c.cut_elem, c.cut_tmpl,
-                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_order, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -130,6 +130,23 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         }
         if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
         if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
+        // cut elements grouped by size class, each class in mesh order
+        std::vector<int> order;
+        order.reserve(hm.n_cut);
+        for (int k = 0; k < kCutClasses; ++k) {
+            c.cut_class_off[k] = (int)order.size();
+            const int lo = k == 0 ? 0 : kCutClassNl[k - 1];
+            for (int ci = 0; ci < hm.n_cut; ++ci) {
+                const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
+                if (nl > lo && nl <= kCutClassNl[k]) order.push_back(ci);
+            }
+        }
+        c.cut_class_off[kCutClasses] = (int)order.size();
+        if (order.size() != (size_t)hm.n_cut) {
+            set_error("cut element with more local nodes than the largest size class");
+            return PG_ERR_MESH;
+        }
+        if ((rc = dev_upload(&c.cut_order, order))) return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;

@@ -23,6 +23,11 @@ struct DevCohLaw {
 };
 
 // Template table entry as the cut-element kernel reads it (constant memory).
+// Cut elements are integrated by one kernel instance per size class: local
+// node count (3 + enrichment slots) at most kCutClassNl[k].
+constexpr int kCutClasses = 4;
+constexpr int kCutClassNl[kCutClasses] = {5, 7, 11, 15};
+
 struct DevTemplate {
     int n_enr, n_child, n_coh, pad;
     int child_n[kMaxChildren];
@@ -63,6 +68,8 @@ struct Ctx {
     int* cut_coh_qp0 = nullptr;
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;
+    int* cut_order = nullptr;          // cut elements grouped by size class (see kCutClassNl)
+    int cut_class_off[5] = {0, 0, 0, 0, 0};
     // system
     double* K = nullptr;               // 4 * n_blocks
     float* Kf = nullptr;               // FP32 copy for mixed precision

@@ -250,6 +250,28 @@ int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
  * switch timing on/off. */
 int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
+/* ---- solve without device allocation ----
+ * No counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory (a host framework that owns every device buffer
+ * through its own allocator or budget, code where an allocation is not
+ * permitted, foreign-language bindings that hold only pointers): block-Jacobi
+ * PCG on a caller-owned 2x2-block CSR system of at most PG_STATIC_MAX_NODES
+ * nodes (2 DOFs each, DOF 2*node+d), solving mask(K) x = mask(b) on the DOFs
+ * with fixed[dof] == 0 and writing x = 0 on the others.  All pointers are
+ * device pointers the caller owns (row_ptr n_nodes+1, col and 4 values per
+ * block, fixed/b/x 2*n_nodes); stats is host memory.  The Krylov vectors live
+ * in one fixed array of about 3 MiB in the library's device image, held on
+ * every GPU that loads the library until exit: the first call on a device
+ * (with that device current) looks its address up, so make that first call
+ * before any stream capture; every call shares the array, so calls that
+ * overlap on the GPU race and must be serialised.  Returns PG_ERR_LIMIT for
+ * more than PG_STATIC_MAX_NODES nodes and never calls cudaMalloc or cudaFree.
+ * stream: cudaStream_t cast to void* (NULL = legacy default stream). */
+#define PG_STATIC_MAX_NODES 32768
+int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, const double* K,
+                        const uint8_t* fixed, const double* b, double* x, double rtol, int32_t max_iter,
+                        void* stream, pg_solve_stats* stats);
+
 const char* pg_last_error(void);
 const char* pg_version(void);
 

@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpigfem_b200.so")
 
 PG_OK = 0
+PG_STATIC_MAX_NODES = 32768
 PG_ERR_ARG = 1
 PG_ERR_MESH = 2
 PG_ERR_CUDA = 3
@@ -126,6 +127,8 @@ def _load() -> C.CDLL:
                                   C.POINTER(_dp)], C.c_int),
         "pg_solver_cfg_default": ([C.POINTER(SolverCfg)], None),
         "pg_solve_linear": ([v, C.POINTER(SolverCfg), C.POINTER(SolveStats)], C.c_int),
+        "pg_pcg_solve_static": ([C.c_int32, v, v, v, v, v, v, C.c_double, C.c_int32, v, C.POINTER(SolveStats)],
+                                C.c_int),
         "pg_get_matrix": ([v, _dp], C.c_int),
         "pg_get_vector": ([v, C.c_int32, _dp], C.c_int),
         "pg_set_vector": ([v, C.c_int32, _dp], C.c_int),
@@ -170,7 +173,7 @@ DECLARED_SYMBOLS = (
     "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
     "pg_solve_nonlinear", "pg_mlp_create", "pg_mlp_destroy", "pg_mlp_param_count", "pg_mlp_params",
     "pg_mlp_grads", "pg_mlp_forward", "pg_mlp_gradient", "pg_mlp_adam", "pg_mlp_train", "pg_predictor_features",
-    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_last_error",
+    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_pcg_solve_static", "pg_last_error",
     "pg_version",
 )
 

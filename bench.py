@@ -288,10 +288,12 @@ def run_b200_arm(args):
     load = None
     if not args.no_load_step:
         load = {}
-        for name, prec in (("plain_fp64", _lib.PG_PRECISION_FP64), ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED)):
+        variants = (("plain_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_MG),
+                    ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED, _lib.PG_PREC_MG),
+                    ("block_jacobi_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_BLOCK_JACOBI))
+        for name, prec, pc in variants:
             solver = pb.Solver(ctx)
-            solver.configure(precision=prec, precond=_lib.PG_PREC_BLOCK_JACOBI, rtol=1e-8, inner_rtol=1e-3,
-                             check_every=64)
+            solver.configure(precision=prec, precond=pc, rtol=1e-8, inner_rtol=1e-3, check_every=64)
             ctx.set_vector(0, np.zeros(info["n_dof"]))
             torch.cuda.synchronize()
             a, b = assemble_timed()

@@ -140,9 +140,13 @@ int pg_ctx_device_arrays(pg_ctx* c, double** K, double** U, double** F_int, doub
 #define PG_PREC_JACOBI 0
 #define PG_PREC_BLOCK_JACOBI 1
 #define PG_PREC_NONE 2
+#define PG_PREC_MG 3               /* one geometric multigrid V-cycle over the structured background grid
+                                      (Galerkin coarse operators, damped block-Jacobi smoothing); with
+                                      PG_PRECISION_MIXED the V-cycle runs in FP32 inside the FP64 Krylov loop */
 #define PG_PRECISION_FP64 0        /* plain FP64 Krylov */
-#define PG_PRECISION_MIXED 1       /* Krylov on the FP32-stored matrix (FP64 vectors and dots) inside
-                                      FP64 iterative refinement on the FP64 residual */
+#define PG_PRECISION_MIXED 1       /* Jacobi preconditioners: Krylov on the FP32-stored matrix (FP64 vectors
+                                      and dots) inside FP64 iterative refinement on the FP64 residual;
+                                      PG_PREC_MG: FP32 V-cycle preconditioning an FP64 Krylov solve */
 
 typedef struct pg_solver_cfg {
     int32_t krylov;                 /* PG_KRYLOV_* */

@@ -29,6 +29,7 @@ PG_KRYLOV_MINRES = 2
 PG_PREC_JACOBI = 0
 PG_PREC_BLOCK_JACOBI = 1
 PG_PREC_NONE = 2
+PG_PREC_MG = 3
 PG_PRECISION_FP64 = 0
 PG_PRECISION_MIXED = 1
 

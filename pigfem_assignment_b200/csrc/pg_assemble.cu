@@ -74,7 +74,10 @@ void upload_tables() {
 // ---------------------------------------------------------------------------
 constexpr int kTileNodes = 64;            // node rows per CTA
 constexpr int kTileThreads = 128;
-constexpr int kTileEntries = 512;         // staged (node, triangle) entries: 64 nodes x valence <= 8 (40 KB)
+constexpr int kTileEntries = 512;         // staged (node, triangle) entries: 64 nodes x valence <= 8
+constexpr int kEntriesPerThread = kTileEntries / kTileThreads;
+constexpr int kTileBlocks = 1024;         // staged column indices of the slice
+constexpr int kTileMats = 32;             // staged material table
 
 struct RowArgs {
     int n_nodes;
@@ -88,6 +91,7 @@ struct RowArgs {
     const double* __restrict__ y;
     const double* __restrict__ u;
     const double* __restrict__ dmat;
+    int n_mat;
     double* K;
     double* f;
     int want_K, want_f;
@@ -145,9 +149,11 @@ __device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, doub
 
 // A CTA owns the 2x2-block CSR slice of kTileNodes consecutive node rows
 // and works in three phases:
-//   1. one thread per (node, adjacent uncut triangle) entry of the slice
-//      computes the triangle's gradients once (b_t, c_t and the node's own
-//      row scaled by 1/(2J)) into shared memory;
+//   1. the slice's (node, adjacent uncut triangle) entries are gathered with
+//      all of a thread's loads in flight together (entry, then triangle, then
+//      coordinates), and each triangle's gradients b_t, c_t and 1/(2J) are
+//      stored once per entry in shared memory, next to the slice's column
+//      indices and the material table;
 //   2. one thread per 2x2 block (i, j) of the slice sums, over the staged
 //      entries of row i whose triangle contains node j, the constant-strain
 //      block B_i^T D B_j (the reference's 4-point rule integrates the constant
@@ -162,43 +168,76 @@ __device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, doub
 // global memory instead.
 template <bool WANT_F>
 __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
-    __shared__ double sG[kTileEntries][8];   // ba, ca, b0, b1, b2, c0, c1, c2
-    __shared__ int4 sN[kTileEntries];        // the triangle's nodes and material
+    __shared__ double sG[kTileEntries][7];   // b0, b1, b2, c0, c1, c2, 1/(2J)
+    __shared__ int4 sN[kTileEntries];        // n0, n1, n2, material | (entry's own vertex << 16)
+    __shared__ int scol[kTileBlocks];
+    __shared__ double sD[3 * kTileMats];
     __shared__ int srp[kTileNodes + 1];
     __shared__ int sne[kTileNodes + 1];
     const int node0 = blockIdx.x * kTileNodes;
     const int node_end = min(node0 + kTileNodes, a.n_nodes);
     const int nn = node_end - node0;
+    // slice bounds read directly (broadcast loads), so that the entry and
+    // column loads need not wait for the shared copies
     const int seg0 = __ldg(&a.row_ptr[node0]);
+    const int nseg = __ldg(&a.row_ptr[node_end]) - seg0;
+    const int k0 = __ldg(&a.ne_ptr[node0]);
+    const int nent = __ldg(&a.ne_ptr[node_end]) - k0;
+    const bool staged = nent <= kTileEntries;
+    const bool cols_staged = nseg <= kTileBlocks;
+    const bool mats_staged = a.n_mat <= kTileMats;
     for (int i = threadIdx.x; i <= nn; i += kTileThreads) {
         srp[i] = __ldg(&a.row_ptr[node0 + i]) - seg0;
-        sne[i] = __ldg(&a.ne_ptr[node0 + i]);
+        sne[i] = __ldg(&a.ne_ptr[node0 + i]) - k0;
+    }
+    if (mats_staged)
+        for (int i = threadIdx.x; i < 3 * a.n_mat; i += kTileThreads) sD[i] = __ldg(&a.dmat[i]);
+    if (cols_staged)
+        for (int i = threadIdx.x; i < nseg; i += kTileThreads) scol[i] = __ldg(&a.col[seg0 + i]);
+    if (staged) {
+        int packed[kEntriesPerThread];
+        int4 el[kEntriesPerThread];
+#pragma unroll
+        for (int u = 0; u < kEntriesPerThread; ++u) {
+            const int k = threadIdx.x + u * kTileThreads;
+            packed[u] = k < nent ? __ldg(&a.ne_list[k0 + k]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kEntriesPerThread; ++u) {
+            const int k = threadIdx.x + u * kTileThreads;
+            el[u] = k < nent ? __ldg(&a.elem4[packed[u] >> 2]) : make_int4(0, 0, 0, 0);
+        }
+        double X[kEntriesPerThread][3], Y[kEntriesPerThread][3];
+#pragma unroll
+        for (int u = 0; u < kEntriesPerThread; ++u) {
+            const int k = threadIdx.x + u * kTileThreads;
+            if (k < nent) {
+                X[u][0] = __ldg(&a.x[el[u].x]);
+                X[u][1] = __ldg(&a.x[el[u].y]);
+                X[u][2] = __ldg(&a.x[el[u].z]);
+                Y[u][0] = __ldg(&a.y[el[u].x]);
+                Y[u][1] = __ldg(&a.y[el[u].y]);
+                Y[u][2] = __ldg(&a.y[el[u].z]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kEntriesPerThread; ++u) {
+            const int k = threadIdx.x + u * kTileThreads;
+            if (k < nent) {
+                const double J = (X[u][1] - X[u][0]) * (Y[u][2] - Y[u][0]) - (X[u][2] - X[u][0]) * (Y[u][1] - Y[u][0]);
+                double* g = sG[k];
+                g[0] = Y[u][1] - Y[u][2];
+                g[1] = Y[u][2] - Y[u][0];
+                g[2] = Y[u][0] - Y[u][1];
+                g[3] = X[u][2] - X[u][1];
+                g[4] = X[u][0] - X[u][2];
+                g[5] = X[u][1] - X[u][0];
+                g[6] = 0.5 / J;
+                sN[k] = make_int4(el[u].x, el[u].y, el[u].z, el[u].w | ((packed[u] & 3) << 16));
+            }
+        }
     }
     __syncthreads();
-    const int nseg = srp[nn];
-    const int k0 = sne[0];
-    const int nent = sne[nn] - k0;
-    const bool staged = nent <= kTileEntries;
-    if (staged) {
-        for (int k = threadIdx.x; k < nent; k += kTileThreads) {
-            const int packed = __ldg(&a.ne_list[k0 + k]);
-            const int e = packed >> 2, v = packed & 3;
-            const int4 el = __ldg(&a.elem4[e]);
-            const double X0 = __ldg(&a.x[el.x]), X1 = __ldg(&a.x[el.y]), X2 = __ldg(&a.x[el.z]);
-            const double Y0 = __ldg(&a.y[el.x]), Y1 = __ldg(&a.y[el.y]), Y2 = __ldg(&a.y[el.z]);
-            const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
-            const double b0 = Y1 - Y2, b1 = Y2 - Y0, b2 = Y0 - Y1;
-            const double c0 = X2 - X1, c1 = X0 - X2, c2 = X1 - X0;
-            const double s = 0.5 / J;
-            double* g = sG[k];
-            g[0] = (v == 0 ? b0 : v == 1 ? b1 : b2) * s;
-            g[1] = (v == 0 ? c0 : v == 1 ? c1 : c2) * s;
-            g[2] = b0; g[3] = b1; g[4] = b2;
-            g[5] = c0; g[6] = c1; g[7] = c2;
-            sN[k] = el;
-        }
-        __syncthreads();
-    }
     for (int sidx = threadIdx.x; sidx < nseg; sidx += kTileThreads) {
         // row of this block: the largest li with srp[li] <= sidx
         int lo = 0, hi = nn - 1;
@@ -206,25 +245,26 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
             const int mid = (lo + hi + 1) >> 1;
             if (srp[mid] <= sidx) lo = mid; else hi = mid - 1;
         }
-        const int j = __ldg(&a.col[seg0 + sidx]);
+        const int j = cols_staged ? scol[sidx] : __ldg(&a.col[seg0 + sidx]);
         double k[4] = {0.0, 0.0, 0.0, 0.0};
         if (staged) {
-            const int kend = sne[lo + 1] - k0;
-            for (int kk = sne[lo] - k0; kk < kend; ++kk) {
+            for (int kk = sne[lo]; kk < sne[lo + 1]; ++kk) {
                 const int4 el = sN[kk];
                 const int t = el.x == j ? 0 : el.y == j ? 1 : el.z == j ? 2 : -1;
                 if (t < 0) continue;
+                const int mat = el.w & 0xffff, v = el.w >> 16;
                 const double* g = sG[kk];
-                const double ba = g[0], ca = g[1], bb = g[2 + t], cb = g[5 + t];
-                const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]);
-                const double d33 = __ldg(&a.dmat[3 * el.w + 2]);
+                const double s = g[6];
+                const double ba = g[v] * s, ca = g[3 + v] * s, bb = g[t], cb = g[3 + t];
+                const double* D = mats_staged ? sD + 3 * mat : a.dmat + 3 * mat;
+                const double d11 = D[0], d12 = D[1], d33 = D[2];
                 k[0] += ba * d11 * bb + ca * d33 * cb;
                 k[1] += ba * d12 * cb + ca * d33 * bb;
                 k[2] += ca * d12 * bb + ba * d33 * cb;
                 k[3] += ca * d11 * cb + ba * d33 * bb;
             }
         } else {
-            for (int kk = sne[lo]; kk < sne[lo + 1]; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
+            for (int kk = k0 + sne[lo]; kk < k0 + sne[lo + 1]; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
         }
         if (a.want_K) {
             double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + sidx));
@@ -237,23 +277,25 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
     for (int li = threadIdx.x; li < nn; li += kTileThreads) {
         double fx = 0.0, fy = 0.0;
         if (staged) {
-            for (int kk = sne[li] - k0; kk < sne[li + 1] - k0; ++kk) {
+            for (int kk = sne[li]; kk < sne[li + 1]; ++kk) {
                 const int4 el = sN[kk];
+                const int mat = el.w & 0xffff, v = el.w >> 16;
                 const double* g = sG[kk];
-                const double ba = g[0], ca = g[1];
-                const double d11 = __ldg(&a.dmat[3 * el.w]), d12 = __ldg(&a.dmat[3 * el.w + 1]);
-                const double d33 = __ldg(&a.dmat[3 * el.w + 2]);
+                const double s = g[6];
+                const double ba = g[v] * s, ca = g[3 + v] * s;
+                const double* D = mats_staged ? sD + 3 * mat : a.dmat + 3 * mat;
+                const double d11 = D[0], d12 = D[1], d33 = D[2];
                 const int nid[3] = {el.x, el.y, el.z};
 #pragma unroll
                 for (int t = 0; t < 3; ++t) {
-                    const double bb = g[2 + t], cb = g[5 + t];
+                    const double bb = g[t], cb = g[3 + t];
                     const double ux = a.u[2 * nid[t]], uy = a.u[2 * nid[t] + 1];
                     fx += (ba * d11 * bb + ca * d33 * cb) * ux + (ba * d12 * cb + ca * d33 * bb) * uy;
                     fy += (ca * d12 * bb + ba * d33 * cb) * ux + (ca * d11 * cb + ba * d33 * bb) * uy;
                 }
             }
         } else {
-            for (int kk = sne[li]; kk < sne[li + 1]; ++kk) cst_force_add(a, __ldg(&a.ne_list[kk]), fx, fy);
+            for (int kk = k0 + sne[li]; kk < k0 + sne[li + 1]; ++kk) cst_force_add(a, __ldg(&a.ne_list[kk]), fx, fy);
         }
         a.f[2 * (node0 + li)] = fx;
         a.f[2 * (node0 + li) + 1] = fy;
@@ -633,6 +675,7 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.y = c.y;
     ra.u = U;
     ra.dmat = c.dmat;
+    ra.n_mat = (int)c.hm.spec.materials.size();
     ra.K = c.K;
     ra.f = c.F;
     ra.want_K = want_K;

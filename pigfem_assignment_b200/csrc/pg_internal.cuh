@@ -44,6 +44,8 @@ struct DevChildQuad {
     double dN[kMaxChildQ * kMaxChildNodes * 2];
 };
 
+struct MgHierarchy;
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -70,6 +72,7 @@ struct Ctx {
     int* cut_slot = nullptr;
     int* cut_order = nullptr;          // cut elements grouped by size class (see kCutClassNl)
     int cut_class_off[5] = {0, 0, 0, 0, 0};
+    MgHierarchy* mg = nullptr;         // multigrid hierarchy, built at the first multigrid solve
     // system
     double* K = nullptr;               // 4 * n_blocks
     float* Kf = nullptr;               // FP32 copy for mixed precision
@@ -134,6 +137,13 @@ int launch_to_fp32(Ctx& c, cudaStream_t s);
 int solve_linear_system(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
 // mask(K) x = b for x (x starts at 0); b = c.b (masked); result in c.dx
 int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
+// out = mask(b - K x) (b nullable: 0); returns ||out||^2
+double residual_into(Ctx& c, cudaStream_t s, const double* x, const double* b, double* out);
+// geometric multigrid (pg_mg.cu)
+int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
+int mg_prepare(Ctx& c, bool f32, cudaStream_t s);
+void mg_precondition(Ctx& c, bool f32, cudaStream_t s, const double* r, double* z);
+void mg_free(Ctx& c);
 // ||v||^2 of a device vector (synchronises)
 double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s);
 void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);

@@ -75,8 +75,10 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
         if (rc != PG_OK) return rc;
         st.krylov_its += ls.iterations;
         if (ls.status == PG_ERR_BREAKDOWN) {
-            // indefinite tangent (cohesive softening): symmetric MINRES
-            lin.krylov = PG_KRYLOV_MINRES;
+            // indefinite tangent (cohesive softening): GMRES with the multigrid
+            // cycle when multigrid is selected, else symmetric MINRES (whose
+            // preconditioner must stay positive definite: |diag| Jacobi)
+            lin.krylov = lin.precond == PG_PREC_MG ? PG_KRYLOV_GMRES : PG_KRYLOV_MINRES;
             pg_solve_stats gs{};
             rc = krylov_solve(c, lin, gs, s);
             if (rc != PG_OK) return rc;

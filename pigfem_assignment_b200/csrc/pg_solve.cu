@@ -83,14 +83,6 @@ int pcg_run(Ctx& c, cudaStream_t s, const MT* K, VT* x, VT* r, VT* z, VT* p, VT*
     return iters;
 }
 
-// out = mask(b - K x) (b nullable: 0); returns ||out||^2
-double residual_into(Ctx& c, cudaStream_t s, const double* x, const double* b, double* out) {
-    const int n = c.n_nodes, nd = c.n_dof;
-    k_spmv_plain<double, double><<<nblk(n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, x, c.fixed, out);
-    k_rhs_minus<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, b, out);
-    return dev_norm2(c, out, nd, s);
-}
-
 // ---------------- GMRES ----------------
 int ensure_gmres(Ctx& c, int m) {
     if (c.V && c.gm >= m) return PG_OK;
@@ -124,7 +116,10 @@ int gmres_solve(Ctx& c, const pg_solver_cfg& cfg, double rtol, int max_iter, pg_
             double* vj = c.V + (size_t)j * nd;
             double* w = c.V + (size_t)(j + 1) * nd;
             // w = K M^-1 v_j
-            k_apply_prec_vec<<<nblk(n), kThreads, 0, s>>>(n, c.minv, vj, c.z);
+            if (cfg.precond == PG_PREC_MG)
+                mg_precondition(c, cfg.precision == PG_PRECISION_MIXED, s, vj, c.z);
+            else
+                k_apply_prec_vec<<<nblk(n), kThreads, 0, s>>>(n, c.minv, vj, c.z);
             k_spmv_plain<double, double><<<nblk(n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.z, c.fixed, w);
             // classical Gram-Schmidt, twice
             std::fill(hcol.begin(), hcol.end(), 0.0);
@@ -170,7 +165,10 @@ int gmres_solve(Ctx& c, const pg_solver_cfg& cfg, double rtol, int max_iter, pg_
         cudaMemcpyAsync(c.hbuf, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
         k_fill<double><<<nblk(nd), kThreads, 0, s>>>(nd, c.q, 0.0);
         k_multi_axpy_add<<<nblk(nd), kThreads, 0, s>>>(nd, j, c.V, c.hbuf, c.q);
-        k_apply_prec_vec<<<nblk(n), kThreads, 0, s>>>(n, c.minv, c.q, c.z);
+        if (cfg.precond == PG_PREC_MG)
+            mg_precondition(c, cfg.precision == PG_PRECISION_MIXED, s, c.q, c.z);
+        else
+            k_apply_prec_vec<<<nblk(n), kThreads, 0, s>>>(n, c.minv, c.q, c.z);
         k_axpy_free<double><<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.dx, c.z, 1.0);
         if (done) {
             rnorm = std::sqrt(residual_into(c, s, c.dx, c.b, c.r));
@@ -247,6 +245,13 @@ int minres_solve(Ctx& c, double rtol, int max_iter, int chunk, pg_solve_stats& s
 
 }  // namespace
 
+double residual_into(Ctx& c, cudaStream_t s, const double* x, const double* b, double* out) {
+    const int n = c.n_nodes, nd = c.n_dof;
+    k_spmv_plain<double, double><<<nblk(n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, x, c.fixed, out);
+    k_rhs_minus<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, b, out);
+    return dev_norm2(c, out, nd, s);
+}
+
 double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s) {
     cudaMemsetAsync(c.scal + S_AUX, 0, sizeof(double), s);
     k_dot_self<<<nblk(n), kThreads, 0, s>>>(n, v, c.scal + S_AUX);
@@ -282,6 +287,16 @@ int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
         // MINRES monitors the M^-1-norm; accept a true residual within a small factor
         st.status = rr <= tol2 * 100.0 ? PG_OK : PG_ERR_NOT_CONVERGED;
         return PG_OK;
+    }
+    if (cfg.precond == PG_PREC_MG) {
+        // one multigrid V-cycle per iteration (FP32 cycle under PG_PRECISION_MIXED)
+        if (cfg.krylov == PG_KRYLOV_GMRES) {
+            const int rc = mg_prepare(c, cfg.precision == PG_PRECISION_MIXED, s);
+            if (rc == PG_ERR_BREAKDOWN) { st.status = rc; return PG_OK; }
+            if (rc != PG_OK) return rc;
+            return gmres_solve(c, cfg, cfg.rtol, cfg.max_iter, st, s, std::sqrt(bb));
+        }
+        return mg_pcg_solve(c, cfg, st, s);
     }
     k_prec_setup<double><<<nblk(n), kThreads, 0, s>>>(n, c.diag, c.K, c.fixed, block, ident, c.minv);
     if (cfg.krylov == PG_KRYLOV_GMRES) {

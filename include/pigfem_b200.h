@@ -41,8 +41,10 @@ typedef struct pg_ctx pg_ctx;    /* device state for one mesh (opaque) */
 
 /* Cohesive laws.  PG_COH_OP: Ortiz-Pandolfi exponential law with linear
  * unloading and viscous regularisation, params {sigma_c, delta_c, beta,
- * viscosity} (src/Material_OPCohesive.cpp:38-253, the reference's active law).
- * PG_COH_BILINEAR: bilinear penalty law, params {sigma_c, G_c, K_p, beta}. */
+ * viscosity, unused} (src/Material_OPCohesive.cpp:38-253, the reference's active law).
+ * PG_COH_BILINEAR: bilinear penalty law, params {sigma_c, G_c, K_p, beta, eta}:
+ * eta >= 0 adds the viscous traction eta * (delta_eff - delta_max) / dt while
+ * the interface loads, the regularisation the OP law carries (0 = none). */
 #define PG_COH_OP 0
 #define PG_COH_BILINEAR 1
 
@@ -65,7 +67,7 @@ typedef struct pg_rve_desc {
     int32_t plane_strain;           /* 1: plane strain (only mode of the configs), 0: plane stress */
     int32_t cohesive;               /* 1: inclusion interfaces carry cohesive elements */
     int32_t coh_law;                /* PG_COH_OP or PG_COH_BILINEAR */
-    double coh_params[4];
+    double coh_params[5];
     double strain;                  /* prescribed x-displacement of the right edge = (x1-x0)*strain */
 } pg_rve_desc;
 
@@ -193,7 +195,14 @@ typedef struct pg_newton_cfg {
     int32_t lin_max_iter;
     int32_t max_repeat;             /* load-step repeats with dt *= 0.25 (reference: 20) */
     int32_t predictor;              /* PG_PREDICT_* */
+    int32_t rtol_base;              /* PG_RTOL_BASE_*: which residual rtol is relative to */
 } pg_newton_cfg;
+/* rtol relative to the residual of the step's own predictor (SNES, the reference) */
+#define PG_RTOL_BASE_PREDICTOR 0
+/* rtol relative to the residual of the zeroth-order predictor (the last converged
+ * U_f with the new prescribed values): one target per load step whatever the
+ * predictor, so predictors are compared at the same accuracy */
+#define PG_RTOL_BASE_ZEROTH 1
 
 typedef struct pg_step_stats {
     double t_frac, dt;
@@ -203,6 +212,7 @@ typedef struct pg_step_stats {
     double seconds;                 /* device time of the step */
     int32_t predictor_used;         /* PG_PREDICT_* actually used for this step */
     double res_linear, res_learned; /* initial residuals of both candidates (learned predictor only) */
+    double res_base;                /* the residual rtol was relative to */
 } pg_step_stats;
 
 void pg_newton_cfg_default(pg_newton_cfg* cfg);

@@ -58,7 +58,7 @@ typedef struct {
     int plane_strain;
     /* cohesive law: 0 = Ortiz-Pandolfi (sigma_c, delta_c, beta, viscosity), 1 = bilinear (sigma_c, G_c, K_p, beta) */
     int coh_law;
-    double coh_p[4];
+    double coh_p[5];
 } orc_mesh;
 
 /* ---------------- constitutive ---------------- */
@@ -129,8 +129,9 @@ static void op_law(const orc_mesh* m, double dt, double dmax, double delta[2], d
                        (T / de) * (beta2 * (i == k) + (1.0 - beta2) * (i == 1) * (k == 1));
 }
 
-/* bilinear penalty law (sigma_c, G_c, K_p, beta) with normal compression penalty */
-static void bilinear_law(const orc_mesh* m, double dmax, double delta[2], double t[2], double Dc[2][2], double* dmax_out) {
+/* bilinear penalty law (sigma_c, G_c, K_p, beta, eta) with normal compression penalty and the
+   viscous traction eta (delta_eff - delta_max) / dt while loading */
+static void bilinear_law(const orc_mesh* m, double dt, double dmax, double delta[2], double t[2], double Dc[2][2], double* dmax_out) {
     const double sc = m->coh_p[0], Gc = m->coh_p[1], Kp = m->coh_p[2], beta2 = m->coh_p[3] * m->coh_p[3];
     const double d0 = sc / Kp, df = 2.0 * Gc / sc;
     double norm = delta[0] * delta[0] + delta[1] * delta[1];
@@ -141,7 +142,7 @@ static void bilinear_law(const orc_mesh* m, double dmax, double delta[2], double
     *dmax_out = dmax;
     #define ENV(dd, T_, dT_) do { if ((dd) <= d0) { T_ = Kp * (dd); dT_ = Kp; } \
         else if ((dd) < df) { T_ = sc * (df - (dd)) / (df - d0); dT_ = -sc / (df - d0); } else { T_ = 0.0; dT_ = 0.0; } } while (0)
-    if (de >= dmax) { ENV(de, T, dT); *dmax_out = de; }
+    if (de >= dmax) { ENV(de, T, dT); T += m->coh_p[4] * (de - dmax) / dt; dT += m->coh_p[4] / dt; *dmax_out = de; }
     else { double Tm, dTm; ENV(dmax, Tm, dTm); (void)dTm; T = Tm * (de / dmax); dT = Tm / dmax; }
     #undef ENV
     double s = T / de, a = dT * de - T, de2 = de * de;
@@ -453,7 +454,7 @@ int orc_assemble(const orc_mesh* m, const int32_t* rp, const int32_t* col, doubl
                     double t[2], Dc[2][2], dnew;
                     double dmax = isv_c ? isv_c[coh_qp] : 0.0;
                     if (m->coh_law == 0) op_law(m, dt, dmax, dl, t, Dc, &dnew);
-                    else bilinear_law(m, dmax, dl, t, Dc, &dnew);
+                    else bilinear_law(m, dt, dmax, dl, t, Dc, &dnew);
                     if (isv_t) isv_t[coh_qp] = dnew;
                     ++coh_qp;
                     double RDR[2][2], tR[2];
@@ -526,14 +527,14 @@ void orc_tri3_K(const double xy[6], double E, double nu, int plane_strain, doubl
 }
 
 /* Cohesive law point evaluation for tests. */
-void orc_cohesive_law(int law, const double p[4], double dt, double dmax, double delta_in[2], double t[2], double Dc[4],
+void orc_cohesive_law(int law, const double p[5], double dt, double dmax, double delta_in[2], double t[2], double Dc[4],
                       double* dmax_out) {
     orc_mesh m;
     memset(&m, 0, sizeof(m));
     m.coh_law = law;
-    for (int i = 0; i < 4; ++i) m.coh_p[i] = p[i];
+    for (int i = 0; i < 5; ++i) m.coh_p[i] = p[i];
     double D2[2][2];
     if (law == 0) op_law(&m, dt, dmax, delta_in, t, D2, dmax_out);
-    else bilinear_law(&m, dmax, delta_in, t, D2, dmax_out);
+    else bilinear_law(&m, dt, dmax, delta_in, t, D2, dmax_out);
     Dc[0] = D2[0][0]; Dc[1] = D2[0][1]; Dc[2] = D2[1][0]; Dc[3] = D2[1][1];
 }

@@ -35,7 +35,7 @@ class _OrcMesh(C.Structure):
         ("n_nodes", C.c_int), ("xy", _dp), ("n_elem", C.c_int), ("conn", _ip), ("elem_mat", _ip), ("is_cut", _ip),
         ("enr_ptr", _ip), ("enr", _ip), ("child_ptr", _ip), ("child_nodes_ptr", _ip), ("child_nodes", _ip),
         ("child_mat", _ip), ("coh_ptr", _ip), ("coh_nodes", _ip), ("n_mat", C.c_int), ("mat_E", _dp),
-        ("mat_nu", _dp), ("plane_strain", C.c_int), ("coh_law", C.c_int), ("coh_p", C.c_double * 4),
+        ("mat_nu", _dp), ("plane_strain", C.c_int), ("coh_law", C.c_int), ("coh_p", C.c_double * 5),
     ]
 
 
@@ -113,7 +113,7 @@ class OracleMesh:
         self.mat_nu = np.ascontiguousarray(mat_nu, dtype=np.float64)
         self.plane_strain = int(plane_strain)
         self.coh_law = int(coh_law)
-        self.coh_p = tuple(float(v) for v in coh_p)
+        self.coh_p = tuple(float(v) for v in coh_p) + (0.0,) * (5 - len(coh_p))
         self.n_coh_qp = 2 * (len(hn) // 4)
         self.ref_dof = None if ref_dof is None else np.asarray(ref_dof, np.int64)
         self.n_free = n_free
@@ -128,7 +128,7 @@ class OracleMesh:
         s.child_mat, s.coh_ptr, s.coh_nodes = _i(self.child_mat), _i(self.coh_ptr), _i(self.coh_nodes)
         s.n_mat, s.mat_E, s.mat_nu = self.mat_E.size, _d(self.mat_E), _d(self.mat_nu)
         s.plane_strain, s.coh_law = self.plane_strain, self.coh_law
-        for k in range(4):
+        for k in range(5):
             s.coh_p[k] = self.coh_p[k]
         return s
 
@@ -256,7 +256,8 @@ def tri3_K(xy, E, nu, plane_strain=True):
 
 
 def cohesive_law(law, params, dt, dmax, delta):
-    p = np.ascontiguousarray(params, dtype=np.float64)
+    p = np.zeros(5)
+    p[:len(params)] = params
     d = np.ascontiguousarray(delta, dtype=np.float64).copy()
     t = np.zeros(2)
     Dc = np.zeros(4)

@@ -30,6 +30,8 @@ PG_PREC_JACOBI = 0
 PG_PREC_BLOCK_JACOBI = 1
 PG_PREC_NONE = 2
 PG_PREC_MG = 3
+PG_RTOL_BASE_PREDICTOR = 0
+PG_RTOL_BASE_ZEROTH = 1
 PG_PRECISION_FP64 = 0
 PG_PRECISION_MIXED = 1
 
@@ -46,7 +48,7 @@ class RveDesc(C.Structure):
         ("inc_cx", _dp), ("inc_cy", _dp), ("inc_r", _dp), ("inc_mat", _ip),
         ("n_materials", C.c_int32), ("mat_E", _dp), ("mat_nu", _dp),
         ("matrix_mat", C.c_int32), ("plane_strain", C.c_int32), ("cohesive", C.c_int32),
-        ("coh_law", C.c_int32), ("coh_params", C.c_double * 4), ("strain", C.c_double),
+        ("coh_law", C.c_int32), ("coh_params", C.c_double * 5), ("strain", C.c_double),
     ]
 
 
@@ -82,7 +84,7 @@ class NewtonCfg(C.Structure):
         ("n_steps", C.c_int32), ("T_final", C.c_double), ("rtol", C.c_double), ("atol", C.c_double),
         ("stol", C.c_double), ("max_it", C.c_int32), ("precision", C.c_int32), ("precond", C.c_int32),
         ("lin_rtol", C.c_double), ("inner_rtol", C.c_double), ("lin_max_iter", C.c_int32),
-        ("max_repeat", C.c_int32), ("predictor", C.c_int32),
+        ("max_repeat", C.c_int32), ("predictor", C.c_int32), ("rtol_base", C.c_int32),
     ]
 
 
@@ -91,7 +93,7 @@ class StepStats(C.Structure):
         ("t_frac", C.c_double), ("dt", C.c_double), ("newton_its", C.c_int32), ("krylov_its", C.c_int32),
         ("gmres_fallbacks", C.c_int32), ("repeats", C.c_int32), ("res0", C.c_double), ("res", C.c_double),
         ("reason", C.c_int32), ("seconds", C.c_double), ("predictor_used", C.c_int32),
-        ("res_linear", C.c_double), ("res_learned", C.c_double),
+        ("res_linear", C.c_double), ("res_learned", C.c_double), ("res_base", C.c_double),
     ]
 
 

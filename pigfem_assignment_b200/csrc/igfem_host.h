@@ -59,10 +59,11 @@ struct Material {
 // Cohesive law parameters.  law 0: Ortiz-Pandolfi exponential with linear
 // unloading and viscous regularisation (the reference's active law,
 // Material_OPCohesive.cpp:38-253): p = {sigma_c, delta_c, beta, viscosity}.
-// law 1: bilinear penalty law: p = {sigma_c, G_c, K_p, 0}.
+// law 1: bilinear penalty law: p = {sigma_c, G_c, K_p, beta, eta} with the
+// viscous traction eta (delta_eff - delta_max) / dt while loading.
 struct CohesiveLaw {
     int law = 0;
-    double p[4] = {0, 0, 0, 0};
+    double p[5] = {0, 0, 0, 0, 0};
 };
 
 struct RveSpec {

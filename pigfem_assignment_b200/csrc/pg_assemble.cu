@@ -33,6 +33,11 @@ namespace pgb {
 
 __constant__ DevTemplate c_tmpl[32];
 __constant__ DevChildQuad c_quad[kNumChildTypes];
+// Global copies for reads whose address differs across a warp's lanes (the
+// per-quadrature-point phase of the cut kernel): constant memory serialises
+// those, the L1 serves them at once.
+__device__ DevTemplate g_tmpl[32];
+__device__ DevChildQuad g_quad[kNumChildTypes];
 
 void upload_tables() {
     static bool done_dev[64] = {false};
@@ -66,6 +71,8 @@ void upload_tables() {
     }
     cudaMemcpyToSymbol(c_tmpl, t, sizeof(t));
     cudaMemcpyToSymbol(c_quad, q, sizeof(q));
+    cudaMemcpyToSymbol(g_tmpl, t, sizeof(t));
+    cudaMemcpyToSymbol(g_quad, q, sizeof(q));
     if (dev >= 0 && dev < 64) done_dev[dev] = true;
 }
 
@@ -147,6 +154,19 @@ __device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, doub
     }
 }
 
+// Adds the staged triangle's block (own vertex, t) to k[4]: g = {b0, b1, b2,
+// c0, c1, c2, 1/(2J)}, w = material | (own vertex << 16).
+__device__ __forceinline__ void cst_staged_add(const double* g, int w, int t, const double* dm, double k[4]) {
+    const int mat = w & 0xffff, v = w >> 16;
+    const double s = g[6];
+    const double ba = g[v] * s, ca = g[3 + v] * s, bb = g[t], cb = g[3 + t];
+    const double d11 = dm[3 * mat], d12 = dm[3 * mat + 1], d33 = dm[3 * mat + 2];
+    k[0] += ba * d11 * bb + ca * d33 * cb;
+    k[1] += ba * d12 * cb + ca * d33 * bb;
+    k[2] += ca * d12 * bb + ba * d33 * cb;
+    k[3] += ca * d11 * cb + ba * d33 * bb;
+}
+
 // A CTA owns the 2x2-block CSR slice of kTileNodes consecutive node rows
 // and works in three phases:
 //   1. the slice's (node, adjacent uncut triangle) entries are gathered with
@@ -154,13 +174,16 @@ __device__ __forceinline__ void cst_force_add(const RowArgs& a, int packed, doub
 //      coordinates), and each triangle's gradients b_t, c_t and 1/(2J) are
 //      stored once per entry in shared memory, next to the slice's column
 //      indices and the material table;
-//   2. one thread per 2x2 block (i, j) of the slice sums, over the staged
-//      entries of row i whose triangle contains node j, the constant-strain
-//      block B_i^T D B_j (the reference's 4-point rule integrates the constant
-//      integrand exactly: its weights sum to 1/2), and stores it once with
-//      coalesced 16-byte stores: no atomics, no prior clear (blocks coupling to
-//      enrichment nodes, and rows of enrichment nodes, are written as zeros
-//      and completed by the cut-element kernel);
+//   2. one thread per off-diagonal 2x2 block (i, j) of the slice finds the
+//      (at most two) staged triangles of row i that contain node j and sums
+//      their constant-strain blocks B_i^T D B_j (the reference's 4-point rule
+//      integrates the constant integrand exactly: its weights sum to 1/2);
+//      one thread per row sums the diagonal block over all the row's
+//      triangles.  Keeping the two apart keeps the warps' FP64 work uniform
+//      (two contributions per off-diagonal block).  Every block is stored once
+//      with coalesced 16-byte stores: no atomics, no prior clear (blocks
+//      coupling to enrichment nodes, and rows of enrichment nodes, are written
+//      as zeros and completed by the cut-element kernel);
 //   3. with WANT_F, one thread per row forms f_int,i = sum_e K_e(i, :) u_e
 //      from the staged entries.
 // A slice with more entries than the staging buffer (never for structured
@@ -246,23 +269,21 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
             if (srp[mid] <= sidx) lo = mid; else hi = mid - 1;
         }
         const int j = cols_staged ? scol[sidx] : __ldg(&a.col[seg0 + sidx]);
+        if (j == node0 + lo && staged) continue;  // diagonal blocks: below
         double k[4] = {0.0, 0.0, 0.0, 0.0};
         if (staged) {
+            // the triangles of row i that contain j: an edge has at most two
+            int m0 = -1, t0 = 0, m1 = -1, t1 = 0;
             for (int kk = sne[lo]; kk < sne[lo + 1]; ++kk) {
                 const int4 el = sN[kk];
                 const int t = el.x == j ? 0 : el.y == j ? 1 : el.z == j ? 2 : -1;
                 if (t < 0) continue;
-                const int mat = el.w & 0xffff, v = el.w >> 16;
-                const double* g = sG[kk];
-                const double s = g[6];
-                const double ba = g[v] * s, ca = g[3 + v] * s, bb = g[t], cb = g[3 + t];
-                const double* D = mats_staged ? sD + 3 * mat : a.dmat + 3 * mat;
-                const double d11 = D[0], d12 = D[1], d33 = D[2];
-                k[0] += ba * d11 * bb + ca * d33 * cb;
-                k[1] += ba * d12 * cb + ca * d33 * bb;
-                k[2] += ca * d12 * bb + ba * d33 * cb;
-                k[3] += ca * d11 * cb + ba * d33 * bb;
+                if (m0 < 0) { m0 = kk; t0 = t; }
+                else if (m1 < 0) { m1 = kk; t1 = t; }
+                else cst_staged_add(sG[kk], sN[kk].w, t, mats_staged ? sD : a.dmat, k);
             }
+            if (m0 >= 0) cst_staged_add(sG[m0], sN[m0].w, t0, mats_staged ? sD : a.dmat, k);
+            if (m1 >= 0) cst_staged_add(sG[m1], sN[m1].w, t1, mats_staged ? sD : a.dmat, k);
         } else {
             for (int kk = k0 + sne[lo]; kk < k0 + sne[lo + 1]; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
         }
@@ -270,6 +291,25 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
             double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + sidx));
             dst[0] = make_double2(k[0], k[1]);
             dst[1] = make_double2(k[2], k[3]);
+        }
+    }
+    if (staged) {
+        // diagonal blocks: every triangle of the row contributes (t = own vertex)
+        for (int li = threadIdx.x; li < nn; li += kTileThreads) {
+            double k[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int kk = sne[li]; kk < sne[li + 1]; ++kk)
+                cst_staged_add(sG[kk], sN[kk].w, sN[kk].w >> 16, mats_staged ? sD : a.dmat, k);
+            if (a.want_K) {
+                // the diagonal block's slot in the row
+                int q = srp[li];
+                const int i = node0 + li;
+                while (q < srp[li + 1] && (cols_staged ? scol[q] : __ldg(&a.col[seg0 + q])) != i) ++q;
+                if (q < srp[li + 1]) {
+                    double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + q));
+                    dst[0] = make_double2(k[0], k[1]);
+                    dst[1] = make_double2(k[2], k[3]);
+                }
+            }
         }
     }
     if (!WANT_F) return;
@@ -345,7 +385,7 @@ __device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, doubl
         return;
     }
     // bilinear penalty law with a compression penalty on the normal opening
-    const double sc = L.p[0], Gc = L.p[1], Kp = L.p[2];
+    const double sc = L.p[0], Gc = L.p[1], Kp = L.p[2], eta = L.p[4];
     const double dlt0 = sc / Kp, dltf = 2.0 * Gc / sc;
     const double dn = d1 > 0.0 ? d1 : 0.0;
     const double de = sqrt(dn * dn + beta2 * (d0 * d0)) + 1e-300;
@@ -358,6 +398,9 @@ __device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, doubl
     dmax_trial = dmax_c;
     if (de >= dmax_c) {
         env(de, T, dT);
+        // viscous regularisation while loading (eta = 0: none)
+        T += eta * (de - dmax_c) / dt;
+        dT += eta / dt;
         dmax_trial = de;
     } else {
         double Tm, dTm;
@@ -475,17 +518,18 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         // geometry of one quadrature point per lane, all points in parallel
         const int l = qbase + lane;
         if (l < nq_total) {
+            const DevTemplate& TG = g_tmpl[a.cut_tmpl[ci]];
             int ch = 0, q = l;
-            while (q >= c_quad[T.child_type[ch]].nq) {
-                q -= c_quad[T.child_type[ch]].nq;
+            while (q >= g_quad[TG.child_type[ch]].nq) {
+                q -= g_quad[TG.child_type[ch]].nq;
                 ++ch;
             }
-            const int nc = T.child_n[ch];
-            const DevChildQuad& Q = c_quad[T.child_type[ch]];
+            const int nc = TG.child_n[ch];
+            const DevChildQuad& Q = g_quad[TG.child_type[ch]];
             const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
             double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
             for (int k = 0; k < nc; ++k) {
-                const int ln = T.child_nodes[ch][k];
+                const int ln = TG.child_nodes[ch][k];
                 const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
                 J00 += dr * sX[w][ln];
                 J01 += dr * sY[w][ln];
@@ -513,7 +557,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
             }
             if (live)
                 for (int k = 0; k < nc; ++k) {
-                    const int ln = T.child_nodes[ch][k];
+                    const int ln = TG.child_nodes[ch][k];
                     if (ln >= 3) {
                         const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
                         row[4 + 2 * ln] = (J11 * dr - J01 * ds) / det;

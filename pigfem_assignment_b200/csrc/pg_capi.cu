@@ -97,7 +97,7 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     c.n_dof = hm.n_dof();
     c.n_coh_qp = hm.n_coh_qp;
     c.coh.law = hm.spec.coh.law;
-    for (int k = 0; k < 4; ++k) c.coh.p[k] = hm.spec.coh.p[k];
+    for (int k = 0; k < 5; ++k) c.coh.p[k] = hm.spec.coh.p[k];
 
     int rc;
     if ((rc = dev_upload(&c.x, hm.x))) return rc;
@@ -217,7 +217,11 @@ int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
     spec.plane_strain = rve->plane_strain != 0;
     spec.cohesive = rve->cohesive != 0;
     spec.coh.law = rve->coh_law;
-    for (int k = 0; k < 4; ++k) spec.coh.p[k] = rve->coh_params[k];
+    for (int k = 0; k < 5; ++k) spec.coh.p[k] = rve->coh_params[k];
+    if (spec.cohesive && spec.coh.law == PG_COH_BILINEAR && !(spec.coh.p[4] >= 0.0)) {
+        set_error("pg_mesh_build: the bilinear law's viscosity must be >= 0");
+        return PG_ERR_ARG;
+    }
     if (spec.cohesive && spec.coh.law != PG_COH_OP && spec.coh.law != PG_COH_BILINEAR) {
         set_error("pg_mesh_build: unknown cohesive law");
         return PG_ERR_ARG;

@@ -19,7 +19,7 @@ namespace pgb {
 // Cohesive law parameters on the device.
 struct DevCohLaw {
     int law;          // PG_COH_OP / PG_COH_BILINEAR
-    double p[4];
+    double p[5];
 };
 
 // Template table entry as the cut-element kernel reads it (constant memory).
@@ -157,7 +157,9 @@ double predictor_app(const Ctx& c);
 double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s);
 
 // Newton (pg_newton.cu)
-int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s);
+// r_base > 0: rtol is relative to it instead of the predictor's residual
+int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s,
+                     double r_base = 0.0);
 
 }  // namespace pgb
 

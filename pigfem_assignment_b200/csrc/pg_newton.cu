@@ -40,7 +40,8 @@ double newton_residual(Ctx& c, const double* U, double dt, cudaStream_t s) {
 
 double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s) { return newton_residual(c, U, dt, s); }
 
-int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s) {
+int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg, pg_step_stats& st, cudaStream_t s,
+                     double r_base) {
     const int nd = c.n_dof;
     st = pg_step_stats{};
     st.t_frac = t_frac;
@@ -50,10 +51,15 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
     double rr = newton_residual(c, c.U, dt, s);
     const double r0 = std::sqrt(rr);
     st.res0 = r0;
+    // rtol is relative to r_base when the caller gives one (the zeroth-order
+    // predictor's residual), else to the predictor's own residual (SNES)
+    const double rb = r_base > 0.0 ? r_base : r0;
+    st.res_base = rb;
     double rnorm = r0;
     int reason = 0;
     if (!(r0 == r0)) reason = -4;
     else if (r0 < cfg.atol) reason = 2;
+    else if (r_base > 0.0 && r0 <= cfg.rtol * rb) reason = 3;  // the predictor already meets the target
     pg_solver_cfg lin;
     pg_solver_cfg_default(&lin);
     lin.precision = cfg.precision;
@@ -101,7 +107,7 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
         const double dn = lambda * std::sqrt(dev_norm2(c, c.dx, nd, s));
         const double un = std::sqrt(dev_norm2(c, c.U, nd, s));
         if (rnorm < cfg.atol) reason = 2;
-        else if (rnorm <= cfg.rtol * r0) reason = 3;
+        else if (rnorm <= cfg.rtol * rb) reason = 3;
         else if (dn < cfg.stol * un) reason = 4;
     }
     if (reason == 0) reason = -5;  // iteration budget exhausted
@@ -139,6 +145,7 @@ void pg_newton_cfg_default(pg_newton_cfg* cfg) {
     cfg->lin_max_iter = 100000;
     cfg->max_repeat = 20;
     cfg->predictor = PG_PREDICT_ZEROTH;
+    cfg->rtol_base = PG_RTOL_BASE_PREDICTOR;
 }
 
 int pg_newton_load_step(pg_ctx* cx, double t_frac, double dt, const pg_newton_cfg* cfg_in, pg_step_stats* stats) {
@@ -187,6 +194,11 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             ++repeat;
             // U holds the last converged solution here (zeroth-order predictor)
             const double tf = (t + dt) / cfg.T_final;
+            double r_base = 0.0;
+            if (cfg.rtol_base == PG_RTOL_BASE_ZEROTH) {
+                set_prescribed(c, tf, s);
+                r_base = std::sqrt(predictor_residual(c, c.U, dt, s));
+            }
             int used = PG_PREDICT_ZEROTH;
             double res_lin = -1.0, res_mlp = -1.0;
             if (cfg.predictor == PG_PREDICT_LINEAR && nrec > 0) {
@@ -214,7 +226,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                     used = PG_PREDICT_LINEAR;
                 }
             }
-            const int rc = newton_load_step(c, tf, dt, cfg, st, s);
+            const int rc = newton_load_step(c, tf, dt, cfg, st, s, r_base);
             st.predictor_used = used;
             st.res_linear = res_lin;
             st.res_learned = res_mlp;

@@ -53,8 +53,8 @@ class Mesh:
         d.plane_strain = 1 if rve.plane_strain else 0
         d.cohesive = 1 if rve.cohesive else 0
         d.coh_law = rve.coh_law
-        for k in range(4):
-            d.coh_params[k] = rve.coh_params[k]
+        for k, v in enumerate(rve.coh_params[:5]):
+            d.coh_params[k] = v
         d.strain = rve.strain
         h = C.c_void_p()
         check(lib.pg_mesh_build(C.byref(d), C.byref(h)), "pg_mesh_build")

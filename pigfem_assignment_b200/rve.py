@@ -43,7 +43,7 @@ class RVE:
     matrix_mat: int = 0
     cohesive: bool = False
     coh_law: int = COH_OP
-    coh_params: Tuple[float, float, float, float] = (0.0, 0.0, 0.0, 0.0)
+    coh_params: Tuple[float, ...] = (0.0, 0.0, 0.0, 0.0, 0.0)
     strain: float = 0.01
     plane_strain: bool = True
     seed: int = -1

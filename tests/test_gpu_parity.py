@@ -135,9 +135,10 @@ def test_gpu_cohesive_residual_and_state_match_reference():
     ctx.close()
 
 
-def test_gpu_bilinear_cohesive_matches_oracle():
+@pytest.mark.parametrize("eta", [0.0, 500.0])
+def test_gpu_bilinear_cohesive_matches_oracle(eta):
     rve = RVE(nx=20, ny=20, inclusions=[(0.45, 0.5, 0.27, 1)], cohesive=True, coh_law=1,
-              coh_params=(30.0, 0.01, 1.0e6, 1.0), strain=0.02)
+              coh_params=(30.0, 0.01, 1.0e6, 1.0, eta), strain=0.02)
     m = pb.Mesh(rve)
     e = m.export()
     ctx = pb.DeviceContext(m)

@@ -131,3 +131,31 @@ def test_bilinear_law_envelope():
     # compression: penalty
     t, D, _ = oracle.cohesive_law(1, p, 0.02, 0.0, np.array([0.0, -1e-6]))
     assert abs(t[1] + Kp * 1e-6) <= 1e-9
+
+
+def test_bilinear_law_viscous_regularisation():
+    """eta adds eta (delta_eff - delta_max) / dt to the loading traction and
+    eta / dt to its slope; the tangent stays the derivative of the traction."""
+    sc, Gc, Kp, eta, dt = 30.0, 0.01, 1.0e6, 500.0, 0.02
+    d0 = sc / Kp
+    dmax = 0.8 * d0
+    delta = np.array([0.0, 2.0 * d0])
+    t0, _, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, 0.0), dt, dmax, delta)
+    t1, D1, dm = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, eta), dt, dmax, delta)
+    assert abs((t1[1] - t0[1]) - eta * (2.0 * d0 - dmax) / dt) <= 1e-9 * sc
+    assert dm == 2.0 * d0
+    # unloading is rate independent
+    tu0, _, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, 0.0), dt, 3.0 * d0, delta)
+    tu1, _, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, eta), dt, 3.0 * d0, delta)
+    assert np.array_equal(tu0, tu1)
+    # mixed-mode loading: central differences of the traction
+    delta = np.array([1.0e-5, 5.0e-5])
+    _, D, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, eta), dt, 2.0e-5, delta)
+    h = 1e-12
+    for k in range(2):
+        dp, dm_ = delta.copy(), delta.copy()
+        dp[k] += h
+        dm_[k] -= h
+        tp, _, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, eta), dt, 2.0e-5, dp)
+        tm, _, _ = oracle.cohesive_law(1, (sc, Gc, Kp, 1.0, eta), dt, 2.0e-5, dm_)
+        np.testing.assert_allclose((tp - tm) / (2 * h), D[:, k], rtol=1e-5, atol=1e-3 * np.abs(D).max())

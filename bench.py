@@ -39,6 +39,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-load-step", action="store_true")
+    ap.add_argument("--no-cohesive", action="store_true")
+    ap.add_argument("--viscosity", type=float, default=200.0,
+                    help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
     return ap.parse_args()
 
 
@@ -307,6 +310,14 @@ def run_b200_arm(args):
                           "krylov_iterations": st.iterations, "refinements": st.refinements,
                           "rel_residual": st.rel_residual}
 
+    # ---- cohesive load step: plain FP64 vs mixed + learned ----
+    coh = None
+    if not args.no_cohesive and not args.no_load_step:
+        try:
+            coh = cohesive_load_steps(local, args.viscosity)
+        except Exception as ex:  # reported, never fatal for the assembly line
+            coh = {"status": f"failed: {ex}"}
+
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -336,6 +347,7 @@ def run_b200_arm(args):
             "gpu_launches": launches_per_pass(mesh) * args.steps,
             "clocks": clocks,
             "load_step": load,
+            "cohesive_load_step": coh,
             "kernel_ms": {"rows_median": statistics.median(rows_ms), "cut_median": statistics.median(cut_ms)},
         }
         print(json.dumps(line), flush=True)
@@ -344,6 +356,102 @@ def run_b200_arm(args):
         dist.barrier()
         dist.destroy_process_group()
 
+
+
+def cohesive_load_steps(local: int, eta: float, n_train: int = 4, train_steps: int = 25, t_window=(0.4, 0.6)):
+    """Time per cohesive load step at 1e-8 relative Newton residual on the
+    256x256 RVE (131,072 TRI3, 40 seeded circles r ~ U[0.03, 0.06], bilinear
+    cohesive interfaces, 2% strain in 50 equal steps).  Every arm must reach
+    the same target: 1e-8 times the residual of the zeroth-order predictor
+    (the reference's), step by step.
+      plain:          FP64 multigrid-preconditioned Newton-Krylov, zeroth-order predictor
+      mixed_learned:  FP32 V-cycle inside the FP64 Krylov solve, learned predictor
+    The learned predictor is trained here, by this library's own kernels, on
+    the first `train_steps` steps of `n_train` other seeded RVEs of the same
+    kind.  The plain method first carries the RVE (untimed) to the load
+    fraction t_window[0]; every arm then starts from that state and steps
+    to t_window[1], timed by the device clock of each step."""
+    import ctypes as C
+    import dataclasses
+
+    import numpy as np
+    import torch
+
+    import pigfem_assignment_b200.problem as pb
+    from pigfem_assignment_b200 import _lib
+    from pigfem_assignment_b200.learned import MLP, trajectory_samples
+    from pigfem_assignment_b200.rve import config2
+
+    def with_eta(rve):
+        return dataclasses.replace(rve, coh_params=tuple(rve.coh_params[:4]) + (eta,))
+
+    newton = dict(precond=_lib.PG_PREC_MG, stol=0.0, rtol_base=_lib.PG_RTOL_BASE_ZEROTH)
+    t0 = time.perf_counter()
+    # training trajectories use the reference's SNES tests (rtol of the predictor, stol)
+    xs, ts = [], []
+    for k in range(n_train):
+        x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.2, seed=k,
+                                     device=local, newton=dict(precond=_lib.PG_PREC_MG))
+        xs.append(x)
+        ts.append(t)
+    X = np.concatenate(xs)
+    T = np.concatenate(ts)
+    perm = np.random.default_rng(0).permutation(len(X))
+    dev = f"cuda:{local}"
+    mlp = MLP(device=local, seed=1)
+    hist = mlp.train(torch.from_numpy(X[perm]).to(dev), torch.from_numpy(T[perm]).to(dev), epochs=40, batch=8192,
+                     lr=2e-3)
+    train_s = time.perf_counter() - t0
+
+    rve = with_eta(config2())
+    prob = pb.ProblemNonlinearStructural(rve, device=local)
+    prob.init()
+    # untimed: the plain method carries the RVE to the start of the window
+    prob.configure(n_steps=50, T_final=1.0, t_start=0.0, t_stop=t_window[0], predictor=_lib.PG_PREDICT_LINEAR,
+                   **newton)
+    prob.solve_problem()
+    U0 = prob.get_solution()
+    isv0 = prob.ctx.isv(committed=True)
+    arms = (("plain_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREDICT_ZEROTH),
+            ("mixed_learned", _lib.PG_PRECISION_MIXED, _lib.PG_PREDICT_LEARNED),
+            ("mixed_linear", _lib.PG_PRECISION_MIXED, _lib.PG_PREDICT_LINEAR))
+    out = {}
+    n_nominal = int(round((t_window[1] - t_window[0]) * 50))
+    for name, prec, pred in arms:
+        prob.ctx.set_vector(0, U0)
+        prob.ctx.set_isv(isv0, committed=True)
+        prob.configure(n_steps=50, T_final=1.0, t_start=t_window[0], t_stop=t_window[1], precision=prec,
+                       predictor=pred, **newton)
+        if pred == _lib.PG_PREDICT_LEARNED:
+            _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, mlp.handle))
+        recs = (_lib.StepStats * 4096)()
+        n = C.c_int32()
+        rc = _lib.lib.pg_solve_nonlinear(prob.ctx.handle, C.byref(prob.cfg), recs, 4096, C.byref(n))
+        R = recs[:min(n.value, 4096)]
+        dev_s = float(sum(r.seconds for r in R))
+        out[name] = {
+            "status": "ok" if rc == 0 else _lib.lib.pg_last_error().decode(),
+            "nominal_steps": n_nominal, "steps_taken": len(R), "t_reached": R[-1].t_frac if R else 0.0,
+            "ms_per_load_step": 1e3 * dev_s / n_nominal,
+            "newton_iterations": int(sum(r.newton_its for r in R)),
+            "krylov_iterations": int(sum(r.krylov_its for r in R)),
+            "repeated_steps": int(sum(1 for r in R if r.repeats > 1)),
+            "learned_used": int(sum(1 for r in R if r.predictor_used == _lib.PG_PREDICT_LEARNED)),
+            "max_final_res_over_base": float(max((r.res / r.res_base) for r in R if r.res_base > 0)) if R else None,
+        }
+        if pred == _lib.PG_PREDICT_LEARNED:
+            _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, None))
+    prob.ctx.close()
+    mlp.close()
+    out["config"] = ("config2: 256x256 TRI3 (131,072 elements), 40 RSA circles r~U[0.03,0.06] gap>=0.01 seed 2, "
+                     f"bilinear law sigma_c 30 MPa, G_c 0.01 N/mm, K_p 1e6 MPa/mm, viscosity {eta} MPa s/mm, "
+                     f"2% strain in 50 steps, timed window of load fractions {t_window[0]}-{t_window[1]}; "
+                     "Newton rtol 1e-8 of the zeroth-order residual")
+    out["training"] = {"rves": n_train, "steps_each": train_steps, "samples": int(len(X)), "seconds": train_s,
+                       "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
+    if out["plain_fp64"]["status"] == "ok" and out["mixed_learned"]["status"] == "ok":
+        out["speedup_mixed_learned"] = out["plain_fp64"]["ms_per_load_step"] / out["mixed_learned"]["ms_per_load_step"]
+    return out
 
 def main():
     args = parse()

@@ -196,6 +196,8 @@ typedef struct pg_newton_cfg {
     int32_t max_repeat;             /* load-step repeats with dt *= 0.25 (reference: 20) */
     int32_t predictor;              /* PG_PREDICT_* */
     int32_t rtol_base;              /* PG_RTOL_BASE_*: which residual rtol is relative to */
+    double t_start, t_stop;         /* pg_solve_nonlinear steps the load fraction from t_start (the current U and
+                                       committed state are converged there) to t_stop; defaults 0 and 1 */
 } pg_newton_cfg;
 /* rtol relative to the residual of the step's own predictor (SNES, the reference) */
 #define PG_RTOL_BASE_PREDICTOR 0

@@ -79,12 +79,40 @@ void upload_tables() {
 // ---------------------------------------------------------------------------
 // Uncut triangles: gather assembly, one thread per 2x2 block of K
 // ---------------------------------------------------------------------------
-constexpr int kTileNodes = 64;            // node rows per CTA
+constexpr int kTileNodes = kTriTileNodes;     // node rows per CTA
 constexpr int kTileThreads = 128;
-constexpr int kTileEntries = 512;         // staged (node, triangle) entries: 64 nodes x valence <= 8
+constexpr int kTileEntries = kTriTileEntries; // staged (node, triangle) entries: 64 nodes x valence <= 8
 constexpr int kEntriesPerThread = kTileEntries / kTileThreads;
-constexpr int kTileBlocks = 1024;         // staged column indices of the slice
-constexpr int kTileMats = 32;             // staged material table
+constexpr int kTileMats = 32;                 // staged material table
+
+void build_tri_map(const HostMesh& hm, std::vector<int>& map) {
+    const int n = hm.n_nodes();
+    map.assign((size_t)hm.n_blocks(), 0);
+    for (int i = 0; i < n; ++i) {
+        const int base = hm.ne_ptr[(i / kTileNodes) * kTileNodes];
+        for (int q = hm.row_ptr[i]; q < hm.row_ptr[i + 1]; ++q) {
+            const int j = hm.col[q];
+            if (j == i) {
+                map[q] = kTriMapDiag;
+                continue;
+            }
+            int cnt = 0, word = 0;
+            bool slow = false;
+            for (int k = hm.ne_ptr[i]; k < hm.ne_ptr[i + 1]; ++k) {
+                const int e = hm.ne_list[k] >> 2;
+                int t = -1;
+                for (int v = 0; v < 3; ++v)
+                    if (hm.conn[3 * e + v] == j) t = v;
+                if (t < 0) continue;
+                const int rel = k - base;
+                if (cnt >= 2 || rel >= kTileEntries) slow = true;
+                else word |= (rel | (t << 10)) << (12 * cnt);
+                ++cnt;
+            }
+            map[q] = slow ? kTriMapSlow : (word | (cnt << 24));
+        }
+    }
+}
 
 struct RowArgs {
     int n_nodes;
@@ -93,6 +121,8 @@ struct RowArgs {
     const int* __restrict__ col;
     const int* __restrict__ ne_ptr;
     const int* __restrict__ ne_list;
+    const int* __restrict__ tri_map;
+    const int* __restrict__ diag;
     const int4* __restrict__ elem4;
     const double* __restrict__ x;
     const double* __restrict__ y;
@@ -193,7 +223,6 @@ template <bool WANT_F>
 __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
     __shared__ double sG[kTileEntries][7];   // b0, b1, b2, c0, c1, c2, 1/(2J)
     __shared__ int4 sN[kTileEntries];        // n0, n1, n2, material | (entry's own vertex << 16)
-    __shared__ int scol[kTileBlocks];
     __shared__ double sD[3 * kTileMats];
     __shared__ int srp[kTileNodes + 1];
     __shared__ int sne[kTileNodes + 1];
@@ -207,7 +236,6 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
     const int k0 = __ldg(&a.ne_ptr[node0]);
     const int nent = __ldg(&a.ne_ptr[node_end]) - k0;
     const bool staged = nent <= kTileEntries;
-    const bool cols_staged = nseg <= kTileBlocks;
     const bool mats_staged = a.n_mat <= kTileMats;
     for (int i = threadIdx.x; i <= nn; i += kTileThreads) {
         srp[i] = __ldg(&a.row_ptr[node0 + i]) - seg0;
@@ -215,8 +243,6 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
     }
     if (mats_staged)
         for (int i = threadIdx.x; i < 3 * a.n_mat; i += kTileThreads) sD[i] = __ldg(&a.dmat[i]);
-    if (cols_staged)
-        for (int i = threadIdx.x; i < nseg; i += kTileThreads) scol[i] = __ldg(&a.col[seg0 + i]);
     if (staged) {
         int packed[kEntriesPerThread];
         int4 el[kEntriesPerThread];
@@ -262,29 +288,28 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
     }
     __syncthreads();
     for (int sidx = threadIdx.x; sidx < nseg; sidx += kTileThreads) {
-        // row of this block: the largest li with srp[li] <= sidx
-        int lo = 0, hi = nn - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (srp[mid] <= sidx) lo = mid; else hi = mid - 1;
-        }
-        const int j = cols_staged ? scol[sidx] : __ldg(&a.col[seg0 + sidx]);
-        if (j == node0 + lo && staged) continue;  // diagonal blocks: below
+        const int w = __ldg(&a.tri_map[seg0 + sidx]);
+        if (staged && (w & kTriMapDiag)) continue;  // diagonal blocks: below
         double k[4] = {0.0, 0.0, 0.0, 0.0};
-        if (staged) {
-            // the triangles of row i that contain j: an edge has at most two
-            int m0 = -1, t0 = 0, m1 = -1, t1 = 0;
-            for (int kk = sne[lo]; kk < sne[lo + 1]; ++kk) {
-                const int4 el = sN[kk];
-                const int t = el.x == j ? 0 : el.y == j ? 1 : el.z == j ? 2 : -1;
-                if (t < 0) continue;
-                if (m0 < 0) { m0 = kk; t0 = t; }
-                else if (m1 < 0) { m1 = kk; t1 = t; }
-                else cst_staged_add(sG[kk], sN[kk].w, t, mats_staged ? sD : a.dmat, k);
+        if (staged && !(w & kTriMapSlow)) {
+            // the (at most two) staged triangles joining the block's two nodes
+            const int cnt = (w >> 24) & 3;
+            if (cnt > 0) {
+                const int e0 = w & 1023;
+                cst_staged_add(sG[e0], sN[e0].w, (w >> 10) & 3, mats_staged ? sD : a.dmat, k);
             }
-            if (m0 >= 0) cst_staged_add(sG[m0], sN[m0].w, t0, mats_staged ? sD : a.dmat, k);
-            if (m1 >= 0) cst_staged_add(sG[m1], sN[m1].w, t1, mats_staged ? sD : a.dmat, k);
+            if (cnt > 1) {
+                const int e1 = (w >> 12) & 1023;
+                cst_staged_add(sG[e1], sN[e1].w, (w >> 22) & 3, mats_staged ? sD : a.dmat, k);
+            }
         } else {
+            // row of this block: the largest li with srp[li] <= sidx
+            int lo = 0, hi = nn - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (srp[mid] <= sidx) lo = mid; else hi = mid - 1;
+            }
+            const int j = __ldg(&a.col[seg0 + sidx]);
             for (int kk = k0 + sne[lo]; kk < k0 + sne[lo + 1]; ++kk) cst_block_add(a, __ldg(&a.ne_list[kk]), j, k);
         }
         if (a.want_K) {
@@ -300,15 +325,9 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
             for (int kk = sne[li]; kk < sne[li + 1]; ++kk)
                 cst_staged_add(sG[kk], sN[kk].w, sN[kk].w >> 16, mats_staged ? sD : a.dmat, k);
             if (a.want_K) {
-                // the diagonal block's slot in the row
-                int q = srp[li];
-                const int i = node0 + li;
-                while (q < srp[li + 1] && (cols_staged ? scol[q] : __ldg(&a.col[seg0 + q])) != i) ++q;
-                if (q < srp[li + 1]) {
-                    double2* dst = reinterpret_cast<double2*>(a.K + 4 * ((size_t)seg0 + q));
-                    dst[0] = make_double2(k[0], k[1]);
-                    dst[1] = make_double2(k[2], k[3]);
-                }
+                double2* dst = reinterpret_cast<double2*>(a.K + 4 * (size_t)__ldg(&a.diag[node0 + li]));
+                dst[0] = make_double2(k[0], k[1]);
+                dst[1] = make_double2(k[2], k[3]);
             }
         }
     }
@@ -714,6 +733,8 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.col = c.col;
     ra.ne_ptr = c.ne_ptr;
     ra.ne_list = c.ne_list;
+    ra.tri_map = c.tri_map;
+    ra.diag = c.diag;
     ra.elem4 = c.elem4;
     ra.x = c.x;
     ra.y = c.y;

@@ -36,7 +36,7 @@ int dev_alloc(T** dst, size_t n) {
 
 void free_ctx(Ctx& c) {
     mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.dmat, c.cut_elem, c.cut_tmpl,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map, c.dmat, c.cut_elem, c.cut_tmpl,
                     c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_order, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
@@ -111,6 +111,11 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     if ((rc = dev_upload(&c.diag, hm.diag_slot))) return rc;
     if ((rc = dev_upload(&c.ne_ptr, hm.ne_ptr))) return rc;
     if ((rc = dev_upload(&c.ne_list, hm.ne_list))) return rc;
+    {
+        std::vector<int> tm;
+        build_tri_map(hm, tm);
+        if ((rc = dev_upload(&c.tri_map, tm))) return rc;
+    }
     std::vector<double> dm(3 * hm.spec.materials.size());
     for (size_t m = 0; m < hm.spec.materials.size(); ++m) dmat_coeffs(hm.spec.materials[m], hm.spec.plane_strain, &dm[3 * m]);
     if ((rc = dev_upload(&c.dmat, dm))) return rc;

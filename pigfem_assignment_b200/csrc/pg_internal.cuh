@@ -46,6 +46,19 @@ struct DevChildQuad {
 
 struct MgHierarchy;
 
+// Uncut-triangle assembly tiling (k_assemble_tri) and the per-block map that
+// tells each 2x2 block which staged (node, triangle) entries of its CTA
+// contribute to it.  Map word of a block: bits 0-9 entry e0 and bits 10-11
+// its vertex t0 that is the block's column node, bits 12-21 / 22-23 the
+// second entry, bits 24-25 the count (0-2); kTriMapDiag marks the diagonal
+// block, kTriMapSlow a block whose entries do not fit the word (evaluated
+// from global memory).  Entries are numbered from the CTA's first entry.
+constexpr int kTriTileNodes = 64;
+constexpr int kTriTileEntries = 512;
+constexpr int kTriMapDiag = 1 << 28;
+constexpr int kTriMapSlow = 1 << 29;
+void build_tri_map(const HostMesh& hm, std::vector<int>& map);
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -61,6 +74,7 @@ struct Ctx {
     int* diag = nullptr;
     int* ne_ptr = nullptr;
     int* ne_list = nullptr;
+    int* tri_map = nullptr;            // one word per block (see kTriMapDiag)
     double* dmat = nullptr;            // 3 per material: D11, D12, D33
     // cut elements
     int* cut_elem = nullptr;

@@ -146,6 +146,8 @@ void pg_newton_cfg_default(pg_newton_cfg* cfg) {
     cfg->max_repeat = 20;
     cfg->predictor = PG_PREDICT_ZEROTH;
     cfg->rtol_base = PG_RTOL_BASE_PREDICTOR;
+    cfg->t_start = 0.0;
+    cfg->t_stop = 1.0;
 }
 
 int pg_newton_load_step(pg_ctx* cx, double t_frac, double dt, const pg_newton_cfg* cfg_in, pg_step_stats* stats) {
@@ -173,15 +175,20 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
     if (cfg_in) cfg = *cfg_in;
     else pg_newton_cfg_default(&cfg);
     if (cfg.n_steps <= 0 || cfg.T_final <= 0) { set_error("pg_solve_nonlinear: bad step count / T_final"); return PG_ERR_ARG; }
+    if (!(cfg.t_start >= 0.0 && cfg.t_start < cfg.t_stop && cfg.t_stop <= 1.0)) {
+        set_error("pg_solve_nonlinear: need 0 <= t_start < t_stop <= 1");
+        return PG_ERR_ARG;
+    }
     cudaStream_t s = c.stream;
     const int nd = c.n_dof;
     const double dt_nom = cfg.T_final / cfg.n_steps;
-    double t = 0.0, dt = dt_nom, dt_prev = dt_nom;
+    const double t_end = cfg.t_stop * cfg.T_final;
+    double t = cfg.t_start * cfg.T_final, dt = std::min(dt_nom, t_end - t), dt_prev = dt_nom;
     int nrec = 0;
     // the previous converged state for predictors / repeats
     cudaMemcpyAsync(c.Uprev, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(c.Uold, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    while (t < cfg.T_final - 1e-12 * cfg.T_final) {
+    while (t < t_end - 1e-12 * cfg.T_final) {
         int repeat = 0;
         bool converged = false;
         pg_step_stats st{};
@@ -250,7 +257,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
         dt_prev = dt;
         if (repeat == 1) dt *= 1.5;
         dt = std::min(dt, dt_nom);
-        if (dt > cfg.T_final - t) dt = cfg.T_final - t;
+        if (dt > t_end - t) dt = t_end - t;
     }
     PG_CUDA(cudaStreamSynchronize(s));
     if (n_records) *n_records = nrec;

@@ -81,15 +81,17 @@ def _dev_ptrs(ctx):
 
 
 def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction: float = 0.1, seed: int = 0,
-                       device: int = 0, rtol: float = 1e-8) -> Tuple["object", "object", List[_lib.StepStats]]:
+                       device: int = 0, rtol: float = 1e-8, newton: dict = None
+                       ) -> Tuple["object", "object", List[_lib.StepStats]]:
     """Runs the first `n_train_steps` of `n_steps` equal load steps of `rve`
     with the linear predictor and returns (features, targets) of the nodes kept
     (every enrichment node, every node with cohesive damage, a random
-    `keep_fraction` of the others), plus the step records."""
+    `keep_fraction` of the others), plus the step records.  `newton` holds
+    further pg_newton_cfg fields (e.g. the preconditioner)."""
     torch = _torch()
     prob = ProblemNonlinearStructural(rve, device=device)
     prob.init()
-    prob.configure(rtol=rtol, n_steps=n_steps)
+    prob.configure(rtol=rtol, n_steps=n_steps, **(newton or {}))
     ctx = prob.ctx
     n_nodes = prob.mesh.info["n_nodes"]
     n_reg = prob.mesh.info["n_regular_nodes"]

@@ -266,6 +266,28 @@ int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
  * switch timing on/off. */
 int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
+/* ---- batches of independent linear-elastic RVEs ----
+ * No counterpart in the reference, which solves one RVE per run
+ * (Problem::solve_problem, src/Problem.cpp:400-418).  A batch is the
+ * block-diagonal union of n_rve meshes (built by pg_mesh_build, any sizes):
+ * one launch of each assembly kernel covers all of them (assemble through
+ * pg_batch_context + pg_assemble_linear), and pg_batch_solve runs CG with
+ * per-RVE step lengths and per-RVE stopping (rtol relative to each RVE's own
+ * right-hand side), preconditioned by block Jacobi or by one V-cycle over the
+ * union of the RVEs' multigrid hierarchies (PG_PREC_MG; FP32 cycle under
+ * PG_PRECISION_MIXED).  The CG iterations run as CUDA graphs. */
+typedef struct pg_batch pg_batch;
+int pg_batch_create(const pg_mesh* const* meshes, int32_t n_rve, int32_t device, pg_batch** out);
+void pg_batch_destroy(pg_batch* b);
+/* the merged system as a context: assembly, timing and host copies work on it */
+pg_ctx* pg_batch_context(pg_batch* b);
+/* first node / element of each RVE in the merged system (n_rve + 1 entries each), multigrid depth per RVE */
+int pg_batch_info(const pg_batch* b, int32_t* node_offset, int32_t* element_offset, int32_t* depth);
+/* solves every RVE (prescribed values at load factor 1); per_rve: n_rve records or NULL; total: worst of all */
+int pg_batch_solve(pg_batch* b, const pg_solver_cfg* cfg, pg_solve_stats* per_rve, pg_solve_stats* total);
+/* the RVE's displacements in its own mesh's DOF order (2 * its node count) */
+int pg_batch_get_solution(pg_batch* b, int32_t rve, double* U_host);
+
 /* ---- solve without device allocation ----
  * No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory (a host framework that owns every device buffer

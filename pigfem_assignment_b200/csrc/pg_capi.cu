@@ -34,22 +34,6 @@ int dev_alloc(T** dst, size_t n) {
     return PG_OK;
 }
 
-void free_ctx(Ctx& c) {
-    mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map, c.dmat, c.cut_elem, c.cut_tmpl,
-                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_order, c.K, c.Kf, c.fixed, c.ubar,
-                    c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
-                    c.minvf, c.scal, c.iflags};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    if (c.h_scal) cudaFreeHost(c.h_scal);
-    if (c.h_iflags) cudaFreeHost(c.h_iflags);
-    if (c.ev0) cudaEventDestroy(c.ev0);
-    if (c.ev1) cudaEventDestroy(c.ev1);
-    for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2})
-        if (e) cudaEventDestroy(e);
-    if (c.stream) cudaStreamDestroy(c.stream);
-}
 
 // D = E/((1+nu)(1-2nu)) [[1-nu, nu, 0], [nu, 1-nu, 0], [0, 0, (1-2nu)/2]]
 // (material_lei.cpp:62-77; plane stress :78-84)
@@ -70,6 +54,23 @@ void dmat_coeffs(const Material& m, bool plane_strain, double out[3]) {
 cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 
 }  // namespace
+
+void free_ctx(Ctx& c) {
+    mg_free(c);
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map, c.dmat, c.cut_elem, c.cut_tmpl,
+                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_order, c.K, c.Kf, c.fixed, c.ubar,
+                    c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
+                    c.minvf, c.scal, c.iflags};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.h_scal) cudaFreeHost(c.h_scal);
+    if (c.h_iflags) cudaFreeHost(c.h_iflags);
+    if (c.ev0) cudaEventDestroy(c.ev0);
+    if (c.ev1) cudaEventDestroy(c.ev1);
+    for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2})
+        if (e) cudaEventDestroy(e);
+    if (c.stream) cudaStreamDestroy(c.stream);
+}
 
 void set_error(const std::string& s) { g_last_error = s; }
 

@@ -140,6 +140,9 @@ struct Ctx {
 
 // error plumbing
 void set_error(const std::string& s);
+// device context of a host mesh (pg_capi.cu)
+int ctx_create(const HostMesh& hm, int device, Ctx& c);
+void free_ctx(Ctx& c);
 int cuda_fail(cudaError_t e, const char* where);
 
 // assembly entry points (pg_assemble.cu)

@@ -74,7 +74,10 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
         launch_assemble(c, c.U, dt, false, true, s);
         // solve K d = -res (forcing term: tighter as Newton converges)
         k_scale_copy<<<nblk(nd), kThreads, 0, s>>>(nd, c.res, c.b, -1.0);
+        // never tighter than what lands this iteration on the Newton target:
+        // ||r_next|| ~ eta ||r|| once the quadratic term is small
         lin.rtol = std::max(cfg.lin_rtol, std::min(1e-2, 1e-3 * rnorm / r0));
+        lin.rtol = std::max(lin.rtol, std::min(1e-2, 0.5 * cfg.rtol * rb / rnorm));
         lin.krylov = PG_KRYLOV_CG;
         pg_solve_stats ls{};
         int rc = krylov_solve(c, lin, ls, s);
@@ -224,11 +227,26 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                 if (rc) return rc;
                 rc = pg_mlp_forward(c.mlp, c.featX, c.n_nodes, c.featY, s);
                 if (rc) return rc;
-                launch_apply(c, c.Uprev, c.Uold, ratio, s_inc, c.featY, c.U, s);
-                k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
-                res_mlp = std::sqrt(predictor_residual(c, c.U, dt, s));
-                used = PG_PREDICT_LEARNED;
-                if (!(res_mlp <= res_lin)) {
+                // the network's correction at full, half and quarter length:
+                // the candidate (linear included) with the smallest residual starts Newton
+                double best = res_lin, best_a = 0.0;
+                for (double a : {1.0, 0.5, 0.25}) {
+                    launch_apply(c, c.Uprev, c.Uold, ratio, a * s_inc, c.featY, c.U, s);
+                    k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
+                    const double ra = std::sqrt(predictor_residual(c, c.U, dt, s));
+                    if (a == 1.0) res_mlp = ra;
+                    if (ra < best) {
+                        best = ra;
+                        best_a = a;
+                    }
+                }
+                if (best_a > 0.0) {
+                    used = PG_PREDICT_LEARNED;
+                    if (best_a != 0.25) {
+                        launch_apply(c, c.Uprev, c.Uold, ratio, best_a * s_inc, c.featY, c.U, s);
+                        k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
+                    }
+                } else {
                     cudaMemcpyAsync(c.U, c.Ut, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
                     used = PG_PREDICT_LINEAR;
                 }

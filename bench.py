@@ -109,6 +109,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes (read + write) of one launch of `kernel` on this workload,
+    from the committed ncu capture summarised under profiles/ (None if absent)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)[kernel]["dram_bytes_per_launch"]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def launches_per_pass(mesh) -> int:
     """Kernels one linear assembly launches: the uncut-triangle kernel plus one
     cut-element kernel per non-empty size class (local node count <= 5, 7, 11, 15)."""
@@ -231,6 +241,16 @@ def run_b200_arm(args):
         _lib.check(_lib.lib.pg_assembly_timing(ctx.handle, 1, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    # pick the assembly launch shapes on this mesh (pg_ctx_autotune), untimed
+    ms_tri = (C.c_float * 4)()
+    ms_cut = (C.c_float * 3)()
+    _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
+    t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
+    _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
+    tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
+              "ms_tri_tile32_tile32p_tile64_tile64p": [round(v, 4) for v in ms_tri],
+              "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
+
     for _ in range(args.warmup):
         flush.fill_(1.0)
         torch.cuda.synchronize()
@@ -347,7 +367,8 @@ def run_b200_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(rve, info),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_assemble_tri",
+                         "frac": achieved / peak, "traffic": profiled_traffic("k_assemble_tri"),
+                         "kernel": "k_assemble_tri",
                          "peak_kind": peak_kind, "bytes_per_launch": rows_bytes, "kernel_share": share,
                          "pass_bytes": pass_bytes,
                          "pass_achieved": pass_bytes / (statistics.mean(step_ms) / 1e3) / 1e9},
@@ -359,6 +380,7 @@ def run_b200_arm(args):
             "load_step": load,
             "cohesive_load_step": coh,
             "batched": batch,
+            "autotune": tuning,
             "kernel_ms": {"rows_median": statistics.median(rows_ms), "cut_median": statistics.median(cut_ms)},
         }
         print(json.dumps(line), flush=True)

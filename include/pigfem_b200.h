@@ -266,6 +266,30 @@ int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
  * switch timing on/off. */
 int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
+/* ---- shape sensitivity ----
+ * SensitivityAdjoint::solveProblem with SensitivityRightLoad (src/SensitivityAdjoint.cpp:23-63,
+ * src/SensitivityRightLoad.cpp:32-125) and the shape-parameter kernels
+ * (src/SensitivityShapeParameterStructural.cpp:18-230) for the radius of every circle.
+ * At the context's current equilibrium U (solve first): C_11 = (sum of the right
+ * edge's x reactions / height) / applied strain, and dC_11/dr_i for every
+ * inclusion from one adjoint solve (cfg: CG/GMRES, any preconditioner) and a
+ * central difference of each cut element's internal force under the move of its
+ * enrichment nodes (h = h_rel * r_i).  dc11_dr: n_inclusions values (NULL allowed). */
+int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double* c11, double* dc11_dr,
+                       pg_solve_stats* adjoint_stats);
+
+/* ---- autotuning of the assembly launch shapes ----
+ * No counterpart in the reference.  Times every launch shape of the two
+ * assembly kernels on this context's mesh (L2 flushed before each launch,
+ * `reps` launches each) and keeps the fastest of each for later assemblies:
+ * ms_tri[4] = triangle kernel with 32 / 64 node rows per CTA, each with one CTA
+ * per tile / a persistent grid; ms_cut[3] = cut-element kernel with 2 / 4 / 8
+ * elements per CTA (NULL allowed).  K is left to be reassembled. */
+int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
+/* the launch shapes in use, and setting them by hand (tile 32 or 64, persistent 0/1, warps 2/4/8) */
+int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
+int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
+
 /* ---- batches of independent linear-elastic RVEs ----
  * No counterpart in the reference, which solves one RVE per run
  * (Problem::solve_problem, src/Problem.cpp:400-418).  A batch is the

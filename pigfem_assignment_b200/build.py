@@ -15,7 +15,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpigfem_b200.so")
 
-SOURCES = ["igfem_host.cpp", "pg_assemble.cu", "pg_solve.cu", "pg_newton.cu", "pg_mlp.cu", "pg_predict.cu", "pg_capi.cu", "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu"]
+SOURCES = ["igfem_host.cpp", "pg_assemble.cu", "pg_solve.cu", "pg_newton.cu", "pg_mlp.cu", "pg_predict.cu", "pg_capi.cu", "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu", "pg_sens.cu"]
 HEADERS = ["igfem_host.h", "pg_internal.cuh", "pg_solve_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -24,6 +24,7 @@
 //     atomics (a few percent of elements).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -79,13 +80,10 @@ void upload_tables() {
 // ---------------------------------------------------------------------------
 // Uncut triangles: gather assembly, one thread per 2x2 block of K
 // ---------------------------------------------------------------------------
-constexpr int kTileNodes = kTriTileNodes;     // node rows per CTA
-constexpr int kTileThreads = 128;
-constexpr int kTileEntries = kTriTileEntries; // staged (node, triangle) entries: 64 nodes x valence <= 8
-constexpr int kEntriesPerThread = kTileEntries / kTileThreads;
 constexpr int kTileMats = 32;                 // staged material table
 
-void build_tri_map(const HostMesh& hm, std::vector<int>& map) {
+void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map) {
+    const int kTileNodes = tile_nodes, kTileEntries = 8 * tile_nodes;
     const int n = hm.n_nodes();
     map.assign((size_t)hm.n_blocks(), 0);
     for (int i = 0; i < n; ++i) {
@@ -219,14 +217,18 @@ __device__ __forceinline__ void cst_staged_add(const double* g, int w, int t, co
 // A slice with more entries than the staging buffer (never for structured
 // meshes, whose valence is at most 8) evaluates the blocks straight from
 // global memory instead.
-template <bool WANT_F>
-__global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
+template <bool WANT_F, int TN>
+__global__ void __launch_bounds__(2 * TN, 320 / TN) k_assemble_tri(RowArgs a, int n_tiles) {
+    constexpr int kTileNodes = TN, kTileThreads = 2 * TN, kTileEntries = 8 * TN;
+    constexpr int kEntriesPerThread = kTileEntries / kTileThreads;
     __shared__ double sG[kTileEntries][7];   // b0, b1, b2, c0, c1, c2, 1/(2J)
     __shared__ int4 sN[kTileEntries];        // n0, n1, n2, material | (entry's own vertex << 16)
     __shared__ double sD[3 * kTileMats];
     __shared__ int srp[kTileNodes + 1];
     __shared__ int sne[kTileNodes + 1];
-    const int node0 = blockIdx.x * kTileNodes;
+    // a grid smaller than the tile count walks the tiles (persistent launch)
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int node0 = tile * kTileNodes;
     const int node_end = min(node0 + kTileNodes, a.n_nodes);
     const int nn = node_end - node0;
     // slice bounds read directly (broadcast loads), so that the entry and
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
             }
         }
     }
-    if (!WANT_F) return;
+    if (WANT_F) {
     // the cut-element kernel adds its own f_int contributions afterwards
     for (int li = threadIdx.x; li < nn; li += kTileThreads) {
         double fx = 0.0, fy = 0.0;
@@ -358,6 +360,9 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble_tri(RowArgs a) {
         }
         a.f[2 * (node0 + li)] = fx;
         a.f[2 * (node0 + li) + 1] = fy;
+    }
+    }
+    __syncthreads();  // the next tile reuses the shared buffers
     }
 }
 
@@ -450,30 +455,6 @@ __device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, doubl
 // ---------------------------------------------------------------------------
 // Cut-element kernel
 // ---------------------------------------------------------------------------
-constexpr int kCutWarps = 4;
-struct CutArgs {
-    int n_cut;                      // elements of this launch: order[0 .. n_cut)
-    const int* __restrict__ order;
-    const int* __restrict__ cut_elem;
-    const int* __restrict__ cut_tmpl;
-    const int* __restrict__ cut_enr;
-    const int* __restrict__ cut_child_mat;
-    const int* __restrict__ cut_coh_qp0;
-    const int* __restrict__ cut_slot_ptr;
-    const int* __restrict__ cut_slot;
-    const int4* __restrict__ elem4;
-    const double* __restrict__ x;
-    const double* __restrict__ y;
-    const double* __restrict__ u;
-    const double* __restrict__ dmat;
-    const double* __restrict__ isv_c;
-    double* isv_t;
-    DevCohLaw coh;
-    double dt;
-    double* K;
-    double* f;
-    int want_K, want_f;
-};
 
 // Per-warp shared tables: one row per quadrature point of the current chunk
 // holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
@@ -483,8 +464,9 @@ struct CutArgs {
 constexpr int kQpChunk = 32;
 constexpr int kCRow = 10;
 
-template <int NL, int PPL>
-__global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
+template <int NL, int PPL, int W, bool SENS = false>
+__global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / W) k_assemble_cut(CutArgs a) {
+    constexpr int kCutWarps = W;
     constexpr int kQRow = 4 + 2 * NL;
     __shared__ double sX[kCutWarps][NL], sY[kCutWarps][NL];
     __shared__ double sU[kCutWarps][2 * NL];
@@ -495,22 +477,53 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
     const int lane = threadIdx.x & 31;
     const int oi = blockIdx.x * kCutWarps + w;
     if (oi >= a.n_cut) return;
-    const int ci = a.order[oi];
-    const DevTemplate& T = c_tmpl[a.cut_tmpl[ci]];
+    const int ci = a.first + oi;  // class-ordered element index
+    const int tmpl = __ldg(&a.cut_tmpl[ci]);
+    const DevTemplate& T = c_tmpl[tmpl];
     const int nl = 3 + T.n_enr;
-    const int e = a.cut_elem[ci];
-    const int4 el = a.elem4[e];
+    // the element's block slots are needed only at the end: issue their loads now
+    const int* slots = a.cut_slot + __ldg(&a.cut_slot_ptr[ci]);
+    int slot[PPL];
+#pragma unroll
+    for (int k = 0; k < PPL; ++k)
+        slot[k] = (!SENS && a.want_K && lane + 32 * k < nl * nl) ? __ldg(&slots[lane + 32 * k]) : -1;
     if (lane < nl) {
-        const int node = lane < 3 ? (lane == 0 ? el.x : (lane == 1 ? el.y : el.z)) : a.cut_enr[ci * kMaxEnr + lane - 3];
+        const int node = __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]);
         sL[w][lane] = node;
         sX[w][lane] = a.x[node];
         sY[w][lane] = a.y[node];
-        if (a.want_f || T.n_coh > 0) {
+        if (SENS || a.want_f || T.n_coh > 0) {
             sU[w][2 * lane] = a.u[2 * node];
             sU[w][2 * lane + 1] = a.u[2 * node + 1];
         }
     }
     __syncwarp();
+    double part = 0.0;    // SENS: this lane's share of wsens . f_e
+    int sel = -1;         // SENS: the inclusion whose radius moves
+    double hstep = 0.0;
+    if (SENS) {
+        const unsigned full = 0xffffffffu;
+        const int my_inc = (lane >= 3 && lane < nl) ? a.node_inc[sL[w][lane]] : -1;
+        // the which-th distinct inclusion among the enrichment slots, in slot order
+        int count = 0;
+        for (int l = 3; l < nl; ++l) {
+            const int v = __shfl_sync(full, my_inc, l);
+            bool seen = false;
+            for (int l2 = 3; l2 < l; ++l2) seen |= __shfl_sync(full, my_inc, l2) == v;
+            if (!seen && v >= 0) {
+                if (count == a.which) sel = v;
+                ++count;
+            }
+        }
+        if (sel < 0) return;  // warp-uniform: no such inclusion in this element
+        hstep = a.h_rel * a.radius[sel];
+        if (lane < nl && my_inc == sel) {
+            const int node = sL[w][lane];
+            sX[w][lane] += a.sgn * hstep * a.vel[2 * node];
+            sY[w][lane] += a.sgn * hstep * a.vel[2 * node + 1];
+        }
+        __syncwarp();
+    }
     // parent (Tri3) gradients are constant over the element
     const double PX0 = sX[w][0], PX1 = sX[w][1], PX2 = sX[w][2];
     const double PY0 = sY[w][0], PY1 = sY[w][1], PY2 = sY[w][2];
@@ -537,7 +550,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         // geometry of one quadrature point per lane, all points in parallel
         const int l = qbase + lane;
         if (l < nq_total) {
-            const DevTemplate& TG = g_tmpl[a.cut_tmpl[ci]];
+            const DevTemplate& TG = g_tmpl[tmpl];
             int ch = 0, q = l;
             while (q >= g_quad[TG.child_type[ch]].nq) {
                 q -= g_quad[TG.child_type[ch]].nq;
@@ -605,7 +618,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         __syncwarp();
     }
     // bulk internal force f_a = sum_b K_ab u_b
-    if (a.want_f) {
+    if (SENS || a.want_f) {
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
             if (lane + 32 * k < npairs) {
@@ -613,8 +626,12 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
                 const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
                 const double fx = acc[k][0] * ux + acc[k][1] * uy;
                 const double fy = acc[k][2] * ux + acc[k][3] * uy;
-                atomicAdd(&a.f[2 * sL[w][ia]], fx);
-                atomicAdd(&a.f[2 * sL[w][ia] + 1], fy);
+                if (SENS) {
+                    part += a.wsens[2 * sL[w][ia]] * fx + a.wsens[2 * sL[w][ia] + 1] * fy;
+                } else {
+                    atomicAdd(&a.f[2 * sL[w][ia]], fx);
+                    atomicAdd(&a.f[2 * sL[w][ia] + 1], fy);
+                }
             }
         }
     }
@@ -639,7 +656,7 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         const double dmax_c = a.isv_c[qp];
         double tr[2], Dc[2][2], dmax_t;
         cohesive_law(a.coh, a.dt, dmax_c, dl, tr, Dc, dmax_t);
-        a.isv_t[qp] = dmax_t;
+        if (!SENS) a.isv_t[qp] = dmax_t;
         double* row = sC[w][lane];
         row[0] = dA * 1.0;
         row[1] = N0;
@@ -656,14 +673,19 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         row[7] = tR0;
         row[8] = tR1;
         const double wgt = row[0];
-        if (a.want_f && wgt != 0.0) {
+        if ((SENS || a.want_f) && wgt != 0.0) {
             const int cn[4] = {c0, c1, c2, c3};
             const double Nn[2] = {N0, N1};
             for (int m = 0; m < 4; ++m) {
                 const double sgn = m < 2 ? -1.0 : 1.0;
                 const int node = sL[w][cn[m]];
-                atomicAdd(&a.f[2 * node], wgt * sgn * Nn[m & 1] * tR0);
-                atomicAdd(&a.f[2 * node + 1], wgt * sgn * Nn[m & 1] * tR1);
+                if (SENS) {
+                    part += a.wsens[2 * node] * (wgt * sgn * Nn[m & 1] * tR0) +
+                            a.wsens[2 * node + 1] * (wgt * sgn * Nn[m & 1] * tR1);
+                } else {
+                    atomicAdd(&a.f[2 * node], wgt * sgn * Nn[m & 1] * tR0);
+                    atomicAdd(&a.f[2 * node + 1], wgt * sgn * Nn[m & 1] * tR1);
+                }
             }
         }
     }
@@ -697,13 +719,19 @@ __global__ void __launch_bounds__(32 * kCutWarps) k_assemble_cut(CutArgs a) {
         }
     }
 scatter:
+    if (SENS) {
+        // central difference of wsens . f_e: this pass adds sgn * (its share) / (2 h)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+        if (lane == 0) atomicAdd(&a.sens[sel], a.sgn * part / (2.0 * hstep));
+        return;
+    }
     if (a.want_K) {
-        const int* slots = a.cut_slot + a.cut_slot_ptr[ci];
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
             const int p = lane + 32 * k;
-            if (p < npairs && slots[p] >= 0) {
-                double* d = a.K + 4 * (size_t)slots[p];
+            if (p < npairs && slot[k] >= 0) {
+                double* d = a.K + 4 * (size_t)slot[k];
                 atomicAdd(d + 0, acc[k][0]);
                 atomicAdd(d + 1, acc[k][1]);
                 atomicAdd(d + 2, acc[k][2]);
@@ -722,10 +750,66 @@ __global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, s
     }
 }
 
-int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
-    if (want_K && c.n_blocks > 0) {
-        // nothing to clear: the row kernel writes every value of K
+template <int W>
+void launch_cut_w(int k, const CutArgs& ck, cudaStream_t s) {
+    // the two large classes keep at most 4 warps per CTA (48 KB of static shared memory)
+    constexpr int WL = W > 4 ? 4 : W;
+    const int cblocks = (ck.n_cut + W - 1) / W, lblocks = (ck.n_cut + WL - 1) / WL;
+    if (k == 0) k_assemble_cut<5, 1, W><<<cblocks, 32 * W, 0, s>>>(ck);
+    else if (k == 1) k_assemble_cut<7, 2, W><<<cblocks, 32 * W, 0, s>>>(ck);
+    else if (k == 2) k_assemble_cut<11, 4, WL><<<lblocks, 32 * WL, 0, s>>>(ck);
+    else k_assemble_cut<15, 8, WL><<<lblocks, 32 * WL, 0, s>>>(ck);
+}
+
+void launch_cut_class(int k, int warps, const CutArgs& ck, cudaStream_t s) {
+    if (warps == 2) launch_cut_w<2>(k, ck, s);
+    else if (warps == 8) launch_cut_w<8>(k, ck, s);
+    else launch_cut_w<4>(k, ck, s);
+}
+
+template <bool WANT_F, int TN>
+void launch_tri_tn(const Ctx& c, const RowArgs& ra, cudaStream_t s) {
+    const int n_tiles = (c.n_nodes + TN - 1) / TN;
+    if (n_tiles <= 0) return;
+    int grid = n_tiles;
+    if (c.tuning.tri_persistent) {
+        int per_sm = 0, dev = 0, n_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_tri<WANT_F, TN>, 2 * TN, 0);
+        grid = std::min(n_tiles, std::max(1, per_sm) * n_sm);
     }
+    k_assemble_tri<WANT_F, TN><<<grid, 2 * TN, 0, s>>>(ra, n_tiles);
+}
+
+void launch_tri(const Ctx& c, const RowArgs& ra, bool want_f, cudaStream_t s) {
+    const int tn = kTriTileSizes[c.tuning.tri_variant];
+    if (tn == 32) {
+        if (want_f) launch_tri_tn<true, 32>(c, ra, s);
+        else launch_tri_tn<false, 32>(c, ra, s);
+    } else {
+        if (want_f) launch_tri_tn<true, 64>(c, ra, s);
+        else launch_tri_tn<false, 64>(c, ra, s);
+    }
+}
+
+// Shape-sensitivity passes of the cut-element kernel (one per size class).
+void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+    for (int k = 0; k < kCutClasses; ++k) {
+        const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
+        if (n == 0) continue;
+        CutArgs ck = ca;
+        ck.n_cut = n;
+        ck.first = c.cut_class_off[k];
+        const int blocks = (n + 3) / 4;
+        if (k == 0) k_assemble_cut<5, 1, 4, true><<<blocks, 128, 0, s>>>(ck);
+        else if (k == 1) k_assemble_cut<7, 2, 4, true><<<blocks, 128, 0, s>>>(ck);
+        else if (k == 2) k_assemble_cut<11, 4, 4, true><<<blocks, 128, 0, s>>>(ck);
+        else k_assemble_cut<15, 8, 4, true><<<blocks, 128, 0, s>>>(ck);
+    }
+}
+
+RowArgs row_args(const Ctx& c, const double* U, bool want_f, bool want_K) {
     RowArgs ra;
     ra.n_nodes = c.n_nodes;
     ra.n_reg = c.n_reg;
@@ -733,7 +817,7 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.col = c.col;
     ra.ne_ptr = c.ne_ptr;
     ra.ne_list = c.ne_list;
-    ra.tri_map = c.tri_map;
+    ra.tri_map = c.tri_map[c.tuning.tri_variant];
     ra.diag = c.diag;
     ra.elem4 = c.elem4;
     ra.x = c.x;
@@ -745,55 +829,125 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     ra.f = c.F;
     ra.want_K = want_K;
     ra.want_f = want_f;
-    const int rblocks = (c.n_nodes + kTileNodes - 1) / kTileNodes;
-    if (c.timing) cudaEventRecord(c.ea0, s);
-    if (rblocks > 0) {
-        if (want_f)
-            k_assemble_tri<true><<<rblocks, kTileThreads, 0, s>>>(ra);
-        else
-            k_assemble_tri<false><<<rblocks, kTileThreads, 0, s>>>(ra);
+    return ra;
+}
+
+CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K) {
+    CutArgs ca;
+    ca.n_cut = c.n_cut;
+    ca.first = 0;
+    ca.cut_nodes = c.cut_nodes;
+    ca.cut_tmpl = c.cut_tmpl;
+    ca.cut_child_mat = c.cut_child_mat;
+    ca.cut_coh_qp0 = c.cut_coh_qp0;
+    ca.cut_slot_ptr = c.cut_slot_ptr;
+    ca.cut_slot = c.cut_slot;
+    ca.x = c.x;
+    ca.y = c.y;
+    ca.u = U;
+    ca.dmat = c.dmat;
+    ca.isv_c = c.isv_c;
+    ca.isv_t = c.isv_t;
+    ca.coh = c.coh;
+    ca.dt = dt;
+    ca.K = c.K;
+    ca.f = c.F;
+    ca.want_K = want_K;
+    ca.want_f = want_f;
+    return ca;
+}
+
+void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+    for (int k = 0; k < kCutClasses; ++k) {
+        const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
+        if (n == 0) continue;
+        CutArgs ck = ca;
+        ck.n_cut = n;
+        ck.first = c.cut_class_off[k];
+        launch_cut_class(k, c.tuning.cut_warps, ck, s);
     }
+}
+
+int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
+    // nothing to clear: the triangle kernel writes every value of K
+    const RowArgs ra = row_args(c, U, want_f, want_K);
+    if (c.timing) cudaEventRecord(c.ea0, s);
+    launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {
-        CutArgs ca;
-        ca.n_cut = c.n_cut;
-        ca.cut_elem = c.cut_elem;
-        ca.cut_tmpl = c.cut_tmpl;
-        ca.cut_enr = c.cut_enr;
-        ca.cut_child_mat = c.cut_child_mat;
-        ca.cut_coh_qp0 = c.cut_coh_qp0;
-        ca.cut_slot_ptr = c.cut_slot_ptr;
-        ca.cut_slot = c.cut_slot;
-        ca.elem4 = c.elem4;
-        ca.x = c.x;
-        ca.y = c.y;
-        ca.u = U;
-        ca.dmat = c.dmat;
-        ca.isv_c = c.isv_c;
-        ca.isv_t = c.isv_t;
-        ca.coh = c.coh;
-        ca.dt = dt;
-        ca.K = c.K;
-        ca.f = c.F;
-        ca.want_K = want_K;
-        ca.want_f = want_f;
-        ca.order = c.cut_order;
-        for (int k = 0; k < kCutClasses; ++k) {
-            const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
-            if (n == 0) continue;
-            CutArgs ck = ca;
-            ck.n_cut = n;
-            ck.order = c.cut_order + c.cut_class_off[k];
-            const int cblocks = (n + kCutWarps - 1) / kCutWarps;
-            if (k == 0) k_assemble_cut<5, 1><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
-            else if (k == 1) k_assemble_cut<7, 2><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
-            else if (k == 2) k_assemble_cut<11, 4><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
-            else k_assemble_cut<15, 8><<<cblocks, 32 * kCutWarps, 0, s>>>(ck);
-        }
+        launch_cut_all(c, cut_args(c, U, dt, want_f, want_K), s);
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);
+    return PG_OK;
+}
+
+// Times every launch shape of the two assembly kernels on this mesh (L2
+// flushed before each launch, `reps` launches each, device events) and keeps
+// the fastest of each kernel in c.tuning.  ms_tri: tile 32/64 x one CTA per
+// tile / persistent (4 values), ms_cut: 2/4/8 warps per CTA (3 values).  K is
+// left undefined (the cut kernel ran repeatedly): the next solve reassembles.
+int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
+    cudaStream_t s = c.stream;
+    reps = std::max(1, reps);
+    const size_t flush_bytes = 256u << 20;  // twice the L2
+    void* flush = nullptr;
+    PG_CUDA(cudaMalloc(&flush, flush_bytes));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timed = [&](auto&& launch) -> float {
+        launch();  // warm-up (first-launch costs)
+        float total = 0.f;
+        for (int r = 0; r < reps; ++r) {
+            cudaMemsetAsync(flush, r & 0xff, flush_bytes, s);
+            cudaEventRecord(e0, s);
+            launch();
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            total += ms;
+        }
+        return total / reps;
+    };
+    AsmTuning best = c.tuning;
+    float best_tri = 1e30f, best_cut = 1e30f;
+    int idx = 0;
+    for (int v = 0; v < kTriTileVariants; ++v)
+        for (int p = 0; p < 2; ++p, ++idx) {
+            c.tuning.tri_variant = v;
+            c.tuning.tri_persistent = p;
+            const RowArgs ra = row_args(c, c.U, false, true);
+            const float ms = timed([&] { launch_tri(c, ra, false, s); });
+            if (ms_tri) ms_tri[idx] = ms;
+            if (ms < best_tri) {
+                best_tri = ms;
+                best.tri_variant = v;
+                best.tri_persistent = p;
+            }
+        }
+    const int warps[3] = {2, 4, 8};
+    for (int k = 0; k < 3; ++k) {
+        c.tuning.cut_warps = warps[k];
+        float ms = 0.f;
+        if (c.n_cut > 0) {
+            const CutArgs ca = cut_args(c, c.U, 1.0, false, true);
+            ms = timed([&] { launch_cut_all(c, ca, s); });
+        }
+        if (ms_cut) ms_cut[k] = ms;
+        if (ms < best_cut) {
+            best_cut = ms;
+            best.cut_warps = warps[k];
+        }
+    }
+    c.tuning = best;
+    c.assembled = false;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(flush);
+    PG_CUDA(cudaGetLastError());
     return PG_OK;
 }
 

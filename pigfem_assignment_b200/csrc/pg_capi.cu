@@ -57,8 +57,8 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 
 void free_ctx(Ctx& c) {
     mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map, c.dmat, c.cut_elem, c.cut_tmpl,
-                    c.cut_enr, c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_order, c.K, c.Kf, c.fixed, c.ubar,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.dmat, c.cut_nodes, c.cut_tmpl,
+                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -112,32 +112,18 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     if ((rc = dev_upload(&c.diag, hm.diag_slot))) return rc;
     if ((rc = dev_upload(&c.ne_ptr, hm.ne_ptr))) return rc;
     if ((rc = dev_upload(&c.ne_list, hm.ne_list))) return rc;
-    {
+    for (int v = 0; v < kTriTileVariants; ++v) {
         std::vector<int> tm;
-        build_tri_map(hm, tm);
-        if ((rc = dev_upload(&c.tri_map, tm))) return rc;
+        build_tri_map(hm, kTriTileSizes[v], tm);
+        if ((rc = dev_upload(&c.tri_map[v], tm))) return rc;
     }
     std::vector<double> dm(3 * hm.spec.materials.size());
     for (size_t m = 0; m < hm.spec.materials.size(); ++m) dmat_coeffs(hm.spec.materials[m], hm.spec.plane_strain, &dm[3 * m]);
     if ((rc = dev_upload(&c.dmat, dm))) return rc;
     if (hm.n_cut > 0) {
-        if ((rc = dev_upload(&c.cut_elem, hm.cut_elem))) return rc;
-        if ((rc = dev_upload(&c.cut_tmpl, hm.cut_tmpl))) return rc;
-        if ((rc = dev_upload(&c.cut_enr, hm.cut_enr))) return rc;
-        if ((rc = dev_upload(&c.cut_child_mat, hm.cut_child_mat))) return rc;
-        if ((rc = dev_upload(&c.cut_coh_qp0, hm.cut_coh_qp0))) return rc;
-        // compact per-element slot tables: (3 + n_enr)^2 entries each
-        std::vector<int> sp(hm.n_cut + 1, 0), sl;
-        constexpr int S = kMaxElemNodes;
-        for (int ci = 0; ci < hm.n_cut; ++ci) {
-            const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
-            for (int a = 0; a < nl; ++a)
-                for (int b = 0; b < nl; ++b) sl.push_back(hm.cut_slot[(size_t)ci * S * S + a * S + b]);
-            sp[ci + 1] = (int)sl.size();
-        }
-        if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
-        if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
-        // cut elements grouped by size class, each class in mesh order
+        // cut elements grouped by size class (each class in mesh order); every
+        // per-element array below is stored in that order, with the element's
+        // local nodes (3 parents, then enrichment slots) as one flat list
         std::vector<int> order;
         order.reserve(hm.n_cut);
         for (int k = 0; k < kCutClasses; ++k) {
@@ -153,7 +139,28 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
             set_error("cut element with more local nodes than the largest size class");
             return PG_ERR_MESH;
         }
-        if ((rc = dev_upload(&c.cut_order, order))) return rc;
+        const int nc = hm.n_cut;
+        constexpr int S = kMaxElemNodes;
+        std::vector<int> nodes((size_t)kCutNodeStride * nc, -1), tmpl(nc), chm((size_t)kMaxChildren * nc), qp0(nc);
+        std::vector<int> sp(nc + 1, 0), sl;
+        for (int oi = 0; oi < nc; ++oi) {
+            const int ci = order[oi], e = hm.cut_elem[ci];
+            const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
+            for (int v = 0; v < 3; ++v) nodes[(size_t)kCutNodeStride * oi + v] = hm.conn[3 * e + v];
+            for (int k = 0; k < nl - 3; ++k) nodes[(size_t)kCutNodeStride * oi + 3 + k] = hm.cut_enr[(size_t)ci * kMaxEnr + k];
+            tmpl[oi] = hm.cut_tmpl[ci];
+            for (int k = 0; k < kMaxChildren; ++k) chm[(size_t)kMaxChildren * oi + k] = hm.cut_child_mat[(size_t)ci * kMaxChildren + k];
+            qp0[oi] = hm.cut_coh_qp0[ci];
+            for (int a = 0; a < nl; ++a)
+                for (int b = 0; b < nl; ++b) sl.push_back(hm.cut_slot[(size_t)ci * S * S + a * S + b]);
+            sp[oi + 1] = (int)sl.size();
+        }
+        if ((rc = dev_upload(&c.cut_nodes, nodes))) return rc;
+        if ((rc = dev_upload(&c.cut_tmpl, tmpl))) return rc;
+        if ((rc = dev_upload(&c.cut_child_mat, chm))) return rc;
+        if ((rc = dev_upload(&c.cut_coh_qp0, qp0))) return rc;
+        if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
+        if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;
@@ -353,6 +360,35 @@ void pg_ctx_destroy(pg_ctx* c) {
     cudaSetDevice(c->c.device);
     free_ctx(c->c);
     delete c;
+}
+
+int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut) {
+    PG_GUARD_CTX(c);
+    cudaSetDevice(c->c.device);
+    return autotune_assembly(c->c, reps, ms_tri, ms_cut);
+}
+
+int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps) {
+    PG_GUARD_CTX(c);
+    if (tri_tile_nodes) *tri_tile_nodes = kTriTileSizes[c->c.tuning.tri_variant];
+    if (tri_persistent) *tri_persistent = c->c.tuning.tri_persistent;
+    if (cut_warps) *cut_warps = c->c.tuning.cut_warps;
+    return PG_OK;
+}
+
+int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps) {
+    PG_GUARD_CTX(c);
+    int v = -1;
+    for (int k = 0; k < kTriTileVariants; ++k)
+        if (kTriTileSizes[k] == tri_tile_nodes) v = k;
+    if (v < 0 || (tri_persistent != 0 && tri_persistent != 1) || (cut_warps != 2 && cut_warps != 4 && cut_warps != 8)) {
+        set_error("pg_ctx_set_tuning: tile 32 or 64, persistent 0 or 1, warps 2, 4 or 8");
+        return PG_ERR_ARG;
+    }
+    c->c.tuning.tri_variant = v;
+    c->c.tuning.tri_persistent = tri_persistent;
+    c->c.tuning.cut_warps = cut_warps;
+    return PG_OK;
 }
 
 int pg_ctx_sync(pg_ctx* c) {

@@ -27,6 +27,7 @@ struct DevCohLaw {
 // node count (3 + enrichment slots) at most kCutClassNl[k].
 constexpr int kCutClasses = 4;
 constexpr int kCutClassNl[kCutClasses] = {5, 7, 11, 15};
+constexpr int kCutNodeStride = 16;
 
 struct DevTemplate {
     int n_enr, n_child, n_coh, pad;
@@ -52,12 +53,22 @@ struct MgHierarchy;
 // its vertex t0 that is the block's column node, bits 12-21 / 22-23 the
 // second entry, bits 24-25 the count (0-2); kTriMapDiag marks the diagonal
 // block, kTriMapSlow a block whose entries do not fit the word (evaluated
-// from global memory).  Entries are numbered from the CTA's first entry.
-constexpr int kTriTileNodes = 64;
-constexpr int kTriTileEntries = 512;
+// from global memory).  Entries are numbered from the CTA's first entry, so
+// the map depends on the tile size: one map per tile size the autotuner may
+// pick (kTriTileSizes node rows per CTA, 2 threads and 8 staged entries per row).
+constexpr int kTriTileVariants = 2;
+constexpr int kTriTileSizes[kTriTileVariants] = {32, 64};
 constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
-void build_tri_map(const HostMesh& hm, std::vector<int>& map);
+void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
+// Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
+// triangle tile size, persistent grid (CTAs walk the tiles) or one CTA per
+// tile, and warps (= cut elements) per CTA of the cut kernel.
+struct AsmTuning {
+    int tri_variant = 1;   // index into kTriTileSizes
+    int tri_persistent = 0;
+    int cut_warps = 4;     // 2, 4 or 8
+};
 
 struct Ctx {
     int device = 0;
@@ -74,17 +85,16 @@ struct Ctx {
     int* diag = nullptr;
     int* ne_ptr = nullptr;
     int* ne_list = nullptr;
-    int* tri_map = nullptr;            // one word per block (see kTriMapDiag)
+    int* tri_map[kTriTileVariants] = {};  // one word per block per tile size (see kTriMapDiag)
+    AsmTuning tuning;
     double* dmat = nullptr;            // 3 per material: D11, D12, D33
-    // cut elements
-    int* cut_elem = nullptr;
+    // cut elements, grouped by size class (kCutClassNl), in that order
+    int* cut_nodes = nullptr;          // kCutNodeStride per element: 3 parent nodes, then enrichment slots, -1 unused
     int* cut_tmpl = nullptr;
-    int* cut_enr = nullptr;
-    int* cut_child_mat = nullptr;
-    int* cut_coh_qp0 = nullptr;
+    int* cut_child_mat = nullptr;      // kMaxChildren per element
+    int* cut_coh_qp0 = nullptr;        // first cohesive quadrature point (mesh numbering)
     int* cut_slot_ptr = nullptr;
-    int* cut_slot = nullptr;
-    int* cut_order = nullptr;          // cut elements grouped by size class (see kCutClassNl)
+    int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
     MgHierarchy* mg = nullptr;         // multigrid hierarchy, built at the first multigrid solve
     // system
@@ -149,6 +159,42 @@ int cuda_fail(cudaError_t e, const char* where);
 void upload_tables();
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s);
 int launch_to_fp32(Ctx& c, cudaStream_t s);
+int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut);
+// shape sensitivity (pg_sens.cu): per-node inclusion / velocity and the cut-kernel passes
+// Arguments of the cut-element kernel (pg_assemble.cu)
+struct CutArgs {
+    int n_cut;                      // elements of this launch (one size class)
+    int first;                      // its first element in the class-ordered arrays
+    const int* __restrict__ cut_nodes;
+    const int* __restrict__ cut_tmpl;
+    const int* __restrict__ cut_child_mat;
+    const int* __restrict__ cut_coh_qp0;
+    const int* __restrict__ cut_slot_ptr;
+    const int* __restrict__ cut_slot;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ dmat;
+    const double* __restrict__ isv_c;
+    double* isv_t;
+    DevCohLaw coh;
+    double dt;
+    double* K;
+    double* f;
+    int want_K, want_f;
+    // shape sensitivity (SENS instances only): the element's enrichment nodes
+    // of its `which`-th inclusion move by sgn * h_rel * r * velocity, and the
+    // element's internal force dotted with wsens goes to sens[inclusion]
+    const int* node_inc;
+    const double* vel;
+    const double* wsens;
+    const double* radius;
+    double* sens;
+    double h_rel, sgn;
+    int which;
+};
+CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K);
+void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s);
 
 // solver entry points (pg_solve.cu)
 int solve_linear_system(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);

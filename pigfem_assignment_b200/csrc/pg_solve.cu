@@ -261,6 +261,7 @@ double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s) {
 }
 
 void set_prescribed(Ctx& c, double t_frac, cudaStream_t s) {
+    c.t_frac = t_frac;
     k_apply_dirichlet<<<nblk(c.n_dof), kThreads, 0, s>>>(c.n_dof, c.fixed, c.ubar, t_frac, c.U);
 }
 

@@ -1,0 +1,54 @@
+"""Assembly launch shapes: every shape the autotuner may pick assembles the
+same K (against the oracle), and the autotuner times them all and keeps the
+fastest."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+import pigfem_assignment_b200.problem as pb
+from helpers import bsr_to_csr, rel_fro
+from pigfem_assignment_b200 import _lib
+from pigfem_assignment_b200.rve import RVE, config0
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_K(ctx, e):
+    return bsr_to_csr(e["row_ptr"], e["col"], ctx.matrix_values())
+
+
+@pytest.mark.parametrize("tile", [32, 64])
+@pytest.mark.parametrize("persistent", [0, 1])
+@pytest.mark.parametrize("warps", [2, 4, 8])
+def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
+    # two inclusions close together give cut elements of several size classes
+    rve = RVE(nx=40, ny=40, inclusions=[(0.3, 0.5, 0.2, 1), (0.72, 0.5, 0.2, 1)], strain=0.01)
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, warps))
+    pb.Assembler(ctx).assemble_linear()
+    Ko, _, _ = oracle.from_product(e, pb.template_table(), rve).assemble()
+    assert rel_fro(gpu_K(ctx, e), Ko) <= 1e-12
+    ctx.close()
+
+
+def test_autotune_times_every_shape_and_keeps_the_fastest():
+    rve = config0()
+    prob = pb.ProblemLinearElasticity(rve)
+    prob.init()
+    ms_tri = (C.c_float * 4)()
+    ms_cut = (C.c_float * 3)()
+    _lib.check(_lib.lib.pg_ctx_autotune(prob.ctx.handle, 3, ms_tri, ms_cut))
+    assert all(v > 0 for v in ms_tri) and all(v > 0 for v in ms_cut)
+    tile, pers, warps = C.c_int32(), C.c_int32(), C.c_int32()
+    _lib.check(_lib.lib.pg_ctx_tuning(prob.ctx.handle, C.byref(tile), C.byref(pers), C.byref(warps)))
+    best_tri = int(np.argmin(list(ms_tri)))
+    assert (tile.value, pers.value) == ((32, 64)[best_tri // 2], best_tri % 2)
+    assert warps.value == (2, 4, 8)[int(np.argmin(list(ms_cut)))]
+    # the tuned context still solves to the reference tolerance
+    st = prob.solve_problem()
+    assert st.status == 0
+    prob.ctx.close()

@@ -242,13 +242,14 @@ def run_b200_arm(args):
         return a.value, b.value
 
     # pick the assembly launch shapes on this mesh (pg_ctx_autotune), untimed
-    ms_tri = (C.c_float * 4)()
+    ms_tri = (C.c_float * 5)()
     ms_cut = (C.c_float * 3)()
     _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
     t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
+    tri_kernel = "k_assemble_grid" if t_tile.value == 128 else "k_assemble_tri"
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
-              "ms_tri_tile32_tile32p_tile64_tile64p": [round(v, 4) for v in ms_tri],
+              "ms_tri_rows32_rows32p_rows64_rows64p_grid32x4": [round(v, 4) for v in ms_tri],
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
 
     for _ in range(args.warmup):
@@ -367,8 +368,8 @@ def run_b200_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(rve, info),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic("k_assemble_tri"),
-                         "kernel": "k_assemble_tri",
+                         "frac": achieved / peak, "traffic": profiled_traffic(tri_kernel),
+                         "kernel": tri_kernel,
                          "peak_kind": peak_kind, "bytes_per_launch": rows_bytes, "kernel_share": share,
                          "pass_bytes": pass_bytes,
                          "pass_achieved": pass_bytes / (statistics.mean(step_ms) / 1e3) / 1e9},

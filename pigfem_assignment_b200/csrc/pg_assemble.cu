@@ -767,6 +767,261 @@ void launch_cut_class(int k, int warps, const CutArgs& ck, cudaStream_t s) {
     else launch_cut_w<4>(k, ck, s);
 }
 
+
+// ---------------------------------------------------------------------------
+// Uncut triangles of a structured background grid: 2D node tiles
+// ---------------------------------------------------------------------------
+// The background mesh is nx x ny cells of two triangles each (element
+// 2 (i + j nx) + t, diagonal alternating with (i + j) % 2), regular node
+// (i, j) = i + j (nx + 1).  A CTA owns a kGridTX x kGridTY tile of regular
+// nodes.  Everything it reads is addressed by the tile's coordinates alone:
+// the materials of the (kGridTX + 1) x (kGridTY + 1) cells around the tile
+// (-1 marks a cut element), the coordinates (and displacements) of the
+// (kGridTX + 2) x (kGridTY + 2) nodes, the row pointers and the block-map
+// words of its rows, so all loads are issued at once, coalesced, without
+// dependent gathers.
+//   1. each staged triangle's gradients are computed once into shared memory;
+//   2. one thread per off-diagonal block reads its map word (the at most two
+//      staged triangles joining the block's nodes, with both local vertices)
+//      and stores the block; one thread per node sums and stores the diagonal
+//      block over its (at most 8) triangles;
+//   3. with WANT_F, one thread per node forms its f_int over its triangles.
+// Rows of enrichment nodes and blocks coupling to them are zero here (the
+// cut-element kernel fills them).
+constexpr int kGridTX = 32, kGridTY = 4;
+constexpr int kGridThreads = kGridTX * kGridTY;
+constexpr int kGridCX = kGridTX + 1, kGridCY = kGridTY + 1;      // staged cells
+constexpr int kGridNX = kGridTX + 2, kGridNY = kGridTY + 2;      // staged nodes
+constexpr int kGridElems = 2 * kGridCX * kGridCY;
+
+struct GridArgs {
+    int nx, ny;
+    const int* __restrict__ row_ptr;
+    const int* __restrict__ emat;       // per element: material, -1 for cut elements
+    const int* __restrict__ map;        // per block: grid-tile map word
+    const int* __restrict__ diag;       // diagonal block slot per node
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ dmat;
+    double* K;
+    double* f;
+    int want_K;
+};
+
+// local vertex numbers of cell (i, j)'s triangle t, as node offsets (di, dj)
+__device__ __forceinline__ void grid_tri_nodes(int i, int j, int t, int di[3], int dj[3]) {
+    if (((i + j) & 1) == 0) {
+        // {n00, n10, n11}, {n00, n11, n01}
+        if (t == 0) { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 0; di[2] = 1; dj[2] = 1; }
+        else        { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 1; di[2] = 0; dj[2] = 1; }
+    } else {
+        // {n00, n10, n01}, {n10, n11, n01}
+        if (t == 0) { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 0; di[2] = 0; dj[2] = 1; }
+        else        { di[0] = 1; dj[0] = 0; di[1] = 1; dj[1] = 1; di[2] = 0; dj[2] = 1; }
+    }
+}
+
+__device__ __forceinline__ void grid_add(const double* g, int v, int t, const double* D, double k[4]) {
+    const double s = g[6];
+    const double ba = g[v] * s, ca = g[3 + v] * s, bb = g[t], cb = g[3 + t];
+    const double d11 = D[0], d12 = D[1], d33 = D[2];
+    k[0] += ba * d11 * bb + ca * d33 * cb;
+    k[1] += ba * d12 * cb + ca * d33 * bb;
+    k[2] += ca * d12 * bb + ba * d33 * cb;
+    k[3] += ca * d11 * cb + ba * d33 * bb;
+}
+
+template <bool WANT_F>
+__global__ void __launch_bounds__(kGridThreads, 6) k_assemble_grid(GridArgs a) {
+    __shared__ double sG[kGridElems][7];           // b0, b1, b2, c0, c1, c2, 1/(2J)
+    __shared__ int sM[kGridElems];                 // material, -1: none (cut or outside)
+    __shared__ double sX[kGridNY][kGridNX], sY[kGridNY][kGridNX];
+    __shared__ double sU[WANT_F ? kGridNY : 1][WANT_F ? 2 * kGridNX : 1];
+    __shared__ int sRow[kGridTY][2];               // block range of each tile row
+    const int tiles_x = (a.nx + 1 + kGridTX - 1) / kGridTX;
+    const int I0 = (blockIdx.x % tiles_x) * kGridTX, J0 = (blockIdx.x / tiles_x) * kGridTY;
+    const int tid = threadIdx.x;
+    // ---- phase 1: independent, coalesced loads ----
+    for (int k = tid; k < kGridElems; k += kGridThreads) {
+        const int t = k & 1, cell = k >> 1;
+        const int ci = I0 - 1 + cell % kGridCX, cj = J0 - 1 + cell / kGridCX;
+        sM[k] = (ci >= 0 && ci < a.nx && cj >= 0 && cj < a.ny) ? __ldg(&a.emat[2 * (ci + cj * a.nx) + t]) : -1;
+    }
+    for (int k = tid; k < kGridNX * kGridNY; k += kGridThreads) {
+        const int gi = I0 - 1 + k % kGridNX, gj = J0 - 1 + k / kGridNX;
+        const bool in = gi >= 0 && gi <= a.nx && gj >= 0 && gj <= a.ny;
+        const int node = gi + gj * (a.nx + 1);
+        sX[k / kGridNX][k % kGridNX] = in ? __ldg(&a.x[node]) : 0.0;
+        sY[k / kGridNX][k % kGridNX] = in ? __ldg(&a.y[node]) : 0.0;
+        if (WANT_F) {
+            sU[k / kGridNX][2 * (k % kGridNX)] = in ? a.u[2 * node] : 0.0;
+            sU[k / kGridNX][2 * (k % kGridNX) + 1] = in ? a.u[2 * node + 1] : 0.0;
+        }
+    }
+    if (tid < kGridTY) {
+        const int gj = J0 + tid;
+        const int i1 = min(I0 + kGridTX, a.nx + 1);
+        if (gj <= a.ny) {
+            sRow[tid][0] = __ldg(&a.row_ptr[I0 + gj * (a.nx + 1)]);
+            sRow[tid][1] = __ldg(&a.row_ptr[i1 + gj * (a.nx + 1)]);
+        } else {
+            sRow[tid][0] = sRow[tid][1] = 0;
+        }
+    }
+    __syncthreads();
+    // ---- phase 1b: gradients of every staged triangle ----
+    for (int k = tid; k < kGridElems; k += kGridThreads) {
+        if (sM[k] < 0) continue;
+        const int t = k & 1, cell = k >> 1;
+        const int lx = cell % kGridCX, ly = cell / kGridCX;  // staged cell = staged node (lx, ly) corner
+        int di[3], dj[3];
+        grid_tri_nodes(I0 - 1 + lx, J0 - 1 + ly, t, di, dj);
+        const double X0 = sX[ly + dj[0]][lx + di[0]], X1 = sX[ly + dj[1]][lx + di[1]], X2 = sX[ly + dj[2]][lx + di[2]];
+        const double Y0 = sY[ly + dj[0]][lx + di[0]], Y1 = sY[ly + dj[1]][lx + di[1]], Y2 = sY[ly + dj[2]][lx + di[2]];
+        const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+        double* g = sG[k];
+        g[0] = Y1 - Y2;
+        g[1] = Y2 - Y0;
+        g[2] = Y0 - Y1;
+        g[3] = X2 - X1;
+        g[4] = X0 - X2;
+        g[5] = X1 - X0;
+        g[6] = 0.5 / J;
+    }
+    __syncthreads();
+    // ---- phase 2: off-diagonal blocks of the tile's rows ----
+    if (a.want_K) {
+        for (int r = 0; r < kGridTY; ++r) {
+            const int q0 = sRow[r][0], q1 = sRow[r][1];
+            for (int q = q0 + tid; q < q1; q += kGridThreads) {
+                const int w = __ldg(&a.map[q]);
+                if (w & kTriMapDiag) continue;
+                double k[4] = {0.0, 0.0, 0.0, 0.0};
+                const int cnt = (w >> 26) & 3;
+                for (int m = 0; m < cnt; ++m) {
+                    const int word = (w >> (13 * m)) & 8191;
+                    const int le = word & 511, v = (word >> 9) & 3, t = (word >> 11) & 3;
+                    grid_add(sG[le], v, t, a.dmat + 3 * sM[le], k);
+                }
+                double2* dst = reinterpret_cast<double2*>(a.K + 4 * (size_t)q);
+                dst[0] = make_double2(k[0], k[1]);
+                dst[1] = make_double2(k[2], k[3]);
+            }
+        }
+    }
+    // ---- phase 2b / 3: per node, diagonal block and f_int ----
+    const int lx = tid % kGridTX, ly = tid / kGridTX;
+    const int gi = I0 + lx, gj = J0 + ly;
+    if (gi > a.nx || gj > a.ny) return;
+    double kd[4] = {0.0, 0.0, 0.0, 0.0};
+    double fx = 0.0, fy = 0.0;
+    // the four cells around the node: staged cell (lx + ox, ly + oy), ox, oy in {0, 1}
+    for (int oy = 0; oy < 2; ++oy)
+        for (int ox = 0; ox < 2; ++ox)
+            for (int t = 0; t < 2; ++t) {
+                const int le = 2 * ((ly + oy) * kGridCX + (lx + ox)) + t;
+                if (sM[le] < 0) continue;
+                int di[3], dj[3];
+                grid_tri_nodes(gi - 1 + ox, gj - 1 + oy, t, di, dj);
+                // the node is staged node (lx + 1, ly + 1); the cell corner is (lx + ox, ly + oy)
+                int v = -1;
+                for (int m = 0; m < 3; ++m)
+                    if (ox + di[m] == 1 && oy + dj[m] == 1) v = m;
+                if (v < 0) continue;
+                const double* D = a.dmat + 3 * sM[le];
+                grid_add(sG[le], v, v, D, kd);
+                if (WANT_F) {
+                    for (int m = 0; m < 3; ++m) {
+                        double kb[4] = {0.0, 0.0, 0.0, 0.0};
+                        grid_add(sG[le], v, m, D, kb);
+                        const int sx = lx + ox + di[m], sy = ly + oy + dj[m];
+                        const double ux = sU[sy][2 * sx], uy = sU[sy][2 * sx + 1];
+                        fx += kb[0] * ux + kb[1] * uy;
+                        fy += kb[2] * ux + kb[3] * uy;
+                    }
+                }
+            }
+    const int node = gi + gj * (a.nx + 1);
+    if (a.want_K) {
+        double2* dst = reinterpret_cast<double2*>(a.K + 4 * (size_t)__ldg(&a.diag[node]));
+        dst[0] = make_double2(kd[0], kd[1]);
+        dst[1] = make_double2(kd[2], kd[3]);
+    }
+    if (WANT_F) {
+        a.f[2 * node] = fx;
+        a.f[2 * node + 1] = fy;
+    }
+}
+
+// Grid-tile map words (see k_assemble_grid): per contribution 13 bits --
+// staged element (9 bits), the row node's vertex (2), the column node's
+// vertex (2); two contributions, the count in bits 26-27.
+void build_grid_map(const HostMesh& hm, std::vector<int>& map) {
+    const int nx = hm.spec.nx, ny = hm.spec.ny;
+    map.assign((size_t)hm.n_blocks(), 0);
+    for (int gj = 0; gj <= ny; ++gj)
+        for (int gi = 0; gi <= nx; ++gi) {
+            const int i = gi + gj * (nx + 1);
+            const int I0 = (gi / kGridTX) * kGridTX, J0 = (gj / kGridTY) * kGridTY;
+            for (int q = hm.row_ptr[i]; q < hm.row_ptr[i + 1]; ++q) {
+                const int j = hm.col[q];
+                if (j == i) {
+                    map[q] = kTriMapDiag;
+                    continue;
+                }
+                if (j >= hm.n_reg) continue;  // enrichment column: zero here
+                int cnt = 0, word = 0;
+                for (int cj = gj - 1; cj <= gj; ++cj)
+                    for (int ci = gi - 1; ci <= gi; ++ci) {
+                        if (ci < 0 || ci >= nx || cj < 0 || cj >= ny) continue;
+                        for (int t = 0; t < 2; ++t) {
+                            const int e = 2 * (ci + cj * nx) + t;
+                            if (hm.elem_cut[e] >= 0) continue;
+                            int v = -1, tc = -1;
+                            for (int m = 0; m < 3; ++m) {
+                                if (hm.conn[3 * e + m] == i) v = m;
+                                if (hm.conn[3 * e + m] == j) tc = m;
+                            }
+                            if (v < 0 || tc < 0) continue;
+                            const int le = 2 * ((cj - (J0 - 1)) * kGridCX + (ci - (I0 - 1))) + t;
+                            if (cnt < 2) word |= (le | (v << 9) | (tc << 11)) << (13 * cnt);
+                            ++cnt;
+                        }
+                    }
+                map[q] = word | (std::min(cnt, 2) << 26);
+            }
+        }
+}
+
+void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
+    GridArgs ga;
+    ga.nx = c.hm.spec.nx;
+    ga.ny = c.hm.spec.ny;
+    ga.row_ptr = c.row_ptr;
+    ga.emat = c.grid_emat;
+    ga.map = c.grid_map;
+    ga.diag = c.diag;
+    ga.x = c.x;
+    ga.y = c.y;
+    ga.u = U;
+    ga.dmat = c.dmat;
+    ga.K = c.K;
+    ga.f = c.F;
+    ga.want_K = want_K;
+    const int tiles = ((ga.nx + 1 + kGridTX - 1) / kGridTX) * ((ga.ny + 1 + kGridTY - 1) / kGridTY);
+    if (want_f)
+        k_assemble_grid<true><<<tiles, kGridThreads, 0, s>>>(ga);
+    else
+        k_assemble_grid<false><<<tiles, kGridThreads, 0, s>>>(ga);
+    // rows of enrichment nodes (after the regular ones) get their values from the cut kernel
+    const size_t q_enr = (size_t)c.hm.row_ptr[c.n_reg];
+    if (want_K && (size_t)c.n_blocks > q_enr)
+        cudaMemsetAsync(c.K + 4 * q_enr, 0, 4 * ((size_t)c.n_blocks - q_enr) * sizeof(double), s);
+    if (want_f && c.n_nodes > c.n_reg)
+        cudaMemsetAsync(c.F + 2 * (size_t)c.n_reg, 0, 2 * (size_t)(c.n_nodes - c.n_reg) * sizeof(double), s);
+}
+
 template <bool WANT_F, int TN>
 void launch_tri_tn(const Ctx& c, const RowArgs& ra, cudaStream_t s) {
     const int n_tiles = (c.n_nodes + TN - 1) / TN;
@@ -783,6 +1038,10 @@ void launch_tri_tn(const Ctx& c, const RowArgs& ra, cudaStream_t s) {
 }
 
 void launch_tri(const Ctx& c, const RowArgs& ra, bool want_f, cudaStream_t s) {
+    if (c.tuning.tri_grid && c.grid_map) {
+        launch_grid(c, ra.u, want_f, ra.want_K, s);
+        return;
+    }
     const int tn = kTriTileSizes[c.tuning.tri_variant];
     if (tn == 32) {
         if (want_f) launch_tri_tn<true, 32>(c, ra, s);
@@ -915,6 +1174,7 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     AsmTuning best = c.tuning;
     float best_tri = 1e30f, best_cut = 1e30f;
     int idx = 0;
+    c.tuning.tri_grid = 0;
     for (int v = 0; v < kTriTileVariants; ++v)
         for (int p = 0; p < 2; ++p, ++idx) {
             c.tuning.tri_variant = v;
@@ -926,8 +1186,21 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
                 best_tri = ms;
                 best.tri_variant = v;
                 best.tri_persistent = p;
+                best.tri_grid = 0;
             }
         }
+    if (c.grid_map) {
+        c.tuning.tri_grid = 1;
+        const RowArgs ra = row_args(c, c.U, false, true);
+        const float ms = timed([&] { launch_tri(c, ra, false, s); });
+        if (ms_tri) ms_tri[4] = ms;
+        if (ms < best_tri) {
+            best_tri = ms;
+            best.tri_grid = 1;
+        }
+    } else if (ms_tri) {
+        ms_tri[4] = 0.f;
+    }
     const int warps[3] = {2, 4, 8};
     for (int k = 0; k < 3; ++k) {
         c.tuning.cut_warps = warps[k];

@@ -61,11 +61,13 @@ constexpr int kTriTileSizes[kTriTileVariants] = {32, 64};
 constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
+void build_grid_map(const HostMesh& hm, std::vector<int>& map);
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // triangle tile size, persistent grid (CTAs walk the tiles) or one CTA per
 // tile, and warps (= cut elements) per CTA of the cut kernel.
 struct AsmTuning {
-    int tri_variant = 1;   // index into kTriTileSizes
+    int tri_grid = 1;      // 1: 2D node tiles of the structured grid (when the mesh has one)
+    int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
     int cut_warps = 4;     // 2, 4 or 8
 };
@@ -87,6 +89,8 @@ struct Ctx {
     int* ne_list = nullptr;
     int* tri_map[kTriTileVariants] = {};  // one word per block per tile size (see kTriMapDiag)
     AsmTuning tuning;
+    int* grid_emat = nullptr;          // structured meshes: material per element, -1 for cut elements
+    int* grid_map = nullptr;           // structured meshes: grid-tile map word per block
     double* dmat = nullptr;            // 3 per material: D11, D12, D33
     // cut elements, grouped by size class (kCutClassNl), in that order
     int* cut_nodes = nullptr;          // kCutNodeStride per element: 3 parent nodes, then enrichment slots, -1 unused

@@ -19,7 +19,7 @@ def gpu_K(ctx, e):
     return bsr_to_csr(e["row_ptr"], e["col"], ctx.matrix_values())
 
 
-@pytest.mark.parametrize("tile", [32, 64])
+@pytest.mark.parametrize("tile", [32, 64, 128])
 @pytest.mark.parametrize("persistent", [0, 1])
 @pytest.mark.parametrize("warps", [2, 4, 8])
 def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
@@ -39,14 +39,17 @@ def test_autotune_times_every_shape_and_keeps_the_fastest():
     rve = config0()
     prob = pb.ProblemLinearElasticity(rve)
     prob.init()
-    ms_tri = (C.c_float * 4)()
+    ms_tri = (C.c_float * 5)()
     ms_cut = (C.c_float * 3)()
     _lib.check(_lib.lib.pg_ctx_autotune(prob.ctx.handle, 3, ms_tri, ms_cut))
     assert all(v > 0 for v in ms_tri) and all(v > 0 for v in ms_cut)
     tile, pers, warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(prob.ctx.handle, C.byref(tile), C.byref(pers), C.byref(warps)))
     best_tri = int(np.argmin(list(ms_tri)))
-    assert (tile.value, pers.value) == ((32, 64)[best_tri // 2], best_tri % 2)
+    if best_tri == 4:
+        assert tile.value == 128  # the 2D tiles of the structured grid
+    else:
+        assert (tile.value, pers.value) == ((32, 64)[best_tri // 2], best_tri % 2)
     assert warps.value == (2, 4, 8)[int(np.argmin(list(ms_cut)))]
     # the tuned context still solves to the reference tolerance
     st = prob.solve_problem()

@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--no-load-step", action="store_true")
     ap.add_argument("--no-cohesive", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (profiling runs: timings under a profiler mislead the tuner)")
     ap.add_argument("--batch-rves", type=int, default=512)
     ap.add_argument("--viscosity", type=float, default=200.0,
                     help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
@@ -244,7 +246,8 @@ def run_b200_arm(args):
     # pick the assembly launch shapes on this mesh (pg_ctx_autotune), untimed
     ms_tri = (C.c_float * 5)()
     ms_cut = (C.c_float * 3)()
-    _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
+    if not args.no_autotune:
+        _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
     t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
     tri_kernel = "k_assemble_grid" if t_tile.value == 128 else "k_assemble_tri"

@@ -870,6 +870,16 @@ __global__ void __launch_bounds__(kGridThreads, 6) k_assemble_grid(GridArgs a) {
         }
     }
     __syncthreads();
+    // the block-map words of the tile's rows: issued now, used after phase 1b
+    constexpr int kPer = 4;  // blocks per thread and tile row held in registers (rows up to 512 blocks)
+    int wv[kGridTY][kPer];
+#pragma unroll
+    for (int r = 0; r < kGridTY; ++r)
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int q = sRow[r][0] + tid + u * kGridThreads;
+            wv[r][u] = (a.want_K && q < sRow[r][1]) ? __ldg(&a.map[q]) : kTriMapDiag;
+        }
     // ---- phase 1b: gradients of every staged triangle ----
     for (int k = tid; k < kGridElems; k += kGridThreads) {
         if (sM[k] < 0) continue;
@@ -892,10 +902,15 @@ __global__ void __launch_bounds__(kGridThreads, 6) k_assemble_grid(GridArgs a) {
     __syncthreads();
     // ---- phase 2: off-diagonal blocks of the tile's rows ----
     if (a.want_K) {
+#pragma unroll
         for (int r = 0; r < kGridTY; ++r) {
             const int q0 = sRow[r][0], q1 = sRow[r][1];
-            for (int q = q0 + tid; q < q1; q += kGridThreads) {
-                const int w = __ldg(&a.map[q]);
+            for (int q = q0 + tid, u = 0; q < q1; q += kGridThreads, ++u) {
+                int w = 0;
+#pragma unroll
+                for (int uu = 0; uu < kPer; ++uu)
+                    if (uu == u) w = wv[r][uu];
+                if (u >= kPer) w = __ldg(&a.map[q]);
                 if (w & kTriMapDiag) continue;
                 double k[4] = {0.0, 0.0, 0.0, 0.0};
                 const int cnt = (w >> 26) & 3;

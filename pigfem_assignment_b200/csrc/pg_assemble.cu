@@ -1142,55 +1142,15 @@ void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
     }
 }
 
-// K(touched slots) += Kc, F(cut nodes) += Fc, and both buffers back to zero
-__global__ void k_fold_cut(int n_touch, const int* __restrict__ touch_slot, double* Kc, double* K, int n_nodes_t,
-                           const int* __restrict__ touch_node, double* Fc, double* F, int want_K, int want_f) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (want_K && i < n_touch) {
-        double4* src = reinterpret_cast<double4*>(Kc) + i;
-        double2* dst = reinterpret_cast<double2*>(K + 4 * (size_t)touch_slot[i]);
-        const double4 v = *src;
-        double2 d0 = dst[0], d1 = dst[1];
-        d0.x += v.x;
-        d0.y += v.y;
-        d1.x += v.z;
-        d1.y += v.w;
-        dst[0] = d0;
-        dst[1] = d1;
-        *src = make_double4(0.0, 0.0, 0.0, 0.0);
-    }
-    if (want_f && i < n_nodes_t) {
-        const int n = touch_node[i];
-        F[2 * n] += Fc[2 * n];
-        F[2 * n + 1] += Fc[2 * n + 1];
-        Fc[2 * n] = 0.0;
-        Fc[2 * n + 1] = 0.0;
-    }
-}
-
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
-    // nothing to clear: the triangle kernel writes every value of K.  The cut
-    // kernels run concurrently on their own stream into Kc / Fc, folded in after.
+    // nothing to clear: the triangle kernel writes every value of K
     const RowArgs ra = row_args(c, U, want_f, want_K);
     if (c.timing) cudaEventRecord(c.ea0, s);
-    if (c.n_cut > 0) {
-        cudaEventRecord(c.ev_fork, s);
-        cudaStreamWaitEvent(c.stream_cut, c.ev_fork, 0);
-        CutArgs ca = cut_args(c, U, dt, want_f, want_K);
-        ca.K = c.Kc;
-        ca.f = c.Fc;
-        launch_cut_all(c, ca, c.stream_cut);
-        PG_CUDA(cudaGetLastError());
-        cudaEventRecord(c.ev_join, c.stream_cut);
-    }
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {
-        cudaStreamWaitEvent(s, c.ev_join, 0);
-        const int n = std::max(c.n_touch, c.n_touch_nodes);
-        k_fold_cut<<<(n + 255) / 256, 256, 0, s>>>(c.n_touch, c.touch_slot, c.Kc, c.K, c.n_touch_nodes, c.touch_node, c.Fc,
-                                                   c.F, want_K, want_f);
+        launch_cut_all(c, cut_args(c, U, dt, want_f, want_K), s);
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);
@@ -1261,9 +1221,7 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
         c.tuning.cut_warps = warps[k];
         float ms = 0.f;
         if (c.n_cut > 0) {
-            CutArgs ca = cut_args(c, c.U, 1.0, false, true);
-            ca.K = c.Kc;  // the cut kernels' own buffer (cleared below)
-            ca.f = c.Fc;
+            const CutArgs ca = cut_args(c, c.U, 1.0, false, true);
             ms = timed([&] { launch_cut_all(c, ca, s); });
         }
         if (ms_cut) ms_cut[k] = ms;
@@ -1274,10 +1232,6 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     }
     c.tuning = best;
     c.assembled = false;
-    if (c.n_cut > 0) {
-        cudaMemsetAsync(c.Kc, 0, 4 * (size_t)std::max(1, c.n_touch) * sizeof(double), s);
-        cudaMemsetAsync(c.Fc, 0, 2 * (size_t)c.n_nodes * sizeof(double), s);
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(flush);

@@ -1,7 +1,6 @@
 // extern "C" entry points of libpigfem_b200 (declared in include/pigfem_b200.h).
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,7 +58,7 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_map, c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
-                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.touch_slot, c.touch_node, c.Kc, c.Fc, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -71,9 +70,6 @@ void free_ctx(Ctx& c) {
     for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2})
         if (e) cudaEventDestroy(e);
     if (c.stream) cudaStreamDestroy(c.stream);
-    if (c.stream_cut) cudaStreamDestroy(c.stream_cut);
-    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
-    if (c.ev_join) cudaEventDestroy(c.ev_join);
 }
 
 void set_error(const std::string& s) { g_last_error = s; }
@@ -88,9 +84,6 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     PG_CUDA(cudaSetDevice(device));
     upload_tables();
     PG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    PG_CUDA(cudaStreamCreateWithFlags(&c.stream_cut, cudaStreamNonBlocking));
-    PG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
-    PG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     PG_CUDA(cudaEventCreate(&c.ev0));
     PG_CUDA(cudaEventCreate(&c.ev1));
     PG_CUDA(cudaEventCreate(&c.ea0));
@@ -175,27 +168,8 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.cut_tmpl, tmpl))) return rc;
         if ((rc = dev_upload(&c.cut_child_mat, chm))) return rc;
         if ((rc = dev_upload(&c.cut_coh_qp0, qp0))) return rc;
-        // compact the slot tables onto the blocks that cut elements touch
-        std::vector<int> touched;
-        for (int v : sl)
-            if (v >= 0) touched.push_back(v);
-        std::sort(touched.begin(), touched.end());
-        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
-        for (int& v : sl)
-            if (v >= 0) v = (int)(std::lower_bound(touched.begin(), touched.end(), v) - touched.begin());
-        std::vector<int> tnodes;
-        for (int v : nodes)
-            if (v >= 0) tnodes.push_back(v);
-        std::sort(tnodes.begin(), tnodes.end());
-        tnodes.erase(std::unique(tnodes.begin(), tnodes.end()), tnodes.end());
-        c.n_touch = (int)touched.size();
-        c.n_touch_nodes = (int)tnodes.size();
         if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
         if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
-        if ((rc = dev_upload(&c.touch_slot, touched))) return rc;
-        if ((rc = dev_upload(&c.touch_node, tnodes))) return rc;
-        if ((rc = dev_alloc(&c.Kc, 4 * (size_t)std::max(1, c.n_touch)))) return rc;
-        if ((rc = dev_alloc(&c.Fc, 2 * (size_t)hm.n_nodes()))) return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;

@@ -75,8 +75,6 @@ struct AsmTuning {
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t stream_cut = nullptr;  // the cut-element kernels run here, beside the triangle kernel
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     HostMesh hm;                       // host copy (sizes, maps, export)
     int n_nodes = 0, n_reg = 0, n_elem = 0, n_cut = 0, n_blocks = 0, n_dof = 0, n_coh_qp = 0;
     DevCohLaw coh{};
@@ -100,14 +98,7 @@ struct Ctx {
     int* cut_child_mat = nullptr;      // kMaxChildren per element
     int* cut_coh_qp0 = nullptr;        // first cohesive quadrature point (mesh numbering)
     int* cut_slot_ptr = nullptr;
-    int* cut_slot = nullptr;           // (3 + n_enr)^2 per element: index into Kc (-1: none)
-    // The cut kernels add into their own buffers while the triangle kernel
-    // writes K; a fold kernel then adds them in and clears them.
-    int n_touch = 0, n_touch_nodes = 0;
-    int* touch_slot = nullptr;         // K block slot of each Kc entry
-    int* touch_node = nullptr;         // nodes of cut elements
-    double* Kc = nullptr;              // 4 per touched block, zero between assemblies
-    double* Fc = nullptr;              // 2 per node, zero between assemblies
+    int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
     MgHierarchy* mg = nullptr;         // multigrid hierarchy, built at the first multigrid solve
     // system

@@ -63,6 +63,7 @@ class SolverCfg(C.Structure):
         ("krylov", C.c_int32), ("precond", C.c_int32), ("precision", C.c_int32),
         ("rtol", C.c_double), ("max_iter", C.c_int32), ("inner_rtol", C.c_double),
         ("max_refine", C.c_int32), ("gmres_restart", C.c_int32), ("check_every", C.c_int32),
+        ("inclusion_modes", C.c_int32),
     ]
 
 
@@ -85,7 +86,7 @@ class NewtonCfg(C.Structure):
         ("stol", C.c_double), ("max_it", C.c_int32), ("precision", C.c_int32), ("precond", C.c_int32),
         ("lin_rtol", C.c_double), ("inner_rtol", C.c_double), ("lin_max_iter", C.c_int32),
         ("max_repeat", C.c_int32), ("predictor", C.c_int32), ("rtol_base", C.c_int32),
-        ("t_start", C.c_double), ("t_stop", C.c_double),
+        ("inclusion_modes", C.c_int32), ("t_start", C.c_double), ("t_stop", C.c_double),
     ]
 
 

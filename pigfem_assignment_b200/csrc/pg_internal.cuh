@@ -208,7 +208,7 @@ int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
 double residual_into(Ctx& c, cudaStream_t s, const double* x, const double* b, double* out);
 // geometric multigrid (pg_mg.cu)
 int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStream_t s);
-int mg_prepare(Ctx& c, bool f32, cudaStream_t s);
+int mg_prepare(Ctx& c, bool f32, bool modes, cudaStream_t s);
 void mg_precondition(Ctx& c, bool f32, cudaStream_t s, const double* r, double* z);
 void mg_free(Ctx& c);
 // ||v||^2 of a device vector (synchronises)

@@ -68,6 +68,14 @@ struct MgHierarchy {
     // CG scalars: 0 pq, 1 rz, 2 rz_new, 3 rr, 4 tol2; flags: 0 done, 1 breakdown, 2 iterations, 3 coarse-singular
     double* sc = nullptr;
     int* fl = nullptr;
+    // inclusion rigid modes (cohesive meshes): 3 per inclusion, supports disjoint
+    int n_inc = 0;                       // 0: no mode space
+    bool use_modes = false;
+    int* z_inc = nullptr;                // per node: the inclusion whose modes touch it, -1 none
+    double* zval = nullptr;              // per node: [d][k], 2 x 3
+    double* E = nullptr;                 // per inclusion: Z_i^T K Z_i (3 x 3)
+    double* Einv = nullptr;
+    double* w = nullptr;                 // per inclusion: Z_i^T r (3)
     std::vector<void*> owned;
 };
 
@@ -536,12 +544,182 @@ __global__ void k_mgcg_tol(double* sc, double rtol2) { sc[4] = rtol2 * sc[3]; }
 
 inline int nb(int n, int t = kThreads) { return (n + t - 1) / t; }
 
+
+// ---------------------------------------------------------------------------
+// Inclusion rigid modes.  With cohesive interfaces an inclusion whose
+// interface has softened can translate and rotate against the matrix at
+// little energy; the grid hierarchy cannot represent those discontinuous
+// modes (its corrections are continuous), so the preconditioner adds the
+// coarse correction Z (Z^T K Z)^-1 Z^T r over them (additively, so it stays
+// symmetric positive definite).  Mode k of inclusion i is the rigid motion
+// R_k (x translation, y translation, rotation about the centre) inside the
+// inclusion and zero outside: R_k at the nodes inside, and at an enrichment
+// node the value that makes the field there R_k (inclusion side) or 0
+// (matrix side), i.e. minus the parent edge's interpolation of the nodal
+// values.  Distinct inclusions share no element, so Z^T K Z is block
+// diagonal with one 3 x 3 block per inclusion.
+// ---------------------------------------------------------------------------
+__global__ void k_modes_E(int n, const int* __restrict__ z_inc, const double* __restrict__ zval,
+                          const int* __restrict__ row_ptr, const int* __restrict__ col, const double* __restrict__ K,
+                          const uint8_t* __restrict__ fixed, double* E) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int zi = z_inc[q];
+    if (zi < 0) return;
+    double y[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    for (int p = row_ptr[q]; p < row_ptr[q + 1]; ++p) {
+        const int cn = col[p];
+        if (z_inc[cn] != zi) continue;
+        const double* blk = K + 4 * (size_t)p;
+        for (int d = 0; d < 2; ++d)
+            for (int e = 0; e < 2; ++e) {
+                if (fixed[2 * cn + e]) continue;
+                const double kde = blk[2 * d + e];
+                for (int l = 0; l < 3; ++l) y[d][l] += kde * zval[6 * (size_t)cn + 3 * e + l];
+            }
+    }
+    for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) {
+            double v = 0.0;
+            for (int d = 0; d < 2; ++d)
+                if (!fixed[2 * q + d]) v += zval[6 * (size_t)q + 3 * d + k] * y[d][l];
+            atomicAdd(&E[9 * zi + 3 * k + l], v);
+        }
+}
+
+// 3 x 3 inverse per inclusion (zero when the block is numerically singular)
+__global__ void k_modes_inv(int n_inc, const double* E, double* Einv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_inc) return;
+    const double* a = E + 9 * i;
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    double scale = 0.0;
+    for (int k = 0; k < 9; ++k) scale = fmax(scale, fabs(a[k]));
+    double* o = Einv + 9 * i;
+    if (!(fabs(det) > 1e-13 * scale * scale * scale)) {
+        for (int k = 0; k < 9; ++k) o[k] = 0.0;
+        return;
+    }
+    const double r = 1.0 / det;
+    o[0] = c00 * r;
+    o[1] = (a[2] * a[7] - a[1] * a[8]) * r;
+    o[2] = (a[1] * a[5] - a[2] * a[4]) * r;
+    o[3] = c01 * r;
+    o[4] = (a[0] * a[8] - a[2] * a[6]) * r;
+    o[5] = (a[2] * a[3] - a[0] * a[5]) * r;
+    o[6] = c02 * r;
+    o[7] = (a[1] * a[6] - a[0] * a[7]) * r;
+    o[8] = (a[0] * a[4] - a[1] * a[3]) * r;
+}
+
+__global__ void k_modes_zero(int n, double* w, const int* done) {
+    if (done && done[0]) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) w[i] = 0.0;
+}
+
+// w_i = Z_i^T r
+__global__ void k_modes_dot(int n, const int* __restrict__ z_inc, const double* __restrict__ zval,
+                            const uint8_t* __restrict__ fixed, const double* __restrict__ r, double* w, const int* done) {
+    if (done && done[0]) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int zi = z_inc[q];
+    if (zi < 0) return;
+    const double r0 = fixed[2 * q] ? 0.0 : r[2 * q], r1 = fixed[2 * q + 1] ? 0.0 : r[2 * q + 1];
+    for (int k = 0; k < 3; ++k)
+        atomicAdd(&w[3 * zi + k], zval[6 * (size_t)q + k] * r0 + zval[6 * (size_t)q + 3 + k] * r1);
+}
+
+// z += Z_i E_i^-1 w_i
+__global__ void k_modes_add(int n, const int* __restrict__ z_inc, const double* __restrict__ zval,
+                            const uint8_t* __restrict__ fixed, const double* __restrict__ Einv,
+                            const double* __restrict__ w, double* z, const int* done) {
+    if (done && done[0]) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int zi = z_inc[q];
+    if (zi < 0) return;
+    const double* B = Einv + 9 * zi;
+    const double* wi = w + 3 * zi;
+    double cc[3];
+    for (int k = 0; k < 3; ++k) cc[k] = B[3 * k] * wi[0] + B[3 * k + 1] * wi[1] + B[3 * k + 2] * wi[2];
+    for (int d = 0; d < 2; ++d) {
+        if (fixed[2 * q + d]) continue;
+        z[2 * q + d] += zval[6 * (size_t)q + 3 * d] * cc[0] + zval[6 * (size_t)q + 3 * d + 1] * cc[1] +
+                        zval[6 * (size_t)q + 3 * d + 2] * cc[2];
+    }
+}
+
 template <typename T>
 int mg_alloc(MgHierarchy& m, T** p, size_t n) {
     *p = nullptr;
     PG_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
     PG_CUDA(cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
     m.owned.push_back((void*)*p);
+    return PG_OK;
+}
+
+// Inclusion rigid modes of a cohesive mesh (host, once per mesh).
+int modes_build(Ctx& c, MgHierarchy& m) {
+    const HostMesh& hm = c.hm;
+    const int ni = (int)hm.spec.inclusions.size();
+    if (!hm.spec.cohesive || ni == 0) return PG_OK;
+    const int nn = hm.n_nodes();
+    // side of every enrichment node: 1 if an inclusion-material child uses it, 0 if a matrix child does
+    std::vector<int> side(hm.n_enr, -1);
+    for (int ci = 0; ci < hm.n_cut; ++ci) {
+        const CutTemplate& T = cut_template(hm.cut_tmpl[ci]);
+        for (int ch = 0; ch < T.n_child; ++ch) {
+            const int mat = hm.cut_child_mat[(size_t)ci * kMaxChildren + ch];
+            for (int k = 0; k < T.child_n[ch]; ++k) {
+                const int ln = T.child_nodes[ch][k];
+                if (ln < 3) continue;
+                const int node = hm.cut_enr[(size_t)ci * kMaxEnr + ln - 3];
+                if (node >= hm.n_reg) side[node - hm.n_reg] = mat == hm.spec.matrix_mat ? 0 : 1;
+            }
+        }
+    }
+    std::vector<int> zinc(nn, -1);
+    std::vector<double> zval(6 * (size_t)nn, 0.0);
+    auto rigid = [&](int i, double x, double y, double out[2][3]) {
+        const Inclusion& I = hm.spec.inclusions[i];
+        out[0][0] = 1.0; out[0][1] = 0.0; out[0][2] = -(y - I.cy);
+        out[1][0] = 0.0; out[1][1] = 1.0; out[1][2] = x - I.cx;
+    };
+    for (int n = 0; n < hm.n_reg; ++n) {
+        const int i = hm.node_detect[n];
+        if (i < 0 || i >= ni) continue;
+        double R[2][3];
+        rigid(i, hm.x[n], hm.y[n], R);
+        zinc[n] = i;
+        for (int d = 0; d < 2; ++d)
+            for (int k = 0; k < 3; ++k) zval[6 * (size_t)n + 3 * d + k] = R[d][k];
+    }
+    for (int k = 0; k < hm.n_enr; ++k) {
+        const int n = hm.n_reg + k, i = hm.enr_inc[k];
+        if (i < 0 || i >= ni || side[k] < 0) continue;
+        const int a = hm.enr_edge[2 * k], b = hm.enr_edge[2 * k + 1];
+        const double ex = hm.x[b] - hm.x[a], ey = hm.y[b] - hm.y[a];
+        const double t = ((hm.x[n] - hm.x[a]) * ex + (hm.y[n] - hm.y[a]) * ey) / (ex * ex + ey * ey);
+        double Ra[2][3] = {}, Rb[2][3] = {}, Rn[2][3] = {};
+        if (hm.node_detect[a] == i) rigid(i, hm.x[a], hm.y[a], Ra);
+        if (hm.node_detect[b] == i) rigid(i, hm.x[b], hm.y[b], Rb);
+        if (side[k] == 1) rigid(i, hm.x[n], hm.y[n], Rn);
+        zinc[n] = i;
+        for (int d = 0; d < 2; ++d)
+            for (int q = 0; q < 3; ++q)
+                zval[6 * (size_t)n + 3 * d + q] = Rn[d][q] - ((1.0 - t) * Ra[d][q] + t * Rb[d][q]);
+    }
+    int rc;
+    if ((rc = mg_alloc(m, &m.z_inc, (size_t)nn)) || (rc = mg_alloc(m, &m.zval, 6 * (size_t)nn)) ||
+        (rc = mg_alloc(m, &m.E, 9 * (size_t)ni)) || (rc = mg_alloc(m, &m.Einv, 9 * (size_t)ni)) ||
+        (rc = mg_alloc(m, &m.w, 3 * (size_t)ni)))
+        return rc;
+    PG_CUDA(cudaMemcpy(m.z_inc, zinc.data(), zinc.size() * sizeof(int), cudaMemcpyHostToDevice));
+    PG_CUDA(cudaMemcpy(m.zval, zval.data(), zval.size() * sizeof(double), cudaMemcpyHostToDevice));
+    m.n_inc = ni;
     return PG_OK;
 }
 
@@ -604,7 +782,7 @@ int mg_build(Ctx& c) {
     }
     PG_CUDA(cudaGetLastError());
     PG_CUDA(cudaStreamSynchronize(s));
-    return PG_OK;
+    return modes_build(c, *m);
 }
 
 // Numeric set-up for the current K (every solve: K changes between Newton iterations).
@@ -641,6 +819,11 @@ int mg_numeric(Ctx& c, bool f32, cudaStream_t s) {
         if (f32) k_mg_to_f32<<<nb(36 * L.n), kThreads, 0, s>>>(36 * (size_t)L.n, L.A, L.Af);
         nxf = L.nx;
         nyf = L.ny;
+    }
+    if (m.n_inc > 0 && m.use_modes) {
+        cudaMemsetAsync(m.E, 0, 9 * (size_t)m.n_inc * sizeof(double), s);
+        k_modes_E<<<nb(n0), kThreads, 0, s>>>(n0, m.z_inc, m.zval, c.row_ptr, c.col, c.K, c.fixed, m.E);
+        k_modes_inv<<<nb(m.n_inc), kThreads, 0, s>>>(m.n_inc, m.E, m.Einv);
     }
     const MgLevel& C = m.L[m.nlev];
     cudaMemsetAsync(m.fl, 0, 8 * sizeof(int), s);
@@ -794,13 +977,20 @@ void mg_apply(Ctx& c, MgHierarchy& m, bool f32, cudaStream_t s, const double* r,
         const double* x = vcycle<double>(c, m, s, r, done);
         k_copy<double><<<nb(nd), kThreads, 0, s>>>(nd, x, z);
     }
+    if (m.n_inc > 0 && m.use_modes) {
+        const int n = c.n_nodes;
+        k_modes_zero<<<nb(3 * m.n_inc), kThreads, 0, s>>>(3 * m.n_inc, m.w, done);
+        k_modes_dot<<<nb(n), kThreads, 0, s>>>(n, m.z_inc, m.zval, c.fixed, r, m.w, done);
+        k_modes_add<<<nb(n), kThreads, 0, s>>>(n, m.z_inc, m.zval, c.fixed, m.Einv, m.w, z, done);
+    }
 }
 
 }  // namespace
 
-int mg_prepare(Ctx& c, bool f32, cudaStream_t s) {
+int mg_prepare(Ctx& c, bool f32, bool modes, cudaStream_t s) {
     int rc = mg_build(c);
     if (rc != PG_OK) return rc;
+    c.mg->use_modes = modes;
     if ((rc = mg_numeric(c, f32, s))) return rc;
     int fl[8] = {};
     cudaMemcpyAsync(fl, c.mg->fl, sizeof fl, cudaMemcpyDeviceToHost, s);
@@ -831,6 +1021,7 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
     if (rc != PG_OK) return rc;
     MgHierarchy& m = *c.mg;
     const bool f32 = cfg.precision == PG_PRECISION_MIXED;
+    m.use_modes = cfg.inclusion_modes != 0;
     if ((rc = mg_numeric(c, f32, s))) return rc;
     const int n = c.n_nodes, nd = c.n_dof;
     cudaMemsetAsync(m.sc, 0, 8 * sizeof(double), s);

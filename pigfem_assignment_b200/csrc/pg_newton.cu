@@ -64,6 +64,7 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
     pg_solver_cfg_default(&lin);
     lin.precision = cfg.precision;
     lin.precond = cfg.precond;
+    lin.inclusion_modes = cfg.inclusion_modes;
     lin.krylov = PG_KRYLOV_CG;
     lin.max_iter = cfg.lin_max_iter;
     lin.inner_rtol = cfg.inner_rtol;
@@ -149,6 +150,7 @@ void pg_newton_cfg_default(pg_newton_cfg* cfg) {
     cfg->max_repeat = 20;
     cfg->predictor = PG_PREDICT_ZEROTH;
     cfg->rtol_base = PG_RTOL_BASE_PREDICTOR;
+    cfg->inclusion_modes = 1;
     cfg->t_start = 0.0;
     cfg->t_stop = 1.0;
 }

@@ -292,7 +292,7 @@ int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
     if (cfg.precond == PG_PREC_MG) {
         // one multigrid V-cycle per iteration (FP32 cycle under PG_PRECISION_MIXED)
         if (cfg.krylov == PG_KRYLOV_GMRES) {
-            const int rc = mg_prepare(c, cfg.precision == PG_PRECISION_MIXED, s);
+            const int rc = mg_prepare(c, cfg.precision == PG_PRECISION_MIXED, cfg.inclusion_modes != 0, s);
             if (rc == PG_ERR_BREAKDOWN) { st.status = rc; return PG_OK; }
             if (rc != PG_OK) return rc;
             return gmres_solve(c, cfg, cfg.rtol, cfg.max_iter, st, s, std::sqrt(bb));

@@ -315,7 +315,7 @@ def run_b200_arm(args):
 
     # ---- load-step time at 1e-8 relative residual: plain FP64 vs mixed ----
     load = None
-    if not args.no_load_step:
+    if not args.no_load_step and world == 1:
         load = {}
         variants = (("plain_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_MG),
                     ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED, _lib.PG_PREC_MG),
@@ -338,7 +338,8 @@ def run_b200_arm(args):
 
     # ---- cohesive load step: plain FP64 vs mixed + learned ----
     coh = None
-    if not args.no_cohesive and not args.no_load_step:
+    # the secondary measurements run on one GPU only (the scaling runs time the assembly alone)
+    if not args.no_cohesive and not args.no_load_step and world == 1:
         try:
             coh = cohesive_load_steps(local, args.viscosity)
         except Exception as ex:  # reported, never fatal for the assembly line
@@ -346,7 +347,7 @@ def run_b200_arm(args):
 
     # ---- batched uneven RVEs (configuration 3) ----
     batch = None
-    if not args.no_batch and not args.no_load_step:
+    if not args.no_batch and not args.no_load_step and world == 1:
         try:
             batch = batched_rves(local, args.batch_rves, 5, 2)
         except Exception as ex:

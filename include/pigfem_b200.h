@@ -211,10 +211,11 @@ typedef struct pg_newton_cfg {
 
 typedef struct pg_step_stats {
     double t_frac, dt;
-    int32_t newton_its, krylov_its, gmres_fallbacks, repeats;
+    int32_t newton_its, krylov_its, gmres_fallbacks, repeats;  /* pg_solve_nonlinear: summed over all attempts */
     double res0, res;               /* FP64 ||r|| of the predictor and at the end */
     int32_t reason;                 /* SNES-style: 2 abs, 3 rel, 4 step; <0 diverged */
-    double seconds;                 /* device time of the step */
+    double seconds;                 /* pg_newton_load_step: device time of the step; pg_solve_nonlinear: wall time
+                                       of the load step from its predictor to acceptance, every attempt included */
     int32_t predictor_used;         /* PG_PREDICT_* actually used for this step */
     double res_linear, res_learned; /* initial residuals of both candidates (learned predictor only) */
     double res_base;                /* the residual rtol was relative to */

@@ -16,6 +16,7 @@
 // The residual (f_int) and the tangent are FP64; the linear Newton systems
 // are solved in FP64 or in FP32 Krylov + FP64 refinement.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <vector>
 
@@ -197,6 +198,11 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
         int repeat = 0;
         bool converged = false;
         pg_step_stats st{};
+        // the record of a load step counts every attempt (failed ones included)
+        // and its wall time from the predictor to the accepted state
+        PG_CUDA(cudaStreamSynchronize(s));
+        const auto t_step = std::chrono::steady_clock::now();
+        int acc_newton = 0, acc_krylov = 0, acc_fallbacks = 0;
         while (!converged) {
             if (repeat >= cfg.max_repeat) {
                 set_error("pg_solve_nonlinear: Newton did not converge within the load-step repeat budget");
@@ -259,6 +265,9 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             st.res_learned = res_mlp;
             if (rc != PG_OK) return rc;
             converged = st.reason > 0;
+            acc_newton += st.newton_its;
+            acc_krylov += st.krylov_its;
+            acc_fallbacks += st.gmres_fallbacks;
             if (!converged) {
                 // restore the last converged solution and cut the step
                 cudaMemcpyAsync(c.U, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -272,6 +281,11 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
         cudaMemcpyAsync(c.Uprev, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
         t += dt;
         st.repeats = repeat;
+        st.newton_its = acc_newton;
+        st.krylov_its = acc_krylov;
+        st.gmres_fallbacks = acc_fallbacks;
+        PG_CUDA(cudaStreamSynchronize(s));
+        st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_step).count();
         if (per_step && nrec < max_records) per_step[nrec] = st;
         ++nrec;
         dt_prev = dt;

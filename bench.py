@@ -423,13 +423,15 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
     def with_eta(rve):
         return dataclasses.replace(rve, coh_params=tuple(rve.coh_params[:4]) + (eta,))
 
-    newton = dict(precond=_lib.PG_PREC_MG, stol=0.0, rtol_base=_lib.PG_RTOL_BASE_ZEROTH)
+    # a Krylov budget of 1000 per Newton iteration: a healthy multigrid solve needs a few hundred, and an attempt on an
+    # indefinite tangent that runs GMRES to a larger budget only delays the step cut
+    newton = dict(precond=_lib.PG_PREC_MG, stol=0.0, rtol_base=_lib.PG_RTOL_BASE_ZEROTH, lin_max_iter=1000)
     t0 = time.perf_counter()
     # training trajectories use the reference's SNES tests (rtol of the predictor, stol)
     xs, ts = [], []
     for k in range(n_train):
         x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.2, seed=k,
-                                     device=local, newton=dict(precond=_lib.PG_PREC_MG))
+                                     device=local, newton=dict(precond=_lib.PG_PREC_MG, lin_max_iter=1000))
         xs.append(x)
         ts.append(t)
     X = np.concatenate(xs)

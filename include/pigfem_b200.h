@@ -160,8 +160,8 @@ typedef struct pg_solver_cfg {
     int32_t max_refine;             /* mixed: refinement budget */
     int32_t gmres_restart;
     int32_t check_every;            /* host residual check cadence (iterations per captured graph) */
-    int32_t inclusion_modes;        /* PG_PREC_MG on cohesive meshes: add the inclusions' rigid motions
-                                       (3 per inclusion) as a coarse space (default 1) */
+    int32_t inclusion_modes;        /* PG_PREC_MG on cohesive meshes: 1 adds the inclusions' rigid motions
+                                       (3 per inclusion) as a coarse space (default 0) */
 } pg_solver_cfg;
 
 typedef struct pg_solve_stats {
@@ -198,7 +198,7 @@ typedef struct pg_newton_cfg {
     int32_t max_repeat;             /* load-step repeats with dt *= 0.25 (reference: 20) */
     int32_t predictor;              /* PG_PREDICT_* */
     int32_t rtol_base;              /* PG_RTOL_BASE_*: which residual rtol is relative to */
-    int32_t inclusion_modes;        /* as in pg_solver_cfg (default 1) */
+    int32_t inclusion_modes;        /* as in pg_solver_cfg (default 0) */
     double t_start, t_stop;         /* pg_solve_nonlinear steps the load fraction from t_start (the current U and
                                        committed state are converged there) to t_stop; defaults 0 and 1 */
 } pg_newton_cfg;

@@ -488,7 +488,7 @@ void pg_solver_cfg_default(pg_solver_cfg* cfg) {
     cfg->max_refine = 50;
     cfg->gmres_restart = 60;
     cfg->check_every = 64;
-    cfg->inclusion_modes = 1;
+    cfg->inclusion_modes = 0;
 }
 
 int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg_in, pg_solve_stats* stats) {

@@ -151,7 +151,7 @@ void pg_newton_cfg_default(pg_newton_cfg* cfg) {
     cfg->max_repeat = 20;
     cfg->predictor = PG_PREDICT_ZEROTH;
     cfg->rtol_base = PG_RTOL_BASE_PREDICTOR;
-    cfg->inclusion_modes = 1;
+    cfg->inclusion_modes = 0;
     cfg->t_start = 0.0;
     cfg->t_stop = 1.0;
 }

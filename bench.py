@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiling runs: timings under a profiler mislead the tuner)")
     ap.add_argument("--batch-rves", type=int, default=512)
+    ap.add_argument("--no-sensitivity", action="store_true")
     ap.add_argument("--viscosity", type=float, default=200.0,
                     help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
     return ap.parse_args()
@@ -353,6 +354,14 @@ def run_b200_arm(args):
         except Exception as ex:
             batch = {"status": f"failed: {ex}"}
 
+    # ---- adjoint shape sensitivity on the configuration-4 geometry ----
+    sens = None
+    if not args.no_sensitivity and not args.no_load_step and world == 1:
+        try:
+            sens = sensitivity_cfg4(local)
+        except Exception as ex:
+            sens = {"status": f"failed: {ex}"}
+
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -385,6 +394,7 @@ def run_b200_arm(args):
             "load_step": load,
             "cohesive_load_step": coh,
             "batched": batch,
+            "sensitivity": sens,
             "autotune": tuning,
             "kernel_ms": {"rows_median": statistics.median(rows_ms), "cut_median": statistics.median(cut_ms)},
         }
@@ -548,6 +558,65 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int):
     out["config"] = (f"config3: {n_rve} RVEs, side in {{64,96,128,192,256}}, 1-64 RSA circles r~U[0.02,0.08], "
                      "E_inc~U[20,100] GPa, seed 3; one launch per assembly kernel for the whole batch")
     return out
+
+
+def sensitivity_cfg4(local: int, n_check: int = 2):
+    """Adjoint sensitivity of C_11 to all 400 inclusion radii on the
+    configuration-4 geometry (1024x1024 TRI3, 400 seeded circles r ~ U[0.01,
+    0.02]) with bonded interfaces: one multigrid-CG solve, one adjoint solve and
+    the cut kernel in sensitivity mode, then central finite differences
+    (h = 1e-6) of C_11 from re-meshed, re-solved RVEs for `n_check` seeded radii."""
+    import ctypes as C
+    import dataclasses
+
+    import numpy as np
+
+    import pigfem_assignment_b200.problem as pb
+    from pigfem_assignment_b200 import _lib
+    from pigfem_assignment_b200.rve import config4
+
+    rve = dataclasses.replace(config4(), cohesive=False)
+
+    def solve(r):
+        prob = pb.ProblemLinearElasticity(r, device=local)
+        prob.init()
+        prob.get_solver().configure(precond=_lib.PG_PREC_MG, rtol=1e-11)
+        st = prob.solve_problem()
+        return prob, st
+
+    cfg = _lib.SolverCfg()
+    _lib.lib.pg_solver_cfg_default(C.byref(cfg))
+    cfg.precond, cfg.rtol = _lib.PG_PREC_MG, 1e-11
+    prob, st = solve(rve)
+    c11 = C.c_double()
+    sens = np.zeros(len(rve.inclusions))
+    ast = _lib.SolveStats()
+    t0 = time.perf_counter()
+    _lib.check(_lib.lib.pg_sensitivity_c11(prob.ctx.handle, C.byref(cfg), 1e-5, C.byref(c11), _lib.dptr(sens),
+                                           C.byref(ast)), "pg_sensitivity_c11")
+    sens_s = time.perf_counter() - t0
+    prob.ctx.close()
+    rng = np.random.default_rng(4)
+    checks = []
+    h = 1e-6
+    for i in rng.choice(len(rve.inclusions), n_check, replace=False):
+        vals = []
+        for sgn in (1.0, -1.0):
+            inc = list(rve.inclusions)
+            x, y, r, m = inc[i]
+            inc[i] = (x, y, r + sgn * h, m)
+            p2, _ = solve(dataclasses.replace(rve, inclusions=inc))
+            c = C.c_double()
+            _lib.check(_lib.lib.pg_sensitivity_c11(p2.ctx.handle, C.byref(cfg), 1e-5, C.byref(c), None, None))
+            p2.ctx.close()
+            vals.append(c.value)
+        fd = (vals[0] - vals[1]) / (2 * h)
+        checks.append({"inclusion": int(i), "adjoint": float(sens[i]), "central_fd": fd,
+                       "rel_diff": abs(sens[i] - fd) / abs(fd)})
+    return {"config": "config4 geometry: 1024x1024 TRI3, 400 RSA circles r~U[0.01,0.02] seed 4, bonded, 1% strain",
+            "C11_MPa": c11.value, "solve_ms": 1e3 * st.seconds, "solve_iterations": st.iterations,
+            "sensitivity_s": sens_s, "adjoint_iterations": ast.iterations, "radii": len(rve.inclusions),
+            "fd_checks_h1e-6": checks}
 
 def main():
     args = parse()

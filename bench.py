@@ -487,6 +487,9 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
             "krylov_iterations": int(sum(r.krylov_its for r in R)),
             "repeated_steps": int(sum(1 for r in R if r.repeats > 1)),
             "learned_used": int(sum(1 for r in R if r.predictor_used == _lib.PG_PREDICT_LEARNED)),
+            "learned_over_linear_start_residual": (
+                float(np.median([r.res_learned / r.res_linear for r in R if r.res_linear > 0 and r.res_learned > 0]))
+                if any(r.res_linear > 0 and r.res_learned > 0 for r in R) else None),
             "max_final_res_over_base": float(max((r.res / r.res_base) for r in R if r.res_base > 0)) if R else None,
         }
         if pred == _lib.PG_PREDICT_LEARNED:

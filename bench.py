@@ -27,6 +27,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from pigfem_assignment_b200.replicas import max_over_ranks, shard_rves, sum_over_ranks  # noqa: E402
+
 METRIC = "elements assembled/s"
 UNIT = "elements/s"
 
@@ -279,12 +281,7 @@ def run_b200_arm(args):
     clocks = sampler.stop()
     step_ms = [a + b for a, b in zip(rows_ms, cut_ms)]
     t_local = sum(step_ms) / 1e3
-    if dist:
-        tt = torch.tensor([t_local], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    else:
-        t_max = t_local
+    t_max = max_over_ranks(t_local, device=f"cuda:{local}")
     n_e = info["n_elements"]
     value = n_e * args.steps * world / t_max
 
@@ -348,9 +345,11 @@ def run_b200_arm(args):
 
     # ---- batched uneven RVEs (configuration 3) ----
     batch = None
-    if not args.no_batch and not args.no_load_step and world == 1:
+    if not args.no_batch and not args.no_load_step:
+        # every rank takes part (the RVEs shard across ranks); an error on one rank ends the others' next
+        # collective through the process-group timeout
         try:
-            batch = batched_rves(local, args.batch_rves, 5, 2)
+            batch = batched_rves(local, args.batch_rves, 5, 2, rank, world)
         except Exception as ex:
             batch = {"status": f"failed: {ex}"}
 
@@ -507,12 +506,14 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
     return out
 
 
-def batched_rves(local: int, n_rve: int, steps: int, warmup: int):
+def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0, world: int = 1):
     """Configuration 3: `n_rve` independent linear RVEs of uneven size (side in
     {64, 96, 128, 192, 256}, 1-64 circles r ~ U[0.02, 0.08], inclusion E ~
     U[20, 100] GPa) assembled by one launch of each assembly kernel and solved
     together by per-RVE CG preconditioned by the union multigrid cycle, FP64
-    and FP32 cycles, each RVE to 1e-8 of its own right-hand side."""
+    and FP32 cycles, each RVE to 1e-8 of its own right-hand side.  With N
+    ranks each takes its share of the RVEs (balanced by element count, no
+    collective on the data path); times are the slowest rank's."""
     import ctypes as C
     from concurrent.futures import ThreadPoolExecutor
 
@@ -524,7 +525,10 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int):
     from pigfem_assignment_b200.rve import config3_rves
 
     t0 = time.perf_counter()
-    rves = config3_rves(count=n_rve)
+    all_rves = config3_rves(count=n_rve)
+    mine = shard_rves([2 * r.nx * r.ny for r in all_rves], world)[rank]
+    rves = [all_rves[i] for i in mine]
+    n_rve = len(rves)
     with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:  # mesh builds release the GIL
         meshes = list(ex.map(pb.Mesh, rves))
     arr = (C.c_void_p * n_rve)(*[m.handle.value for m in meshes])
@@ -545,8 +549,13 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int):
         _lib.check(_lib.lib.pg_assembly_timing(ctx, 1, C.byref(a), C.byref(b)))
         if k >= warmup:
             times.append(a.value + b.value)
-    out = {"rves": n_rve, "elements": n_elem, "dof": n_dof, "host_setup_s": setup_s,
-           "assembly_ms": statistics.median(times), "elements_per_s": n_elem / (statistics.median(times) / 1e3)}
+    dev = f"cuda:{local}"
+    t_asm = max_over_ranks(statistics.median(times), device=dev)
+    tot_elem = sum_over_ranks(n_elem, device=dev)
+    out = {"rves": int(sum_over_ranks(n_rve, device=dev)), "elements": int(tot_elem),
+           "dof": int(sum_over_ranks(n_dof, device=dev)), "ranks": world,
+           "host_setup_s": max_over_ranks(setup_s, device=dev), "assembly_ms": t_asm,
+           "elements_per_s": tot_elem / (t_asm / 1e3)}
     for name, prec in (("solve_fp64_mg", _lib.PG_PRECISION_FP64), ("solve_mixed_mg", _lib.PG_PRECISION_MIXED)):
         cfg = _lib.SolverCfg()
         _lib.lib.pg_solver_cfg_default(C.byref(cfg))
@@ -555,8 +564,10 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int):
         _lib.check(_lib.lib.pg_set_vector(ctx, 0, _lib.dptr(zero)))
         tot = _lib.SolveStats()
         rc = _lib.lib.pg_batch_solve(h, C.byref(cfg), None, C.byref(tot))
-        out[name] = {"status": "ok" if rc == 0 else _lib.lib.pg_last_error().decode(), "ms": 1e3 * tot.seconds,
-                     "max_iterations": tot.iterations, "worst_rel_residual": tot.rel_residual}
+        out[name] = {"status": "ok" if rc == 0 else _lib.lib.pg_last_error().decode(),
+                     "ms": 1e3 * max_over_ranks(tot.seconds, device=dev),
+                     "max_iterations": int(max_over_ranks(tot.iterations, device=dev)),
+                     "worst_rel_residual": max_over_ranks(tot.rel_residual, device=dev)}
     _lib.lib.pg_batch_destroy(h)
     out["config"] = (f"config3: {n_rve} RVEs, side in {{64,96,128,192,256}}, 1-64 RSA circles r~U[0.02,0.08], "
                      "E_inc~U[20,100] GPa, seed 3; one launch per assembly kernel for the whole batch")

@@ -528,8 +528,9 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
     const double PX0 = sX[w][0], PX1 = sX[w][1], PX2 = sX[w][2];
     const double PY0 = sY[w][0], PY1 = sY[w][1], PY2 = sY[w][2];
     const double PJ = (PX1 - PX0) * (PY2 - PY0) - (PX2 - PX0) * (PY1 - PY0);
-    const double pbx[3] = {(PY1 - PY2) / PJ, (PY2 - PY0) / PJ, (PY0 - PY1) / PJ};
-    const double pby[3] = {(PX2 - PX1) / PJ, (PX0 - PX2) / PJ, (PX1 - PX0) / PJ};
+    const double iPJ = 1.0 / PJ;  // one division per element instead of six
+    const double pbx[3] = {(PY1 - PY2) * iPJ, (PY2 - PY0) * iPJ, (PY0 - PY1) * iPJ};
+    const double pby[3] = {(PX2 - PX1) * iPJ, (PX0 - PX2) * iPJ, (PX1 - PX0) * iPJ};
 
     int nq_total = 0;
     for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
@@ -587,15 +588,17 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
                 row[4 + 2 * j] = 0.0;
                 row[5 + 2 * j] = 0.0;
             }
-            if (live)
+            if (live) {
+                const double idet = 1.0 / det;
                 for (int k = 0; k < nc; ++k) {
                     const int ln = TG.child_nodes[ch][k];
                     if (ln >= 3) {
                         const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
-                        row[4 + 2 * ln] = (J11 * dr - J01 * ds) / det;
-                        row[5 + 2 * ln] = (-J10 * dr + J00 * ds) / det;
+                        row[4 + 2 * ln] = (J11 * dr - J01 * ds) * idet;
+                        row[5 + 2 * ln] = (-J10 * dr + J00 * ds) * idet;
                     }
                 }
+            }
         }
         __syncwarp();
         // each lane integrates its node-pair blocks over the chunk's points

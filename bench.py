@@ -75,7 +75,9 @@ def workload_config(rve, info):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """Samples SM clocks and throttle reasons during the timed region: NVML
+    reads every 5 ms where pynvml is importable, else nvidia-smi every 200 ms.
+    Only reads; no GPU setting is touched."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -88,6 +90,31 @@ class ClockSampler:
         self._t = None
 
     def start(self):
+        try:  # short timed regions need the faster NVML path to get samples at all
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            bits = [("hw_slowdown", getattr(pynvml, "nvmlClocksEventReasonHwSlowdown", 0x8)),
+                    ("hw_thermal_slowdown", getattr(pynvml, "nvmlClocksEventReasonHwThermalSlowdown", 0x40)),
+                    ("sw_thermal_slowdown", getattr(pynvml, "nvmlClocksEventReasonSwThermalSlowdown", 0x20)),
+                    ("sw_power_cap", getattr(pynvml, "nvmlClocksEventReasonSwPowerCap", 0x4))]
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def run_nvml():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                        self.rows.append([str(sm), str(mx), ""] + ["Active" if rs & b else "Not Active" for _, b in bits])
+                    except Exception:
+                        pass
+                    self._stop.wait(0.005)
+            self._t = threading.Thread(target=run_nvml, daemon=True)
+            self._t.start()
+            return
+        except Exception:
+            pass
+
         def run():
             while not self._stop.is_set():
                 try:

@@ -478,17 +478,20 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
     const int oi = blockIdx.x * kCutWarps + w;
     if (oi >= a.n_cut) return;
     const int ci = a.first + oi;  // class-ordered element index
+    // the node list (padded with -1), the template and the slot pointer do
+    // not depend on each other: their loads go out together
+    const int node = lane < NL ? __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]) : -1;
     const int tmpl = __ldg(&a.cut_tmpl[ci]);
+    const int slot0 = __ldg(&a.cut_slot_ptr[ci]);
     const DevTemplate& T = c_tmpl[tmpl];
     const int nl = 3 + T.n_enr;
     // the element's block slots are needed only at the end: issue their loads now
-    const int* slots = a.cut_slot + __ldg(&a.cut_slot_ptr[ci]);
+    const int* slots = a.cut_slot + slot0;
     int slot[PPL];
 #pragma unroll
     for (int k = 0; k < PPL; ++k)
         slot[k] = (!SENS && a.want_K && lane + 32 * k < nl * nl) ? __ldg(&slots[lane + 32 * k]) : -1;
     if (lane < nl) {
-        const int node = __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]);
         sL[w][lane] = node;
         sX[w][lane] = a.x[node];
         sY[w][lane] = a.y[node];

@@ -64,7 +64,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-Xlinker", "--no-undefined"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -70,6 +70,20 @@ void upload_tables() {
         for (size_t i = 0; i < Q.N.size(); ++i) q[ty].N[i] = Q.N[i];
         for (size_t i = 0; i < Q.dN.size(); ++i) q[ty].dN[i] = Q.dN[i];
     }
+    // A Tri3 child's shape gradients (and so its B^T D B) are the same at all
+    // four points of its rule: the device integrates it at one point carrying
+    // the summed weight, which equals the four-point sum up to rounding.
+    {
+        DevChildQuad& t3 = q[kChildTri3];
+        double wsum = 0.0;
+        for (int i = 0; i < t3.nq; ++i) wsum += t3.w[i];
+        t3.nq = 1;
+        t3.w[0] = wsum;
+        const double third = 1.0 / 3.0;
+        t3.N[0] = third;
+        t3.N[1] = third;
+        t3.N[2] = third;
+    }
     cudaMemcpyToSymbol(c_tmpl, t, sizeof(t));
     cudaMemcpyToSymbol(c_quad, q, sizeof(q));
     cudaMemcpyToSymbol(g_tmpl, t, sizeof(t));
@@ -775,37 +789,57 @@ void launch_cut_class(int k, int warps, const CutArgs& ck, cudaStream_t s) {
 
 
 // ---------------------------------------------------------------------------
-// Uncut triangles of a structured background grid: 2D node tiles
+// Uncut triangles of a structured background grid: edge-centric tiles
 // ---------------------------------------------------------------------------
 // The background mesh is nx x ny cells of two triangles each (element
 // 2 (i + j nx) + t, diagonal alternating with (i + j) % 2), regular node
-// (i, j) = i + j (nx + 1).  A CTA owns a kGridTX x kGridTY tile of regular
-// nodes.  Everything it reads is addressed by the tile's coordinates alone:
-// the materials of the (kGridTX + 1) x (kGridTY + 1) cells around the tile
-// (-1 marks a cut element), the coordinates (and displacements) of the
-// (kGridTX + 2) x (kGridTY + 2) nodes, the row pointers and the block-map
-// words of its rows, so all loads are issued at once, coalesced, without
-// dependent gathers.
-//   1. each staged triangle's gradients are computed once into shared memory;
-//   2. one thread per off-diagonal block reads its map word (the at most two
-//      staged triangles joining the block's nodes, with both local vertices)
-//      and stores the block; one thread per node sums and stores the diagonal
-//      block over its (at most 8) triangles;
-//   3. with WANT_F, one thread per node forms its f_int over its triangles.
-// Rows of enrichment nodes and blocks coupling to them are zero here (the
-// cut-element kernel fills them).
-constexpr int kGridTX = 32, kGridTY = 4;
-constexpr int kGridThreads = kGridTX * kGridTY;
-constexpr int kGridCX = kGridTX + 1, kGridCY = kGridTY + 1;      // staged cells
-constexpr int kGridNX = kGridTX + 2, kGridNY = kGridTY + 2;      // staged nodes
-constexpr int kGridElems = 2 * kGridCX * kGridCY;
+// (i, j) = i + j (nx + 1).  On such a mesh every off-diagonal block of a
+// regular row is a mesh edge: horizontal, vertical, or the diagonal of a
+// cell, with at most two triangles on it whose local vertices follow from
+// the cells' parities.  Its place in the row is fixed too: the row holds the
+// node's grid neighbours (all four axis neighbours; the four diagonal ones
+// for even nodes only) in ascending order, then enrichment columns.
+// grid_pattern_ok checks that layout on the host before this kernel is used.
+//
+// A CTA owns a tile of kTileX node columns and TR node rows (3 or 7, picked by
+// the autotuner), with the TR + 1 cell rows around them, and runs one thread
+// per staged triangle ((TR + 1) x 64) in three phases between two barriers:
+//   1. one load per thread of each staged quantity, all in flight at once
+//      and addressed by the tile alone: the materials of the staged
+//      triangles (-1 marks a cut element), the coordinates (and
+//      displacements) of the (TR + 2) x 33 staged nodes, the rows' pointers
+//      and the material table;
+//   2. one staged triangle per thread: its 6 x 6 stiffness (21 distinct
+//      values) into shared memory.  A cell row's triangles are kept t-major
+//      (slot 32 t + cell column) at an odd stride of 21 doubles, so the 16
+//      lanes of a half-warp reading 16 consecutive cells of one t, or one
+//      column each of either t, touch 16 distinct bank pairs;
+//   3. per warp two tasks: warps w < TR the horizontal edges and then the
+//      diagonal blocks of node row w (zeroing the row's enrichment columns);
+//      warps TR .. 2 TR the vertical edges and the cell diagonals of staged
+//      cell row w - TR; with WANT_F, the last warp the tile's f_int.
+// An edge's block is formed once and stored in both rows (the second as its
+// transpose) wherever the tile owns that row; blocks whose triangles are all
+// cut are stored as zeros for the cut-element kernel to add to.
+constexpr int kTileX = kGridTileX;             // node columns per tile (31)
+constexpr int kTileCells = kTileX + 1;         // staged cells per cell row (32)
+constexpr int kTileElems = 2 * kTileCells;     // staged triangles per cell row (64)
+constexpr int kTileNX = kTileX + 2;            // staged node columns (33)
+// Element stiffness in shared memory, kKeStride doubles per triangle: blocks
+// (0,1), (0,2), (1,2) row-major at 0, 4, 8 (pair a < b at 4 (a + b - 1));
+// diagonal block of vertex v as (k00, k01, k11) at kKeDiag + 3 v.
+constexpr int kKeStride = 21;
+constexpr int kKeDiag = 12;
+constexpr int kKeRow = kTileElems * kKeStride;
+// slot of triangle t of staged cell column cc within its cell row
+__host__ __device__ constexpr int tile_slot(int cc, int t) { return t * kTileCells + cc; }
 
 struct GridArgs {
     int nx, ny;
+    int n_mat;                          // materials (at most kSweepMaxMat)
+    int strips;                         // tiles across
     const int* __restrict__ row_ptr;
     const int* __restrict__ emat;       // per element: material, -1 for cut elements
-    const int* __restrict__ map;        // per block: grid-tile map word
-    const int* __restrict__ diag;       // diagonal block slot per node
     const double* __restrict__ x;
     const double* __restrict__ y;
     const double* __restrict__ u;
@@ -815,214 +849,347 @@ struct GridArgs {
     int want_K;
 };
 
-// local vertex numbers of cell (i, j)'s triangle t, as node offsets (di, dj)
-__device__ __forceinline__ void grid_tri_nodes(int i, int j, int t, int di[3], int dj[3]) {
-    if (((i + j) & 1) == 0) {
-        // {n00, n10, n11}, {n00, n11, n01}
-        if (t == 0) { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 0; di[2] = 1; dj[2] = 1; }
-        else        { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 1; di[2] = 0; dj[2] = 1; }
-    } else {
-        // {n00, n10, n01}, {n10, n11, n01}
-        if (t == 0) { di[0] = 0; dj[0] = 0; di[1] = 1; dj[1] = 0; di[2] = 0; dj[2] = 1; }
-        else        { di[0] = 1; dj[0] = 0; di[1] = 1; dj[1] = 1; di[2] = 0; dj[2] = 1; }
+// Corner (di + 2 dj) of local vertex m of triangle t in a cell of parity cp
+// ((i + j) % 2): {n00, n10, n11}, {n00, n11, n01} for even cells,
+// {n00, n10, n01}, {n10, n11, n01} for odd ones.
+__host__ __device__ constexpr int tri_corner(int cp, int t, int m) {
+    return cp == 0 ? (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 3) : (m == 0 ? 0 : m == 1 ? 3 : 2))
+                   : (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 2) : (m == 0 ? 1 : m == 1 ? 3 : 2));
+}
+
+// Local vertex, in triangle t of a cell of parity cp, of the node at the
+// cell's corner (1 - ox, 1 - oy); -1 if the triangle does not touch it.
+__host__ __device__ constexpr int sweep_vertex(int cp, int t, int ox, int oy) {
+    return tri_corner(cp, t, 0) == (1 - ox) + 2 * (1 - oy) ? 0
+         : tri_corner(cp, t, 1) == (1 - ox) + 2 * (1 - oy) ? 1
+         : tri_corner(cp, t, 2) == (1 - ox) + 2 * (1 - oy) ? 2 : -1;
+}
+
+// Grid neighbours of node (gi, gj) present in its row, as bits d = 3 (dy + 1)
+// + (dx + 1) (bit 4 the node itself): axis neighbours inside the grid, and
+// the diagonal ones too for even nodes.  A block's place in the row is the
+// number of lower bits set.
+__host__ __device__ inline unsigned grid_nbr_mask(int gi, int gj, int nx, int ny) {
+    const bool even = ((gi + gj) & 1) == 0;
+    const bool w = gi > 0, e = gi < nx, s = gj > 0, n = gj < ny;
+    return (s && even && w ? 1u : 0u) | (s ? 2u : 0u) | (s && even && e ? 4u : 0u) | (w ? 8u : 0u) | 16u |
+           (e ? 32u : 0u) | (n && even && w ? 64u : 0u) | (n ? 128u : 0u) | (n && even && e ? 256u : 0u);
+}
+
+__device__ __forceinline__ int grid_slot(int row_start, int gi, int gj, int nx, int ny, int d) {
+    return row_start + __popc(grid_nbr_mask(gi, gj, nx, ny) & ((1u << d) - 1u));
+}
+
+__device__ __forceinline__ void store_block(double* K, int q, double k0, double k1, double k2, double k3) {
+    double2* dst = reinterpret_cast<double2*>(K + 4 * (size_t)q);
+    dst[0] = make_double2(k0, k1);
+    dst[1] = make_double2(k2, k3);
+}
+
+// adds the stored element block at e (4 values, row-major) to k
+__device__ __forceinline__ void add_block(const double* e, double k[4]) {
+    k[0] += e[0];
+    k[1] += e[1];
+    k[2] += e[2];
+    k[3] += e[3];
+}
+
+size_t grid_smem_bytes(bool want_f, int tr) {
+    const size_t nodes = (size_t)(tr + 2) * kTileNX;
+    return sizeof(double) * ((tr + 1) * (size_t)kKeRow + 2 * nodes + (want_f ? 2 * nodes : 0) + 3 * kSweepMaxMat) +
+           sizeof(int) * ((tr + 1) * (size_t)kTileElems + tr * (kTileX + 1));
+}
+
+// Stiffness of triangle t of staged cell (cc, cr) (material mat >= 0).
+__device__ __forceinline__ void tile_element(double* ke, const double* sX, const double* sY, const double* sD,
+                                             int mat, int I0, int J0, int cr, int cc, int t) {
+    const int cp = (I0 + J0 + cc + cr) & 1;  // parity of cell (I0 - 1 + cc, J0 - 1 + cr)
+    double X[3], Y[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int code = tri_corner(cp, t, m);
+        const int k = (cr + (code >> 1)) * kTileNX + cc + (code & 1);
+        X[m] = sX[k];
+        Y[m] = sY[k];
+    }
+    const double J = (X[1] - X[0]) * (Y[2] - Y[0]) - (X[2] - X[0]) * (Y[1] - Y[0]);
+    const double s = 0.5 / J;
+    const double b[3] = {Y[1] - Y[2], Y[2] - Y[0], Y[0] - Y[1]};
+    const double c[3] = {X[2] - X[1], X[0] - X[2], X[1] - X[0]};
+    const double E0 = s * sD[3 * mat], E1 = s * sD[3 * mat + 1], E2 = s * sD[3 * mat + 2];
+    // K_ab = [Xa bb + Wa cb, Ya cb + Wa bb; Va bb + Za cb, Ua cb + Za bb] with
+    // X, Y, Z = b (E0, E1, E2), U, V, W = c (E0, E1, E2), E = D / (4 A)
+    double Xv[3], Yv[3], Zv[3], Uv[3], Vv[3], Wv[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        Xv[m] = b[m] * E0; Yv[m] = b[m] * E1; Zv[m] = b[m] * E2;
+        Uv[m] = c[m] * E0; Vv[m] = c[m] * E1; Wv[m] = c[m] * E2;
+    }
+#pragma unroll
+    for (int pa = 0; pa < 2; ++pa)
+#pragma unroll
+        for (int pb = pa + 1; pb < 3; ++pb) {
+            double* d = ke + 4 * (pa + pb - 1);
+            d[0] = Xv[pa] * b[pb] + Wv[pa] * c[pb];
+            d[1] = Yv[pa] * c[pb] + Wv[pa] * b[pb];
+            d[2] = Vv[pa] * b[pb] + Zv[pa] * c[pb];
+            d[3] = Uv[pa] * c[pb] + Zv[pa] * b[pb];
+        }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        double* d = ke + kKeDiag + 3 * m;
+        d[0] = Xv[m] * b[m] + Wv[m] * c[m];
+        d[1] = Yv[m] * c[m] + Wv[m] * b[m];
+        d[2] = Uv[m] * c[m] + Zv[m] * b[m];
     }
 }
 
-__device__ __forceinline__ void grid_add(const double* g, int v, int t, const double* D, double k[4]) {
-    const double s = g[6];
-    const double ba = g[v] * s, ca = g[3 + v] * s, bb = g[t], cb = g[3 + t];
-    const double d11 = D[0], d12 = D[1], d33 = D[2];
-    k[0] += ba * d11 * bb + ca * d33 * cb;
-    k[1] += ba * d12 * cb + ca * d33 * bb;
-    k[2] += ca * d12 * bb + ba * d33 * cb;
-    k[3] += ca * d11 * cb + ba * d33 * bb;
-}
-
-template <bool WANT_F>
-__global__ void __launch_bounds__(kGridThreads, 6) k_assemble_grid(GridArgs a) {
-    __shared__ double sG[kGridElems][7];           // b0, b1, b2, c0, c1, c2, 1/(2J)
-    __shared__ int sM[kGridElems];                 // material, -1: none (cut or outside)
-    __shared__ double sX[kGridNY][kGridNX], sY[kGridNY][kGridNX];
-    __shared__ double sU[WANT_F ? kGridNY : 1][WANT_F ? 2 * kGridNX : 1];
-    __shared__ int sRow[kGridTY][2];               // block range of each tile row
-    const int tiles_x = (a.nx + 1 + kGridTX - 1) / kGridTX;
-    const int I0 = (blockIdx.x % tiles_x) * kGridTX, J0 = (blockIdx.x / tiles_x) * kGridTY;
-    const int tid = threadIdx.x;
-    // ---- phase 1: independent, coalesced loads ----
-    for (int k = tid; k < kGridElems; k += kGridThreads) {
-        const int t = k & 1, cell = k >> 1;
-        const int ci = I0 - 1 + cell % kGridCX, cj = J0 - 1 + cell / kGridCX;
-        sM[k] = (ci >= 0 && ci < a.nx && cj >= 0 && cj < a.ny) ? __ldg(&a.emat[2 * (ci + cj * a.nx) + t]) : -1;
-    }
-    for (int k = tid; k < kGridNX * kGridNY; k += kGridThreads) {
-        const int gi = I0 - 1 + k % kGridNX, gj = J0 - 1 + k / kGridNX;
-        const bool in = gi >= 0 && gi <= a.nx && gj >= 0 && gj <= a.ny;
-        const int node = gi + gj * (a.nx + 1);
-        sX[k / kGridNX][k % kGridNX] = in ? __ldg(&a.x[node]) : 0.0;
-        sY[k / kGridNX][k % kGridNX] = in ? __ldg(&a.y[node]) : 0.0;
-        if (WANT_F) {
-            sU[k / kGridNX][2 * (k % kGridNX)] = in ? a.u[2 * node] : 0.0;
-            sU[k / kGridNX][2 * (k % kGridNX) + 1] = in ? a.u[2 * node + 1] : 0.0;
+template <bool WANT_F, int TR>
+__global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : 2) k_assemble_grid(GridArgs a) {
+    constexpr int kTileThreads = (TR + 1) * kTileElems;  // one staged triangle per thread
+    static_assert((TR + 2) * kTileNX <= kTileThreads && TR * (kTileX + 1) <= kTileThreads &&
+                  2 * TR + 2 <= kTileThreads / 32, "one staged node and row pointer per thread; warps per task");
+    extern __shared__ __align__(16) unsigned char g_tile_smem[];
+    constexpr int kNodes = (TR + 2) * kTileNX;
+    double* sKe = reinterpret_cast<double*>(g_tile_smem);     // [TR + 1][kTileElems][kKeStride]
+    double* sX = sKe + (TR + 1) * kKeRow;                  // [TR + 2][kTileNX]
+    double* sY = sX + kNodes;
+    double* sU = sY + kNodes;                                  // WANT_F: [TR + 2][2 kTileNX]
+    double* sD = sU + (WANT_F ? 2 * kNodes : 0);               // [n_mat][3]: d11, d12, d33
+    int* sM = reinterpret_cast<int*>(sD + 3 * kSweepMaxMat);   // [TR + 1][kTileElems]
+    int* sRp = sM + (TR + 1) * kTileElems;                 // [TR][kTileX + 1]: row pointers
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nx = a.nx, ny = a.ny, NXn = nx + 1;
+    const int I0 = (blockIdx.x % a.strips) * kTileX, J0 = (blockIdx.x / a.strips) * TR;
+    const int R = min(TR, ny + 1 - J0);  // node rows of this tile
+    // ---- phase 1: one load per thread of each staged quantity ----
+    {
+        const int cr = tid / kTileElems, sl = tid % kTileElems;  // slot sl = tile_slot(cc, t)
+        const int ci = I0 - 1 + sl % kTileCells, cj = J0 - 1 + cr;
+        const int m = (ci >= 0 && ci < nx && cj >= 0 && cj < ny) ? __ldg(&a.emat[2 * (ci + cj * nx) + sl / kTileCells])
+                                                                 : -1;
+        double xv = 0.0, yv = 0.0, ux = 0.0, uy = 0.0;
+        const int gi = I0 - 1 + tid % kTileNX, gj = J0 - 1 + tid / kTileNX;
+        const bool in = tid < kNodes && gi >= 0 && gi <= nx && gj >= 0 && gj <= ny;
+        if (in) {
+            const int node = gi + gj * NXn;
+            xv = __ldg(&a.x[node]);
+            yv = __ldg(&a.y[node]);
+            if (WANT_F) {
+                ux = a.u[2 * node];
+                uy = a.u[2 * node + 1];
+            }
         }
-    }
-    if (tid < kGridTY) {
-        const int gj = J0 + tid;
-        const int i1 = min(I0 + kGridTX, a.nx + 1);
-        if (gj <= a.ny) {
-            sRow[tid][0] = __ldg(&a.row_ptr[I0 + gj * (a.nx + 1)]);
-            sRow[tid][1] = __ldg(&a.row_ptr[i1 + gj * (a.nx + 1)]);
-        } else {
-            sRow[tid][0] = sRow[tid][1] = 0;
+        // row_ptr of tile node (I0 + k, J0 + r); k = kTileX gives the row end of the last one
+        const int rk = tid % (kTileX + 1), rr = tid / (kTileX + 1);
+        const int rp = rr < R ? __ldg(&a.row_ptr[min(I0 + rk, NXn) + (J0 + rr) * NXn]) : 0;
+        const double dm = tid < 3 * a.n_mat ? __ldg(&a.dmat[tid]) : 0.0;
+        sM[tid] = m;
+        if (tid < kNodes) {
+            sX[tid] = xv;
+            sY[tid] = yv;
+            if (WANT_F) {
+                sU[2 * tid] = ux;
+                sU[2 * tid + 1] = uy;
+            }
         }
+        if (rr < TR) sRp[tid] = rp;
+        if (tid < 3 * a.n_mat) sD[tid] = dm;
     }
     __syncthreads();
-    // the block-map words of the tile's rows: issued now, used after phase 1b
-    constexpr int kPer = 4;  // blocks per thread and tile row held in registers (rows up to 512 blocks)
-    int wv[kGridTY][kPer];
-#pragma unroll
-    for (int r = 0; r < kGridTY; ++r)
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int q = sRow[r][0] + tid + u * kGridThreads;
-            wv[r][u] = (a.want_K && q < sRow[r][1]) ? __ldg(&a.map[q]) : kTriMapDiag;
-        }
-    // ---- phase 1b: gradients of every staged triangle ----
-    for (int k = tid; k < kGridElems; k += kGridThreads) {
-        if (sM[k] < 0) continue;
-        const int t = k & 1, cell = k >> 1;
-        const int lx = cell % kGridCX, ly = cell / kGridCX;  // staged cell = staged node (lx, ly) corner
-        int di[3], dj[3];
-        grid_tri_nodes(I0 - 1 + lx, J0 - 1 + ly, t, di, dj);
-        const double X0 = sX[ly + dj[0]][lx + di[0]], X1 = sX[ly + dj[1]][lx + di[1]], X2 = sX[ly + dj[2]][lx + di[2]];
-        const double Y0 = sY[ly + dj[0]][lx + di[0]], Y1 = sY[ly + dj[1]][lx + di[1]], Y2 = sY[ly + dj[2]][lx + di[2]];
-        const double J = (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
-        double* g = sG[k];
-        g[0] = Y1 - Y2;
-        g[1] = Y2 - Y0;
-        g[2] = Y0 - Y1;
-        g[3] = X2 - X1;
-        g[4] = X0 - X2;
-        g[5] = X1 - X0;
-        g[6] = 0.5 / J;
+    // ---- phase 2: one staged triangle per thread ----
+    {
+        const int m = sM[tid], sl = tid % kTileElems;
+        if (m >= 0)
+            tile_element(sKe + tid * kKeStride, sX, sY, sD, m, I0, J0, tid / kTileElems, sl % kTileCells, sl / kTileCells);
     }
     __syncthreads();
-    // ---- phase 2: off-diagonal blocks of the tile's rows ----
-    if (a.want_K) {
-#pragma unroll
-        for (int r = 0; r < kGridTY; ++r) {
-            const int q0 = sRow[r][0], q1 = sRow[r][1];
-            for (int q = q0 + tid, u = 0; q < q1; q += kGridThreads, ++u) {
-                int w = 0;
-#pragma unroll
-                for (int uu = 0; uu < kPer; ++uu)
-                    if (uu == u) w = wv[r][uu];
-                if (u >= kPer) w = __ldg(&a.map[q]);
-                if (w & kTriMapDiag) continue;
+    // ---- phase 3: edges, diagonal blocks, f_int ----
+    if (warp < TR) {
+        const int r = warp, gj = J0 + r;
+        if (r < R) {
+            const double* kBelow = sKe + r * kKeRow;        // staged cell row r (global gj - 1)
+            const double* kAbove = sKe + (r + 1) * kKeRow;  // staged cell row r + 1 (global gj)
+            const int rs = r * (kTileX + 1);
+            // horizontal edge A = (gi, gj) - B = (gi + 1, gj), gi = I0 - 1 + lane (tile columns
+            // lane - 1 and lane): the top triangle (t = 1, vertices 2, 1) of the cell below,
+            // the bottom one (t = 0, vertices 0, 1) of the cell above
+            const int gi = I0 - 1 + lane;
+            if (a.want_K && gi >= 0 && gi + 1 <= nx) {
                 double k[4] = {0.0, 0.0, 0.0, 0.0};
-                const int cnt = (w >> 26) & 3;
-                for (int m = 0; m < cnt; ++m) {
-                    const int word = (w >> (13 * m)) & 8191;
-                    const int le = word & 511, v = (word >> 9) & 3, t = (word >> 11) & 3;
-                    grid_add(sG[le], v, t, a.dmat + 3 * sM[le], k);
+                const int eb = tile_slot(lane, 1), ea = tile_slot(lane, 0);
+                if (sM[r * kTileElems + eb] >= 0) {
+                    double t[4] = {0.0, 0.0, 0.0, 0.0};
+                    add_block(kBelow + eb * kKeStride + 8, t);  // block (1, 2): used transposed
+                    k[0] += t[0]; k[1] += t[2]; k[2] += t[1]; k[3] += t[3];
                 }
-                double2* dst = reinterpret_cast<double2*>(a.K + 4 * (size_t)q);
-                dst[0] = make_double2(k[0], k[1]);
-                dst[1] = make_double2(k[2], k[3]);
+                if (sM[(r + 1) * kTileElems + ea] >= 0) add_block(kAbove + ea * kKeStride + 0, k);
+                if (lane >= 1) store_block(a.K, grid_slot(sRp[rs + lane - 1], gi, gj, nx, ny, 5), k[0], k[1], k[2], k[3]);
+                if (lane < kTileX) store_block(a.K, grid_slot(sRp[rs + lane], gi + 1, gj, nx, ny, 3), k[0], k[2], k[1], k[3]);
+            }
+            // diagonal block of node (I0 + lane, gj) over its (at most 8) triangles; zeros in
+            // its enrichment columns
+            const int gn = I0 + lane;
+            if (a.want_K && lane < kTileX && gn <= nx) {
+                const int p = (gn + gj) & 1;
+                double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+                for (int oy = 0; oy < 2; ++oy) {
+                    const double* kb = oy ? kAbove : kBelow;
+#pragma unroll
+                    for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+                        for (int t = 0; t < 2; ++t) {
+                            // staged cell (lane + ox, r + oy), the node at its corner (1 - ox, 1 - oy)
+                            const int e = tile_slot(lane + ox, t);
+                            const int cp = p ^ ((ox + oy) & 1);
+                            const int v = cp ? sweep_vertex(1, t, ox, oy) : sweep_vertex(0, t, ox, oy);
+                            if (v < 0 || sM[(r + oy) * kTileElems + e] < 0) continue;
+                            const double* dv = kb + e * kKeStride + kKeDiag + 3 * v;
+                            d0 += dv[0];
+                            d1 += dv[1];
+                            d2 += dv[2];
+                        }
+                }
+                const int q0 = sRp[rs + lane], q1 = sRp[rs + lane + 1];
+                const unsigned mask = grid_nbr_mask(gn, gj, nx, ny);
+                store_block(a.K, q0 + __popc(mask & 15u), d0, d1, d1, d2);
+                for (int q = q0 + __popc(mask); q < q1; ++q) store_block(a.K, q, 0.0, 0.0, 0.0, 0.0);
             }
         }
-    }
-    // ---- phase 2b / 3: per node, diagonal block and f_int ----
-    const int lx = tid % kGridTX, ly = tid / kGridTX;
-    const int gi = I0 + lx, gj = J0 + ly;
-    if (gi > a.nx || gj > a.ny) return;
-    double kd[4] = {0.0, 0.0, 0.0, 0.0};
-    double fx = 0.0, fy = 0.0;
-    // the four cells around the node: staged cell (lx + ox, ly + oy), ox, oy in {0, 1}
-    for (int oy = 0; oy < 2; ++oy)
-        for (int ox = 0; ox < 2; ++ox)
-            for (int t = 0; t < 2; ++t) {
-                const int le = 2 * ((ly + oy) * kGridCX + (lx + ox)) + t;
-                if (sM[le] < 0) continue;
-                int di[3], dj[3];
-                grid_tri_nodes(gi - 1 + ox, gj - 1 + oy, t, di, dj);
-                // the node is staged node (lx + 1, ly + 1); the cell corner is (lx + ox, ly + oy)
-                int v = -1;
-                for (int m = 0; m < 3; ++m)
-                    if (ox + di[m] == 1 && oy + dj[m] == 1) v = m;
-                if (v < 0) continue;
-                const double* D = a.dmat + 3 * sM[le];
-                grid_add(sG[le], v, v, D, kd);
-                if (WANT_F) {
-                    for (int m = 0; m < 3; ++m) {
-                        double kb[4] = {0.0, 0.0, 0.0, 0.0};
-                        grid_add(sG[le], v, m, D, kb);
-                        const int sx = lx + ox + di[m], sy = ly + oy + dj[m];
-                        const double ux = sU[sy][2 * sx], uy = sU[sy][2 * sx + 1];
-                        fx += kb[0] * ux + kb[1] * uy;
-                        fy += kb[2] * ux + kb[3] * uy;
-                    }
-                }
+    } else if (warp < TR + TR + 1) {
+        // staged cell row s (global gj = J0 - 1 + s) between node rows s - 1 and s
+        const int s = warp - TR, gj = J0 - 1 + s;
+        const double* kc = sKe + s * kKeRow;
+        const bool ownLo = s >= 1 && s - 1 < R, ownHi = s < R;
+        if (a.want_K && gj >= 0 && gj < ny) {
+            // vertical edge A = (gi, gj) - B = (gi, gj + 1), gi = I0 + lane: in the left cell
+            // (parity cl) triangle t = cl with vertices (1, 2) if cl = 0, (0, 1) if cl = 1; in
+            // the right cell triangle t = cl with vertices (0, 2)
+            const int gi = I0 + lane;
+            if (lane < kTileX && gi <= nx) {
+                const int cl = (gi - 1 + gj) & 1;
+                double k[4] = {0.0, 0.0, 0.0, 0.0};
+                const int el = tile_slot(lane, cl), er = tile_slot(lane + 1, cl);
+                if (sM[s * kTileElems + el] >= 0) add_block(kc + el * kKeStride + (cl ? 0 : 8), k);
+                if (sM[s * kTileElems + er] >= 0) add_block(kc + er * kKeStride + 4, k);
+                if (ownLo)
+                    store_block(a.K, grid_slot(sRp[(s - 1) * (kTileX + 1) + lane], gi, gj, nx, ny, 7),
+                                k[0], k[1], k[2], k[3]);
+                if (ownHi)
+                    store_block(a.K, grid_slot(sRp[s * (kTileX + 1) + lane], gi, gj + 1, nx, ny, 1),
+                                k[0], k[2], k[1], k[3]);
             }
-    const int node = gi + gj * (a.nx + 1);
-    if (a.want_K) {
-        double2* dst = reinterpret_cast<double2*>(a.K + 4 * (size_t)__ldg(&a.diag[node]));
-        dst[0] = make_double2(kd[0], kd[1]);
-        dst[1] = make_double2(kd[2], kd[3]);
-    }
-    if (WANT_F) {
-        a.f[2 * node] = fx;
-        a.f[2 * node + 1] = fy;
+            // diagonal of cell (gc, gj), gc = I0 - 1 + lane, parity cp.  cp = 0: A = (gc, gj),
+            // B = (gc + 1, gj + 1), t0 vertices (0, 2), t1 (0, 1).  cp = 1: A = (gc + 1, gj),
+            // B = (gc, gj + 1), t0 vertices (1, 2), t1 (0, 2).
+            const int gc = I0 - 1 + lane;
+            if (gc >= 0 && gc < nx) {
+                const int cp = (gc + gj) & 1;
+                double k[4] = {0.0, 0.0, 0.0, 0.0};
+                const int e0 = tile_slot(lane, 0), e1 = tile_slot(lane, 1);
+                if (sM[s * kTileElems + e0] >= 0) add_block(kc + e0 * kKeStride + (cp ? 8 : 4), k);
+                if (sM[s * kTileElems + e1] >= 0) add_block(kc + e1 * kKeStride + (cp ? 4 : 0), k);
+                const int la = cp ? lane : lane - 1, lb = cp ? lane - 1 : lane;  // tile columns of A, B
+                if (ownLo && la >= 0 && la < kTileX)
+                    store_block(a.K, grid_slot(sRp[(s - 1) * (kTileX + 1) + la], I0 + la, gj, nx, ny, cp ? 6 : 8),
+                                k[0], k[1], k[2], k[3]);
+                if (ownHi && lb >= 0 && lb < kTileX)
+                    store_block(a.K, grid_slot(sRp[s * (kTileX + 1) + lb], I0 + lb, gj + 1, nx, ny, cp ? 2 : 0),
+                                k[0], k[2], k[1], k[3]);
+            }
+        }
+    } else if (WANT_F) {
+        // f_int of the tile's nodes, lane = node column
+        const int gn = I0 + lane;
+        for (int r = 0; r < R; ++r) {
+            const int gj = J0 + r;
+            if (lane >= kTileX || gn > nx) break;
+            const int p = (gn + gj) & 1;
+            double fx = 0.0, fy = 0.0;
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy) {
+                const double* kb = sKe + (r + oy) * kKeRow;
+#pragma unroll
+                for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        const int e = tile_slot(lane + ox, t);
+                        const int cp = p ^ ((ox + oy) & 1);
+                        const int v = cp ? sweep_vertex(1, t, ox, oy) : sweep_vertex(0, t, ox, oy);
+                        if (v < 0 || sM[(r + oy) * kTileElems + e] < 0) continue;
+                        const double* ke = kb + e * kKeStride;
+#pragma unroll
+                        for (int m = 0; m < 3; ++m) {
+                            double k0, k1, k2, k3;
+                            if (m == v) {
+                                const double* dv = ke + kKeDiag + 3 * v;
+                                k0 = dv[0]; k1 = dv[1]; k2 = dv[1]; k3 = dv[2];
+                            } else {
+                                const double* eb = ke + 4 * (v + m - 1);
+                                k0 = eb[0]; k3 = eb[3];
+                                k1 = v < m ? eb[1] : eb[2];
+                                k2 = v < m ? eb[2] : eb[1];
+                            }
+                            const int code = tri_corner(cp, t, m);
+                            const int k = (r + oy + (code >> 1)) * kTileNX + lane + ox + (code & 1);
+                            const double ux = sU[2 * k], uy = sU[2 * k + 1];
+                            fx += k0 * ux + k1 * uy;
+                            fy += k2 * ux + k3 * uy;
+                        }
+                    }
+            }
+            const int node = gn + gj * NXn;
+            a.f[2 * node] = fx;
+            a.f[2 * node + 1] = fy;
+        }
     }
 }
 
-// Grid-tile map words (see k_assemble_grid): per contribution 13 bits --
-// staged element (9 bits), the row node's vertex (2), the column node's
-// vertex (2); two contributions, the count in bits 26-27.
-void build_grid_map(const HostMesh& hm, std::vector<int>& map) {
+// True when every regular row of the block pattern is laid out as
+// k_assemble_grid assumes: the node's grid neighbours (grid_nbr_mask) and
+// itself in ascending order, then only enrichment columns.
+bool grid_pattern_ok(const HostMesh& hm) {
     const int nx = hm.spec.nx, ny = hm.spec.ny;
-    map.assign((size_t)hm.n_blocks(), 0);
+    if ((long long)(nx + 1) * (ny + 1) != hm.n_reg) return false;
     for (int gj = 0; gj <= ny; ++gj)
         for (int gi = 0; gi <= nx; ++gi) {
             const int i = gi + gj * (nx + 1);
-            const int I0 = (gi / kGridTX) * kGridTX, J0 = (gj / kGridTY) * kGridTY;
-            for (int q = hm.row_ptr[i]; q < hm.row_ptr[i + 1]; ++q) {
-                const int j = hm.col[q];
-                if (j == i) {
-                    map[q] = kTriMapDiag;
-                    continue;
-                }
-                if (j >= hm.n_reg) continue;  // enrichment column: zero here
-                int cnt = 0, word = 0;
-                for (int cj = gj - 1; cj <= gj; ++cj)
-                    for (int ci = gi - 1; ci <= gi; ++ci) {
-                        if (ci < 0 || ci >= nx || cj < 0 || cj >= ny) continue;
-                        for (int t = 0; t < 2; ++t) {
-                            const int e = 2 * (ci + cj * nx) + t;
-                            if (hm.elem_cut[e] >= 0) continue;
-                            int v = -1, tc = -1;
-                            for (int m = 0; m < 3; ++m) {
-                                if (hm.conn[3 * e + m] == i) v = m;
-                                if (hm.conn[3 * e + m] == j) tc = m;
-                            }
-                            if (v < 0 || tc < 0) continue;
-                            const int le = 2 * ((cj - (J0 - 1)) * kGridCX + (ci - (I0 - 1))) + t;
-                            if (cnt < 2) word |= (le | (v << 9) | (tc << 11)) << (13 * cnt);
-                            ++cnt;
-                        }
-                    }
-                map[q] = word | (std::min(cnt, 2) << 26);
+            const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+            int q = hm.row_ptr[i];
+            for (int d = 0; d < 9; ++d) {
+                if (!(mask & (1u << d))) continue;
+                const int j = (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
+                if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
+                ++q;
             }
+            for (; q < hm.row_ptr[i + 1]; ++q)
+                if (hm.col[q] < hm.n_reg) return false;
         }
+    return true;
+}
+
+// Lifts k_assemble_grid's dynamic shared-memory limit, once per device and
+// outside any graph capture (called when a context is created).
+void grid_prepare() {
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    cudaFuncSetAttribute(k_assemble_grid<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 3));
+    cudaFuncSetAttribute(k_assemble_grid<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 3));
+    cudaFuncSetAttribute(k_assemble_grid<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 7));
+    cudaFuncSetAttribute(k_assemble_grid<true, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 7));
+    if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
 void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
     GridArgs ga;
     ga.nx = c.hm.spec.nx;
     ga.ny = c.hm.spec.ny;
+    ga.n_mat = (int)c.hm.spec.materials.size();
     ga.row_ptr = c.row_ptr;
     ga.emat = c.grid_emat;
-    ga.map = c.grid_map;
-    ga.diag = c.diag;
     ga.x = c.x;
     ga.y = c.y;
     ga.u = U;
@@ -1030,11 +1197,18 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.K = c.K;
     ga.f = c.F;
     ga.want_K = want_K;
-    const int tiles = ((ga.nx + 1 + kGridTX - 1) / kGridTX) * ((ga.ny + 1 + kGridTY - 1) / kGridTY);
-    if (want_f)
-        k_assemble_grid<true><<<tiles, kGridThreads, 0, s>>>(ga);
-    else
-        k_assemble_grid<false><<<tiles, kGridThreads, 0, s>>>(ga);
+    ga.strips = (ga.nx + 1 + kTileX - 1) / kTileX;
+    const int tr = c.tuning.grid_rows == 3 ? 3 : 7;
+    const int tiles = ga.strips * ((ga.ny + 1 + tr - 1) / tr);
+    const int threads = (tr + 1) * kTileElems;
+    grid_prepare();
+    if (tr == 3) {
+        if (want_f) k_assemble_grid<true, 3><<<tiles, threads, grid_smem_bytes(true, 3), s>>>(ga);
+        else k_assemble_grid<false, 3><<<tiles, threads, grid_smem_bytes(false, 3), s>>>(ga);
+    } else {
+        if (want_f) k_assemble_grid<true, 7><<<tiles, threads, grid_smem_bytes(true, 7), s>>>(ga);
+        else k_assemble_grid<false, 7><<<tiles, threads, grid_smem_bytes(false, 7), s>>>(ga);
+    }
     // rows of enrichment nodes (after the regular ones) get their values from the cut kernel
     const size_t q_enr = (size_t)c.hm.row_ptr[c.n_reg];
     if (want_K && (size_t)c.n_blocks > q_enr)
@@ -1059,7 +1233,7 @@ void launch_tri_tn(const Ctx& c, const RowArgs& ra, cudaStream_t s) {
 }
 
 void launch_tri(const Ctx& c, const RowArgs& ra, bool want_f, cudaStream_t s) {
-    if (c.tuning.tri_grid && c.grid_map) {
+    if (c.tuning.tri_grid && c.grid_emat) {
         launch_grid(c, ra.u, want_f, ra.want_K, s);
         return;
     }
@@ -1210,15 +1384,22 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
                 best.tri_grid = 0;
             }
         }
-    if (c.grid_map) {
+    if (c.grid_emat) {
+        // the structured-grid kernel at both tile heights; ms_tri[4] reports the faster
         c.tuning.tri_grid = 1;
-        const RowArgs ra = row_args(c, c.U, false, true);
-        const float ms = timed([&] { launch_tri(c, ra, false, s); });
-        if (ms_tri) ms_tri[4] = ms;
-        if (ms < best_tri) {
-            best_tri = ms;
-            best.tri_grid = 1;
+        float ms_grid = 0.f;
+        for (int tr : {3, 7}) {
+            c.tuning.grid_rows = tr;
+            const RowArgs ra = row_args(c, c.U, false, true);
+            const float ms = timed([&] { launch_tri(c, ra, false, s); });
+            if (ms_grid == 0.f || ms < ms_grid) ms_grid = ms;
+            if (ms < best_tri) {
+                best_tri = ms;
+                best.tri_grid = 1;
+                best.grid_rows = tr;
+            }
         }
+        if (ms_tri) ms_tri[4] = ms_grid;
     } else if (ms_tri) {
         ms_tri[4] = 0.f;
     }

@@ -57,7 +57,7 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 
 void free_ctx(Ctx& c) {
     mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_map, c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
@@ -117,12 +117,13 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         build_tri_map(hm, kTriTileSizes[v], tm);
         if ((rc = dev_upload(&c.tri_map[v], tm))) return rc;
     }
-    if (hm.spec.nx > 0 && hm.spec.ny > 0 && hm.n_elem == 2 * hm.spec.nx * hm.spec.ny) {
-        // one structured background grid: the 2D-tile triangle kernel applies
-        std::vector<int> gm, em(hm.n_elem);
-        build_grid_map(hm, gm);
+    if (hm.spec.nx > 0 && hm.spec.ny > 0 && hm.n_elem == 2 * hm.spec.nx * hm.spec.ny &&
+        hm.spec.materials.size() <= (size_t)kSweepMaxMat && grid_pattern_ok(hm)) {
+        // one structured background grid: the edge-centric sweep kernel applies
+        std::vector<int> em(hm.n_elem);
         for (int e = 0; e < hm.n_elem; ++e) em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e];
-        if ((rc = dev_upload(&c.grid_map, gm)) || (rc = dev_upload(&c.grid_emat, em))) return rc;
+        if ((rc = dev_upload(&c.grid_emat, em))) return rc;
+        grid_prepare();  // kernel attributes set here, outside any graph capture
     } else {
         c.tuning.tri_grid = 0;
     }
@@ -379,7 +380,8 @@ int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut) {
 
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps) {
     PG_GUARD_CTX(c);
-    if (tri_tile_nodes) *tri_tile_nodes = c->c.tuning.tri_grid ? 128 : kTriTileSizes[c->c.tuning.tri_variant];
+    if (tri_tile_nodes)
+        *tri_tile_nodes = c->c.tuning.tri_grid ? kGridTileX * c->c.tuning.grid_rows : kTriTileSizes[c->c.tuning.tri_variant];
     if (tri_persistent) *tri_persistent = c->c.tuning.tri_persistent;
     if (cut_warps) *cut_warps = c->c.tuning.cut_warps;
     return PG_OK;
@@ -390,13 +392,15 @@ int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent,
     int v = -1;
     for (int k = 0; k < kTriTileVariants; ++k)
         if (kTriTileSizes[k] == tri_tile_nodes) v = k;
-    const bool grid = tri_tile_nodes == 128;
-    if ((v < 0 && !(grid && c->c.grid_map)) || (tri_persistent != 0 && tri_persistent != 1) ||
+    const bool grid = tri_tile_nodes == 3 * kGridTileX || tri_tile_nodes == 7 * kGridTileX;
+    if ((v < 0 && !(grid && c->c.grid_emat)) || (tri_persistent != 0 && tri_persistent != 1) ||
         (cut_warps != 2 && cut_warps != 4 && cut_warps != 8)) {
-        set_error("pg_ctx_set_tuning: tile 32, 64 or 128 (structured grid), persistent 0 or 1, warps 2, 4 or 8");
+        set_error("pg_ctx_set_tuning: tile 32 or 64 (row tiles), 93 or 217 (structured grid, 31 x 3 or 31 x 7 "
+                  "nodes), persistent 0 or 1, warps 2, 4 or 8");
         return PG_ERR_ARG;
     }
     c->c.tuning.tri_grid = grid ? 1 : 0;
+    if (grid) c->c.tuning.grid_rows = tri_tile_nodes / kGridTileX;
     if (!grid) c->c.tuning.tri_variant = v;
     c->c.tuning.tri_persistent = tri_persistent;
     c->c.tuning.cut_warps = cut_warps;

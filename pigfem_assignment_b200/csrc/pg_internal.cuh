@@ -61,12 +61,16 @@ constexpr int kTriTileSizes[kTriTileVariants] = {32, 64};
 constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
-void build_grid_map(const HostMesh& hm, std::vector<int>& map);
+bool grid_pattern_ok(const HostMesh& hm);  // block rows laid out as the structured-grid kernel assumes
+void grid_prepare();  // sets the structured-grid kernel's shared-memory limit on this device
+constexpr int kSweepMaxMat = 16;  // materials the structured-grid kernel stages in shared memory
+constexpr int kGridTileX = 31;    // node columns per structured-grid tile
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // triangle tile size, persistent grid (CTAs walk the tiles) or one CTA per
 // tile, and warps (= cut elements) per CTA of the cut kernel.
 struct AsmTuning {
-    int tri_grid = 1;      // 1: 2D node tiles of the structured grid (when the mesh has one)
+    int tri_grid = 1;      // 1: edge-centric tiles of the structured grid (when the mesh has one)
+    int grid_rows = 7;     // node rows per structured-grid tile: 3 or 7
     int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
     int cut_warps = 4;     // 2, 4 or 8
@@ -90,7 +94,7 @@ struct Ctx {
     int* tri_map[kTriTileVariants] = {};  // one word per block per tile size (see kTriMapDiag)
     AsmTuning tuning;
     int* grid_emat = nullptr;          // structured meshes: material per element, -1 for cut elements
-    int* grid_map = nullptr;           // structured meshes: grid-tile map word per block
+                                       // (set only where the structured-grid kernel applies)
     double* dmat = nullptr;            // 3 per material: D11, D12, D33
     // cut elements, grouped by size class (kCutClassNl), in that order
     int* cut_nodes = nullptr;          // kCutNodeStride per element: 3 parent nodes, then enrichment slots, -1 unused

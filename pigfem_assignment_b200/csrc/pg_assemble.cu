@@ -838,6 +838,11 @@ struct GridArgs {
     int nx, ny;
     int n_mat;                          // materials (at most kSweepMaxMat)
     int strips;                         // tiles across
+    int n_tiles;
+    // enrichment rows, cleared here for the cut-element kernel to add to:
+    // blocks [q_enr, n_blocks) and, with WANT_F, f entries [2 n_reg, 2 n_nodes)
+    long long q_enr, n_blocks;
+    int n_reg, n_nodes;
     const int* __restrict__ row_ptr;
     const int* __restrict__ emat;       // per element: material, -1 for cut elements
     const double* __restrict__ x;
@@ -880,10 +885,11 @@ __device__ __forceinline__ int grid_slot(int row_start, int gi, int gj, int nx, 
     return row_start + __popc(grid_nbr_mask(gi, gj, nx, ny) & ((1u << d) - 1u));
 }
 
+// One 2x2 block as a single 256-bit store (K is a cudaMalloc allocation, so
+// every block is 32-byte aligned): half the store requests of two 128-bit ones.
 __device__ __forceinline__ void store_block(double* K, int q, double k0, double k1, double k2, double k3) {
-    double2* dst = reinterpret_cast<double2*>(K + 4 * (size_t)q);
-    dst[0] = make_double2(k0, k1);
-    dst[1] = make_double2(k2, k3);
+    double* dst = K + 4 * (size_t)q;
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "d"(k0), "d"(k1), "d"(k2), "d"(k3) : "memory");
 }
 
 // adds the stored element block at e (4 values, row-major) to k
@@ -962,6 +968,17 @@ __global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : 2) k_asse
     const int nx = a.nx, ny = a.ny, NXn = nx + 1;
     const int I0 = (blockIdx.x % a.strips) * kTileX, J0 = (blockIdx.x / a.strips) * TR;
     const int R = min(TR, ny + 1 - J0);  // node rows of this tile
+    // this CTA's share of the enrichment rows: cleared (no launch of its own)
+    if (a.want_K) {
+        const long long n = a.n_blocks - a.q_enr, chunk = (n + a.n_tiles - 1) / a.n_tiles;
+        const long long q0 = a.q_enr + blockIdx.x * chunk, q1 = min(q0 + chunk, a.n_blocks);
+        for (long long q = q0 + tid; q < q1; q += kTileThreads) store_block(a.K, (int)q, 0.0, 0.0, 0.0, 0.0);
+    }
+    if (WANT_F) {
+        const int n = 2 * (a.n_nodes - a.n_reg), chunk = (n + a.n_tiles - 1) / a.n_tiles;
+        const int i0 = 2 * a.n_reg + blockIdx.x * chunk, i1 = min(i0 + chunk, 2 * a.n_nodes);
+        for (int i = i0 + tid; i < i1; i += kTileThreads) a.f[i] = 0.0;
+    }
     // ---- phase 1: one load per thread of each staged quantity ----
     {
         const int cr = tid / kTileElems, sl = tid % kTileElems;  // slot sl = tile_slot(cc, t)
@@ -1200,6 +1217,11 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.strips = (ga.nx + 1 + kTileX - 1) / kTileX;
     const int tr = c.tuning.grid_rows == 3 ? 3 : 7;
     const int tiles = ga.strips * ((ga.ny + 1 + tr - 1) / tr);
+    ga.n_tiles = tiles;
+    ga.q_enr = c.hm.row_ptr[c.n_reg];
+    ga.n_blocks = c.n_blocks;
+    ga.n_reg = c.n_reg;
+    ga.n_nodes = c.n_nodes;
     const int threads = (tr + 1) * kTileElems;
     grid_prepare();
     if (tr == 3) {
@@ -1209,12 +1231,6 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
         if (want_f) k_assemble_grid<true, 7><<<tiles, threads, grid_smem_bytes(true, 7), s>>>(ga);
         else k_assemble_grid<false, 7><<<tiles, threads, grid_smem_bytes(false, 7), s>>>(ga);
     }
-    // rows of enrichment nodes (after the regular ones) get their values from the cut kernel
-    const size_t q_enr = (size_t)c.hm.row_ptr[c.n_reg];
-    if (want_K && (size_t)c.n_blocks > q_enr)
-        cudaMemsetAsync(c.K + 4 * q_enr, 0, 4 * ((size_t)c.n_blocks - q_enr) * sizeof(double), s);
-    if (want_f && c.n_nodes > c.n_reg)
-        cudaMemsetAsync(c.F + 2 * (size_t)c.n_reg, 0, 2 * (size_t)(c.n_nodes - c.n_reg) * sizeof(double), s);
 }
 
 template <bool WANT_F, int TN>

@@ -467,8 +467,148 @@ __device__ void cohesive_law(const DevCohLaw& L, double dt, double dmax_c, doubl
 }
 
 // ---------------------------------------------------------------------------
-// Cut-element kernel
+// Cut-element kernels
 // ---------------------------------------------------------------------------
+
+// Quadrature points of a child type on the device (a Tri3 child: one, see upload_tables)
+int device_child_nq(int type) { return type == kChildTri3 ? 1 : child_quadrature(type).nq; }
+
+int device_point_count(int tmpl) {
+    const CutTemplate& T = cut_template(tmpl);
+    int n = 0;
+    for (int c = 0; c < T.n_child; ++c)
+        n += device_child_nq(T.child_n[c] == 3 ? kChildTri3 : T.child_n[c] == 4 ? kChildQuad4
+                             : T.child_n[c] == 5 ? kChildPoly5 : kChildPoly6);
+    return n;
+}
+
+// One quadrature row: point q of a child with nc nodes (local numbers ln,
+// coordinates cx, cy) of a cut element with nl local functions, material dm
+// and parent (Tri3) gradients pbx, pby:
+//   {w det, d11, d12, d33, (gx, gy) of each local function}.
+__device__ __forceinline__ void cut_row(double* row, int nl, const DevChildQuad& Q, int q, int nc, const int* ln,
+                                        const double* cx, const double* cy, const double* dm, const double* pbx,
+                                        const double* pby) {
+    double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxChildNodes; ++k) {
+        if (k < nc) {
+            const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+            J00 += dr * cx[k];
+            J01 += dr * cy[k];
+            J10 += ds * cx[k];
+            J11 += ds * cy[k];
+        }
+    }
+    const double det = J00 * J11 - J01 * J10;
+    const double wgt = det * Q.w[q];
+    // a zero weight (collapsed child) contributes nothing: the reference's
+    // K_el.AXPY is cblas_daxpy, which returns at once for alpha == 0;
+    // the row is zeroed so that no 0/0 gradient enters the sums
+    const bool live = wgt != 0.0;
+    row[0] = live ? wgt : 0.0;
+    row[1] = dm[0];
+    row[2] = dm[1];
+    row[3] = dm[2];
+    for (int j = 0; j < 3; ++j) {
+        row[4 + 2 * j] = pbx[j];
+        row[5 + 2 * j] = pby[j];
+    }
+    for (int j = 3; j < nl; ++j) {
+        row[4 + 2 * j] = 0.0;
+        row[5 + 2 * j] = 0.0;
+    }
+    if (live) {
+        const double idet = 1.0 / det;
+#pragma unroll
+        for (int k = 0; k < kMaxChildNodes; ++k) {
+            if (k < nc && ln[k] >= 3) {
+                const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+                row[4 + 2 * ln[k]] = (J11 * dr - J01 * ds) * idet;
+                row[5 + 2 * ln[k]] = (-J10 * dr + J00 * ds) * idet;
+            }
+        }
+    }
+}
+
+// parent (Tri3) gradients from the three parent coordinates
+__device__ __forceinline__ void parent_gradients(const double* PX, const double* PY, double* pbx, double* pby) {
+    const double PJ = (PX[1] - PX[0]) * (PY[2] - PY[0]) - (PX[2] - PX[0]) * (PY[1] - PY[0]);
+    const double iPJ = 1.0 / PJ;  // one division per element instead of six
+    pbx[0] = (PY[1] - PY[2]) * iPJ;
+    pbx[1] = (PY[2] - PY[0]) * iPJ;
+    pbx[2] = (PY[0] - PY[1]) * iPJ;
+    pby[0] = (PX[2] - PX[1]) * iPJ;
+    pby[1] = (PX[0] - PX[2]) * iPJ;
+    pby[2] = (PX[1] - PX[0]) * iPJ;
+}
+
+// child ch and its point q holding point l of a template
+__device__ __forceinline__ void point_child(const DevTemplate& TG, int l, int& ch, int& q) {
+    ch = 0;
+    q = l;
+    while (q >= g_quad[TG.child_type[ch]].nq) {
+        q -= g_quad[TG.child_type[ch]].nq;
+        ++ch;
+    }
+}
+
+// Quadrature rows of every cut element, one thread per point, all points of
+// all elements at once (a cut element has 1 to ~100 points; one per lane of
+// a per-element warp would leave most lanes idle).
+struct CutPointArgs {
+    int n_pts;
+    int class_off[kCutClasses + 1];
+    int class_stride[kCutClasses];      // row length 4 + 2 NL of each size class
+    const int* __restrict__ pt_elem;
+    const int* __restrict__ pt_q;
+    const long long* __restrict__ row_off;
+    const int* __restrict__ cut_nodes;
+    const int* __restrict__ cut_tmpl;
+    const int* __restrict__ cut_child_mat;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ dmat;
+    double* rows;
+};
+
+__global__ void __launch_bounds__(256) k_cut_points(CutPointArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n_pts) return;
+    const int ci = __ldg(&a.pt_elem[p]), l = __ldg(&a.pt_q[p]);
+    const int tmpl = __ldg(&a.cut_tmpl[ci]);
+    const long long off = __ldg(&a.row_off[ci]);
+    const int* nodes = a.cut_nodes + kCutNodeStride * ci;
+    const int n0 = __ldg(&nodes[0]), n1 = __ldg(&nodes[1]), n2 = __ldg(&nodes[2]);
+    int cls = 0;
+    while (cls < kCutClasses - 1 && ci >= a.class_off[cls + 1]) ++cls;
+    const int stride = a.class_stride[cls];
+    const DevTemplate& TG = g_tmpl[tmpl];
+    int ch, q;
+    point_child(TG, l, ch, q);
+    const int nc = TG.child_n[ch];
+    const int mat = __ldg(&a.cut_child_mat[ci * kMaxChildren + ch]);
+    int ln[kMaxChildNodes];
+    double cx[kMaxChildNodes], cy[kMaxChildNodes];
+#pragma unroll
+    for (int k = 0; k < kMaxChildNodes; ++k) {
+        ln[k] = 0;
+        cx[k] = cy[k] = 0.0;
+        if (k < nc) {  // no loads for the unused node slots
+            ln[k] = TG.child_nodes[ch][k];
+            const int node = __ldg(&nodes[ln[k]]);
+            cx[k] = __ldg(&a.x[node]);
+            cy[k] = __ldg(&a.y[node]);
+        }
+    }
+    const double PX[3] = {__ldg(&a.x[n0]), __ldg(&a.x[n1]), __ldg(&a.x[n2])};
+    const double PY[3] = {__ldg(&a.y[n0]), __ldg(&a.y[n1]), __ldg(&a.y[n2])};
+    double pbx[3], pby[3];
+    parent_gradients(PX, PY, pbx, pby);
+    const double dm[3] = {__ldg(&a.dmat[3 * mat]), __ldg(&a.dmat[3 * mat + 1]), __ldg(&a.dmat[3 * mat + 2])};
+    cut_row(a.rows + off + (long long)l * stride, 3 + TG.n_enr, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm,
+            pbx, pby);
+}
 
 // Per-warp shared tables: one row per quadrature point of the current chunk
 // holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
@@ -497,6 +637,7 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
     const int node = lane < NL ? __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]) : -1;
     const int tmpl = __ldg(&a.cut_tmpl[ci]);
     const int slot0 = __ldg(&a.cut_slot_ptr[ci]);
+    const long long roff = SENS ? 0 : __ldg(&a.row_off[ci]);
     const DevTemplate& T = c_tmpl[tmpl];
     const int nl = 3 + T.n_enr;
     // the element's block slots are needed only at the end: issue their loads now
@@ -507,8 +648,10 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
         slot[k] = (!SENS && a.want_K && lane + 32 * k < nl * nl) ? __ldg(&slots[lane + 32 * k]) : -1;
     if (lane < nl) {
         sL[w][lane] = node;
-        sX[w][lane] = a.x[node];
-        sY[w][lane] = a.y[node];
+        if (SENS || T.n_coh > 0) {  // otherwise the quadrature rows carry all the geometry
+            sX[w][lane] = a.x[node];
+            sY[w][lane] = a.y[node];
+        }
         if (SENS || a.want_f || T.n_coh > 0) {
             sU[w][2 * lane] = a.u[2 * node];
             sU[w][2 * lane + 1] = a.u[2 * node + 1];
@@ -541,13 +684,9 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
         }
         __syncwarp();
     }
-    // parent (Tri3) gradients are constant over the element
-    const double PX0 = sX[w][0], PX1 = sX[w][1], PX2 = sX[w][2];
-    const double PY0 = sY[w][0], PY1 = sY[w][1], PY2 = sY[w][2];
-    const double PJ = (PX1 - PX0) * (PY2 - PY0) - (PX2 - PX0) * (PY1 - PY0);
-    const double iPJ = 1.0 / PJ;  // one division per element instead of six
-    const double pbx[3] = {(PY1 - PY2) * iPJ, (PY2 - PY0) * iPJ, (PY0 - PY1) * iPJ};
-    const double pby[3] = {(PX2 - PX1) * iPJ, (PX0 - PX2) * iPJ, (PX1 - PX0) * iPJ};
+    // parent (Tri3) gradients are constant over the element (SENS: its nodes have moved)
+    double pbx[3] = {0.0, 0.0, 0.0}, pby[3] = {0.0, 0.0, 0.0};
+    if (SENS) parent_gradients(sX[w], sY[w], pbx, pby);
 
     int nq_total = 0;
     for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
@@ -565,57 +704,32 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
     }
 
     for (int qbase = 0; qbase < nq_total; qbase += kQpChunk) {
-        // geometry of one quadrature point per lane, all points in parallel
-        const int l = qbase + lane;
-        if (l < nq_total) {
-            const DevTemplate& TG = g_tmpl[tmpl];
-            int ch = 0, q = l;
-            while (q >= g_quad[TG.child_type[ch]].nq) {
-                q -= g_quad[TG.child_type[ch]].nq;
-                ++ch;
-            }
-            const int nc = TG.child_n[ch];
-            const DevChildQuad& Q = g_quad[TG.child_type[ch]];
-            const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
-            double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
-            for (int k = 0; k < nc; ++k) {
-                const int ln = TG.child_nodes[ch][k];
-                const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
-                J00 += dr * sX[w][ln];
-                J01 += dr * sY[w][ln];
-                J10 += ds * sX[w][ln];
-                J11 += ds * sY[w][ln];
-            }
-            const double det = J00 * J11 - J01 * J10;
-            const double wgt = det * Q.w[q];
-            double* row = sQ[w][lane];
-            // a zero weight (collapsed child) contributes nothing: the reference's
-            // K_el.AXPY is cblas_daxpy, which returns at once for alpha == 0;
-            // the row is zeroed so that no 0/0 gradient enters the sums
-            const bool live = wgt != 0.0;
-            row[0] = live ? wgt : 0.0;
-            row[1] = a.dmat[3 * mat];
-            row[2] = a.dmat[3 * mat + 1];
-            row[3] = a.dmat[3 * mat + 2];
-            for (int j = 0; j < 3; ++j) {
-                row[4 + 2 * j] = pbx[j];
-                row[5 + 2 * j] = pby[j];
-            }
-            for (int j = 3; j < nl; ++j) {
-                row[4 + 2 * j] = 0.0;
-                row[5 + 2 * j] = 0.0;
-            }
-            if (live) {
-                const double idet = 1.0 / det;
-                for (int k = 0; k < nc; ++k) {
-                    const int ln = TG.child_nodes[ch][k];
-                    if (ln >= 3) {
-                        const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
-                        row[4 + 2 * ln] = (J11 * dr - J01 * ds) * idet;
-                        row[5 + 2 * ln] = (-J10 * dr + J00 * ds) * idet;
-                    }
+        if (SENS) {
+            // geometry of one quadrature point per lane, all points in parallel
+            const int l = qbase + lane;
+            if (l < nq_total) {
+                const DevTemplate& TG = g_tmpl[tmpl];
+                int ch, q;
+                point_child(TG, l, ch, q);
+                const int nc = TG.child_n[ch];
+                const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
+                int ln[kMaxChildNodes];
+                double cx[kMaxChildNodes], cy[kMaxChildNodes];
+#pragma unroll
+                for (int k = 0; k < kMaxChildNodes; ++k) {
+                    ln[k] = k < nc ? TG.child_nodes[ch][k] : 0;
+                    cx[k] = sX[w][ln[k]];
+                    cy[k] = sY[w][ln[k]];
                 }
+                const double dm[3] = {a.dmat[3 * mat], a.dmat[3 * mat + 1], a.dmat[3 * mat + 2]};
+                cut_row(sQ[w][lane], nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm, pbx, pby);
             }
+        } else {
+            // the chunk's rows, formed by k_cut_points: one coalesced copy
+            const int n = min(kQpChunk, nq_total - qbase) * kQRow;
+            const double* src = a.rows + roff + (long long)qbase * kQRow;
+            double* dst = &sQ[w][0][0];
+            for (int i = lane; i < n; i += 32) dst[i] = __ldg(&src[i]);
         }
         __syncwarp();
         // each lane integrates its node-pair blocks over the chunk's points
@@ -1318,6 +1432,8 @@ CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool wan
     ca.dmat = c.dmat;
     ca.isv_c = c.isv_c;
     ca.isv_t = c.isv_t;
+    ca.rows = c.cut_rows;
+    ca.row_off = c.cut_row_off;
     ca.coh = c.coh;
     ca.dt = dt;
     ca.K = c.K;
@@ -1327,7 +1443,27 @@ CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool wan
     return ca;
 }
 
-void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+void launch_cut_points(const Ctx& c, cudaStream_t s) {
+    if (c.n_cut_pts > 0) {
+        CutPointArgs pa;
+        pa.n_pts = c.n_cut_pts;
+        for (int k = 0; k <= kCutClasses; ++k) pa.class_off[k] = c.cut_class_off[k];
+        for (int k = 0; k < kCutClasses; ++k) pa.class_stride[k] = 4 + 2 * kCutClassNl[k];
+        pa.pt_elem = c.cut_pt_elem;
+        pa.pt_q = c.cut_pt_q;
+        pa.row_off = c.cut_row_off;
+        pa.cut_nodes = c.cut_nodes;
+        pa.cut_tmpl = c.cut_tmpl;
+        pa.cut_child_mat = c.cut_child_mat;
+        pa.x = c.x;
+        pa.y = c.y;
+        pa.dmat = c.dmat;
+        pa.rows = c.cut_rows;
+        k_cut_points<<<(c.n_cut_pts + 255) / 256, 256, 0, s>>>(pa);
+    }
+}
+
+void launch_cut_classes(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
     for (int k = 0; k < kCutClasses; ++k) {
         const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
         if (n == 0) continue;
@@ -1338,15 +1474,30 @@ void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
     }
 }
 
+void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+    launch_cut_points(c, s);
+    launch_cut_classes(c, ca, s);
+}
+
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
     // nothing to clear: the triangle kernel writes every value of K
     const RowArgs ra = row_args(c, U, want_f, want_K);
+    // the cut elements' quadrature rows depend on the coordinates only: they
+    // are formed on the second stream while the triangle kernel runs
+    const bool fork = c.n_cut_pts > 0;
+    if (fork) {
+        PG_CUDA(cudaEventRecord(c.fork_ev, s));
+        PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
+        launch_cut_points(c, c.aux);
+        PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
+    }
     if (c.timing) cudaEventRecord(c.ea0, s);
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
+    if (fork) PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
     if (c.n_cut > 0) {
-        launch_cut_all(c, cut_args(c, U, dt, want_f, want_K), s);
+        launch_cut_classes(c, cut_args(c, U, dt, want_f, want_K), s);
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);

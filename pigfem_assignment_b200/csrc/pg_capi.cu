@@ -58,7 +58,8 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
-                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off,
+                    c.cut_pt_elem, c.cut_pt_q, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -67,8 +68,9 @@ void free_ctx(Ctx& c) {
     if (c.h_iflags) cudaFreeHost(c.h_iflags);
     if (c.ev0) cudaEventDestroy(c.ev0);
     if (c.ev1) cudaEventDestroy(c.ev1);
-    for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2})
+    for (cudaEvent_t e : {c.ea0, c.ea1, c.ea2, c.fork_ev, c.join_ev})
         if (e) cudaEventDestroy(e);
+    if (c.aux) cudaStreamDestroy(c.aux);
     if (c.stream) cudaStreamDestroy(c.stream);
 }
 
@@ -84,6 +86,9 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     PG_CUDA(cudaSetDevice(device));
     upload_tables();
     PG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    PG_CUDA(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
+    PG_CUDA(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
+    PG_CUDA(cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming));
     PG_CUDA(cudaEventCreate(&c.ev0));
     PG_CUDA(cudaEventCreate(&c.ev1));
     PG_CUDA(cudaEventCreate(&c.ea0));
@@ -171,6 +176,22 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.cut_coh_qp0, qp0))) return rc;
         if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
         if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
+        // quadrature points of every cut element and where its rows go
+        std::vector<long long> roff(nc + 1, 0);
+        std::vector<int> pe, pq;
+        for (int k = 0; k < kCutClasses; ++k)
+            for (int oi = c.cut_class_off[k]; oi < c.cut_class_off[k + 1]; ++oi) {
+                const int nq = device_point_count(tmpl[oi]);
+                for (int q = 0; q < nq; ++q) {
+                    pe.push_back(oi);
+                    pq.push_back(q);
+                }
+                roff[oi + 1] = roff[oi] + (long long)nq * (4 + 2 * kCutClassNl[k]);
+            }
+        c.n_cut_pts = (int)pe.size();
+        if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pt_elem, pe)) ||
+            (rc = dev_upload(&c.cut_pt_q, pq)) || (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
+            return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;

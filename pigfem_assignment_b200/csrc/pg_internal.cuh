@@ -101,6 +101,14 @@ struct Ctx {
     int* cut_tmpl = nullptr;
     int* cut_child_mat = nullptr;      // kMaxChildren per element
     int* cut_coh_qp0 = nullptr;        // first cohesive quadrature point (mesh numbering)
+    // quadrature rows of the cut elements ({w det, d11, d12, d33, (gx, gy) per
+    // local function} per point, 4 + 2 NL doubles for size class NL), formed by
+    // k_cut_points at every assembly and integrated by k_assemble_cut
+    double* cut_rows = nullptr;
+    long long* cut_row_off = nullptr;  // per element (class order): its first row's offset
+    int* cut_pt_elem = nullptr;        // per point: element (class order)
+    int* cut_pt_q = nullptr;           // per point: number within its element
+    int n_cut_pts = 0;
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
@@ -153,6 +161,10 @@ struct Ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // events bracketing the two assembly kernels of the last assembly (rows, cut)
     cudaEvent_t ea0 = nullptr, ea1 = nullptr, ea2 = nullptr;
+    // second stream: the cut elements' quadrature rows are formed on it while
+    // the structured-grid kernel runs (fork / join events)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool timing = false;
 };
 
@@ -185,6 +197,8 @@ struct CutArgs {
     const double* __restrict__ dmat;
     const double* __restrict__ isv_c;
     double* isv_t;
+    const double* __restrict__ rows;          // quadrature rows from k_cut_points (not SENS)
+    const long long* __restrict__ row_off;
     DevCohLaw coh;
     double dt;
     double* K;
@@ -202,6 +216,7 @@ struct CutArgs {
     int which;
 };
 CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K);
+int device_point_count(int tmpl);  // quadrature points of a cut template on the device
 void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s);
 
 // solver entry points (pg_solve.cu)

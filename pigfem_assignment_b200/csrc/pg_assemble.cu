@@ -619,7 +619,7 @@ constexpr int kQpChunk = 32;
 constexpr int kCRow = 10;
 
 template <int NL, int PPL, int W, bool SENS = false>
-__global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / W) k_assemble_cut(CutArgs a) {
+__global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7 ? 16 : 8)) / W) k_assemble_cut(CutArgs a) {
     constexpr int kCutWarps = W;
     constexpr int kQRow = 4 + 2 * NL;
     __shared__ double sX[kCutWarps][NL], sY[kCutWarps][NL];

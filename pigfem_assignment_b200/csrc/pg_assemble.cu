@@ -485,10 +485,11 @@ int device_point_count(int tmpl) {
 // One quadrature row: point q of a child with nc nodes (local numbers ln,
 // coordinates cx, cy) of a cut element with nl local functions, material dm
 // and parent (Tri3) gradients pbx, pby:
-//   {w det, d11, d12, d33, (gx, gy) of each local function}.
-__device__ __forceinline__ void cut_row(double* row, int nl, const DevChildQuad& Q, int q, int nc, const int* ln,
-                                        const double* cx, const double* cy, const double* dm, const double* pbx,
-                                        const double* pby) {
+//   {w det, d11, d12, d33, (gx, gy) of each local function},
+// value i at row[i * rs].
+__device__ __forceinline__ void cut_row(double* row, int rs, int nl, const DevChildQuad& Q, int q, int nc,
+                                        const int* ln, const double* cx, const double* cy, const double* dm,
+                                        const double* pbx, const double* pby) {
     double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
 #pragma unroll
     for (int k = 0; k < kMaxChildNodes; ++k) {
@@ -507,16 +508,16 @@ __device__ __forceinline__ void cut_row(double* row, int nl, const DevChildQuad&
     // the row is zeroed so that no 0/0 gradient enters the sums
     const bool live = wgt != 0.0;
     row[0] = live ? wgt : 0.0;
-    row[1] = dm[0];
-    row[2] = dm[1];
-    row[3] = dm[2];
+    row[rs] = dm[0];
+    row[2 * rs] = dm[1];
+    row[3 * rs] = dm[2];
     for (int j = 0; j < 3; ++j) {
-        row[4 + 2 * j] = pbx[j];
-        row[5 + 2 * j] = pby[j];
+        row[(4 + 2 * j) * rs] = pbx[j];
+        row[(5 + 2 * j) * rs] = pby[j];
     }
     for (int j = 3; j < nl; ++j) {
-        row[4 + 2 * j] = 0.0;
-        row[5 + 2 * j] = 0.0;
+        row[(4 + 2 * j) * rs] = 0.0;
+        row[(5 + 2 * j) * rs] = 0.0;
     }
     if (live) {
         const double idet = 1.0 / det;
@@ -524,8 +525,8 @@ __device__ __forceinline__ void cut_row(double* row, int nl, const DevChildQuad&
         for (int k = 0; k < kMaxChildNodes; ++k) {
             if (k < nc && ln[k] >= 3) {
                 const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
-                row[4 + 2 * ln[k]] = (J11 * dr - J01 * ds) * idet;
-                row[5 + 2 * ln[k]] = (-J10 * dr + J00 * ds) * idet;
+                row[(4 + 2 * ln[k]) * rs] = (J11 * dr - J01 * ds) * idet;
+                row[(5 + 2 * ln[k]) * rs] = (-J10 * dr + J00 * ds) * idet;
             }
         }
     }
@@ -553,19 +554,14 @@ __device__ __forceinline__ void point_child(const DevTemplate& TG, int l, int& c
     }
 }
 
-// Quadrature rows of every cut element, one thread per point, all points of
-// all elements at once (a cut element has 1 to ~100 points; one per lane of
-// a per-element warp would leave most lanes idle).
+// Quadrature rows of every cut element, one thread per point.  What a point
+// needs of the mesh is static, so the host packs it into one 64-byte record
+// (kCutPointInts ints, see build_cut_points): the thread reads its record,
+// then the coordinates it names, and writes its row.  It runs on a second
+// stream beside the structured-grid kernel.
 struct CutPointArgs {
     int n_pts;
-    int class_off[kCutClasses + 1];
-    int class_stride[kCutClasses];      // row length 4 + 2 NL of each size class
-    const int* __restrict__ pt_elem;
-    const int* __restrict__ pt_q;
-    const long long* __restrict__ row_off;
-    const int* __restrict__ cut_nodes;
-    const int* __restrict__ cut_tmpl;
-    const int* __restrict__ cut_child_mat;
+    const int4* __restrict__ pts;
     const double* __restrict__ x;
     const double* __restrict__ y;
     const double* __restrict__ dmat;
@@ -575,39 +571,72 @@ struct CutPointArgs {
 __global__ void __launch_bounds__(256) k_cut_points(CutPointArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n_pts) return;
-    const int ci = __ldg(&a.pt_elem[p]), l = __ldg(&a.pt_q[p]);
-    const int tmpl = __ldg(&a.cut_tmpl[ci]);
-    const long long off = __ldg(&a.row_off[ci]);
-    const int* nodes = a.cut_nodes + kCutNodeStride * ci;
-    const int n0 = __ldg(&nodes[0]), n1 = __ldg(&nodes[1]), n2 = __ldg(&nodes[2]);
-    int cls = 0;
-    while (cls < kCutClasses - 1 && ci >= a.class_off[cls + 1]) ++cls;
-    const int stride = a.class_stride[cls];
-    const DevTemplate& TG = g_tmpl[tmpl];
-    int ch, q;
-    point_child(TG, l, ch, q);
-    const int nc = TG.child_n[ch];
-    const int mat = __ldg(&a.cut_child_mat[ci * kMaxChildren + ch]);
+    const int4* rec = a.pts + 4 * (size_t)p;
+    const int4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3);
+    const int gn[kMaxChildNodes] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y};
+    const int mat = r2.y, lnp = r2.z, meta = r2.w;
+    const int q = meta & 255, type = (meta >> 8) & 3, nc = (meta >> 10) & 7, nl = (meta >> 13) & 15;
+    const long long base = (long long)(unsigned)r3.x | ((long long)r3.y << 32);
+    const int nq_e = r3.z, l = r3.w;
     int ln[kMaxChildNodes];
     double cx[kMaxChildNodes], cy[kMaxChildNodes];
 #pragma unroll
     for (int k = 0; k < kMaxChildNodes; ++k) {
-        ln[k] = 0;
+        ln[k] = (lnp >> (4 * k)) & 15;
         cx[k] = cy[k] = 0.0;
-        if (k < nc) {  // no loads for the unused node slots
-            ln[k] = TG.child_nodes[ch][k];
-            const int node = __ldg(&nodes[ln[k]]);
-            cx[k] = __ldg(&a.x[node]);
-            cy[k] = __ldg(&a.y[node]);
+        if (k < nc) {
+            cx[k] = __ldg(&a.x[gn[k]]);
+            cy[k] = __ldg(&a.y[gn[k]]);
         }
     }
-    const double PX[3] = {__ldg(&a.x[n0]), __ldg(&a.x[n1]), __ldg(&a.x[n2])};
-    const double PY[3] = {__ldg(&a.y[n0]), __ldg(&a.y[n1]), __ldg(&a.y[n2])};
+    const double PX[3] = {__ldg(&a.x[r1.z]), __ldg(&a.x[r1.w]), __ldg(&a.x[r2.x])};
+    const double PY[3] = {__ldg(&a.y[r1.z]), __ldg(&a.y[r1.w]), __ldg(&a.y[r2.x])};
     double pbx[3], pby[3];
     parent_gradients(PX, PY, pbx, pby);
     const double dm[3] = {__ldg(&a.dmat[3 * mat]), __ldg(&a.dmat[3 * mat + 1]), __ldg(&a.dmat[3 * mat + 2])};
-    cut_row(a.rows + off + (long long)l * stride, 3 + TG.n_enr, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm,
-            pbx, pby);
+    cut_row(a.rows + base + l, nq_e, nl, g_quad[type], q, nc, ln, cx, cy, dm, pbx, pby);
+}
+
+// Point records of k_cut_points, per point kCutPointInts ints: global nodes of
+// its child (6, unused ones repeat the first), of the parent (3), the child's
+// material, the child nodes' local numbers (4 bits each), then point q (8
+// bits), child type (2), child node count (3) and the element's local-function
+// count (4), then the element's first row offset in doubles (2 ints, low
+// first), its point count and this point's number within it.  An element's
+// rows are stored value-major (value j of point l at j nq + l), so that the
+// threads of consecutive points write consecutive doubles.  Points are in
+// class order, each element's in the order of its rows.
+void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
+                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out) {
+    out.clear();
+    for (int k = 0; k < kCutClasses; ++k)
+        for (int oi = class_off[k]; oi < class_off[k + 1]; ++oi) {
+            const CutTemplate& T = cut_template(tmpl[oi]);
+            const int* en = &nodes[(size_t)kCutNodeStride * oi];
+            const int nq_e = device_point_count(tmpl[oi]);
+            int l = 0;
+            for (int ch = 0; ch < T.n_child; ++ch) {
+                const int nc = T.child_n[ch];
+                const int type = nc == 3 ? kChildTri3 : nc == 4 ? kChildQuad4 : nc == 5 ? kChildPoly5 : kChildPoly6;
+                int lnp = 0;
+                for (int c = 0; c < nc; ++c) lnp |= T.child_nodes[ch][c] << (4 * c);
+                for (int q = 0; q < device_child_nq(type); ++q, ++l) {
+                    int r[kCutPointInts] = {};
+                    for (int c = 0; c < kMaxChildNodes; ++c) r[c] = en[c < nc ? T.child_nodes[ch][c] : 0];
+                    r[6] = en[0];
+                    r[7] = en[1];
+                    r[8] = en[2];
+                    r[9] = chm[(size_t)kMaxChildren * oi + ch];
+                    r[10] = lnp;
+                    r[11] = q | (type << 8) | (nc << 10) | ((3 + T.n_enr) << 13);
+                    r[12] = (int)(unsigned)(roff[oi] & 0xffffffffLL);
+                    r[13] = (int)(roff[oi] >> 32);
+                    r[14] = nq_e;
+                    r[15] = l;
+                    out.insert(out.end(), r, r + kCutPointInts);
+                }
+            }
+        }
 }
 
 // Per-warp shared tables: one row per quadrature point of the current chunk
@@ -722,14 +751,17 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7
                     cy[k] = sY[w][ln[k]];
                 }
                 const double dm[3] = {a.dmat[3 * mat], a.dmat[3 * mat + 1], a.dmat[3 * mat + 2]};
-                cut_row(sQ[w][lane], nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm, pbx, pby);
+                cut_row(sQ[w][lane], 1, nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm, pbx, pby);
             }
         } else {
-            // the chunk's rows, formed by k_cut_points: one coalesced copy
-            const int n = min(kQpChunk, nq_total - qbase) * kQRow;
-            const double* src = a.rows + roff + (long long)qbase * kQRow;
-            double* dst = &sQ[w][0][0];
-            for (int i = lane; i < n; i += 32) dst[i] = __ldg(&src[i]);
+            // the chunk's rows, formed by k_cut_points (value-major: value j of
+            // point q at j nq_total + q): a coalesced read, transposed into sQ
+            const int nqc = min(kQpChunk, nq_total - qbase);
+            const double* src = a.rows + roff + qbase;
+            for (int i = lane; i < nqc * kQRow; i += 32) {
+                const int j = i / nqc, q = i - j * nqc;
+                sQ[w][q][j] = __ldg(&src[(long long)j * nq_total + q]);
+            }
         }
         __syncwarp();
         // each lane integrates its node-pair blocks over the chunk's points
@@ -1447,14 +1479,7 @@ void launch_cut_points(const Ctx& c, cudaStream_t s) {
     if (c.n_cut_pts > 0) {
         CutPointArgs pa;
         pa.n_pts = c.n_cut_pts;
-        for (int k = 0; k <= kCutClasses; ++k) pa.class_off[k] = c.cut_class_off[k];
-        for (int k = 0; k < kCutClasses; ++k) pa.class_stride[k] = 4 + 2 * kCutClassNl[k];
-        pa.pt_elem = c.cut_pt_elem;
-        pa.pt_q = c.cut_pt_q;
-        pa.row_off = c.cut_row_off;
-        pa.cut_nodes = c.cut_nodes;
-        pa.cut_tmpl = c.cut_tmpl;
-        pa.cut_child_mat = c.cut_child_mat;
+        pa.pts = reinterpret_cast<const int4*>(c.cut_pts);
         pa.x = c.x;
         pa.y = c.y;
         pa.dmat = c.dmat;
@@ -1483,17 +1508,19 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     // nothing to clear: the triangle kernel writes every value of K
     const RowArgs ra = row_args(c, U, want_f, want_K);
     // the cut elements' quadrature rows depend on the coordinates only: they
-    // are formed on the second stream while the triangle kernel runs
+    // are formed on the second stream beside the triangle kernel.  That one is
+    // launched first, so its CTAs are dispatched first and the row kernel's
+    // fill the SMs its last wave leaves free.
     const bool fork = c.n_cut_pts > 0;
+    if (fork) PG_CUDA(cudaEventRecord(c.fork_ev, s));
+    if (c.timing) cudaEventRecord(c.ea0, s);
+    launch_tri(c, ra, want_f, s);
+    PG_CUDA(cudaGetLastError());
     if (fork) {
-        PG_CUDA(cudaEventRecord(c.fork_ev, s));
         PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
         launch_cut_points(c, c.aux);
         PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
     }
-    if (c.timing) cudaEventRecord(c.ea0, s);
-    launch_tri(c, ra, want_f, s);
-    PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
     if (fork) PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
     if (c.n_cut > 0) {

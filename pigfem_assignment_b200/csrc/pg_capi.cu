@@ -58,8 +58,7 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
-                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off,
-                    c.cut_pt_elem, c.cut_pt_q, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -176,21 +175,16 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.cut_coh_qp0, qp0))) return rc;
         if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
         if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
-        // quadrature points of every cut element and where its rows go
+        // where each cut element's quadrature rows go (4 + 2 NL doubles per point)
         std::vector<long long> roff(nc + 1, 0);
-        std::vector<int> pe, pq;
         for (int k = 0; k < kCutClasses; ++k)
-            for (int oi = c.cut_class_off[k]; oi < c.cut_class_off[k + 1]; ++oi) {
-                const int nq = device_point_count(tmpl[oi]);
-                for (int q = 0; q < nq; ++q) {
-                    pe.push_back(oi);
-                    pq.push_back(q);
-                }
-                roff[oi + 1] = roff[oi] + (long long)nq * (4 + 2 * kCutClassNl[k]);
-            }
-        c.n_cut_pts = (int)pe.size();
-        if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pt_elem, pe)) ||
-            (rc = dev_upload(&c.cut_pt_q, pq)) || (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
+            for (int oi = c.cut_class_off[k]; oi < c.cut_class_off[k + 1]; ++oi)
+                roff[oi + 1] = roff[oi] + (long long)device_point_count(tmpl[oi]) * (4 + 2 * kCutClassNl[k]);
+        std::vector<int> pts;
+        build_cut_points(nodes, tmpl, chm, roff, c.cut_class_off, pts);
+        c.n_cut_pts = (int)(pts.size() / kCutPointInts);
+        if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pts, pts)) ||
+            (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
             return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;

@@ -106,8 +106,7 @@ struct Ctx {
     // k_cut_points at every assembly and integrated by k_assemble_cut
     double* cut_rows = nullptr;
     long long* cut_row_off = nullptr;  // per element (class order): its first row's offset
-    int* cut_pt_elem = nullptr;        // per point: element (class order)
-    int* cut_pt_q = nullptr;           // per point: number within its element
+    int* cut_pts = nullptr;            // per point: its record (build_cut_points)
     int n_cut_pts = 0;
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
@@ -217,6 +216,9 @@ struct CutArgs {
 };
 CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K);
 int device_point_count(int tmpl);  // quadrature points of a cut template on the device
+constexpr int kCutPointInts = 16;  // ints per point record of the cut-row kernel
+void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
+                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out);
 void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s);
 
 // solver entry points (pg_solve.cu)

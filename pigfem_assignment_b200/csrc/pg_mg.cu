@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <vector>
 
@@ -274,7 +275,30 @@ __global__ void k_mg_coarse_factor(int nx, int ny, const double* A, const uint8_
         }
         __syncthreads();
     }
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) LU[e] = M[e / n][e % n];
+    // The coarse solve runs once per V-cycle; two substitutions of n steps,
+    // each behind a barrier, cost tens of microseconds.  So the inverse is
+    // formed here (column j solves L U x = P e_j, one thread per column) and
+    // stored transposed in LU (LU[j n + r] = X[r][j]), with the rows and
+    // columns of fixed DOFs zeroed: the solve is then one matrix-vector product.
+    __shared__ double W[kMgCoarseMaxDof][kMgCoarseMaxDof + 1];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double* y = W[j];
+        for (int r = 0; r < n; ++r) y[r] = (sp[r] == j && !fixed[j]) ? 1.0 : 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double yk = y[k];
+            for (int r = k + 1; r < n; ++r) y[r] -= M[r][k] * yk;
+        }
+        for (int k = n - 1; k >= 0; --k) {
+            y[k] = M[k][k] != 0.0 ? y[k] / M[k][k] : 0.0;
+            const double yk = y[k];
+            for (int r = 0; r < k; ++r) y[r] -= M[r][k] * yk;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int j = e / n, r = e - j * n;
+        LU[e] = fixed[r] ? 0.0 : W[j][r];
+    }
     for (int r = threadIdx.x; r < n; r += blockDim.x) piv[r] = sp[r];
 }
 
@@ -318,13 +342,10 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_bsr(int n, const int* __
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_mg_smooth_st(int nx, int ny, const T* __restrict__ A,
-                                                           const T* __restrict__ Dinv, const uint8_t* __restrict__ fixed,
-                                                           const T* __restrict__ b, const T* __restrict__ xin,
-                                                           T* __restrict__ xout, T omega, const int* done, int resid_only) {
-    if (done && done[0]) return;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= (nx + 1) * (ny + 1)) return;
+__device__ __forceinline__ void mg_smooth_node(int i, int nx, int ny, const T* __restrict__ A,
+                                               const T* __restrict__ Dinv, const uint8_t* __restrict__ fixed,
+                                               const T* __restrict__ b, const T* __restrict__ xin, T* __restrict__ xout,
+                                               T omega, int resid_only) {
     T r0 = b[2 * i], r1 = b[2 * i + 1];
     if (xin) {
         const int I = i % (nx + 1), J = i / (nx + 1);
@@ -354,13 +375,21 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_st(int nx, int ny, const
     xout[2 * i + 1] = (xin ? xin[2 * i + 1] : (T)0) + omega * z1;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_mg_smooth_st(int nx, int ny, const T* __restrict__ A,
+                                                           const T* __restrict__ Dinv, const uint8_t* __restrict__ fixed,
+                                                           const T* __restrict__ b, const T* __restrict__ xin,
+                                                           T* __restrict__ xout, T omega, const int* done, int resid_only) {
+    if (done && done[0]) return;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= (nx + 1) * (ny + 1)) return;
+    mg_smooth_node(i, nx, ny, A, Dinv, fixed, b, xin, xout, omega, resid_only);
+}
+
 // bc(a) = mask_c(sum_{i child of a} P_ia rf(i))
 template <typename T>
-__global__ void k_mg_restrict(int nxf, int nyf, int nxc, int nyc, const T* __restrict__ rf, const uint8_t* fixed_c,
-                              T* __restrict__ bc, const int* done) {
-    if (done && done[0]) return;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= (nxc + 1) * (nyc + 1)) return;
+__device__ __forceinline__ void mg_restrict_node(int a, int nxf, int nyf, int nxc, const T* __restrict__ rf,
+                                                 const uint8_t* fixed_c, T* __restrict__ bc) {
     const int Ia = a % (nxc + 1), Ja = a / (nxc + 1);
     const int px = mg_pos(Ia, nxf), py = mg_pos(Ja, nyf);
     T s0 = 0, s1 = 0;
@@ -382,13 +411,19 @@ __global__ void k_mg_restrict(int nxf, int nyf, int nxc, int nyc, const T* __res
     bc[2 * a + 1] = fixed_c[2 * a + 1] ? (T)0 : s1;
 }
 
+template <typename T>
+__global__ void k_mg_restrict(int nxf, int nyf, int nxc, int nyc, const T* __restrict__ rf, const uint8_t* fixed_c,
+                              T* __restrict__ bc, const int* done) {
+    if (done && done[0]) return;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (nxc + 1) * (nyc + 1)) return;
+    mg_restrict_node(a, nxf, nyf, nxc, rf, fixed_c, bc);
+}
+
 // xf(i) += mask_f(sum_a P_ia xc(a)) over the finer grid's nodes
 template <typename T>
-__global__ void k_mg_prolong(int nxf, int nyf, int nxc, const T* __restrict__ xc, const uint8_t* fixed_f,
-                             T* __restrict__ xf, const int* done) {
-    if (done && done[0]) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (nxf + 1) * (nyf + 1)) return;
+__device__ __forceinline__ void mg_prolong_node(int i, int nxf, int nyf, int nxc, const T* __restrict__ xc,
+                                                const uint8_t* fixed_f, T* __restrict__ xf) {
     const int gx = i % (nxf + 1), gy = i / (nxf + 1);
     int Ix[2], Iy[2];
     T wxs[2], wys[2];
@@ -411,27 +446,148 @@ __global__ void k_mg_prolong(int nxf, int nyf, int nxc, const T* __restrict__ xc
     if (!fixed_f[2 * i + 1]) xf[2 * i + 1] += s1;
 }
 
-// x = U^-1 L^-1 P b on the coarsest level, one CTA (fixed DOFs return 0).
 template <typename T>
-__global__ void k_mg_coarse_solve(int n, const double* __restrict__ LU, const int* __restrict__ piv,
-                                  const uint8_t* fixed, const T* __restrict__ b, T* __restrict__ x, const int* done) {
+__global__ void k_mg_prolong(int nxf, int nyf, int nxc, const T* __restrict__ xc, const uint8_t* fixed_f,
+                             T* __restrict__ xf, const int* done) {
     if (done && done[0]) return;
-    __shared__ double y[kMgCoarseMaxDof];
-    for (int r = threadIdx.x; r < n; r += blockDim.x) y[r] = fixed[piv[r]] ? 0.0 : (double)b[piv[r]];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (nxf + 1) * (nyf + 1)) return;
+    mg_prolong_node(i, nxf, nyf, nxc, xc, fixed_f, xf);
+}
+
+// The bottom of the V-cycle in one launch.  Below a few hundred nodes every
+// level's kernels are latency-bound (a launch of one block costs about as
+// much as one of a thousand), and the V-cycle has seven of them per level.
+// So the levels from `first` down to the coarsest run in one CTA, phase after
+// phase between block barriers, in the same order and with the same per-node
+// arithmetic as the per-level kernels: restrict the finer residual,
+// pre-smooth, residual, ..., coarse solve, then prolongate and post-smooth
+// back up.  Their operators, diagonal inverses and vectors are first copied
+// into shared memory (one coalesced pass), so no phase waits on L2; the
+// result of level `first` goes back to its x for the caller's prolongation.
+constexpr int kMgBottomNodes = 300;        // levels at most this size may run in k_mg_bottom
+constexpr int kMgBottomSmem = 200 * 1024;  // and their shared-memory copy at most this many bytes
+constexpr int kMgBottomThreads = 512;
+constexpr int kMgBottomLevels = 8;
+
+template <typename T>
+struct MgBottomArgs {
+    int nlev;                               // levels here, the last the coarsest
+    int nxf, nyf;                           // grid of the finer level restricted first
+    const T* rf;                            // its residual
+    int nx[kMgBottomLevels], ny[kMgBottomLevels];
+    const T* A[kMgBottomLevels];
+    const T* Dinv[kMgBottomLevels];
+    const uint8_t* fixed[kMgBottomLevels];
+    T* x0;                                  // level `first`'s x (global): the result
+    const double* XT;                       // coarsest: transposed masked inverse
+    int nc;
+    T omega;
+};
+
+// shared-memory bytes of k_mg_bottom for levels of n nodes: A (36 n), D^-1 (4 n),
+// b, x, x2, r (2 n each), fixed (2 n bytes, rounded to 8)
+template <typename T>
+size_t mg_bottom_level_bytes(int n) {
+    return (size_t)(36 + 4 + 8) * n * sizeof(T) + (((size_t)2 * n + 7) & ~(size_t)7);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMgBottomThreads) k_mg_bottom(MgBottomArgs<T> a, const int* done) {
+    if (done && done[0]) return;
+    extern __shared__ __align__(16) unsigned char g_bottom_smem[];
+    __shared__ double bs[kMgCoarseMaxDof];
+    const int tid = threadIdx.x;
+    // carve and stage
+    T* sA[kMgBottomLevels];
+    T* sD[kMgBottomLevels];
+    T* sb[kMgBottomLevels];
+    T* sx[kMgBottomLevels];
+    T* sx2[kMgBottomLevels];
+    T* sr[kMgBottomLevels];
+    uint8_t* sf[kMgBottomLevels];
+    unsigned char* p = g_bottom_smem;
+    for (int k = 0; k < a.nlev; ++k) {
+        const int n = (a.nx[k] + 1) * (a.ny[k] + 1);
+        sA[k] = reinterpret_cast<T*>(p);
+        sD[k] = sA[k] + 36 * n;
+        sb[k] = sD[k] + 4 * n;
+        sx[k] = sb[k] + 2 * n;
+        sx2[k] = sx[k] + 2 * n;
+        sr[k] = sx2[k] + 2 * n;
+        sf[k] = reinterpret_cast<uint8_t*>(sr[k] + 2 * n);
+        p = reinterpret_cast<unsigned char*>(sf[k]) + ((2 * n + 7) & ~7);
+        if (k < a.nlev - 1) {
+            for (int q = tid; q < 36 * n; q += kMgBottomThreads) sA[k][q] = a.A[k][q];
+            for (int q = tid; q < 4 * n; q += kMgBottomThreads) sD[k][q] = a.Dinv[k][q];
+        }
+        for (int q = tid; q < 2 * n; q += kMgBottomThreads) sf[k][q] = a.fixed[k][q];
+    }
     __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        const double yk = y[k];
-        for (int r = k + 1 + threadIdx.x; r < n; r += blockDim.x) y[r] -= LU[r * n + k] * yk;
+    int nxf = a.nxf, nyf = a.nyf;
+    const T* rf = a.rf;
+    T* xs[kMgBottomLevels];
+    for (int k = 0; k < a.nlev; ++k) {
+        const int nx = a.nx[k], ny = a.ny[k], n = (nx + 1) * (ny + 1);
+        for (int i = tid; i < n; i += kMgBottomThreads) mg_restrict_node(i, nxf, nyf, nx, rf, sf[k], sb[k]);
         __syncthreads();
+        if (k == a.nlev - 1) {
+            // coarsest: x = XT^T b (fixed DOFs 0)
+            for (int q = tid; q < a.nc; q += kMgBottomThreads) bs[q] = sf[k][q] ? 0.0 : (double)sb[k][q];
+            __syncthreads();
+            for (int q = tid; q < a.nc; q += kMgBottomThreads) {
+                double acc = 0.0;
+                for (int j = 0; j < a.nc; ++j) acc += a.XT[(size_t)j * a.nc + q] * bs[j];
+                sx[k][q] = sf[k][q] ? (T)0 : (T)acc;
+            }
+            __syncthreads();
+            xs[k] = sx[k];
+            break;
+        }
+        T* lc = sx[k];
+        T* la = sx2[k];
+        for (int i = tid; i < n; i += kMgBottomThreads)
+            mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)nullptr, lc,
+                           a.omega, 0);
+        __syncthreads();
+        for (int it = 1; it < kMgNu1; ++it) {
+            for (int i = tid; i < n; i += kMgBottomThreads)
+                mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
+                               a.omega, 0);
+            __syncthreads();
+            T* t = lc;
+            lc = la;
+            la = t;
+        }
+        for (int i = tid; i < n; i += kMgBottomThreads)
+            mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, sr[k],
+                           a.omega, 1);
+        __syncthreads();
+        xs[k] = lc;
+        rf = sr[k];
+        nxf = nx;
+        nyf = ny;
     }
-    for (int k = n - 1; k >= 0; --k) {
-        if (threadIdx.x == 0) y[k] = LU[k * n + k] != 0.0 ? y[k] / LU[k * n + k] : 0.0;
+    for (int k = a.nlev - 2; k >= 0; --k) {
+        const int nx = a.nx[k], ny = a.ny[k], n = (nx + 1) * (ny + 1);
+        T* lc = xs[k];
+        T* la = lc == sx[k] ? sx2[k] : sx[k];
+        for (int i = tid; i < n; i += kMgBottomThreads)
+            mg_prolong_node(i, nx, ny, a.nx[k + 1], (const T*)xs[k + 1], sf[k], lc);
         __syncthreads();
-        const double yk = y[k];
-        for (int r = threadIdx.x; r < k; r += blockDim.x) y[r] -= LU[r * n + k] * yk;
-        __syncthreads();
+        for (int it = 0; it < kMgNu2; ++it) {
+            for (int i = tid; i < n; i += kMgBottomThreads)
+                mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
+                               a.omega, 0);
+            __syncthreads();
+            T* t = lc;
+            lc = la;
+            la = t;
+        }
+        xs[k] = lc;
     }
-    for (int r = threadIdx.x; r < n; r += blockDim.x) x[r] = fixed[r] ? (T)0 : (T)y[r];
+    const int n0 = 2 * (a.nx[0] + 1) * (a.ny[0] + 1);
+    for (int q = tid; q < n0; q += kMgBottomThreads) a.x0[q] = xs[0][q];
 }
 
 __global__ void k_mg_f64_to_f32(int n, const double* __restrict__ a, float* __restrict__ b, const int* done) {
@@ -726,6 +882,16 @@ int modes_build(Ctx& c, MgHierarchy& m) {
 // Structure of the hierarchy (once per mesh).
 int mg_build(Ctx& c) {
     if (c.mg) return PG_OK;
+    {   // k_mg_bottom's shared-memory limit, once per device (before any graph capture)
+        static bool done_dev[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !done_dev[dev]) {
+            PG_CUDA(cudaFuncSetAttribute(k_mg_bottom<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMgBottomSmem));
+            PG_CUDA(cudaFuncSetAttribute(k_mg_bottom<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMgBottomSmem));
+            if (dev >= 0 && dev < 64) done_dev[dev] = true;
+        }
+    }
     const int nx0 = c.hm.spec.nx, ny0 = c.hm.spec.ny;
     if (nx0 < 1 || ny0 < 1) {
         set_error("multigrid: mesh without a structured background grid");
@@ -836,6 +1002,54 @@ int mg_numeric(Ctx& c, bool f32, cudaStream_t s) {
 template <typename T>
 const T* vcycle(Ctx& c, MgHierarchy& m, cudaStream_t s, const T* b0, const int* done);
 
+// First level of the fused bottom (k_mg_bottom): going up from the coarsest,
+// levels of at most kMgBottomNodes nodes while their shared-memory copy stays
+// within kMgBottomSmem bytes (and at most kMgBottomLevels levels).
+template <typename T>
+int mg_bottom_first(const MgHierarchy& m, size_t* smem) {
+    int kb = m.nlev;
+    size_t bytes = mg_bottom_level_bytes<T>(m.L[m.nlev].n);
+    for (int k = m.nlev - 1; k >= 1 && m.nlev - k + 1 <= kMgBottomLevels; --k) {
+        const size_t add = mg_bottom_level_bytes<T>(m.L[k].n);
+        if (m.L[k].n > kMgBottomNodes || bytes + add > (size_t)kMgBottomSmem) break;
+        bytes += add;
+        kb = k;
+    }
+    *smem = bytes;
+    return kb;
+}
+
+// Levels kb .. nlev in one launch; level kb's result ends in its x (xf).
+template <typename T>
+void launch_bottom(MgHierarchy& m, int kb, size_t smem, int nxf, int nyf, const T* rf, cudaStream_t s,
+                   const int* done) {
+    MgBottomArgs<T> a;
+    a.nlev = m.nlev - kb + 1;
+    a.nxf = nxf;
+    a.nyf = nyf;
+    a.rf = rf;
+    for (int k = kb; k <= m.nlev; ++k) {
+        MgLevel& L = m.L[k];
+        const int j = k - kb;
+        a.nx[j] = L.nx;
+        a.ny[j] = L.ny;
+        a.fixed[j] = L.fixed;
+        if constexpr (std::is_same<T, float>::value) {
+            a.A[j] = L.Af;
+            a.Dinv[j] = L.Dinvf;
+        } else {
+            a.A[j] = L.A;
+            a.Dinv[j] = L.Dinv;
+        }
+    }
+    if constexpr (std::is_same<T, float>::value) a.x0 = m.L[kb].xf;
+    else a.x0 = m.L[kb].x;
+    a.XT = m.LU;
+    a.nc = m.nc;
+    a.omega = (T)kMgOmega;
+    k_mg_bottom<T><<<1, kMgBottomThreads, smem, s>>>(a, done);
+}
+
 template <>
 const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const double* b0, const int* done) {
     const int n0 = c.n_nodes;
@@ -856,14 +1070,16 @@ const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const doubl
     const double* rf = m.r0;
     double* xs[kMgMaxLevels + 1];
     xs[0] = cur;
+    size_t bsm = 0;
+    const int kb = mg_bottom_first<double>(m, &bsm);
     for (int k = 1; k <= m.nlev; ++k) {
         MgLevel& L = m.L[k];
-        k_mg_restrict<double><<<nb(L.n), kThreads, 0, s>>>(nxf, nyf, L.nx, L.ny, rf, L.fixed, L.b, done);
-        if (k == m.nlev) {
-            k_mg_coarse_solve<double><<<1, 128, 0, s>>>(m.nc, m.LU, m.piv, L.fixed, L.b, L.x, done);
+        if (k == kb) {  // this level and all coarser ones: one launch
+            launch_bottom<double>(m, kb, bsm, nxf, nyf, rf, s, done);
             xs[k] = L.x;
             break;
         }
+        k_mg_restrict<double><<<nb(L.n), kThreads, 0, s>>>(nxf, nyf, L.nx, L.ny, rf, L.fixed, L.b, done);
         double* lc = L.x;
         double* la = L.x2;
         k_mg_smooth_st<double><<<nb(L.n), kThreads, 0, s>>>(L.nx, L.ny, L.A, L.Dinv, L.fixed, L.b, nullptr, lc, om, done, 0);
@@ -877,7 +1093,7 @@ const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const doubl
         nxf = L.nx;
         nyf = L.ny;
     }
-    for (int k = m.nlev - 1; k >= 0; --k) {
+    for (int k = kb - 1; k >= 0; --k) {
         const MgLevel& Lc = m.L[k + 1];
         if (k == 0) {
             k_mg_prolong<double><<<nb(c.n_reg), kThreads, 0, s>>>(c.hm.spec.nx, c.hm.spec.ny, Lc.nx, xs[1], c.fixed, cur,
@@ -921,14 +1137,16 @@ const float* vcycle<float>(Ctx& c, MgHierarchy& m, cudaStream_t s, const float* 
     const float* rf = m.r0f;
     float* xs[kMgMaxLevels + 1];
     xs[0] = cur;
+    size_t bsm = 0;
+    const int kb = mg_bottom_first<float>(m, &bsm);
     for (int k = 1; k <= m.nlev; ++k) {
         MgLevel& L = m.L[k];
-        k_mg_restrict<float><<<nb(L.n), kThreads, 0, s>>>(nxf, nyf, L.nx, L.ny, rf, L.fixed, L.bf, done);
-        if (k == m.nlev) {
-            k_mg_coarse_solve<float><<<1, 128, 0, s>>>(m.nc, m.LU, m.piv, L.fixed, L.bf, L.xf, done);
+        if (k == kb) {  // this level and all coarser ones: one launch
+            launch_bottom<float>(m, kb, bsm, nxf, nyf, rf, s, done);
             xs[k] = L.xf;
             break;
         }
+        k_mg_restrict<float><<<nb(L.n), kThreads, 0, s>>>(nxf, nyf, L.nx, L.ny, rf, L.fixed, L.bf, done);
         float* lc = L.xf;
         float* la = L.x2f;
         k_mg_smooth_st<float><<<nb(L.n), kThreads, 0, s>>>(L.nx, L.ny, L.Af, L.Dinvf, L.fixed, L.bf, nullptr, lc, om, done, 0);
@@ -942,7 +1160,7 @@ const float* vcycle<float>(Ctx& c, MgHierarchy& m, cudaStream_t s, const float* 
         nxf = L.nx;
         nyf = L.ny;
     }
-    for (int k = m.nlev - 1; k >= 0; --k) {
+    for (int k = kb - 1; k >= 0; --k) {
         const MgLevel& Lc = m.L[k + 1];
         if (k == 0) {
             k_mg_prolong<float><<<nb(c.n_reg), kThreads, 0, s>>>(c.hm.spec.nx, c.hm.spec.ny, Lc.nx, xs[1], c.fixed, cur, done);

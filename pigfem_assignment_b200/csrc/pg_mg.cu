@@ -313,20 +313,16 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_bsr(int n, const int* __
                                                             const T* __restrict__ b, const T* __restrict__ xin,
                                                             T* __restrict__ xout, T omega, const int* done, int resid_only) {
     if (done && done[0]) return;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= n) return;
+    // kRowLanes lanes per block row (bsr_row_group); lane 0 of each group finishes the row
+    const int t = blockIdx.x * kThreads + threadIdx.x;
+    const int i = t / kRowLanes, g = t % kRowLanes;
+    double y0 = 0.0, y1 = 0.0;
+    if (xin) bsr_row_group<T, T>(i, i < n, g, row_ptr, col, K, xin, y0, y1);
+    if (i >= n || g != 0) return;
     T r0 = b[2 * i], r1 = b[2 * i + 1];
     if (xin) {
-        T y0 = 0, y1 = 0;
-        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
-            const int j = col[q];
-            const T* k = K + 4 * (size_t)q;
-            const T x0 = xin[2 * j], x1 = xin[2 * j + 1];
-            y0 += k[0] * x0 + k[1] * x1;
-            y1 += k[2] * x0 + k[3] * x1;
-        }
-        r0 -= y0;
-        r1 -= y1;
+        r0 -= (T)y0;
+        r1 -= (T)y1;
     }
     if (fixed[2 * i]) r0 = 0;
     if (fixed[2 * i + 1]) r1 = 0;
@@ -617,11 +613,13 @@ __global__ void __launch_bounds__(kThreads) k_mgcg_spmv(int n, const int* __rest
                                                         const double* __restrict__ p, const uint8_t* __restrict__ fixed,
                                                         double* __restrict__ q, double* sc, const int* fl) {
     if (fl[0]) return;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
+    // kRowLanes lanes per block row (bsr_row_group); lane 0 of each group finishes the row
+    const int t = blockIdx.x * kThreads + threadIdx.x;
+    const int i = t / kRowLanes, g = t % kRowLanes;
     double part = 0.0;
-    if (i < n) {
-        double y0, y1;
-        bsr_row<double, double>(i, row_ptr, col, K, p, y0, y1);
+    double y0, y1;
+    bsr_row_group<double, double>(i, i < n, g, row_ptr, col, K, p, y0, y1);
+    if (i < n && g == 0) {
         if (fixed[2 * i]) y0 = 0.0;
         if (fixed[2 * i + 1]) y1 = 0.0;
         q[2 * i] = y0;
@@ -1057,14 +1055,14 @@ const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const doubl
     // level 0 pre-smoothing
     double* cur = m.x0;
     double* alt = m.x0b;
-    k_mg_smooth_bsr<double><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, nullptr, cur, om,
+    k_mg_smooth_bsr<double><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, nullptr, cur, om,
                                                           done, 0);
     for (int it = 1; it < kMgNu1; ++it) {
-        k_mg_smooth_bsr<double><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur, alt, om,
+        k_mg_smooth_bsr<double><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur, alt, om,
                                                               done, 0);
         std::swap(cur, alt);
     }
-    k_mg_smooth_bsr<double><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur, m.r0, om,
+    k_mg_smooth_bsr<double><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur, m.r0, om,
                                                           done, 1);
     int nxf = c.hm.spec.nx, nyf = c.hm.spec.ny;
     const double* rf = m.r0;
@@ -1099,7 +1097,7 @@ const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const doubl
             k_mg_prolong<double><<<nb(c.n_reg), kThreads, 0, s>>>(c.hm.spec.nx, c.hm.spec.ny, Lc.nx, xs[1], c.fixed, cur,
                                                                     done);
             for (int it = 0; it < kMgNu2; ++it) {
-                k_mg_smooth_bsr<double><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur,
+                k_mg_smooth_bsr<double><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.K, c.minv, c.fixed, b0, cur,
                                                                       alt, om, done, 0);
                 std::swap(cur, alt);
             }
@@ -1124,14 +1122,14 @@ const float* vcycle<float>(Ctx& c, MgHierarchy& m, cudaStream_t s, const float* 
     const float om = (float)kMgOmega;
     float* cur = m.x0f;
     float* alt = m.x0bf;
-    k_mg_smooth_bsr<float><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, nullptr, cur, om,
+    k_mg_smooth_bsr<float><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, nullptr, cur, om,
                                                          done, 0);
     for (int it = 1; it < kMgNu1; ++it) {
-        k_mg_smooth_bsr<float><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur, alt, om,
+        k_mg_smooth_bsr<float><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur, alt, om,
                                                              done, 0);
         std::swap(cur, alt);
     }
-    k_mg_smooth_bsr<float><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur, m.r0f, om,
+    k_mg_smooth_bsr<float><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur, m.r0f, om,
                                                          done, 1);
     int nxf = c.hm.spec.nx, nyf = c.hm.spec.ny;
     const float* rf = m.r0f;
@@ -1165,7 +1163,7 @@ const float* vcycle<float>(Ctx& c, MgHierarchy& m, cudaStream_t s, const float* 
         if (k == 0) {
             k_mg_prolong<float><<<nb(c.n_reg), kThreads, 0, s>>>(c.hm.spec.nx, c.hm.spec.ny, Lc.nx, xs[1], c.fixed, cur, done);
             for (int it = 0; it < kMgNu2; ++it) {
-                k_mg_smooth_bsr<float><<<nb(n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur,
+                k_mg_smooth_bsr<float><<<nb(kRowLanes * n0), kThreads, 0, s>>>(n0, c.row_ptr, c.col, c.Kf, m.Dinv0f, c.fixed, b0, cur,
                                                                      alt, om, done, 0);
                 std::swap(cur, alt);
             }
@@ -1268,7 +1266,7 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
         PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int it = 0; it < kChunk; ++it) {
             k_mgcg_s1<<<1, 1, 0, s>>>(m.sc, m.fl);
-            k_mgcg_spmv<<<nb(n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.p, c.fixed, c.q, m.sc, m.fl);
+            k_mgcg_spmv<<<nb(kRowLanes * n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.p, c.fixed, c.q, m.sc, m.fl);
             k_mgcg_update<<<nb(nd), kThreads, 0, s>>>(nd, c.dx, c.r, c.p, c.q, m.sc, m.fl);
             k_mgcg_s2<<<1, 1, 0, s>>>(m.sc, m.fl);
             mg_apply(c, m, f32, s, c.r, c.z, m.fl);

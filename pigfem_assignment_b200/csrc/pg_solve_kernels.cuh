@@ -51,6 +51,49 @@ __device__ __forceinline__ void bsr_row(int i, const int* __restrict__ row_ptr, 
     }
 }
 
+// One 2x2 block of K (row-major), read-only: one 256-bit load for FP64 blocks
+// (K is a cudaMalloc allocation, so every block is 32-byte aligned), one
+// 128-bit load for FP32 ones.
+__device__ __forceinline__ void load_block(const double* p, double& a, double& b, double& c, double& d) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+__device__ __forceinline__ void load_block(const float* p, double& a, double& b, double& c, double& d) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    a = v.x;
+    b = v.y;
+    c = v.z;
+    d = v.w;
+}
+
+// Block row i of K times x with kRowLanes lanes per row: lane g of the row's
+// group takes blocks r0 + g, r0 + g + kRowLanes, ..., so a group's loads of K
+// are contiguous; two shuffles give every lane of the group the row's sum.
+// Every lane of the warp must call it (valid = false for padding rows).
+constexpr int kRowLanes = 4;
+template <typename MT, typename VT>
+__device__ __forceinline__ void bsr_row_group(int i, bool valid, int g, const int* __restrict__ row_ptr,
+                                              const int* __restrict__ col, const MT* __restrict__ K,
+                                              const VT* __restrict__ x, double& y0, double& y1) {
+    double a0 = 0.0, a1 = 0.0;
+    if (valid) {
+        const int r1 = __ldg(&row_ptr[i + 1]);
+        for (int k = __ldg(&row_ptr[i]) + g; k < r1; k += kRowLanes) {
+            const int j = __ldg(&col[k]);
+            double b0, b1, b2, b3;
+            load_block(K + 4 * (size_t)k, b0, b1, b2, b3);
+            const double x0 = (double)x[2 * j], x1 = (double)x[2 * j + 1];
+            a0 += b0 * x0 + b1 * x1;
+            a1 += b2 * x0 + b3 * x1;
+        }
+    }
+    a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+    a0 += __shfl_xor_sync(0xffffffffu, a0, 2);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
+    y0 = a0;
+    y1 = a1;
+}
+
 template <typename MT, typename VT>
 __global__ void __launch_bounds__(kThreads) k_spmv_plain(int n, const int* __restrict__ row_ptr, const int* __restrict__ col,
                                                           const MT* __restrict__ K, const VT* __restrict__ x,

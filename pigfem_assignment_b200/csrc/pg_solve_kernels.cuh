@@ -68,8 +68,11 @@ __device__ __forceinline__ void load_block(const float* p, double& a, double& b,
 // Block row i of K times x with kRowLanes lanes per row: lane g of the row's
 // group takes blocks r0 + g, r0 + g + kRowLanes, ..., so a group's loads of K
 // are contiguous; two shuffles give every lane of the group the row's sum.
+// A lane issues the column and block loads of kRowUnroll of its blocks at
+// once, then their x gathers (a row of up to 12 blocks: one round of each).
 // Every lane of the warp must call it (valid = false for padding rows).
 constexpr int kRowLanes = 4;
+constexpr int kRowUnroll = 3;
 template <typename MT, typename VT>
 __device__ __forceinline__ void bsr_row_group(int i, bool valid, int g, const int* __restrict__ row_ptr,
                                               const int* __restrict__ col, const MT* __restrict__ K,
@@ -77,13 +80,27 @@ __device__ __forceinline__ void bsr_row_group(int i, bool valid, int g, const in
     double a0 = 0.0, a1 = 0.0;
     if (valid) {
         const int r1 = __ldg(&row_ptr[i + 1]);
-        for (int k = __ldg(&row_ptr[i]) + g; k < r1; k += kRowLanes) {
-            const int j = __ldg(&col[k]);
-            double b0, b1, b2, b3;
-            load_block(K + 4 * (size_t)k, b0, b1, b2, b3);
-            const double x0 = (double)x[2 * j], x1 = (double)x[2 * j + 1];
-            a0 += b0 * x0 + b1 * x1;
-            a1 += b2 * x0 + b3 * x1;
+        for (int base = __ldg(&row_ptr[i]) + g; base < r1; base += kRowLanes * kRowUnroll) {
+            int j[kRowUnroll];
+            double b[kRowUnroll][4];
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; ++u) {
+                const int k = base + u * kRowLanes;
+                j[u] = -1;
+                b[u][0] = b[u][1] = b[u][2] = b[u][3] = 0.0;
+                if (k < r1) {
+                    j[u] = __ldg(&col[k]);
+                    load_block(K + 4 * (size_t)k, b[u][0], b[u][1], b[u][2], b[u][3]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; ++u) {
+                if (j[u] >= 0) {
+                    const double x0 = (double)x[2 * j[u]], x1 = (double)x[2 * j[u] + 1];
+                    a0 += b[u][0] * x0 + b[u][1] * x1;
+                    a1 += b[u][2] * x0 + b[u][3] * x1;
+                }
+            }
         }
     }
     a0 += __shfl_xor_sync(0xffffffffu, a0, 1);

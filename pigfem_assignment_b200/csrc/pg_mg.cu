@@ -337,7 +337,9 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_bsr(int n, const int* __
     xout[2 * i + 1] = (xin ? xin[2 * i + 1] : (T)0) + omega * z1;
 }
 
-template <typename T>
+// GLOBAL: A and Dinv are in global memory and read as whole 2x2 blocks
+// (load_block); otherwise (shared memory) element by element.
+template <typename T, bool GLOBAL>
 __device__ __forceinline__ void mg_smooth_node(int i, int nx, int ny, const T* __restrict__ A,
                                                const T* __restrict__ Dinv, const uint8_t* __restrict__ fixed,
                                                const T* __restrict__ b, const T* __restrict__ xin, T* __restrict__ xout,
@@ -351,9 +353,17 @@ __device__ __forceinline__ void mg_smooth_node(int i, int nx, int ny, const T* _
             if (gx < 0 || gx > nx || gy < 0 || gy > ny) continue;
             const int j = gx + gy * (nx + 1);
             const T* k = A + 36 * (size_t)i + 4 * s;
+            T k0, k1, k2, k3;
+            if constexpr (GLOBAL) {
+                double d0, d1, d2, d3;
+                load_block(k, d0, d1, d2, d3);
+                k0 = (T)d0; k1 = (T)d1; k2 = (T)d2; k3 = (T)d3;
+            } else {
+                k0 = k[0]; k1 = k[1]; k2 = k[2]; k3 = k[3];
+            }
             const T x0 = xin[2 * j], x1 = xin[2 * j + 1];
-            y0 += k[0] * x0 + k[1] * x1;
-            y1 += k[2] * x0 + k[3] * x1;
+            y0 += k0 * x0 + k1 * x1;
+            y1 += k2 * x0 + k3 * x1;
         }
         r0 -= y0;
         r1 -= y1;
@@ -366,7 +376,15 @@ __device__ __forceinline__ void mg_smooth_node(int i, int nx, int ny, const T* _
         return;
     }
     const T* m = Dinv + 4 * (size_t)i;
-    const T z0 = m[0] * r0 + m[1] * r1, z1 = m[2] * r0 + m[3] * r1;
+    T m0, m1, m2, m3;
+    if constexpr (GLOBAL) {
+        double d0, d1, d2, d3;
+        load_block(m, d0, d1, d2, d3);
+        m0 = (T)d0; m1 = (T)d1; m2 = (T)d2; m3 = (T)d3;
+    } else {
+        m0 = m[0]; m1 = m[1]; m2 = m[2]; m3 = m[3];
+    }
+    const T z0 = m0 * r0 + m1 * r1, z1 = m2 * r0 + m3 * r1;
     xout[2 * i] = (xin ? xin[2 * i] : (T)0) + omega * z0;
     xout[2 * i + 1] = (xin ? xin[2 * i + 1] : (T)0) + omega * z1;
 }
@@ -379,7 +397,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_st(int nx, int ny, const
     if (done && done[0]) return;
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= (nx + 1) * (ny + 1)) return;
-    mg_smooth_node(i, nx, ny, A, Dinv, fixed, b, xin, xout, omega, resid_only);
+    mg_smooth_node<T, true>(i, nx, ny, A, Dinv, fixed, b, xin, xout, omega, resid_only);
 }
 
 // bc(a) = mask_c(sum_{i child of a} P_ia rf(i))
@@ -543,12 +561,12 @@ __global__ void __launch_bounds__(kMgBottomThreads) k_mg_bottom(MgBottomArgs<T> 
         T* lc = sx[k];
         T* la = sx2[k];
         for (int i = tid; i < n; i += kMgBottomThreads)
-            mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)nullptr, lc,
+            mg_smooth_node<T, false>(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)nullptr, lc,
                            a.omega, 0);
         __syncthreads();
         for (int it = 1; it < kMgNu1; ++it) {
             for (int i = tid; i < n; i += kMgBottomThreads)
-                mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
+                mg_smooth_node<T, false>(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
                                a.omega, 0);
             __syncthreads();
             T* t = lc;
@@ -556,7 +574,7 @@ __global__ void __launch_bounds__(kMgBottomThreads) k_mg_bottom(MgBottomArgs<T> 
             la = t;
         }
         for (int i = tid; i < n; i += kMgBottomThreads)
-            mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, sr[k],
+            mg_smooth_node<T, false>(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, sr[k],
                            a.omega, 1);
         __syncthreads();
         xs[k] = lc;
@@ -573,7 +591,7 @@ __global__ void __launch_bounds__(kMgBottomThreads) k_mg_bottom(MgBottomArgs<T> 
         __syncthreads();
         for (int it = 0; it < kMgNu2; ++it) {
             for (int i = tid; i < n; i += kMgBottomThreads)
-                mg_smooth_node(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
+                mg_smooth_node<T, false>(i, nx, ny, (const T*)sA[k], (const T*)sD[k], sf[k], (const T*)sb[k], (const T*)lc, la,
                                a.omega, 0);
             __syncthreads();
             T* t = lc;

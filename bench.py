@@ -47,6 +47,9 @@ def parse():
                     help="keep the default launch shapes (profiling runs: timings under a profiler mislead the tuner)")
     ap.add_argument("--batch-rves", type=int, default=512)
     ap.add_argument("--no-sensitivity", action="store_true")
+    ap.add_argument("--profile-range", choices=["load_step"], default=None,
+                    help="bracket the timed FP64 multigrid solve of the load step with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--viscosity", type=float, default=200.0,
                     help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
     return ap.parse_args()
@@ -357,12 +360,18 @@ def run_b200_arm(args):
                 ctx.set_vector(0, np.zeros(info["n_dof"]))
                 torch.cuda.synchronize()
                 a, b = assemble_timed()
+                profiled = args.profile_range == "load_step" and name == "plain_fp64" and rep == 1
+                if profiled:
+                    torch.cuda.profiler.start()
                 try:
                     st = solver.solve_linear()
                 except _lib.PgError as ex:
                     st = solver.stats
                     status = str(ex)
                     break
+                if profiled:
+                    torch.cuda.synchronize()
+                    torch.cuda.profiler.stop()
                 if rep == 0:
                     first_ms = 1e3 * st.seconds
             load[name] = {"status": status, "ms": a + b + 1e3 * st.seconds, "assemble_ms": a + b, "solve_ms": 1e3 * st.seconds,

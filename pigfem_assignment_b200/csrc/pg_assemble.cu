@@ -982,7 +982,7 @@ __host__ __device__ constexpr int tile_slot(int cc, int t) { return t * kTileCel
 
 struct GridArgs {
     int nx, ny;
-    int n_mat;                          // materials (at most kSweepMaxMat)
+    int n_mat;                          // materials (at most kGridMaxMat)
     int strips;                         // tiles across
     int n_tiles;
     // enrichment rows, cleared here for the cut-element kernel to add to:
@@ -1048,7 +1048,7 @@ __device__ __forceinline__ void add_block(const double* e, double k[4]) {
 
 size_t grid_smem_bytes(bool want_f, int tr) {
     const size_t nodes = (size_t)(tr + 2) * kTileNX;
-    return sizeof(double) * ((tr + 1) * (size_t)kKeRow + 2 * nodes + (want_f ? 2 * nodes : 0) + 3 * kSweepMaxMat) +
+    return sizeof(double) * ((tr + 1) * (size_t)kKeRow + 2 * nodes + (want_f ? 2 * nodes : 0) + 3 * kGridMaxMat) +
            sizeof(int) * ((tr + 1) * (size_t)kTileElems + tr * (kTileX + 1));
 }
 
@@ -1108,7 +1108,7 @@ __global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : 2) k_asse
     double* sY = sX + kNodes;
     double* sU = sY + kNodes;                                  // WANT_F: [TR + 2][2 kTileNX]
     double* sD = sU + (WANT_F ? 2 * kNodes : 0);               // [n_mat][3]: d11, d12, d33
-    int* sM = reinterpret_cast<int*>(sD + 3 * kSweepMaxMat);   // [TR + 1][kTileElems]
+    int* sM = reinterpret_cast<int*>(sD + 3 * kGridMaxMat);   // [TR + 1][kTileElems]
     int* sRp = sM + (TR + 1) * kTileElems;                 // [TR][kTileX + 1]: row pointers
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nx = a.nx, ny = a.ny, NXn = nx + 1;

@@ -122,7 +122,7 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.tri_map[v], tm))) return rc;
     }
     if (hm.spec.nx > 0 && hm.spec.ny > 0 && hm.n_elem == 2 * hm.spec.nx * hm.spec.ny &&
-        hm.spec.materials.size() <= (size_t)kSweepMaxMat && grid_pattern_ok(hm)) {
+        hm.spec.materials.size() <= (size_t)kGridMaxMat && grid_pattern_ok(hm)) {
         // one structured background grid: the edge-centric sweep kernel applies
         std::vector<int> em(hm.n_elem);
         for (int e = 0; e < hm.n_elem; ++e) em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e];

@@ -63,7 +63,7 @@ constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
 bool grid_pattern_ok(const HostMesh& hm);  // block rows laid out as the structured-grid kernel assumes
 void grid_prepare();  // sets the structured-grid kernel's shared-memory limit on this device
-constexpr int kSweepMaxMat = 16;  // materials the structured-grid kernel stages in shared memory
+constexpr int kGridMaxMat = 16;  // materials the structured-grid kernel stages in shared memory
 constexpr int kGridTileX = 31;    // node columns per structured-grid tile
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // triangle tile size, persistent grid (CTAs walk the tiles) or one CTA per

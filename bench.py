@@ -483,7 +483,7 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
     # training trajectories use the reference's SNES tests (rtol of the predictor, stol)
     xs, ts = [], []
     for k in range(n_train):
-        x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.2, seed=k,
+        x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.0, seed=k,
                                      device=local, newton=dict(precond=_lib.PG_PREC_MG, lin_max_iter=1000))
         xs.append(x)
         ts.append(t)

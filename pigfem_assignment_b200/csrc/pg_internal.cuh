@@ -239,8 +239,9 @@ void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
 // learned predictor (pg_predict.cu)
 int launch_features(Ctx& c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc, float* X,
                     cudaStream_t s);
+// gate: features of the step (k_features) to apply Y only at enrichment and damaged nodes; null: everywhere
 int launch_apply(Ctx& c, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y, double* U,
-                 cudaStream_t s);
+                 cudaStream_t s, const float* gate = nullptr);
 double predictor_app(const Ctx& c);
 double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s);
 

@@ -239,7 +239,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                 // the candidate (linear included) with the smallest residual starts Newton
                 double best = res_lin, best_a = 0.0;
                 for (double a : {1.0, 0.5, 0.25}) {
-                    launch_apply(c, c.Uprev, c.Uold, ratio, a * s_inc, c.featY, c.U, s);
+                    launch_apply(c, c.Uprev, c.Uold, ratio, a * s_inc, c.featY, c.U, s, c.featX);
                     k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
                     const double ra = std::sqrt(predictor_residual(c, c.U, dt, s));
                     if (a == 1.0) res_mlp = ra;
@@ -251,7 +251,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                 if (best_a > 0.0) {
                     used = PG_PREDICT_LEARNED;
                     if (best_a != 0.25) {
-                        launch_apply(c, c.Uprev, c.Uold, ratio, best_a * s_inc, c.featY, c.U, s);
+                        launch_apply(c, c.Uprev, c.Uold, ratio, best_a * s_inc, c.featY, c.U, s, c.featX);
                         k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
                     }
                 } else {

@@ -67,12 +67,21 @@ __global__ void k_targets(int nd, const uint8_t* __restrict__ fixed, const doubl
     T[i] = fixed[i] ? 0.f : (float)((Un1[i] - lin) / s_inc);
 }
 
+// gate (features, may be null): the correction is applied only at nodes that
+// are enrichment nodes or carry cohesive damage (features 6 and 8); in the
+// elastic bulk the linear extrapolation is already close, and any network
+// output there only adds error.
 __global__ void k_apply(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ Un,
                         const double* __restrict__ Unm1, double ratio, double s_inc, const float* __restrict__ Y,
-                        double* __restrict__ U) {
+                        const float* __restrict__ gate, double* __restrict__ U) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= nd || fixed[i]) return;
-    U[i] = Un[i] + ratio * (Un[i] - Unm1[i]) + (Y ? s_inc * (double)Y[i] : 0.0);
+    bool on = Y != nullptr;
+    if (on && gate) {
+        const float* f = gate + 16 * (size_t)(i >> 1);
+        on = f[6] > 0.5f || f[8] > 0.f;
+    }
+    U[i] = Un[i] + ratio * (Un[i] - Unm1[i]) + (on ? s_inc * (double)Y[i] : 0.0);
 }
 
 // node -> cohesive quadrature points (for the damage feature)
@@ -125,8 +134,8 @@ int launch_features(Ctx& c, const double* Un, const double* Unm1, double t_frac,
 }
 
 int launch_apply(Ctx& c, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y, double* U,
-                 cudaStream_t s) {
-    k_apply<<<nblk(c.n_dof), kThreads, 0, s>>>(c.n_dof, c.fixed, Un, Unm1, ratio, s_inc, Y, U);
+                 cudaStream_t s, const float* gate) {
+    k_apply<<<nblk(c.n_dof), kThreads, 0, s>>>(c.n_dof, c.fixed, Un, Unm1, ratio, s_inc, Y, gate, U);
     PG_CUDA(cudaGetLastError());
     return PG_OK;
 }

@@ -7,6 +7,10 @@ extrapolation of every node's displacement at the start of a load step:
 
     U_pred = U_n + ratio (U_n - U_{n-1}) + s * MLP(features)
 
+at enrichment nodes and nodes with cohesive damage (elsewhere the linear
+extrapolation is kept: in the elastic bulk it is already close, and any
+network output there only adds error).
+
 Training data are trajectories the GPU Newton solver itself generates
 (features at the start of step n+1, targets from the converged U_{n+1}).
 Inside pg_solve_nonlinear (predictor PG_PREDICT_LEARNED) the plain linear
@@ -80,13 +84,14 @@ def _dev_ptrs(ctx):
     return C.cast(U, C.c_void_p).value
 
 
-def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction: float = 0.1, seed: int = 0,
+def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction: float = 0.0, seed: int = 0,
                        device: int = 0, rtol: float = 1e-8, newton: dict = None
                        ) -> Tuple["object", "object", List[_lib.StepStats]]:
     """Runs the first `n_train_steps` of `n_steps` equal load steps of `rve`
     with the linear predictor and returns (features, targets) of the nodes kept
-    (every enrichment node, every node with cohesive damage, a random
-    `keep_fraction` of the others), plus the step records.  `newton` holds
+    (every enrichment node, every node with cohesive damage, and a random
+    `keep_fraction` of the others; the Newton solver applies the network's
+    correction at the first two kinds only), plus the step records.  `newton` holds
     further pg_newton_cfg fields (e.g. the preconditioner)."""
     torch = _torch()
     prob = ProblemNonlinearStructural(rve, device=device)

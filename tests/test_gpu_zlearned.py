@@ -34,7 +34,7 @@ def test_learned_warm_start_trains_and_helps():
     n_steps, n_train = 20, 10
     xs, ts = [], []
     for seed in range(4):
-        x, t, recs = trajectory_samples(small_rve(100 + seed), n_steps, n_train, keep_fraction=0.2, seed=seed)
+        x, t, recs = trajectory_samples(small_rve(100 + seed), n_steps, n_train, keep_fraction=0.0, seed=seed)
         assert len(recs) == n_train, [(r.t_frac, r.reason) for r in recs]
         xs.append(x)
         ts.append(t)

@@ -284,7 +284,7 @@ def run_b200_arm(args):
         _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
     t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
-    tri_kernel = "k_assemble_grid" if t_tile.value in (93, 217) else "k_assemble_tri"
+    tri_kernel = "k_assemble_grid" if t_tile.value in (93, 124, 217) else "k_assemble_tri"
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
               "ms_tri_rows32_rows32p_rows64_rows64p_gridsweep": [round(v, 4) for v in ms_tri],
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}

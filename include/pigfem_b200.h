@@ -288,13 +288,13 @@ int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double
  * `reps` launches each) and keeps the fastest of each for later assemblies:
  * ms_tri[5] = triangle kernel gathering over 32 / 64 consecutive node rows per
  * CTA, each with one CTA per tile / a persistent grid, then the edge-centric
- * kernel of the structured background grid (the faster of its 31 x 3 and
- * 31 x 7 node tiles; 0 if the mesh has none); ms_cut[3] = cut-element kernel with 2 / 4 / 8 elements per CTA (NULL
+ * kernel of the structured background grid (the fastest of its 31 x 3,
+ * 31 x 4 and 31 x 7 node tiles; 0 if the mesh has none); ms_cut[3] = cut-element kernel with 2 / 4 / 8 elements per CTA (NULL
  * allowed).  K is left to be reassembled. */
 int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
-/* the launch shapes in use, and setting them by hand (tile 32 or 64 rows, or 93 / 217 for the
- * structured-grid kernel's 31 x 3 / 31 x 7 node tiles; persistent 0/1 for the row tiles;
- * warps 2/4/8) */
+/* the launch shapes in use, and setting them by hand (tile 32 or 64 rows, or 93 / 124 / 217 for
+ * the structured-grid kernel's 31 x 3 / 31 x 4 / 31 x 7 node tiles; persistent 0/1 for the row
+ * tiles; warps 2/4/8) */
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
 int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
 

@@ -947,7 +947,7 @@ void launch_cut_class(int k, int warps, const CutArgs& ck, cudaStream_t s) {
 // for even nodes only) in ascending order, then enrichment columns.
 // grid_pattern_ok checks that layout on the host before this kernel is used.
 //
-// A CTA owns a tile of kTileX node columns and TR node rows (3 or 7, picked by
+// A CTA owns a tile of kTileX node columns and TR node rows (3, 4 or 7, picked by
 // the autotuner), with the TR + 1 cell rows around them, and runs one thread
 // per staged triangle ((TR + 1) x 64) in three phases between two barriers:
 //   1. one load per thread of each staged quantity, all in flight at once
@@ -1097,7 +1097,7 @@ __device__ __forceinline__ void tile_element(double* ke, const double* sX, const
 }
 
 template <bool WANT_F, int TR>
-__global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : 2) k_assemble_grid(GridArgs a) {
+__global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : (TR <= 4 ? 3 : 2)) k_assemble_grid(GridArgs a) {
     constexpr int kTileThreads = (TR + 1) * kTileElems;  // one staged triangle per thread
     static_assert((TR + 2) * kTileNX <= kTileThreads && TR * (kTileX + 1) <= kTileThreads &&
                   2 * TR + 2 <= kTileThreads / 32, "one staged node and row pointer per thread; warps per task");
@@ -1341,6 +1341,8 @@ void grid_prepare() {
     if (dev >= 0 && dev < 64 && done[dev]) return;
     cudaFuncSetAttribute(k_assemble_grid<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 3));
     cudaFuncSetAttribute(k_assemble_grid<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 3));
+    cudaFuncSetAttribute(k_assemble_grid<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 4));
+    cudaFuncSetAttribute(k_assemble_grid<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 4));
     cudaFuncSetAttribute(k_assemble_grid<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 7));
     cudaFuncSetAttribute(k_assemble_grid<true, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 7));
     if (dev >= 0 && dev < 64) done[dev] = true;
@@ -1361,7 +1363,7 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.f = c.F;
     ga.want_K = want_K;
     ga.strips = (ga.nx + 1 + kTileX - 1) / kTileX;
-    const int tr = c.tuning.grid_rows == 3 ? 3 : 7;
+    const int tr = c.tuning.grid_rows == 3 ? 3 : c.tuning.grid_rows == 4 ? 4 : 7;
     const int tiles = ga.strips * ((ga.ny + 1 + tr - 1) / tr);
     ga.n_tiles = tiles;
     ga.q_enr = c.hm.row_ptr[c.n_reg];
@@ -1373,6 +1375,9 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     if (tr == 3) {
         if (want_f) k_assemble_grid<true, 3><<<tiles, threads, grid_smem_bytes(true, 3), s>>>(ga);
         else k_assemble_grid<false, 3><<<tiles, threads, grid_smem_bytes(false, 3), s>>>(ga);
+    } else if (tr == 4) {
+        if (want_f) k_assemble_grid<true, 4><<<tiles, threads, grid_smem_bytes(true, 4), s>>>(ga);
+        else k_assemble_grid<false, 4><<<tiles, threads, grid_smem_bytes(false, 4), s>>>(ga);
     } else {
         if (want_f) k_assemble_grid<true, 7><<<tiles, threads, grid_smem_bytes(true, 7), s>>>(ga);
         else k_assemble_grid<false, 7><<<tiles, threads, grid_smem_bytes(false, 7), s>>>(ga);
@@ -1582,7 +1587,7 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
         // the structured-grid kernel at both tile heights; ms_tri[4] reports the faster
         c.tuning.tri_grid = 1;
         float ms_grid = 0.f;
-        for (int tr : {3, 7}) {
+        for (int tr : {3, 4, 7}) {
             c.tuning.grid_rows = tr;
             const RowArgs ra = row_args(c, c.U, false, true);
             const float ms = timed([&] { launch_tri(c, ra, false, s); });

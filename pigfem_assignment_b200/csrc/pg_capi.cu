@@ -407,11 +407,12 @@ int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent,
     int v = -1;
     for (int k = 0; k < kTriTileVariants; ++k)
         if (kTriTileSizes[k] == tri_tile_nodes) v = k;
-    const bool grid = tri_tile_nodes == 3 * kGridTileX || tri_tile_nodes == 7 * kGridTileX;
+    const bool grid = tri_tile_nodes == 3 * kGridTileX || tri_tile_nodes == 4 * kGridTileX ||
+                      tri_tile_nodes == 7 * kGridTileX;
     if ((v < 0 && !(grid && c->c.grid_emat)) || (tri_persistent != 0 && tri_persistent != 1) ||
         (cut_warps != 2 && cut_warps != 4 && cut_warps != 8)) {
-        set_error("pg_ctx_set_tuning: tile 32 or 64 (row tiles), 93 or 217 (structured grid, 31 x 3 or 31 x 7 "
-                  "nodes), persistent 0 or 1, warps 2, 4 or 8");
+        set_error("pg_ctx_set_tuning: tile 32 or 64 (row tiles), 93, 124 or 217 (structured grid, 31 x 3, 31 x 4 "
+                  "or 31 x 7 nodes), persistent 0 or 1, warps 2, 4 or 8");
         return PG_ERR_ARG;
     }
     c->c.tuning.tri_grid = grid ? 1 : 0;

@@ -70,7 +70,7 @@ constexpr int kGridTileX = 31;    // node columns per structured-grid tile
 // tile, and warps (= cut elements) per CTA of the cut kernel.
 struct AsmTuning {
     int tri_grid = 1;      // 1: edge-centric tiles of the structured grid (when the mesh has one)
-    int grid_rows = 3;     // node rows per structured-grid tile: 3 or 7
+    int grid_rows = 3;     // node rows per structured-grid tile: 3, 4 or 7
     int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
     int cut_warps = 2;     // 2, 4 or 8

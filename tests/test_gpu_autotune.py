@@ -19,7 +19,7 @@ def gpu_K(ctx, e):
     return bsr_to_csr(e["row_ptr"], e["col"], ctx.matrix_values())
 
 
-@pytest.mark.parametrize("tile", [32, 64, 93, 217])
+@pytest.mark.parametrize("tile", [32, 64, 93, 124, 217])
 @pytest.mark.parametrize("persistent", [0, 1])
 @pytest.mark.parametrize("warps", [2, 4, 8])
 def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
@@ -47,7 +47,7 @@ def test_autotune_times_every_shape_and_keeps_the_fastest():
     _lib.check(_lib.lib.pg_ctx_tuning(prob.ctx.handle, C.byref(tile), C.byref(pers), C.byref(warps)))
     best_tri = int(np.argmin(list(ms_tri)))
     if best_tri == 4:
-        assert tile.value in (93, 217)  # the 31 x 3 or 31 x 7 tiles of the structured grid
+        assert tile.value in (93, 124, 217)  # the 31 x 3, 31 x 4 or 31 x 7 tiles of the structured grid
     else:
         assert (tile.value, pers.value) == ((32, 64)[best_tri // 2], best_tri % 2)
     assert warps.value == (2, 4, 8)[int(np.argmin(list(ms_cut)))]

@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiling runs: timings under a profiler mislead the tuner)")
+    ap.add_argument("--tile", type=int, choices=[32, 64, 93, 124, 217], default=None,
+                    help="fix the triangle kernel's launch shape after any autotuning (32 / 64 node rows: "
+                         "the gather kernel; 93 / 124 / 217: the structured-grid kernel's 31 x 3 / 4 / 7 tiles)")
     ap.add_argument("--batch-rves", type=int, default=512)
     ap.add_argument("--no-sensitivity", action="store_true")
     ap.add_argument("--profile-range", choices=["load_step"], default=None,
@@ -284,6 +287,9 @@ def run_b200_arm(args):
         _lib.check(_lib.lib.pg_ctx_autotune(ctx.handle, 5, ms_tri, ms_cut))
     t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
+    if args.tile is not None:
+        _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, args.tile, t_pers.value, t_warps.value))
+        _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
     tri_kernel = "k_assemble_grid" if t_tile.value in (93, 124, 217) else "k_assemble_tri"
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
               "ms_tri_rows32_rows32p_rows64_rows64p_gridsweep": [round(v, 4) for v in ms_tri],

@@ -246,6 +246,12 @@ int pg_mlp_gradient(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n
 int pg_mlp_adam(pg_mlp* m, float lr);
 int pg_mlp_train(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n, int32_t epochs, int32_t batch,
                  float lr, double* loss_hist);
+/* Self-test of the kernels' bounded completion waits (the failure path the
+ * reference has no counterpart for): one forward tile whose first GEMM is
+ * not issued, so its mbarrier is never signalled and the wait gives up after
+ * `polls` polls with nothing in flight.  Returns PG_ERR_STATE ("timed out");
+ * the network and the device stay usable. */
+int pg_mlp_wait_selftest(pg_mlp* m, int32_t polls);
 
 /* Learned-predictor plumbing (device pointers).  s_inc = prescribed displacement
  * increment of the step, ratio = dt_{n+1}/dt_n.  Features: 16 floats per node;

@@ -4,12 +4,12 @@
 # gsl + gslcblas (PIGFEM4.6.1/Makefile:32-36); the reference build in
 # oracle/Makefile.ref needs both.  Outputs go only under oracle/_ref/.
 #
-# Usage: oracle/build_gsl.sh [REFERENCE_ROOT]
+# Usage: oracle/build_gsl.sh <PIGFEM4.6.1 directory>
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:?usage: build_gsl.sh <PIGFEM4.6.1 directory>}"
 OUT="$HERE/_ref"
-TARBALL="$REF/PIGFEM4.6.1/gsl-2.1.tar.gz"
+TARBALL="$REF/gsl-2.1.tar.gz"
 if [ -f "$OUT/gsl/lib/libgsl.a" ]; then
   echo "gsl already built in $OUT/gsl"; exit 0
 fi

@@ -72,6 +72,7 @@ struct Config {
     int max_iter = 40;
     int assemble_repeats = 0;   // >0: time assemble_linear this many times (linear only)
     int dump_K = 1;
+    double snes_rtol = 0.0, snes_stol = -1.0;  // > 0 / >= 0: the shim's SNES defaults (PETSc: 1e-8, 1e-8)
 };
 
 Config read_config(const char* path) {
@@ -105,6 +106,8 @@ Config read_config(const char* path) {
         else if (k == "max_iter") ss >> c.max_iter;
         else if (k == "assemble_repeats") ss >> c.assemble_repeats;
         else if (k == "dump_K") ss >> c.dump_K;
+        else if (k == "snes_rtol") ss >> c.snes_rtol;
+        else if (k == "snes_stol") ss >> c.snes_stol;
         else { fprintf(stderr, "unknown config key %s\n", k.c_str()); exit(2); }
     }
     return c;
@@ -160,6 +163,16 @@ double now_s() {
 int main(int argc, char** argv) {
     if (argc < 4) { fprintf(stderr, "usage: %s config out.bin scratch_dir\n", argv[0]); return 2; }
     Config cfg = read_config(argv[1]);
+    // SNES tolerances the shim takes as its defaults (see SNESCreate there)
+    char tolbuf[64];
+    if (cfg.snes_rtol > 0.0) {
+        snprintf(tolbuf, sizeof tolbuf, "%.17g", cfg.snes_rtol);
+        setenv("PGSHIM_SNES_RTOL", tolbuf, 1);
+    }
+    if (cfg.snes_stol >= 0.0) {
+        snprintf(tolbuf, sizeof tolbuf, "%.17g", cfg.snes_stol);
+        setenv("PGSHIM_SNES_STOL", tolbuf, 1);
+    }
     std::string scratch = std::string(argv[3]);
     if (scratch.back() != '/') scratch += "/";
 

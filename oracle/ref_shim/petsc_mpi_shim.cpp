@@ -570,7 +570,17 @@ PetscErrorCode PCHYPRESetType(PC, const char*) { return 0; }
 PetscErrorCode PCSetCoordinates(PC, PetscInt, PetscInt, PetscReal*) { return 0; }
 
 // ---- SNES -------------------------------------------------------------
-PetscErrorCode SNESCreate(MPI_Comm, SNES* s) { *s = new _p_SNES; return 0; }
+// PETSc's SNES defaults are rtol = stol = 1e-8 (what the reference runs with:
+// its SNESSetTolerances passes PETSC_DEFAULT, SolverNonlinearSNES.cpp:78).
+// PGSHIM_SNES_RTOL / PGSHIM_SNES_STOL replace those defaults when set -- the
+// stand-in for PETSc's -snes_rtol / -snes_stol options, used to record
+// tightly converged reference trajectories for parity tests.
+PetscErrorCode SNESCreate(MPI_Comm, SNES* s) {
+    *s = new _p_SNES;
+    if (const char* v = std::getenv("PGSHIM_SNES_RTOL")) (*s)->rtol = std::atof(v);
+    if (const char* v = std::getenv("PGSHIM_SNES_STOL")) (*s)->stol = std::atof(v);
+    return 0;
+}
 PetscErrorCode SNESDestroy(SNES* s) { if (s && *s) { delete *s; *s = nullptr; } return 0; }
 PetscErrorCode SNESGetKSP(SNES s, KSP* ksp) { *ksp = &s->ksp; return 0; }
 PetscErrorCode SNESSetType(SNES, SNESType) { return 0; }

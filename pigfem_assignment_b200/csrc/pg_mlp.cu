@@ -98,8 +98,10 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (int it = 0; it < (1 << 22); ++it) {
+constexpr int kPollLimit = 1 << 22;  // polls of a completion wait before it gives up
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int polls) {
+    for (int it = 0; it < polls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -143,14 +145,25 @@ __device__ __forceinline__ void st_row(uint8_t* base, int row, const float* v, i
     }
 }
 
+// How the completion waits of one launch behave: polls before a wait gives
+// up, and (self-test only) a GEMM whose MMAs are not issued, so that nothing
+// ever arrives on its mbarrier and its wait must run out.
+struct WaitCfg {
+    int polls;
+    int skip_gemm;  // index of the GEMM not issued, -1: none
+};
+
 // Issues the K/16 MMAs of one GEMM (thread 0) and waits for them (all threads).
-// Returns false on a timed-out wait.
+// Returns false on a timed-out wait; `inflight` then says whether MMAs of this
+// CTA are still pending on the phase `phase` (left unflipped).
 __device__ __forceinline__ bool gemm(uint32_t sbase, uint32_t a_off, uint32_t b_off, int K, int N, uint32_t d_tmem,
-                                     bool accumulate, uint32_t mbar, uint32_t& phase) {
+                                     bool accumulate, uint32_t mbar, uint32_t& phase, const WaitCfg& wc, int& index,
+                                     bool& inflight) {
+    const bool issue = index++ != wc.skip_gemm;
     fence_async_smem();
     fence_before();
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && issue) {
         fence_after();
         const uint32_t id = idesc_bf16(128, N);
         for (int ks = 0; ks < K / 16; ++ks) {
@@ -160,9 +173,13 @@ __device__ __forceinline__ bool gemm(uint32_t sbase, uint32_t a_off, uint32_t b_
         }
         umma_commit(mbar);
     }
-    bool ok = mbar_wait(mbar, phase);
-    phase ^= 1u;
+    bool ok = mbar_wait(mbar, phase, wc.polls);
     ok = __syncthreads_and(ok) != 0;  // every thread takes the same branch afterwards
+    if (!ok) {
+        inflight = issue;
+        return false;
+    }
+    phase ^= 1u;
     fence_after();
     return ok;
 }
@@ -170,7 +187,8 @@ __device__ __forceinline__ bool gemm(uint32_t sbase, uint32_t a_off, uint32_t b_
 // Training (want_grad) or inference pass over n rows.
 template <bool kTrain>
 __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, const float* __restrict__ T, int n,
-                                               Params p, Params g, float* Y_out, double* loss, int* err) {
+                                               Params p, Params g, float* Y_out, double* loss, int* err,
+                                               WaitCfg wc) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
@@ -219,6 +237,8 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
     uint32_t phase = 0;
     bool ok = true;
     bool first = true;
+    int gi = 0;             // GEMMs issued so far (WaitCfg::skip_gemm)
+    bool inflight = false;  // a timed-out wait left MMAs of this CTA pending
     const int ntiles = (n + TILE - 1) / TILE;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int row = tile * TILE + tid;
@@ -230,7 +250,7 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         if (kTrain)
             for (int i = 0; i < IN; ++i) st_bf16(sm, O_BT + kmaj(HID + i, tid, TILE), x[i]);
         // ---- layer 1
-        ok = gemm(sbase, O_X, O_W1, IN, HID, tmem + C_Z1, false, mbar, phase);
+        ok = gemm(sbase, O_X, O_W1, IN, HID, tmem + C_Z1, false, mbar, phase, wc, gi, inflight);
         if (!ok) break;
         float h1[HID];
         uint64_t m1 = 0;
@@ -244,7 +264,7 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         if (kTrain)
             for (int j = 0; j < HID; ++j) st_bf16(sm, O_BT + kmaj(j, tid, TILE), h1[j]);
         // ---- layer 2
-        ok = gemm(sbase, O_H1, O_W2, HID, HID, tmem + C_Z2, false, mbar, phase);
+        ok = gemm(sbase, O_H1, O_W2, HID, HID, tmem + C_Z2, false, mbar, phase, wc, gi, inflight);
         if (!ok) break;
         float h2[HID];
         uint64_t m2 = 0;
@@ -258,7 +278,7 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         if (kTrain)
             for (int j = 0; j < HID; ++j) st_bf16(sm, O_B3 + kmaj(j, tid, TILE), h2[j]);
         // ---- layer 3
-        ok = gemm(sbase, O_H2, O_W3, HID, OUT, tmem + C_Y, false, mbar, phase);
+        ok = gemm(sbase, O_H2, O_W3, HID, OUT, tmem + C_Y, false, mbar, phase, wc, gi, inflight);
         if (!ok) break;
         float y[OUT];
         tmem_ld16(tmem + lane_base + C_Y, y);
@@ -284,7 +304,7 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         for (int o = 0; o < USED; ++o) atomicAdd(&sgb[2 * HID + o], dy[o]);
         st_row(sm + O_DY, tid, dy, OUT);
         for (int o = 0; o < USED; ++o) st_bf16(sm, O_A3 + kmaj(o, tid, TILE), dy[o]);
-        ok = gemm(sbase, O_DY, O_W3T, OUT, HID, tmem + C_Z1, false, mbar, phase);  // dH2
+        ok = gemm(sbase, O_DY, O_W3T, OUT, HID, tmem + C_Z1, false, mbar, phase, wc, gi, inflight);  // dH2
         if (!ok) break;
         float d2[HID];
         for (int c = 0; c < HID; c += 16) tmem_ld16(tmem + lane_base + C_Z1 + c, d2 + c);
@@ -294,7 +314,7 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         }
         st_row(sm + O_DZ2, tid, d2, HID);
         for (int j = 0; j < HID; ++j) st_bf16(sm, O_AT + kmaj(j, tid, TILE), d2[j]);
-        ok = gemm(sbase, O_DZ2, O_W2T, HID, HID, tmem + C_Z2, false, mbar, phase);  // dH1
+        ok = gemm(sbase, O_DZ2, O_W2T, HID, HID, tmem + C_Z2, false, mbar, phase, wc, gi, inflight);  // dH1
         if (!ok) break;
         float d1[HID];
         for (int c = 0; c < HID; c += 16) tmem_ld16(tmem + lane_base + C_Z2 + c, d1 + c);
@@ -304,13 +324,16 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
             st_bf16(sm, O_AT + kmaj(HID + j, tid, TILE), d1[j]);
         }
         // weight gradients, accumulated in tensor memory over this CTA's tiles
-        ok = gemm(sbase, O_AT, O_BT, TILE, HID + IN, tmem + C_DW12, !first, mbar, phase);
+        ok = gemm(sbase, O_AT, O_BT, TILE, HID + IN, tmem + C_DW12, !first, mbar, phase, wc, gi, inflight);
         if (!ok) break;
-        ok = gemm(sbase, O_A3, O_B3, TILE, HID, tmem + C_DW3, !first, mbar, phase);
+        ok = gemm(sbase, O_A3, O_B3, TILE, HID, tmem + C_DW3, !first, mbar, phase, wc, gi, inflight);
         if (!ok) break;
         first = false;
     }
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    // MMAs still pending after a timed-out wait write tensor memory: wait for
+    // them (bounded again) before that memory is freed below
+    if (!ok && inflight) mbar_wait(mbar, phase, kPollLimit);
     if (kTrain && ok && !first) {
         // D12 rows 0..63: dW2 (cols 0..63); rows 64..127: dW1 (cols 64..79); D3 rows 0..15: dW3
         const int m = tid;
@@ -382,6 +405,7 @@ struct pg_mlp {
     float* v = nullptr;
     double* loss = nullptr;
     int* err = nullptr;
+    float* probe = nullptr;    // one tile of inputs and outputs for pg_mlp_wait_selftest
     int step = 0;
     int n_sms = 148;
 };
@@ -407,6 +431,8 @@ int pg_mlp_create(int32_t device, uint64_t seed, pg_mlp** out) {
     PG_CUDA(cudaMalloc((void**)&m->loss, sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&m->err, sizeof(int)));
     PG_CUDA(cudaMemset(m->err, 0, sizeof(int)));
+    PG_CUDA(cudaMalloc((void**)&m->probe, TILE * (IN + 2) * sizeof(float)));
+    PG_CUDA(cudaMemset(m->probe, 0, TILE * (IN + 2) * sizeof(float)));
     cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, device);
     PG_CUDA(cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
     PG_CUDA(cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
@@ -430,6 +456,7 @@ void pg_mlp_destroy(pg_mlp* m) {
     if (m->params) cudaFree(m->params);
     if (m->loss) cudaFree(m->loss);
     if (m->err) cudaFree(m->err);
+    if (m->probe) cudaFree(m->probe);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
 }
@@ -479,10 +506,25 @@ int pg_mlp_forward(pg_mlp* m, const float* X_dev, int32_t n, float* Y_dev, void*
     const int tiles = (n + TILE - 1) / TILE;
     const int grid = tiles < m->n_sms ? tiles : m->n_sms;
     Params p = carve(m->params), g = carve(m->grads);
-    k_mlp<false><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, nullptr, n, p, g, Y_dev, m->loss, m->err);
+    k_mlp<false><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, nullptr, n, p, g, Y_dev, m->loss, m->err, WaitCfg{kPollLimit, -1});
     PG_CUDA(cudaGetLastError());
     if (s == m->stream) return mlp_check_err(m);
     return PG_OK;
+}
+
+// Self-test of the bounded completion wait: one forward tile whose first GEMM
+// is not issued, so nothing arrives on its mbarrier and the wait must give up
+// after `polls` polls.  Nothing is in flight when it does, so the kernel
+// records its error word, frees its tensor memory and returns; the call
+// returns the timeout status and the network stays usable.
+int pg_mlp_wait_selftest(pg_mlp* m, int32_t polls) {
+    if (!m || polls < 1) { set_error("pg_mlp_wait_selftest: bad argument"); return PG_ERR_ARG; }
+    cudaSetDevice(m->device);
+    Params p = carve(m->params), g = carve(m->grads);
+    k_mlp<false><<<1, NT, SMEM_ALLOC, m->stream>>>(m->probe, nullptr, TILE, p, g, m->probe + TILE * IN, m->loss, m->err,
+                                                   WaitCfg{polls, 0});
+    PG_CUDA(cudaGetLastError());
+    return mlp_check_err(m);
 }
 
 // gradients of the mean-squared loss over all n rows into the internal buffer; loss to *loss_host
@@ -495,7 +537,7 @@ int pg_mlp_gradient(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n
     const int tiles = (n + TILE - 1) / TILE;
     const int grid = tiles < m->n_sms ? tiles : m->n_sms;
     Params p = carve(m->params), g = carve(m->grads);
-    k_mlp<true><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, T_dev, n, p, g, nullptr, m->loss, m->err);
+    k_mlp<true><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, T_dev, n, p, g, nullptr, m->loss, m->err, WaitCfg{kPollLimit, -1});
     PG_CUDA(cudaGetLastError());
     int rc = mlp_check_err(m);
     if (rc) return rc;

@@ -17,7 +17,10 @@
 // the one array and finds the previous call's contents there; everything
 // the solve reads before writing is cleared by the call itself.  Calls that
 // overlap on the GPU (several streams or host threads at once) race on the
-// array and must be serialised by the caller.
+// array and must be serialised by the caller.  The looked-up address belongs
+// to the device's current CUDA context: after cudaDeviceReset on that device
+// it is stale, so a process that resets a device must not call this entry
+// point on it again.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -34,6 +37,9 @@ namespace {
 
 constexpr int kStaticMaxNodes = PG_STATIC_MAX_NODES;
 constexpr int kStaticChunk = 32;   // iterations launched between two host reads of the status flags
+// set-up verdicts in the breakdown flag (CG itself writes 1 there)
+constexpr int kStaticNoDiag = 2;    // a free DOF whose row has no diagonal block
+constexpr int kStaticSingular = 3;  // a free DOF's diagonal block (or pivot) is zero or not finite
 
 // Layout (doubles): r, z, p, q (2 * kStaticMaxNodes each), minv (4 per
 // node), the CG scalars (S_NSCAL), the CG flags (F_NFLAGS ints, 8 bytes
@@ -72,14 +78,17 @@ __global__ void k_static_prec(int n, const int* __restrict__ row_ptr, const int*
     double m[4] = {0.0, 0.0, 0.0, 0.0};
     const bool f0 = fixed[2 * i], f1 = fixed[2 * i + 1];
     if (b == nullptr) {
-        if (!f0 || !f1) flags[F_BREAKDOWN] = 2;  // a free DOF without a diagonal block
+        if (!f0 || !f1) flags[F_BREAKDOWN] = kStaticNoDiag;  // a free DOF without a diagonal block
     } else if (!f0 && !f1) {
         const double det = b[0] * b[3] - b[1] * b[2];
+        if (det == 0.0 || !isfinite(det)) flags[F_BREAKDOWN] = kStaticSingular;
         m[0] = b[3] / det;
         m[1] = -b[1] / det;
         m[2] = -b[2] / det;
         m[3] = b[0] / det;
     } else {
+        const double piv = f0 ? b[3] : b[0];
+        if (!(f0 && f1) && (piv == 0.0 || !isfinite(piv))) flags[F_BREAKDOWN] = kStaticSingular;
         m[0] = f0 ? 0.0 : 1.0 / b[0];
         m[3] = f1 ? 0.0 : 1.0 / b[3];
     }
@@ -148,9 +157,10 @@ int scratch_on_current_device(double** out) {
 
 using namespace pgb;
 
-extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, const double* K,
-                                   const uint8_t* fixed, const double* b, double* x, double rtol, int32_t max_iter,
-                                   void* stream, pg_solve_stats* stats) {
+namespace {
+
+int pcg_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, const double* K, const uint8_t* fixed,
+               const double* b, double* x, double rtol, int32_t max_iter, void* stream, pg_solve_stats* stats) {
     if (n_nodes > kStaticMaxNodes) {
         char msg[160];
         std::snprintf(msg, sizeof msg, "pg_pcg_solve_static: %d nodes exceed the fixed scratch capacity of %d nodes",
@@ -177,12 +187,13 @@ extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, cons
     int* flags = reinterpret_cast<int*>(base + kOffFlags);
     const int gb = (n + kThreads - 1) / kThreads, gd = (nd + kThreads - 1) / kThreads;
 
-    cudaMemsetAsync(scal, 0, (S_NSCAL + F_NFLAGS) * sizeof(double), s);
+    cudaError_t e = cudaMemsetAsync(scal, 0, (S_NSCAL + F_NFLAGS) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: clearing the scalars and flags");
     k_static_start<<<gd, kThreads, 0, s>>>(nd, fixed, b, r, x);
     k_static_prec<<<gb, kThreads, 0, s>>>(n, row_ptr, col, K, fixed, minv, flags);
     k_cg_init<double, double><<<gb, kThreads, 0, s>>>(n, r, z, p, minv, scal);
     k_static_tol<<<1, 1, 0, s>>>(scal, rtol * rtol);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: launch");
 
     int hf[F_NFLAGS] = {};
@@ -191,9 +202,13 @@ extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, cons
     if (e == cudaSuccess) e = cudaMemcpyAsync(hf, flags, sizeof hf, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: set-up");
-    if (hf[F_BREAKDOWN] == 2) {
+    if (hf[F_BREAKDOWN] == kStaticNoDiag) {
         set_error("pg_pcg_solve_static: a free DOF has no diagonal block in the pattern");
         return PG_ERR_ARG;
+    }
+    if (hf[F_BREAKDOWN] == kStaticSingular) {
+        set_error("pg_pcg_solve_static: singular diagonal block (zero or non-finite determinant or pivot)");
+        return PG_ERR_BREAKDOWN;
     }
     int iters = 0, launched = 0;
     bool done = hs[S_RR0 + 1] <= hs[S_TOL2] || hs[S_RR0 + 1] == 0.0;
@@ -214,7 +229,8 @@ extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, cons
         done = hf[F_DONE] != 0;
     }
     // true residual of the returned x (the q slot of the scratch is free now)
-    cudaMemsetAsync(q, 0, 2 * sizeof(double), s);
+    e = cudaMemsetAsync(q, 0, 2 * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: clearing the residual accumulator");
     k_static_resid<<<gb, kThreads, 0, s>>>(n, row_ptr, col, K, x, fixed, b, q);
     double res[2] = {0.0, 0.0};
     e = cudaMemcpyAsync(res, q, sizeof res, cudaMemcpyDeviceToHost, s);
@@ -239,4 +255,20 @@ extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, cons
     }
     stats->status = PG_OK;
     return PG_OK;
+}
+
+}  // namespace
+
+extern "C" int pg_pcg_solve_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, const double* K,
+                                   const uint8_t* fixed, const double* b, double* x, double rtol, int32_t max_iter,
+                                   void* stream, pg_solve_stats* stats) {
+    // stats describes this call on every return, the early ones included
+    constexpr int kUnset = -1;
+    if (stats) {
+        *stats = pg_solve_stats{};
+        stats->status = kUnset;
+    }
+    const int rc = pcg_static(n_nodes, row_ptr, col, K, fixed, b, x, rtol, max_iter, stream, stats);
+    if (stats && stats->status == kUnset) stats->status = rc;
+    return rc;
 }

@@ -47,6 +47,8 @@ int pcg_run(Ctx& c, cudaStream_t s, const MT* K, VT* x, VT* r, VT* z, VT* p, VT*
     PG_CUDA(cudaStreamSynchronize(s));
     rr_final = c.h_scal[S_RR0 + 1];
     if (rr_final <= tol2 || max_iter <= 0) return 0;
+    // a budget below one graph's worth of iterations is honoured exactly
+    chunk = std::max(1, std::min(chunk, max_iter));
 
     cudaGraph_t graph;
     PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));

@@ -13,7 +13,10 @@ Fixtures (numpy .npz):
                       node on an interface that escapes the node-moving rule
                       (a zero-area child element)
   cohesive_16x16.npz  Ortiz-Pandolfi cohesive interface, four load steps from
-                      four prefix-consistent runs (committed state per step)
+                      four prefix-consistent runs (committed state per step),
+                      each Newton solve converged to SNES rtol 1e-12 (stol off)
+                      instead of PETSc's default 1e-8, so that the trajectory
+                      itself is accurate to well below the parity bounds
 Each holds the reference's enriched mesh, DOF numbering, K_ff/K_fp/K_pf/K_pp
 (linear), the solution, and (cohesive) the internal force and delta_max.
 """
@@ -58,7 +61,7 @@ def main() -> None:
     # same load history as the first k steps of any longer run of this family
     base = dict(nx=16, ny=16, E_matrix=3000.0, nu_matrix=0.35, problem="cohesive",
                 inclusions=[(0.5, 0.5, 0.25, 70000.0, 0.2)], coh_sigma=10.0, coh_delta=1.5e-4, coh_beta=1.0,
-                coh_visc=0.5, min_dt=1e-6, max_iter=40)
+                coh_visc=0.5, min_dt=1e-6, max_iter=40, snes_rtol=1e-12, snes_stol=0.0)
     dt = 0.1
     steps = {}
     for k in range(1, 5):
@@ -70,7 +73,7 @@ def main() -> None:
     save("cohesive_16x16.npz", last, dict(steps, **{
         "cfg.nx": np.array([16]), "cfg.inc": np.array([[0.5, 0.5, 0.25, 70000.0, 0.2]]),
         "cfg.coh": np.array([10.0, 1.5e-4, 1.0, 0.5]), "cfg.dt": np.array([dt]), "cfg.strain_per_step": np.array([0.0025]),
-        "cfg.nsteps": np.array([4])}))
+        "cfg.nsteps": np.array([4]), "cfg.snes_rtol": np.array([1e-12])}))
 
 
 if __name__ == "__main__":

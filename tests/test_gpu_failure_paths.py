@@ -1,0 +1,169 @@
+"""Failure paths of the solver stack, driven from the host: a Newton budget
+that runs out (load-step repeats, then PG_ERR_NOT_CONVERGED), the step-cut
+sequence of SolverNonlinear::update_time_step (src/SolverNonlinear.cpp:455-491),
+a Krylov budget that runs out, an indefinite cohesive tangent that trips the
+CG -> MINRES / GMRES switch, and the MLP kernels' bounded completion wait.
+Nothing here faults or hangs a GPU: every failure is a status the host reads."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+import pigfem_assignment_b200.problem as pb
+from pigfem_assignment_b200 import _lib
+from pigfem_assignment_b200.rve import RVE, config0
+
+pytestmark = pytest.mark.gpu
+
+SOFT = (30.0, 0.01, 1.0e6, 1.0)  # bilinear law: sigma_c 30 MPa, G_c 0.01 N/mm, K_p 1e6 MPa/mm, beta 1
+
+
+def _cohesive_problem(**cfg):
+    rve = RVE(nx=16, ny=16, inclusions=[(0.5, 0.5, 0.25, 1)], cohesive=True, coh_law=1, coh_params=SOFT,
+              strain=0.004)
+    prob = pb.ProblemNonlinearStructural(rve)
+    prob.init()
+    prob.configure(**cfg)
+    return rve, prob
+
+
+def expected_dt_sequence(records, dt_nom, t_end):
+    """The accepted steps' dt under SolverNonlinear::update_time_step: a failed
+    attempt multiplies dt by 0.25; a step accepted at its first attempt lets
+    the next one grow by 1.5; dt never exceeds the nominal step (max_dt) nor
+    the remaining load."""
+    out, t, dt = [], 0.0, min(dt_nom, t_end)
+    for r in records:
+        dt_acc = dt * 0.25 ** (r.repeats - 1)
+        out.append(dt_acc)
+        t += dt_acc
+        dt = dt_acc * (1.5 if r.repeats == 1 else 1.0)
+        dt = min(dt, dt_nom, t_end - t)
+    return np.array(out)
+
+
+def test_newton_budget_exhausted_reports_not_converged():
+    # one Newton iteration cannot reach rtol 1e-8 (the first Krylov solve is
+    # only asked for 1e-3): every attempt fails, the step is cut max_repeat
+    # times, then the driver gives up with a status instead of exiting
+    _, prob = _cohesive_problem(n_steps=4, max_it=1, max_repeat=3)
+    recs = (_lib.StepStats * 8)()
+    n = C.c_int32(-1)
+    rc = _lib.lib.pg_solve_nonlinear(prob.ctx.handle, C.byref(prob.cfg), recs, 8, C.byref(n))
+    assert rc == _lib.PG_ERR_NOT_CONVERGED
+    assert b"repeat budget" in _lib.lib.pg_last_error()
+    assert n.value == 0
+    prob.ctx.close()
+
+
+def test_step_cuts_follow_update_time_step():
+    # three Newton iterations are enough for an elastic step (forcing terms
+    # 1e-3, then ~1e-6, then the target), not for the steps that debond the
+    # interface: those are cut by 4 until they converge
+    n_steps = 5
+    _, prob = _cohesive_problem(n_steps=n_steps, T_final=1.0, max_it=3, max_repeat=20,
+                                predictor=_lib.PG_PREDICT_ZEROTH)
+    recs = prob.solve_problem()
+    assert all(r.reason > 0 for r in recs)
+    dts = np.array([r.dt for r in recs])
+    assert abs(dts.sum() - 1.0) < 1e-12
+    assert max(r.repeats for r in recs) > 1, "no step was cut: the budget did not bind"
+    np.testing.assert_allclose(dts, expected_dt_sequence(recs, 1.0 / n_steps, 1.0), rtol=1e-12)
+    prob.ctx.close()
+
+
+def test_krylov_budget_of_five_iterations():
+    prob = pb.ProblemLinearElasticity(config0())
+    prob.init()
+    prob.get_solver().configure(rtol=1e-12, max_iter=5, check_every=64)
+    with pytest.raises(_lib.PgError) as ei:
+        prob.solve_problem()
+    assert ei.value.code == _lib.PG_ERR_NOT_CONVERGED
+    st = prob.get_solver().stats
+    assert st.status == _lib.PG_ERR_NOT_CONVERGED
+    assert st.iterations == 5
+    assert st.rel_residual > 1e-12
+    prob.ctx.close()
+
+
+def _translated_inclusion(e, rve, a):
+    """Displacement field in which the inclusion translates rigidly by `a`
+    against a matrix at rest.  In the IGFEM basis: a at the regular nodes
+    inside the circle; at an enrichment node, the field there minus the
+    parent edge's interpolation of the nodal values (a on the inclusion side,
+    0 on the matrix side)."""
+    xy = e["xy"]
+    cx, cy, r, inc_mat = rve.inclusions[0]
+    inside = (xy[:, 0] - cx) ** 2 + (xy[:, 1] - cy) ** 2 < r * r
+    nreg = e["n_regular_nodes"]
+    U = np.zeros(2 * xy.shape[0])
+    reg_in = np.flatnonzero(inside[:nreg])
+    U[2 * reg_in] = a[0]
+    U[2 * reg_in + 1] = a[1]
+    T = pb.template_table()
+    for c, el in enumerate(e["cut_elem"]):
+        tm = T[e["cut_tmpl"][c]]
+        n_child = tm[2]
+        par = e["conn"][el]
+        P = xy[par]
+        A = np.array([[P[1, 0] - P[0, 0], P[2, 0] - P[0, 0]], [P[1, 1] - P[0, 1], P[2, 1] - P[0, 1]]])
+        for k in range(n_child):
+            nodes = tm[24 + 6 * k: 24 + 6 * k + tm[16 + k]]
+            inc_side = e["cut_child_mat"][c][k] == inc_mat
+            for ln in nodes:
+                if ln < 3:
+                    continue
+                node = e["cut_enr"][c][ln - 3]
+                l1, l2 = np.linalg.solve(A, xy[node] - P[0])
+                lam = np.array([1.0 - l1 - l2, l1, l2])
+                n_in = lam[inside[par]].sum()
+                for d in range(2):
+                    U[2 * node + d] = a[d] * ((1.0 - n_in) if inc_side else -n_in)
+    return U
+
+
+@pytest.mark.parametrize("precond,fallback", [(_lib.PG_PREC_BLOCK_JACOBI, "MINRES"), (_lib.PG_PREC_MG, "GMRES")])
+def test_indefinite_tangent_switches_krylov_method(precond, fallback):
+    # the inclusion translated by |a| = 5e-4 mm against the matrix, from an
+    # undamaged committed state: on the half of the interface that opens,
+    # every cohesive point loads on the softening branch (delta_0 = 3e-5 <
+    # 5e-4 < delta_f = 6.67e-4 mm), where the normal tangent (-4.7e4 MPa/mm)
+    # outweighs the tangential secant (1.6e4), so the tangent is indefinite;
+    # on the closing half the law counts only the tangential opening
+    rve, prob = _cohesive_problem(max_it=2, precond=precond)
+    e = prob.mesh.export()
+    a = np.array([5e-4 / np.sqrt(2.0), 5e-4 / np.sqrt(2.0)])
+    U = _translated_inclusion(e, rve, a)
+    om = oracle.from_product(e, pb.template_table(), rve)
+    nq = prob.mesh.info["n_cohesive_qp"]
+    K, _, isv_t = om.assemble(u=U, dt=1.0, isv_c=np.zeros(nq), want_K=True)
+    assert abs(isv_t.max() - 5e-4) <= 1e-12 and (isv_t > 3e-5).sum() >= isv_t.size // 2
+    free = ~e["fixed"]
+    Kff = K.toarray()[np.ix_(free, free)]
+    assert np.linalg.eigvalsh(0.5 * (Kff + Kff.T)).min() < 0.0
+
+    prob.ctx.set_vector(0, U)
+    prob.ctx.set_isv(np.zeros(nq), committed=True)
+    st = prob.load_step(0.0, 1.0)
+    assert st.gmres_fallbacks >= 1, f"CG never broke down; expected a {fallback} fallback"
+    prob.ctx.close()
+
+
+def test_mlp_bounded_wait_times_out_then_recovers():
+    torch = pytest.importorskip("torch")
+    h = C.c_void_p()
+    _lib.check(_lib.lib.pg_mlp_create(0, 7, C.byref(h)))
+    try:
+        rc = _lib.lib.pg_mlp_wait_selftest(h, 1000)
+        assert rc == _lib.PG_ERR_STATE
+        assert b"timed out" in _lib.lib.pg_last_error()
+        # the device and the network are still usable: a normal forward pass
+        n = 300
+        X = torch.randn(n, 16, device="cuda:0", dtype=torch.float32)
+        Y = torch.zeros(n, 2, device="cuda:0", dtype=torch.float32)
+        _lib.check(_lib.lib.pg_mlp_forward(h, C.c_void_p(X.data_ptr()), n, C.c_void_p(Y.data_ptr()), None))
+        torch.cuda.synchronize()
+        assert torch.isfinite(Y).all()
+    finally:
+        _lib.lib.pg_mlp_destroy(h)

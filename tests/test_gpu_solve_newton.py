@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 def test_gpu_newton_follows_reference_trajectory(precision):
     """Four load steps (dt = 0.1, 0.25% strain each) from zero state: the
     converged displacements and delta_max after every step match the
-    reference's (its SNES Newton with rtol 1e-8)."""
+    reference's (its SNES Newton, run to rtol 1e-12 for the fixture) within
+    the north star's displacement bound 1e-8, delta_max within 1e-10."""
     g = golden("cohesive_16x16.npz")
     rve = rve_from_golden(g, cohesive=True)
     nsteps = int(g["cfg.nsteps"][0])
@@ -24,7 +25,7 @@ def test_gpu_newton_follows_reference_trajectory(precision):
     rve.strain = float(g["cfg.strain_per_step"][0]) * nsteps
     prob = pb.ProblemNonlinearStructural(rve)
     prob.init()
-    prob.configure(rtol=1e-10, precision=precision)
+    prob.configure(rtol=1e-12, stol=0.0, precision=precision)
     e = prob.mesh.export()
     ref = e["ref_dof"]
     for k in range(1, nsteps + 1):
@@ -33,9 +34,8 @@ def test_gpu_newton_follows_reference_trajectory(precision):
         prob.commit()
         u = prob.get_solution()
         uref = np.concatenate([g[f"step{k}.U.f"], g[f"step{k}.U.p"]])[ref]
-        # the reference stops at ||r|| <= 1e-8 ||r0||; its U carries that error
-        assert np.linalg.norm(u - uref) / np.linalg.norm(uref) <= 1e-6
-        np.testing.assert_allclose(prob.ctx.isv(committed=True), g[f"step{k}.isv.delta_max"], rtol=1e-5, atol=1e-12)
+        assert np.linalg.norm(u - uref) / np.linalg.norm(uref) <= 1e-8
+        np.testing.assert_allclose(prob.ctx.isv(committed=True), g[f"step{k}.isv.delta_max"], rtol=1e-10, atol=1e-18)
     prob.ctx.close()
 
 

@@ -24,6 +24,8 @@ def test_static_solve_rejects_sizes_beyond_the_scratch():
                                       None, C.byref(st))
     assert rc == _lib.PG_ERR_LIMIT
     assert b"exceed" in _lib.lib.pg_last_error()
+    # the early return still describes this call in stats
+    assert st.status == _lib.PG_ERR_LIMIT and st.iterations == 0
 
 
 @pytest.mark.gpu
@@ -59,12 +61,36 @@ def test_static_solve_matches_context_solver_on_two_calls():
     for call in range(2):
         x.fill_(123.0)  # the entry point must overwrite every value
         torch.cuda.synchronize()
+        # the module (and its scratch array) is loaded before the second call:
+        # from then on the call must leave the device's free memory unchanged
+        free_before = torch.cuda.mem_get_info(dev)[0]
         st = _lib.SolveStats()
         rc = _lib.lib.pg_pcg_solve_static(n_nodes, row_ptr.data_ptr(), col.data_ptr(), K.data_ptr(), fx.data_ptr(),
                                           bd.data_ptr(), x.data_ptr(), 1e-12, 200000, None, C.byref(st))
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info(dev)[0]
         assert rc == 0, (call, rc, _lib.lib.pg_last_error())
+        if call == 1:
+            assert free_after == free_before, (free_before, free_after)
         assert st.status == 0 and st.rel_residual <= 4e-12, (call, st.rel_residual)
         xh = x.cpu().numpy()
         assert np.all(xh[fixed] == 0.0)
         assert np.linalg.norm(xh[free] - ref) / np.linalg.norm(ref) <= U_TOL, call
+
+    # a free node whose diagonal block is zero: reported as a singular block,
+    # with stats describing this call
+    Ks = Kv.copy()
+    i = int(np.flatnonzero(~fixed.reshape(-1, 2).any(axis=1))[0])
+    rp = np.asarray(e["row_ptr"])
+    cl = np.asarray(e["col"])
+    q = rp[i] + int(np.flatnonzero(cl[rp[i]:rp[i + 1]] == i)[0])
+    Ks[4 * q:4 * q + 4] = 0.0
+    K.copy_(torch.as_tensor(Ks, device=dev))
+    st = _lib.SolveStats()
+    st.status = 77
+    st.iterations = 999
+    rc = _lib.lib.pg_pcg_solve_static(n_nodes, row_ptr.data_ptr(), col.data_ptr(), K.data_ptr(), fx.data_ptr(),
+                                      bd.data_ptr(), x.data_ptr(), 1e-12, 100, None, C.byref(st))
+    assert rc == _lib.PG_ERR_BREAKDOWN and b"singular" in _lib.lib.pg_last_error()
+    assert st.status == rc and st.iterations == 0
     prob.ctx.close()

@@ -7,7 +7,9 @@ with FP64 refinement), on configuration 1: a 512x512 structured TRI3 mesh
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-One step = one full assembly pass (node-row kernel + cut-element kernel) of K.
+One step = one full assembly pass of K: the structured-grid kernel (uncut
+triangles, one thread per node row) with the cut elements' kernels beside it
+on a second stream, then the deterministic fold of the cut elements' blocks.
 Timing: CUDA events on the assembly stream around each step; the L2 (126 MB)
 is flushed by writing a 512 MB buffer between steps; max over ranks.  For N > 1
 every rank assembles its own replica of the RVE (replicas only: a single RVE
@@ -45,9 +47,9 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiling runs: timings under a profiler mislead the tuner)")
-    ap.add_argument("--tile", type=int, choices=[32, 64, 93, 124, 217], default=None,
+    ap.add_argument("--tile", type=int, choices=[32, 64, 128, 256], default=None,
                     help="fix the triangle kernel's launch shape after any autotuning (32 / 64 node rows: "
-                         "the gather kernel; 93 / 124 / 217: the structured-grid kernel's 31 x 3 / 4 / 7 tiles)")
+                         "the gather kernel; 128 / 256: threads per CTA of the structured-grid kernel)")
     ap.add_argument("--batch-rves", type=int, default=512)
     ap.add_argument("--no-sensitivity", action="store_true")
     ap.add_argument("--profile-range", choices=["load_step"], default=None,
@@ -159,8 +161,8 @@ def profiled_traffic(kernel: str):
 
 def launches_per_pass(mesh) -> int:
     """Kernels one linear assembly launches: the uncut-triangle kernel, the
-    cut elements' quadrature-row kernel and one cut-element kernel per
-    non-empty size class (local node count <= 5, 7, 11, 15)."""
+    cut elements' quadrature-row kernel, one pair kernel per non-empty size
+    class (local node count <= 5, 7, 11, 15) and the fold of K."""
     import numpy as np
 
     import pigfem_assignment_b200.problem as pb
@@ -168,7 +170,7 @@ def launches_per_pass(mesh) -> int:
     n_enr = tmpl[np.asarray(mesh.export()["cut_tmpl"], dtype=np.int64), 1] if mesh.info["n_cut_elements"] else []
     nl = 3 + np.asarray(n_enr)
     classes = {int(np.searchsorted([5, 7, 11, 15], v)) for v in nl}
-    return 1 + (1 if classes else 0) + len(classes)
+    return 1 + (2 if classes else 0) + len(classes)
 
 
 def measured_peak_hbm():
@@ -290,9 +292,9 @@ def run_b200_arm(args):
     if args.tile is not None:
         _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, args.tile, t_pers.value, t_warps.value))
         _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
-    tri_kernel = "k_assemble_grid" if t_tile.value in (93, 124, 217) else "k_assemble_tri"
+    tri_kernel = "k_grid_rows" if t_tile.value in (128, 256) else "k_assemble_tri"
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
-              "ms_tri_rows32_rows32p_rows64_rows64p_gridsweep": [round(v, 4) for v in ms_tri],
+              "ms_tri_rows32_rows32p_rows64_rows64p_grid": [round(v, 4) for v in ms_tri],
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
 
     for _ in range(args.warmup):
@@ -325,8 +327,17 @@ def run_b200_arm(args):
     # ---- roofline of the dominant kernel (node rows) ----
     n_blocks, n_nodes, n_cut = info["n_blocks"], info["n_nodes"], info["n_cut_elements"]
     n_uncut = n_e - n_cut
-    rows_bytes = 32 * n_blocks + 13 * n_uncut + 16 * n_nodes
-    pass_bytes = rows_bytes + 64 * n_cut + 16 * info["n_enrichment_nodes"]
+    n_reg = info["n_regular_nodes"]
+    if tri_kernel == "k_grid_rows":
+        # the grid kernel writes the blocks between regular nodes; the fold writes the
+        # enrichment rows and columns
+        ex = mesh.export()
+        row_of = np.repeat(np.arange(n_nodes), np.diff(ex["row_ptr"]))
+        reg_blocks = int(np.count_nonzero((row_of < n_reg) & (ex["col"] < n_reg)))
+        rows_bytes = 32 * reg_blocks + 13 * n_uncut + 16 * n_reg
+    else:
+        rows_bytes = 32 * n_blocks + 13 * n_uncut + 16 * n_nodes
+    pass_bytes = 32 * n_blocks + 13 * n_uncut + 16 * n_nodes + 64 * n_cut
     peak, peak_kind = measured_peak_hbm()
     avg_rows = statistics.mean(rows_ms) / 1e3
     achieved = rows_bytes / avg_rows / 1e9

@@ -271,9 +271,11 @@ int pg_get_vector(pg_ctx* c, int32_t which, double* out); /* which: 0=U, 1=F_int
 int pg_set_vector(pg_ctx* c, int32_t which, const double* in);
 int pg_get_isv(pg_ctx* c, int32_t committed, double* out);/* n_cohesive_qp delta_max values */
 int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
-/* Device time of the last assembly's two kernels (node rows, cut elements), from CUDA
- * events recorded on the assembly stream while timing is enabled; pass NULLs to only
- * switch timing on/off. */
+/* Device time of the last assembly, from CUDA events recorded on the assembly stream
+ * while timing is enabled: ms_rows = the triangle kernel, ms_cut = from its end to the end
+ * of the pass (the cut elements' work on the second stream, as far as it outlasts the
+ * triangle kernel, and the fold).  Their sum is the pass.  Pass NULLs to only switch
+ * timing on/off. */
 int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
 /* ---- shape sensitivity ----
@@ -290,17 +292,19 @@ int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double
 
 /* ---- autotuning of the assembly launch shapes ----
  * No counterpart in the reference.  Times every launch shape of the two
- * assembly kernels on this context's mesh (L2 flushed before each launch,
+ * assembly stages on this context's mesh (L2 flushed before each launch,
  * `reps` launches each) and keeps the fastest of each for later assemblies:
- * ms_tri[5] = triangle kernel gathering over 32 / 64 consecutive node rows per
- * CTA, each with one CTA per tile / a persistent grid, then the edge-centric
- * kernel of the structured background grid (the fastest of its 31 x 3,
- * 31 x 4 and 31 x 7 node tiles; 0 if the mesh has none); ms_cut[3] = cut-element kernel with 2 / 4 / 8 elements per CTA (NULL
+ * ms_tri[5] = the row-tile triangle kernel gathering over 32 / 64 consecutive
+ * node rows per CTA, each with one CTA per tile / a persistent grid, then the
+ * structured-grid kernel (one thread per regular node row; the faster of 128
+ * and 256 threads per CTA; 0 if the mesh is not one structured grid);
+ * ms_cut[3] = the cut elements' work (quadrature rows, cohesive points, pair
+ * blocks, fold) with 2 / 4 / 8 warps per CTA of the pair kernel (NULL
  * allowed).  K is left to be reassembled. */
 int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
-/* the launch shapes in use, and setting them by hand (tile 32 or 64 rows, or 93 / 124 / 217 for
- * the structured-grid kernel's 31 x 3 / 31 x 4 / 31 x 7 node tiles; persistent 0/1 for the row
- * tiles; warps 2/4/8) */
+/* the launch shapes in use, and setting them by hand (tile 32 or 64 node rows per CTA of the
+ * row-tile kernel, or 128 / 256 threads per CTA of the structured-grid kernel; persistent 0/1
+ * for the row tiles; warps 2/4/8 per CTA of the cut elements' pair kernel) */
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
 int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
 

@@ -639,6 +639,545 @@ void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmp
         }
 }
 
+// ---------------------------------------------------------------------------
+// Uncut triangles of a structured background grid: one thread per node row
+// ---------------------------------------------------------------------------
+// The background mesh is nx x ny cells of two triangles each (element
+// 2 (i + j nx) + t, diagonal alternating with (i + j) % 2), regular node
+// (i, j) = i + j (nx + 1).  Row (i, j) of K holds the node's grid neighbours
+// -- all four axis neighbours, and the four diagonal ones for even nodes
+// ((i + j) % 2 == 0), the only nodes a cell diagonal passes through -- in
+// ascending order, then enrichment columns; grid_pattern_ok checks that
+// layout on the host before this kernel is used.
+//
+// A thread owns one regular node and writes its row: in registers, it forms
+// row v of the constant-strain stiffness of every uncut triangle around the
+// node (8 for an even node, 4 for an odd one; the reference's 4-point rule
+// integrates the constant integrand exactly, its weights summing to 1/2),
+// sums them into the node's grid-neighbour blocks and stores each block
+// once with a 256-bit store.  A triangle is thus formed by each of its three
+// vertices' threads; the FP64 pipe has room for that, and nothing is staged
+// in shared memory, exchanged between threads or waited for.  The lanes of
+// a warp take nodes of one parity from one grid row (every other node
+// column), so every lane runs the same, fully unrolled triangle code.
+// Enrichment columns and enrichment rows are not touched: the cut-element
+// fold writes them whole.  With WF the thread also forms its two f_int
+// entries from the same row blocks.
+constexpr int kGridLanes = 32;  // lanes of a (row, parity) segment are padded to whole warps
+
+// Corner (di + 2 dj) of local vertex m of triangle t in a cell of parity cp
+// ((i + j) % 2): {n00, n10, n11}, {n00, n11, n01} for even cells,
+// {n00, n10, n01}, {n10, n11, n01} for odd ones.
+__host__ __device__ constexpr int tri_corner(int cp, int t, int m) {
+    return cp == 0 ? (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 3) : (m == 0 ? 0 : m == 1 ? 3 : 2))
+                   : (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 2) : (m == 0 ? 1 : m == 1 ? 3 : 2));
+}
+
+// Grid neighbours of node (gi, gj) present in its row, as bits d = 3 (dy + 1)
+// + (dx + 1) (bit 4 the node itself): axis neighbours inside the grid, and
+// the diagonal ones too for even nodes.  A block's place in the row is the
+// number of lower bits set.
+__host__ __device__ inline unsigned grid_nbr_mask(int gi, int gj, int nx, int ny) {
+    const bool even = ((gi + gj) & 1) == 0;
+    const bool w = gi > 0, e = gi < nx, s = gj > 0, n = gj < ny;
+    return (s && even && w ? 1u : 0u) | (s ? 2u : 0u) | (s && even && e ? 4u : 0u) | (w ? 8u : 0u) | 16u |
+           (e ? 32u : 0u) | (n && even && w ? 64u : 0u) | (n ? 128u : 0u) | (n && even && e ? 256u : 0u);
+}
+
+// One 2x2 block as a single 256-bit store (K is a cudaMalloc allocation, so
+// every block is 32-byte aligned).
+__device__ __forceinline__ void store_block(double* K, long long q, double k0, double k1, double k2, double k3) {
+    double* dst = K + 4 * q;
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "d"(k0), "d"(k1), "d"(k2), "d"(k3) : "memory");
+}
+
+// One 2x2 block as a single 256-bit load through the read-only path (data
+// the launch does not write).
+__device__ __forceinline__ double4 load_block_nc(const double* K, long long q) {
+    double4 v;
+    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+                 : "l"(K + 4 * q));
+    return v;
+}
+
+// The same from memory the launch also writes (plain load).
+__device__ __forceinline__ double4 load_block(const double* K, long long q) {
+    double4 v;
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+                 : "l"(K + 4 * q)
+                 : "memory");
+    return v;
+}
+
+struct GridArgs {
+    int nx, ny;
+    int kpad;                           // threads per (grid row, parity) segment, a multiple of kGridLanes
+    const int* __restrict__ row_ptr;
+    const int* __restrict__ emat;       // per element: material, -1 for cut elements
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ dmat;
+    double* K;
+    double* f;
+};
+
+// Local vertex of the node in triangle T of the cell at offset (OX - 1,
+// OY - 1) from a node of parity Q (the node is that cell's corner
+// (1 - OX, 1 - OY)); -1 when the triangle does not contain it.
+template <int Q, int OX, int OY, int T>
+struct GridTri {
+    static constexpr int cp = (Q + OX + OY) & 1;  // parity of the cell
+    static constexpr int cn = (1 - OX) + 2 * (1 - OY);
+    static constexpr int v = tri_corner(cp, T, 0) == cn ? 0 : tri_corner(cp, T, 1) == cn ? 1
+                           : tri_corner(cp, T, 2) == cn ? 2 : -1;
+    // position of vertex m in the node's 3 x 3 neighbourhood
+    __host__ __device__ static constexpr int dx(int m) { return OX + (tri_corner(cp, T, m) & 1); }
+    __host__ __device__ static constexpr int dy(int m) { return OY + (tri_corner(cp, T, m) >> 1); }
+};
+
+// 2 x (signed area) of triangle T of the cell
+template <int Q, int OX, int OY, int T>
+__device__ __forceinline__ double grid_tri_J(const double (&X)[3][3], const double (&Y)[3][3]) {
+    using G = GridTri<Q, OX, OY, T>;
+    const double X0 = X[G::dy(0)][G::dx(0)], X1 = X[G::dy(1)][G::dx(1)], X2 = X[G::dy(2)][G::dx(2)];
+    const double Y0 = Y[G::dy(0)][G::dx(0)], Y1 = Y[G::dy(1)][G::dx(1)], Y2 = Y[G::dy(2)][G::dx(2)];
+    return (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+}
+
+// Adds row v (the node's) of triangle T's stiffness, scaled by s = 1 / (2 J),
+// to the neighbour blocks acc[d] (d = 3 dy + dx; acc[4] = diagonal block as
+// k00, k01, k11) and, with WF, K_vw u_w to (fx, fy).
+template <int Q, int OX, int OY, int T, bool WK, bool WF>
+__device__ __forceinline__ void grid_tri_row(const double (&X)[3][3], const double (&Y)[3][3],
+                                             const double (&UX)[3][3], const double (&UY)[3][3], double s,
+                                             const double* __restrict__ D, double (&acc)[9][4], double& fx,
+                                             double& fy) {
+    using G = GridTri<Q, OX, OY, T>;
+    constexpr int v = G::v;
+    const double X0 = X[G::dy(0)][G::dx(0)], X1 = X[G::dy(1)][G::dx(1)], X2 = X[G::dy(2)][G::dx(2)];
+    const double Y0 = Y[G::dy(0)][G::dx(0)], Y1 = Y[G::dy(1)][G::dx(1)], Y2 = Y[G::dy(2)][G::dx(2)];
+    const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
+    const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
+    const double E0 = s * __ldg(&D[0]), E1 = s * __ldg(&D[1]), E2 = s * __ldg(&D[2]);
+    const double bv = b[v], cv = c[v];
+    const double Xv = bv * E0, Yv = bv * E1, Zv = bv * E2, Uv = cv * E0, Vv = cv * E1, Wv = cv * E2;
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+        const int d = 3 * G::dy(w) + G::dx(w);
+        const double k0 = Xv * b[w] + Wv * c[w];
+        const double k1 = Yv * c[w] + Wv * b[w];
+        const double k2 = Vv * b[w] + Zv * c[w];
+        const double k3 = Uv * c[w] + Zv * b[w];
+        if (WK) {
+            if (w == v) {
+                acc[4][0] += k0;
+                acc[4][1] += k1;
+                acc[4][2] += k3;
+            } else {
+                acc[d][0] += k0;
+                acc[d][1] += k1;
+                acc[d][2] += k2;
+                acc[d][3] += k3;
+            }
+        }
+        if (WF) {
+            const double ux = UX[G::dy(w)][G::dx(w)], uy = UY[G::dy(w)][G::dx(w)];
+            fx += k0 * ux + k1 * uy;
+            fy += k2 * ux + k3 * uy;
+        }
+    }
+}
+
+// The uncut triangles of cell (OX, OY) around the node (cell (gi - 1 + OX,
+// gj - 1 + OY), materials m0, m1, -1 for cut or absent triangles).  When
+// both contain the node, their two scales share one division.
+template <int Q, int OX, int OY, bool WK, bool WF>
+__device__ __forceinline__ void grid_cell(const double (&X)[3][3], const double (&Y)[3][3], const double (&UX)[3][3],
+                                          const double (&UY)[3][3], int m0, int m1,
+                                          const double* __restrict__ dmat, double (&acc)[9][4], double& fx,
+                                          double& fy) {
+    constexpr bool h0 = GridTri<Q, OX, OY, 0>::v >= 0, h1 = GridTri<Q, OX, OY, 1>::v >= 0;
+    if constexpr (h0 && h1) {
+        if (m0 < 0 && m1 < 0) return;
+        const double J0 = grid_tri_J<Q, OX, OY, 0>(X, Y), J1 = grid_tri_J<Q, OX, OY, 1>(X, Y);
+        const double r = 0.5 / (J0 * J1);
+        if (m0 >= 0) grid_tri_row<Q, OX, OY, 0, WK, WF>(X, Y, UX, UY, r * J1, dmat + 3 * m0, acc, fx, fy);
+        if (m1 >= 0) grid_tri_row<Q, OX, OY, 1, WK, WF>(X, Y, UX, UY, r * J0, dmat + 3 * m1, acc, fx, fy);
+    } else if constexpr (h0) {
+        if (m0 < 0) return;
+        const double s = 0.5 / grid_tri_J<Q, OX, OY, 0>(X, Y);
+        grid_tri_row<Q, OX, OY, 0, WK, WF>(X, Y, UX, UY, s, dmat + 3 * m0, acc, fx, fy);
+    } else {
+        if (m1 < 0) return;
+        const double s = 0.5 / grid_tri_J<Q, OX, OY, 1>(X, Y);
+        grid_tri_row<Q, OX, OY, 1, WK, WF>(X, Y, UX, UY, s, dmat + 3 * m1, acc, fx, fy);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void grid_store(double* K, int q0, unsigned mask, const double (&acc)[9][4]) {
+    if (mask & (1u << D)) {
+        const long long q = q0 + __popc(mask & ((1u << D) - 1u));
+        if (D == 4) store_block(K, q, acc[4][0], acc[4][1], acc[4][1], acc[4][2]);
+        else store_block(K, q, acc[D][0], acc[D][1], acc[D][2], acc[D][3]);
+    }
+}
+
+template <int Q, bool WK, bool WF>
+__device__ __forceinline__ void grid_node(const GridArgs& a, int gi, int gj) {
+    const int nx = a.nx, ny = a.ny, NX1 = nx + 1;
+    const int node = gi + gj * NX1;
+    // coordinates (and displacements) of the node's 3 x 3 neighbourhood,
+    // [dy + 1][dx + 1]; entries outside the grid are never read (an odd
+    // node's triangles do not reach the diagonal ones at all)
+    double X[3][3], Y[3][3], UX[3][3], UY[3][3];
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+            const int ni = gi + dx - 1, nj = gj + dy - 1;
+            const bool in = ni >= 0 && ni <= nx && nj >= 0 && nj <= ny;
+            const int n = in ? ni + nj * NX1 : node;
+            X[dy][dx] = __ldg(&a.x[n]);
+            Y[dy][dx] = __ldg(&a.y[n]);
+            UX[dy][dx] = WF ? __ldg(&a.u[2 * n]) : 0.0;
+            UY[dy][dx] = WF ? __ldg(&a.u[2 * n + 1]) : 0.0;
+        }
+    // materials of the two triangles of the four cells around the node
+    // (cell (gi - 1 + ox, gj - 1 + oy)); -1 for a cut or absent triangle
+    int2 M[2][2];
+#pragma unroll
+    for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+        for (int ox = 0; ox < 2; ++ox) {
+            const int ci = gi - 1 + ox, cj = gj - 1 + oy;
+            const bool in = ci >= 0 && ci < nx && cj >= 0 && cj < ny;
+            M[oy][ox] = in ? __ldg(reinterpret_cast<const int2*>(a.emat) + (ci + (size_t)cj * nx)) : make_int2(-1, -1);
+        }
+    const int q0 = WK ? __ldg(&a.row_ptr[node]) : 0;
+    const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+    double acc[9][4];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) acc[d][0] = acc[d][1] = acc[d][2] = acc[d][3] = 0.0;
+    double fx = 0.0, fy = 0.0;
+    // cells in the order that completes blocks early: below (d = 0, 1, 2
+    // done), above left (d = 3, 6), above right (d = 4, 5, 7, 8)
+    grid_cell<Q, 0, 0, WK, WF>(X, Y, UX, UY, M[0][0].x, M[0][0].y, a.dmat, acc, fx, fy);
+    grid_cell<Q, 1, 0, WK, WF>(X, Y, UX, UY, M[0][1].x, M[0][1].y, a.dmat, acc, fx, fy);
+    if (WK) {
+        if (Q == 0) grid_store<0>(a.K, q0, mask, acc);
+        grid_store<1>(a.K, q0, mask, acc);
+        if (Q == 0) grid_store<2>(a.K, q0, mask, acc);
+    }
+    grid_cell<Q, 0, 1, WK, WF>(X, Y, UX, UY, M[1][0].x, M[1][0].y, a.dmat, acc, fx, fy);
+    if (WK) {
+        grid_store<3>(a.K, q0, mask, acc);
+        if (Q == 0) grid_store<6>(a.K, q0, mask, acc);
+    }
+    grid_cell<Q, 1, 1, WK, WF>(X, Y, UX, UY, M[1][1].x, M[1][1].y, a.dmat, acc, fx, fy);
+    if (WK) {
+        grid_store<4>(a.K, q0, mask, acc);
+        grid_store<5>(a.K, q0, mask, acc);
+        grid_store<7>(a.K, q0, mask, acc);
+        if (Q == 0) grid_store<8>(a.K, q0, mask, acc);
+    }
+    if (WF) {
+        a.f[2 * (size_t)node] = fx;
+        a.f[2 * (size_t)node + 1] = fy;
+    }
+}
+
+// Thread t: segment t / kpad = 2 gj + q (grid row gj, parity q), lane
+// k = t % kpad, node column gi = 2 k + ((gj + q) & 1).
+template <bool WK, bool WF>
+__global__ void __launch_bounds__(256) k_grid_rows(GridArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int seg = t / a.kpad, k = t - seg * a.kpad;
+    const int gj = seg >> 1, q = seg & 1;
+    if (gj > a.ny) return;
+    const int gi = 2 * k + ((gj + q) & 1);
+    if (gi > a.nx) return;
+    if (q == 0) grid_node<0, WK, WF>(a, gi, gj);
+    else grid_node<1, WK, WF>(a, gi, gj);
+}
+
+// True when every regular row of the block pattern is laid out as
+// k_grid_rows assumes: the node's grid neighbours (grid_nbr_mask) and
+// itself in ascending order, then only enrichment columns.
+bool grid_pattern_ok(const HostMesh& hm) {
+    const int nx = hm.spec.nx, ny = hm.spec.ny;
+    if ((long long)(nx + 1) * (ny + 1) != hm.n_reg) return false;
+    for (int gj = 0; gj <= ny; ++gj)
+        for (int gi = 0; gi <= nx; ++gi) {
+            const int i = gi + gj * (nx + 1);
+            const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+            int q = hm.row_ptr[i];
+            for (int d = 0; d < 9; ++d) {
+                if (!(mask & (1u << d))) continue;
+                const int j = (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
+                if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
+                ++q;
+            }
+            for (; q < hm.row_ptr[i + 1]; ++q)
+                if (hm.col[q] < hm.n_reg) return false;
+        }
+    return true;
+}
+
+int grid_kpad(int nx) { return ((nx + 2) / 2 + kGridLanes - 1) / kGridLanes * kGridLanes; }
+
+void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
+    GridArgs ga;
+    ga.nx = c.hm.spec.nx;
+    ga.ny = c.hm.spec.ny;
+    ga.kpad = grid_kpad(ga.nx);
+    ga.row_ptr = c.row_ptr;
+    ga.emat = c.grid_emat;
+    ga.x = c.x;
+    ga.y = c.y;
+    ga.u = U;
+    ga.dmat = c.dmat;
+    ga.K = c.K;
+    ga.f = c.F;
+    const long long threads = 2LL * (ga.ny + 1) * ga.kpad;
+    const int bs = c.tuning.grid_block;
+    const int blocks = (int)((threads + bs - 1) / bs);
+    if (want_K && want_f) k_grid_rows<true, true><<<blocks, bs, 0, s>>>(ga);
+    else if (want_K) k_grid_rows<true, false><<<blocks, bs, 0, s>>>(ga);
+    else if (want_f) k_grid_rows<false, true><<<blocks, bs, 0, s>>>(ga);
+}
+
+// ---------------------------------------------------------------------------
+// Cut elements: per-pair integration into a compact buffer, then a fold
+// ---------------------------------------------------------------------------
+// Every cut element's (3 + n_enr)^2 node-pair blocks have a fixed place in
+// the element's slot table (cut_slot: pair (a, b) at cut_slot_ptr + a nl +
+// b, holding the block's K slot).  k_cut_pairs integrates one pair per
+// thread into the compact buffer cut_ke at the pair's slot-table position
+// (and, for residual passes, K_ab u_b into cut_fe); nothing is added into K
+// there.  k_fold_K then gives every K slot that cut elements touch its final
+// value in one thread: the regular-element value the triangle kernel wrote
+// (or zero, for blocks in enrichment rows or columns, which only cut
+// elements reach) plus its contributions in a fixed order, a list built once
+// per mesh and sorted by (element, pair).  k_fold_f does the same per node
+// for f_int.  The sums are the same on every run: no atomics.
+//
+// The quadrature rows (k_cut_points), the cohesive points (k_coh_points)
+// and the pairs depend on the coordinates, the displacements and the
+// committed cohesive state only, so they run on a second stream beside the
+// triangle kernel; only the fold waits for both.
+
+// Rows of the cohesive Gauss points (CohEdge2, 2 points, w = 1): one thread
+// per point evaluates the traction-separation law at its opening (writing
+// the trial delta_max) and stores {w dA, N0, N1, (R^T D R) 4, (R^T t) 2} for
+// the pair kernel.  Point qp of a cohesive sub-element ce of element ci
+// (class order) is qp = cut_coh_qp0[ci] + 2 ce + q; coh_rec[qp] packs
+// ci << 8 | ce << 1 | q.
+constexpr int kCohRow = kCohRowDoubles;
+
+struct CohArgs {
+    int n_qp;
+    const int* __restrict__ coh_rec;
+    const int* __restrict__ cut_nodes;
+    const int* __restrict__ cut_tmpl;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ u;
+    const double* __restrict__ isv_c;
+    double* isv_t;
+    double* coh_rows;
+    DevCohLaw coh;
+    double dt;
+};
+
+__global__ void __launch_bounds__(128) k_coh_points(CohArgs a) {
+    const int qp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qp >= a.n_qp) return;
+    const int rec = __ldg(&a.coh_rec[qp]);
+    const int ci = rec >> 8, ce = (rec >> 1) & 127, q = rec & 1;
+    const DevTemplate& T = g_tmpl[__ldg(&a.cut_tmpl[ci])];
+    const int* en = a.cut_nodes + (size_t)kCutNodeStride * ci;
+    int n[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) n[m] = __ldg(&en[T.coh_nodes[ce][m]]);
+    const double jx = 0.5 * (__ldg(&a.x[n[1]]) - __ldg(&a.x[n[0]]));
+    const double jy = 0.5 * (__ldg(&a.y[n[1]]) - __ldg(&a.y[n[0]]));
+    const double mag = sqrt(jx * jx + jy * jy);
+    const double nx = -jy, ny = jx;
+    const double dA = sqrt(nx * nx + ny * ny);
+    const double R[2][2] = {{jx / mag, jy / mag}, {nx / dA, ny / dA}};
+    const double xi = q == 0 ? -0.57735026918962576450914878050196 : 0.57735026918962576450914878050196;
+    const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+    double dg[2];
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+        dg[d] = N0 * (__ldg(&a.u[2 * n[2] + d]) - __ldg(&a.u[2 * n[0] + d])) +
+                N1 * (__ldg(&a.u[2 * n[3] + d]) - __ldg(&a.u[2 * n[1] + d]));
+    double dl[2] = {R[0][0] * dg[0] + R[0][1] * dg[1], R[1][0] * dg[0] + R[1][1] * dg[1]};
+    double tr[2], Dc[2][2], dmax_t;
+    cohesive_law(a.coh, a.dt, __ldg(&a.isv_c[qp]), dl, tr, Dc, dmax_t);
+    a.isv_t[qp] = dmax_t;
+    double* row = a.coh_rows + (size_t)kCohRow * qp;
+    row[0] = dA * 1.0;
+    row[1] = N0;
+    row[2] = N1;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int k1 = 0; k1 < 2; ++k1)
+#pragma unroll
+                for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
+            row[3 + 2 * i + j] = s;
+        }
+    row[7] = R[0][0] * tr[0] + R[1][0] * tr[1];
+    row[8] = R[0][1] * tr[0] + R[1][1] * tr[1];
+    row[9] = 0.0;
+}
+
+struct PairArgs {
+    int n_elem;                     // elements of this size class
+    int first;                      // its first element in class order
+    const int* __restrict__ cut_nodes;
+    const int* __restrict__ cut_tmpl;
+    const int* __restrict__ cut_coh_qp0;
+    const int* __restrict__ cut_slot_ptr;
+    const double* __restrict__ rows;
+    const long long* __restrict__ row_off;
+    const double* __restrict__ coh_rows;
+    const double* __restrict__ u;
+    double* ke;                     // 4 per slot-table entry
+    double* fe;                     // 2 per slot-table entry
+    int want_K, want_f;
+};
+
+// One thread per node pair (a, b) of a cut element of size class NL (NL^2
+// threads per element; pairs beyond the element's nl^2 idle): the block
+// K_ab = sum_q w_q B_a^T D B_b over the element's quadrature rows
+// (value-major: value j of point q at j nq + q, so the threads of an element
+// read the same addresses), plus the cohesive sub-elements' N_a N_b (+-)
+// R^T D R R terms when both nodes are cohesive nodes.  Residual passes store
+// K_ab u_b, and on the diagonal pair the node's cohesive traction term.
+template <int NL>
+__global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
+    constexpr int P = NL * NL, W = 4 + 2 * NL;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int oi = (int)(t / P), p = (int)(t - (long long)oi * P);
+    if (oi >= a.n_elem) return;
+    const int ci = a.first + oi;
+    const DevTemplate& T = g_tmpl[__ldg(&a.cut_tmpl[ci])];
+    const int nl = 3 + T.n_enr;
+    if (p >= nl * nl) return;
+    const int pa = p / nl, pb = p - pa * nl;
+    const long long r0 = __ldg(&a.row_off[ci]);
+    const int nq = (int)((__ldg(&a.row_off[ci + 1]) - r0) / W);
+    const double* rw = a.rows + r0;
+    double k0 = 0.0, k1 = 0.0, k2 = 0.0, k3 = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        const double wgt = __ldg(&rw[q]), d11 = __ldg(&rw[nq + q]), d12 = __ldg(&rw[2 * nq + q]),
+                     d33 = __ldg(&rw[3 * nq + q]);
+        const double ba = __ldg(&rw[(4 + 2 * pa) * nq + q]) * wgt, ca = __ldg(&rw[(5 + 2 * pa) * nq + q]) * wgt;
+        const double bb = __ldg(&rw[(4 + 2 * pb) * nq + q]), cb = __ldg(&rw[(5 + 2 * pb) * nq + q]);
+        k0 += ba * d11 * bb + ca * d33 * cb;
+        k1 += ba * d12 * cb + ca * d33 * bb;
+        k2 += ca * d12 * bb + ba * d33 * cb;
+        k3 += ca * d11 * cb + ba * d33 * bb;
+    }
+    // bulk internal force term K_ab u_b (the cohesive part of f_int is the
+    // traction integral below, not the cohesive tangent times u)
+    double fx = 0.0, fy = 0.0;
+    if (a.want_f) {
+        const int node_b = __ldg(&a.cut_nodes[(size_t)kCutNodeStride * ci + pb]);
+        const double ux = __ldg(&a.u[2 * node_b]), uy = __ldg(&a.u[2 * node_b + 1]);
+        fx = k0 * ux + k1 * uy;
+        fy = k2 * ux + k3 * uy;
+    }
+    double tx = 0.0, ty = 0.0;  // cohesive traction of node a (diagonal pair only)
+    if (T.n_coh > 0) {
+        const int qp0 = __ldg(&a.cut_coh_qp0[ci]);
+        for (int ce = 0; ce < T.n_coh; ++ce) {
+            int i = -1, j = -1;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                if (T.coh_nodes[ce][m] == pa) i = m;
+                if (T.coh_nodes[ce][m] == pb) j = m;
+            }
+            if (i < 0 || j < 0) continue;
+            const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
+            const double sa = i < 2 ? -1.0 : 1.0;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const double* row = a.coh_rows + (size_t)kCohRow * (qp0 + 2 * ce + q);
+                const double wgt = __ldg(&row[0]);
+                if (wgt == 0.0) continue;
+                const double Na = __ldg(&row[1 + (i & 1)]), Nb = __ldg(&row[1 + (j & 1)]);
+                const double v = wgt * sgn * Na * Nb;
+                k0 += v * __ldg(&row[3]);
+                k1 += v * __ldg(&row[4]);
+                k2 += v * __ldg(&row[5]);
+                k3 += v * __ldg(&row[6]);
+                if (pa == pb) {
+                    tx += wgt * sa * Na * __ldg(&row[7]);
+                    ty += wgt * sa * Na * __ldg(&row[8]);
+                }
+            }
+        }
+    }
+    const long long sidx = __ldg(&a.cut_slot_ptr[ci]) + (long long)p;
+    if (a.want_K) store_block(a.ke, sidx, k0, k1, k2, k3);
+    if (a.want_f) reinterpret_cast<double2*>(a.fe)[sidx] = make_double2(fx + tx, fy + ty);
+}
+
+// K slots that cut elements touch, one thread each: K[slot] = (the triangle
+// kernel's value, or 0 where flagged as cut-only) + the slot's pair blocks
+// in list order.  Entry j: fold_slot[j] = slot << 1 | cut_only, pairs
+// fold_idx[fold_ptr[j] .. fold_ptr[j + 1]).
+__global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restrict__ fold_slot,
+                                                const int* __restrict__ fold_ptr, const int* __restrict__ fold_idx,
+                                                const double* __restrict__ ke, double* K) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const long long sw = __ldg(&fold_slot[j]);
+    const long long slot = sw >> 1;
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (!(sw & 1)) acc = load_block(K, slot);
+    const int i1 = __ldg(&fold_ptr[j + 1]);
+    for (int i = __ldg(&fold_ptr[j]); i < i1; ++i) {
+        const double4 v = load_block_nc(ke, __ldg(&fold_idx[i]));
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
+    }
+    store_block(K, slot, acc.x, acc.y, acc.z, acc.w);
+}
+
+// f_int of the nodes cut elements touch, one thread each: f = (the triangle
+// kernel's value, or 0 for enrichment nodes) + the node's pair terms in
+// list order.  fold_node[j] = node << 1 | cut_only.
+__global__ void __launch_bounds__(256) k_fold_f(int n, const int* __restrict__ fold_node,
+                                                const int* __restrict__ fold_ptr, const int* __restrict__ fold_idx,
+                                                const double* __restrict__ fe, double* f) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int nw = __ldg(&fold_node[j]);
+    const int node = nw >> 1;
+    double2 acc = make_double2(0.0, 0.0);
+    if (!(nw & 1)) acc = reinterpret_cast<const double2*>(f)[node];
+    const int i1 = __ldg(&fold_ptr[j + 1]);
+    for (int i = __ldg(&fold_ptr[j]); i < i1; ++i) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(fe) + __ldg(&fold_idx[i]));
+        acc.x += v.x;
+        acc.y += v.y;
+    }
+    reinterpret_cast<double2*>(f)[node] = acc;
+}
+
 // Per-warp shared tables: one row per quadrature point of the current chunk
 // holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
 // row per cohesive point holding {wgt, N0, N1, (R^T D R) 4, (R^T t) 2}.
@@ -916,473 +1455,8 @@ __global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, s
     }
 }
 
-template <int W>
-void launch_cut_w(int k, const CutArgs& ck, cudaStream_t s) {
-    // the two large classes keep at most 4 warps per CTA (48 KB of static shared memory)
-    constexpr int WL = W > 4 ? 4 : W;
-    const int cblocks = (ck.n_cut + W - 1) / W, lblocks = (ck.n_cut + WL - 1) / WL;
-    if (k == 0) k_assemble_cut<5, 1, W><<<cblocks, 32 * W, 0, s>>>(ck);
-    else if (k == 1) k_assemble_cut<7, 2, W><<<cblocks, 32 * W, 0, s>>>(ck);
-    else if (k == 2) k_assemble_cut<11, 4, WL><<<lblocks, 32 * WL, 0, s>>>(ck);
-    else k_assemble_cut<15, 8, WL><<<lblocks, 32 * WL, 0, s>>>(ck);
-}
-
-void launch_cut_class(int k, int warps, const CutArgs& ck, cudaStream_t s) {
-    if (warps == 2) launch_cut_w<2>(k, ck, s);
-    else if (warps == 8) launch_cut_w<8>(k, ck, s);
-    else launch_cut_w<4>(k, ck, s);
-}
 
 
-// ---------------------------------------------------------------------------
-// Uncut triangles of a structured background grid: edge-centric tiles
-// ---------------------------------------------------------------------------
-// The background mesh is nx x ny cells of two triangles each (element
-// 2 (i + j nx) + t, diagonal alternating with (i + j) % 2), regular node
-// (i, j) = i + j (nx + 1).  On such a mesh every off-diagonal block of a
-// regular row is a mesh edge: horizontal, vertical, or the diagonal of a
-// cell, with at most two triangles on it whose local vertices follow from
-// the cells' parities.  Its place in the row is fixed too: the row holds the
-// node's grid neighbours (all four axis neighbours; the four diagonal ones
-// for even nodes only) in ascending order, then enrichment columns.
-// grid_pattern_ok checks that layout on the host before this kernel is used.
-//
-// A CTA owns a tile of kTileX node columns and TR node rows (3, 4 or 7, picked by
-// the autotuner), with the TR + 1 cell rows around them, and runs one thread
-// per staged triangle ((TR + 1) x 64) in three phases between two barriers:
-//   1. one load per thread of each staged quantity, all in flight at once
-//      and addressed by the tile alone: the materials of the staged
-//      triangles (-1 marks a cut element), the coordinates (and
-//      displacements) of the (TR + 2) x 33 staged nodes, the rows' pointers
-//      and the material table;
-//   2. one staged triangle per thread: its 6 x 6 stiffness (21 distinct
-//      values) into shared memory.  A cell row's triangles are kept t-major
-//      (slot 32 t + cell column) at an odd stride of 21 doubles, so the 16
-//      lanes of a half-warp reading 16 consecutive cells of one t, or one
-//      column each of either t, touch 16 distinct bank pairs;
-//   3. per warp two tasks: warps w < TR the horizontal edges and then the
-//      diagonal blocks of node row w (zeroing the row's enrichment columns);
-//      warps TR .. 2 TR the vertical edges and the cell diagonals of staged
-//      cell row w - TR; with WANT_F, the last warp the tile's f_int.
-// An edge's block is formed once and stored in both rows (the second as its
-// transpose) wherever the tile owns that row; blocks whose triangles are all
-// cut are stored as zeros for the cut-element kernel to add to.
-constexpr int kTileX = kGridTileX;             // node columns per tile (31)
-constexpr int kTileCells = kTileX + 1;         // staged cells per cell row (32)
-constexpr int kTileElems = 2 * kTileCells;     // staged triangles per cell row (64)
-constexpr int kTileNX = kTileX + 2;            // staged node columns (33)
-// Element stiffness in shared memory, kKeStride doubles per triangle: blocks
-// (0,1), (0,2), (1,2) row-major at 0, 4, 8 (pair a < b at 4 (a + b - 1));
-// diagonal block of vertex v as (k00, k01, k11) at kKeDiag + 3 v.
-constexpr int kKeStride = 21;
-constexpr int kKeDiag = 12;
-constexpr int kKeRow = kTileElems * kKeStride;
-// slot of triangle t of staged cell column cc within its cell row
-__host__ __device__ constexpr int tile_slot(int cc, int t) { return t * kTileCells + cc; }
-
-struct GridArgs {
-    int nx, ny;
-    int n_mat;                          // materials (at most kGridMaxMat)
-    int strips;                         // tiles across
-    int n_tiles;
-    // enrichment rows, cleared here for the cut-element kernel to add to:
-    // blocks [q_enr, n_blocks) and, with WANT_F, f entries [2 n_reg, 2 n_nodes)
-    long long q_enr, n_blocks;
-    int n_reg, n_nodes;
-    const int* __restrict__ row_ptr;
-    const int* __restrict__ emat;       // per element: material, -1 for cut elements
-    const double* __restrict__ x;
-    const double* __restrict__ y;
-    const double* __restrict__ u;
-    const double* __restrict__ dmat;
-    double* K;
-    double* f;
-    int want_K;
-};
-
-// Corner (di + 2 dj) of local vertex m of triangle t in a cell of parity cp
-// ((i + j) % 2): {n00, n10, n11}, {n00, n11, n01} for even cells,
-// {n00, n10, n01}, {n10, n11, n01} for odd ones.
-__host__ __device__ constexpr int tri_corner(int cp, int t, int m) {
-    return cp == 0 ? (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 3) : (m == 0 ? 0 : m == 1 ? 3 : 2))
-                   : (t == 0 ? (m == 0 ? 0 : m == 1 ? 1 : 2) : (m == 0 ? 1 : m == 1 ? 3 : 2));
-}
-
-// Local vertex, in triangle t of a cell of parity cp, of the node at the
-// cell's corner (1 - ox, 1 - oy); -1 if the triangle does not touch it.
-__host__ __device__ constexpr int sweep_vertex(int cp, int t, int ox, int oy) {
-    return tri_corner(cp, t, 0) == (1 - ox) + 2 * (1 - oy) ? 0
-         : tri_corner(cp, t, 1) == (1 - ox) + 2 * (1 - oy) ? 1
-         : tri_corner(cp, t, 2) == (1 - ox) + 2 * (1 - oy) ? 2 : -1;
-}
-
-// Grid neighbours of node (gi, gj) present in its row, as bits d = 3 (dy + 1)
-// + (dx + 1) (bit 4 the node itself): axis neighbours inside the grid, and
-// the diagonal ones too for even nodes.  A block's place in the row is the
-// number of lower bits set.
-__host__ __device__ inline unsigned grid_nbr_mask(int gi, int gj, int nx, int ny) {
-    const bool even = ((gi + gj) & 1) == 0;
-    const bool w = gi > 0, e = gi < nx, s = gj > 0, n = gj < ny;
-    return (s && even && w ? 1u : 0u) | (s ? 2u : 0u) | (s && even && e ? 4u : 0u) | (w ? 8u : 0u) | 16u |
-           (e ? 32u : 0u) | (n && even && w ? 64u : 0u) | (n ? 128u : 0u) | (n && even && e ? 256u : 0u);
-}
-
-__device__ __forceinline__ int grid_slot(int row_start, int gi, int gj, int nx, int ny, int d) {
-    return row_start + __popc(grid_nbr_mask(gi, gj, nx, ny) & ((1u << d) - 1u));
-}
-
-// One 2x2 block as a single 256-bit store (K is a cudaMalloc allocation, so
-// every block is 32-byte aligned): half the store requests of two 128-bit ones.
-__device__ __forceinline__ void store_block(double* K, int q, double k0, double k1, double k2, double k3) {
-    double* dst = K + 4 * (size_t)q;
-    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "d"(k0), "d"(k1), "d"(k2), "d"(k3) : "memory");
-}
-
-// adds the stored element block at e (4 values, row-major) to k
-__device__ __forceinline__ void add_block(const double* e, double k[4]) {
-    k[0] += e[0];
-    k[1] += e[1];
-    k[2] += e[2];
-    k[3] += e[3];
-}
-
-size_t grid_smem_bytes(bool want_f, int tr) {
-    const size_t nodes = (size_t)(tr + 2) * kTileNX;
-    return sizeof(double) * ((tr + 1) * (size_t)kKeRow + 2 * nodes + (want_f ? 2 * nodes : 0) + 3 * kGridMaxMat) +
-           sizeof(int) * ((tr + 1) * (size_t)kTileElems + tr * (kTileX + 1));
-}
-
-// Stiffness of triangle t of staged cell (cc, cr) (material mat >= 0).
-__device__ __forceinline__ void tile_element(double* ke, const double* sX, const double* sY, const double* sD,
-                                             int mat, int I0, int J0, int cr, int cc, int t) {
-    const int cp = (I0 + J0 + cc + cr) & 1;  // parity of cell (I0 - 1 + cc, J0 - 1 + cr)
-    double X[3], Y[3];
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const int code = tri_corner(cp, t, m);
-        const int k = (cr + (code >> 1)) * kTileNX + cc + (code & 1);
-        X[m] = sX[k];
-        Y[m] = sY[k];
-    }
-    const double J = (X[1] - X[0]) * (Y[2] - Y[0]) - (X[2] - X[0]) * (Y[1] - Y[0]);
-    const double s = 0.5 / J;
-    const double b[3] = {Y[1] - Y[2], Y[2] - Y[0], Y[0] - Y[1]};
-    const double c[3] = {X[2] - X[1], X[0] - X[2], X[1] - X[0]};
-    const double E0 = s * sD[3 * mat], E1 = s * sD[3 * mat + 1], E2 = s * sD[3 * mat + 2];
-    // K_ab = [Xa bb + Wa cb, Ya cb + Wa bb; Va bb + Za cb, Ua cb + Za bb] with
-    // X, Y, Z = b (E0, E1, E2), U, V, W = c (E0, E1, E2), E = D / (4 A)
-    double Xv[3], Yv[3], Zv[3], Uv[3], Vv[3], Wv[3];
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        Xv[m] = b[m] * E0; Yv[m] = b[m] * E1; Zv[m] = b[m] * E2;
-        Uv[m] = c[m] * E0; Vv[m] = c[m] * E1; Wv[m] = c[m] * E2;
-    }
-#pragma unroll
-    for (int pa = 0; pa < 2; ++pa)
-#pragma unroll
-        for (int pb = pa + 1; pb < 3; ++pb) {
-            double* d = ke + 4 * (pa + pb - 1);
-            d[0] = Xv[pa] * b[pb] + Wv[pa] * c[pb];
-            d[1] = Yv[pa] * c[pb] + Wv[pa] * b[pb];
-            d[2] = Vv[pa] * b[pb] + Zv[pa] * c[pb];
-            d[3] = Uv[pa] * c[pb] + Zv[pa] * b[pb];
-        }
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        double* d = ke + kKeDiag + 3 * m;
-        d[0] = Xv[m] * b[m] + Wv[m] * c[m];
-        d[1] = Yv[m] * c[m] + Wv[m] * b[m];
-        d[2] = Uv[m] * c[m] + Zv[m] * b[m];
-    }
-}
-
-template <bool WANT_F, int TR>
-__global__ void __launch_bounds__((TR + 1) * kTileElems, TR <= 3 ? 4 : (TR <= 4 ? 3 : 2)) k_assemble_grid(GridArgs a) {
-    constexpr int kTileThreads = (TR + 1) * kTileElems;  // one staged triangle per thread
-    static_assert((TR + 2) * kTileNX <= kTileThreads && TR * (kTileX + 1) <= kTileThreads &&
-                  2 * TR + 2 <= kTileThreads / 32, "one staged node and row pointer per thread; warps per task");
-    extern __shared__ __align__(16) unsigned char g_tile_smem[];
-    constexpr int kNodes = (TR + 2) * kTileNX;
-    double* sKe = reinterpret_cast<double*>(g_tile_smem);     // [TR + 1][kTileElems][kKeStride]
-    double* sX = sKe + (TR + 1) * kKeRow;                  // [TR + 2][kTileNX]
-    double* sY = sX + kNodes;
-    double* sU = sY + kNodes;                                  // WANT_F: [TR + 2][2 kTileNX]
-    double* sD = sU + (WANT_F ? 2 * kNodes : 0);               // [n_mat][3]: d11, d12, d33
-    int* sM = reinterpret_cast<int*>(sD + 3 * kGridMaxMat);   // [TR + 1][kTileElems]
-    int* sRp = sM + (TR + 1) * kTileElems;                 // [TR][kTileX + 1]: row pointers
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nx = a.nx, ny = a.ny, NXn = nx + 1;
-    const int I0 = (blockIdx.x % a.strips) * kTileX, J0 = (blockIdx.x / a.strips) * TR;
-    const int R = min(TR, ny + 1 - J0);  // node rows of this tile
-    // this CTA's share of the enrichment rows: cleared (no launch of its own)
-    if (a.want_K) {
-        const long long n = a.n_blocks - a.q_enr, chunk = (n + a.n_tiles - 1) / a.n_tiles;
-        const long long q0 = a.q_enr + blockIdx.x * chunk, q1 = min(q0 + chunk, a.n_blocks);
-        for (long long q = q0 + tid; q < q1; q += kTileThreads) store_block(a.K, (int)q, 0.0, 0.0, 0.0, 0.0);
-    }
-    if (WANT_F) {
-        const int n = 2 * (a.n_nodes - a.n_reg), chunk = (n + a.n_tiles - 1) / a.n_tiles;
-        const int i0 = 2 * a.n_reg + blockIdx.x * chunk, i1 = min(i0 + chunk, 2 * a.n_nodes);
-        for (int i = i0 + tid; i < i1; i += kTileThreads) a.f[i] = 0.0;
-    }
-    // ---- phase 1: one load per thread of each staged quantity ----
-    {
-        const int cr = tid / kTileElems, sl = tid % kTileElems;  // slot sl = tile_slot(cc, t)
-        const int ci = I0 - 1 + sl % kTileCells, cj = J0 - 1 + cr;
-        const int m = (ci >= 0 && ci < nx && cj >= 0 && cj < ny) ? __ldg(&a.emat[2 * (ci + cj * nx) + sl / kTileCells])
-                                                                 : -1;
-        double xv = 0.0, yv = 0.0, ux = 0.0, uy = 0.0;
-        const int gi = I0 - 1 + tid % kTileNX, gj = J0 - 1 + tid / kTileNX;
-        const bool in = tid < kNodes && gi >= 0 && gi <= nx && gj >= 0 && gj <= ny;
-        if (in) {
-            const int node = gi + gj * NXn;
-            xv = __ldg(&a.x[node]);
-            yv = __ldg(&a.y[node]);
-            if (WANT_F) {
-                ux = a.u[2 * node];
-                uy = a.u[2 * node + 1];
-            }
-        }
-        // row_ptr of tile node (I0 + k, J0 + r); k = kTileX gives the row end of the last one
-        const int rk = tid % (kTileX + 1), rr = tid / (kTileX + 1);
-        const int rp = rr < R ? __ldg(&a.row_ptr[min(I0 + rk, NXn) + (J0 + rr) * NXn]) : 0;
-        const double dm = tid < 3 * a.n_mat ? __ldg(&a.dmat[tid]) : 0.0;
-        sM[tid] = m;
-        if (tid < kNodes) {
-            sX[tid] = xv;
-            sY[tid] = yv;
-            if (WANT_F) {
-                sU[2 * tid] = ux;
-                sU[2 * tid + 1] = uy;
-            }
-        }
-        if (rr < TR) sRp[tid] = rp;
-        if (tid < 3 * a.n_mat) sD[tid] = dm;
-    }
-    __syncthreads();
-    // ---- phase 2: one staged triangle per thread ----
-    {
-        const int m = sM[tid], sl = tid % kTileElems;
-        if (m >= 0)
-            tile_element(sKe + tid * kKeStride, sX, sY, sD, m, I0, J0, tid / kTileElems, sl % kTileCells, sl / kTileCells);
-    }
-    __syncthreads();
-    // ---- phase 3: edges, diagonal blocks, f_int ----
-    if (warp < TR) {
-        const int r = warp, gj = J0 + r;
-        if (r < R) {
-            const double* kBelow = sKe + r * kKeRow;        // staged cell row r (global gj - 1)
-            const double* kAbove = sKe + (r + 1) * kKeRow;  // staged cell row r + 1 (global gj)
-            const int rs = r * (kTileX + 1);
-            // horizontal edge A = (gi, gj) - B = (gi + 1, gj), gi = I0 - 1 + lane (tile columns
-            // lane - 1 and lane): the top triangle (t = 1, vertices 2, 1) of the cell below,
-            // the bottom one (t = 0, vertices 0, 1) of the cell above
-            const int gi = I0 - 1 + lane;
-            if (a.want_K && gi >= 0 && gi + 1 <= nx) {
-                double k[4] = {0.0, 0.0, 0.0, 0.0};
-                const int eb = tile_slot(lane, 1), ea = tile_slot(lane, 0);
-                if (sM[r * kTileElems + eb] >= 0) {
-                    double t[4] = {0.0, 0.0, 0.0, 0.0};
-                    add_block(kBelow + eb * kKeStride + 8, t);  // block (1, 2): used transposed
-                    k[0] += t[0]; k[1] += t[2]; k[2] += t[1]; k[3] += t[3];
-                }
-                if (sM[(r + 1) * kTileElems + ea] >= 0) add_block(kAbove + ea * kKeStride + 0, k);
-                if (lane >= 1) store_block(a.K, grid_slot(sRp[rs + lane - 1], gi, gj, nx, ny, 5), k[0], k[1], k[2], k[3]);
-                if (lane < kTileX) store_block(a.K, grid_slot(sRp[rs + lane], gi + 1, gj, nx, ny, 3), k[0], k[2], k[1], k[3]);
-            }
-            // diagonal block of node (I0 + lane, gj) over its (at most 8) triangles; zeros in
-            // its enrichment columns
-            const int gn = I0 + lane;
-            if (a.want_K && lane < kTileX && gn <= nx) {
-                const int p = (gn + gj) & 1;
-                double d0 = 0.0, d1 = 0.0, d2 = 0.0;
-#pragma unroll
-                for (int oy = 0; oy < 2; ++oy) {
-                    const double* kb = oy ? kAbove : kBelow;
-#pragma unroll
-                    for (int ox = 0; ox < 2; ++ox)
-#pragma unroll
-                        for (int t = 0; t < 2; ++t) {
-                            // staged cell (lane + ox, r + oy), the node at its corner (1 - ox, 1 - oy)
-                            const int e = tile_slot(lane + ox, t);
-                            const int cp = p ^ ((ox + oy) & 1);
-                            const int v = cp ? sweep_vertex(1, t, ox, oy) : sweep_vertex(0, t, ox, oy);
-                            if (v < 0 || sM[(r + oy) * kTileElems + e] < 0) continue;
-                            const double* dv = kb + e * kKeStride + kKeDiag + 3 * v;
-                            d0 += dv[0];
-                            d1 += dv[1];
-                            d2 += dv[2];
-                        }
-                }
-                const int q0 = sRp[rs + lane], q1 = sRp[rs + lane + 1];
-                const unsigned mask = grid_nbr_mask(gn, gj, nx, ny);
-                store_block(a.K, q0 + __popc(mask & 15u), d0, d1, d1, d2);
-                for (int q = q0 + __popc(mask); q < q1; ++q) store_block(a.K, q, 0.0, 0.0, 0.0, 0.0);
-            }
-        }
-    } else if (warp < TR + TR + 1) {
-        // staged cell row s (global gj = J0 - 1 + s) between node rows s - 1 and s
-        const int s = warp - TR, gj = J0 - 1 + s;
-        const double* kc = sKe + s * kKeRow;
-        const bool ownLo = s >= 1 && s - 1 < R, ownHi = s < R;
-        if (a.want_K && gj >= 0 && gj < ny) {
-            // vertical edge A = (gi, gj) - B = (gi, gj + 1), gi = I0 + lane: in the left cell
-            // (parity cl) triangle t = cl with vertices (1, 2) if cl = 0, (0, 1) if cl = 1; in
-            // the right cell triangle t = cl with vertices (0, 2)
-            const int gi = I0 + lane;
-            if (lane < kTileX && gi <= nx) {
-                const int cl = (gi - 1 + gj) & 1;
-                double k[4] = {0.0, 0.0, 0.0, 0.0};
-                const int el = tile_slot(lane, cl), er = tile_slot(lane + 1, cl);
-                if (sM[s * kTileElems + el] >= 0) add_block(kc + el * kKeStride + (cl ? 0 : 8), k);
-                if (sM[s * kTileElems + er] >= 0) add_block(kc + er * kKeStride + 4, k);
-                if (ownLo)
-                    store_block(a.K, grid_slot(sRp[(s - 1) * (kTileX + 1) + lane], gi, gj, nx, ny, 7),
-                                k[0], k[1], k[2], k[3]);
-                if (ownHi)
-                    store_block(a.K, grid_slot(sRp[s * (kTileX + 1) + lane], gi, gj + 1, nx, ny, 1),
-                                k[0], k[2], k[1], k[3]);
-            }
-            // diagonal of cell (gc, gj), gc = I0 - 1 + lane, parity cp.  cp = 0: A = (gc, gj),
-            // B = (gc + 1, gj + 1), t0 vertices (0, 2), t1 (0, 1).  cp = 1: A = (gc + 1, gj),
-            // B = (gc, gj + 1), t0 vertices (1, 2), t1 (0, 2).
-            const int gc = I0 - 1 + lane;
-            if (gc >= 0 && gc < nx) {
-                const int cp = (gc + gj) & 1;
-                double k[4] = {0.0, 0.0, 0.0, 0.0};
-                const int e0 = tile_slot(lane, 0), e1 = tile_slot(lane, 1);
-                if (sM[s * kTileElems + e0] >= 0) add_block(kc + e0 * kKeStride + (cp ? 8 : 4), k);
-                if (sM[s * kTileElems + e1] >= 0) add_block(kc + e1 * kKeStride + (cp ? 4 : 0), k);
-                const int la = cp ? lane : lane - 1, lb = cp ? lane - 1 : lane;  // tile columns of A, B
-                if (ownLo && la >= 0 && la < kTileX)
-                    store_block(a.K, grid_slot(sRp[(s - 1) * (kTileX + 1) + la], I0 + la, gj, nx, ny, cp ? 6 : 8),
-                                k[0], k[1], k[2], k[3]);
-                if (ownHi && lb >= 0 && lb < kTileX)
-                    store_block(a.K, grid_slot(sRp[s * (kTileX + 1) + lb], I0 + lb, gj + 1, nx, ny, cp ? 2 : 0),
-                                k[0], k[2], k[1], k[3]);
-            }
-        }
-    } else if (WANT_F) {
-        // f_int of the tile's nodes, lane = node column
-        const int gn = I0 + lane;
-        for (int r = 0; r < R; ++r) {
-            const int gj = J0 + r;
-            if (lane >= kTileX || gn > nx) break;
-            const int p = (gn + gj) & 1;
-            double fx = 0.0, fy = 0.0;
-#pragma unroll
-            for (int oy = 0; oy < 2; ++oy) {
-                const double* kb = sKe + (r + oy) * kKeRow;
-#pragma unroll
-                for (int ox = 0; ox < 2; ++ox)
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        const int e = tile_slot(lane + ox, t);
-                        const int cp = p ^ ((ox + oy) & 1);
-                        const int v = cp ? sweep_vertex(1, t, ox, oy) : sweep_vertex(0, t, ox, oy);
-                        if (v < 0 || sM[(r + oy) * kTileElems + e] < 0) continue;
-                        const double* ke = kb + e * kKeStride;
-#pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            double k0, k1, k2, k3;
-                            if (m == v) {
-                                const double* dv = ke + kKeDiag + 3 * v;
-                                k0 = dv[0]; k1 = dv[1]; k2 = dv[1]; k3 = dv[2];
-                            } else {
-                                const double* eb = ke + 4 * (v + m - 1);
-                                k0 = eb[0]; k3 = eb[3];
-                                k1 = v < m ? eb[1] : eb[2];
-                                k2 = v < m ? eb[2] : eb[1];
-                            }
-                            const int code = tri_corner(cp, t, m);
-                            const int k = (r + oy + (code >> 1)) * kTileNX + lane + ox + (code & 1);
-                            const double ux = sU[2 * k], uy = sU[2 * k + 1];
-                            fx += k0 * ux + k1 * uy;
-                            fy += k2 * ux + k3 * uy;
-                        }
-                    }
-            }
-            const int node = gn + gj * NXn;
-            a.f[2 * node] = fx;
-            a.f[2 * node + 1] = fy;
-        }
-    }
-}
-
-// True when every regular row of the block pattern is laid out as
-// k_assemble_grid assumes: the node's grid neighbours (grid_nbr_mask) and
-// itself in ascending order, then only enrichment columns.
-bool grid_pattern_ok(const HostMesh& hm) {
-    const int nx = hm.spec.nx, ny = hm.spec.ny;
-    if ((long long)(nx + 1) * (ny + 1) != hm.n_reg) return false;
-    for (int gj = 0; gj <= ny; ++gj)
-        for (int gi = 0; gi <= nx; ++gi) {
-            const int i = gi + gj * (nx + 1);
-            const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
-            int q = hm.row_ptr[i];
-            for (int d = 0; d < 9; ++d) {
-                if (!(mask & (1u << d))) continue;
-                const int j = (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
-                if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
-                ++q;
-            }
-            for (; q < hm.row_ptr[i + 1]; ++q)
-                if (hm.col[q] < hm.n_reg) return false;
-        }
-    return true;
-}
-
-// Lifts k_assemble_grid's dynamic shared-memory limit, once per device and
-// outside any graph capture (called when a context is created).
-void grid_prepare() {
-    static bool done[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && done[dev]) return;
-    cudaFuncSetAttribute(k_assemble_grid<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 3));
-    cudaFuncSetAttribute(k_assemble_grid<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 3));
-    cudaFuncSetAttribute(k_assemble_grid<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 4));
-    cudaFuncSetAttribute(k_assemble_grid<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 4));
-    cudaFuncSetAttribute(k_assemble_grid<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(false, 7));
-    cudaFuncSetAttribute(k_assemble_grid<true, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem_bytes(true, 7));
-    if (dev >= 0 && dev < 64) done[dev] = true;
-}
-
-void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
-    GridArgs ga;
-    ga.nx = c.hm.spec.nx;
-    ga.ny = c.hm.spec.ny;
-    ga.n_mat = (int)c.hm.spec.materials.size();
-    ga.row_ptr = c.row_ptr;
-    ga.emat = c.grid_emat;
-    ga.x = c.x;
-    ga.y = c.y;
-    ga.u = U;
-    ga.dmat = c.dmat;
-    ga.K = c.K;
-    ga.f = c.F;
-    ga.want_K = want_K;
-    ga.strips = (ga.nx + 1 + kTileX - 1) / kTileX;
-    const int tr = c.tuning.grid_rows == 3 ? 3 : c.tuning.grid_rows == 4 ? 4 : 7;
-    const int tiles = ga.strips * ((ga.ny + 1 + tr - 1) / tr);
-    ga.n_tiles = tiles;
-    ga.q_enr = c.hm.row_ptr[c.n_reg];
-    ga.n_blocks = c.n_blocks;
-    ga.n_reg = c.n_reg;
-    ga.n_nodes = c.n_nodes;
-    const int threads = (tr + 1) * kTileElems;
-    grid_prepare();
-    if (tr == 3) {
-        if (want_f) k_assemble_grid<true, 3><<<tiles, threads, grid_smem_bytes(true, 3), s>>>(ga);
-        else k_assemble_grid<false, 3><<<tiles, threads, grid_smem_bytes(false, 3), s>>>(ga);
-    } else if (tr == 4) {
-        if (want_f) k_assemble_grid<true, 4><<<tiles, threads, grid_smem_bytes(true, 4), s>>>(ga);
-        else k_assemble_grid<false, 4><<<tiles, threads, grid_smem_bytes(false, 4), s>>>(ga);
-    } else {
-        if (want_f) k_assemble_grid<true, 7><<<tiles, threads, grid_smem_bytes(true, 7), s>>>(ga);
-        else k_assemble_grid<false, 7><<<tiles, threads, grid_smem_bytes(false, 7), s>>>(ga);
-    }
-}
 
 template <bool WANT_F, int TN>
 void launch_tri_tn(const Ctx& c, const RowArgs& ra, cudaStream_t s) {
@@ -1493,54 +1567,153 @@ void launch_cut_points(const Ctx& c, cudaStream_t s) {
     }
 }
 
-void launch_cut_classes(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+// Fold lists from the class-ordered slot tables (sp: per element its first
+// slot-table entry, sl: K slot of every pair, -1 none; nodes: kCutNodeStride
+// local nodes per element).  K: every touched slot with its pair entries in
+// slot-table order (element, then pair), flagged cut_only when its row or
+// column node is an enrichment node (no triangle-kernel value to add to).
+// f: every touched node with the entries of its pairs (a, *), in the same
+// order, flagged cut_only for enrichment nodes.
+void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
+                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& k_idx,
+                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& f_idx) {
+    const int nc = (int)sp.size() - 1;
+    std::vector<std::pair<long long, int>> ke, fe;  // (key, slot-table entry)
+    ke.reserve(sl.size());
+    fe.reserve(sl.size());
+    std::vector<char> k_cut_only;
+    for (int oi = 0; oi < nc; ++oi) {
+        const int np = sp[oi + 1] - sp[oi];
+        int nl = 0;
+        while (nl * nl < np) ++nl;
+        for (int p = 0; p < np; ++p) {
+            const int idx = sp[oi] + p, a = p / nl, b = p % nl;
+            const int na = nodes[(size_t)kCutNodeStride * oi + a], nb = nodes[(size_t)kCutNodeStride * oi + b];
+            const bool cut_only = na >= n_reg || nb >= n_reg;
+            if (sl[idx] >= 0) ke.emplace_back(((long long)sl[idx] << 1) | (cut_only ? 1 : 0), idx);
+            fe.emplace_back(((long long)na << 1) | (na >= n_reg ? 1 : 0), idx);
+        }
+    }
+    auto to_csr = [](std::vector<std::pair<long long, int>>& v, auto& keys, std::vector<int>& ptr,
+                     std::vector<int>& idx) {
+        std::sort(v.begin(), v.end());
+        keys.clear();
+        ptr.assign(1, 0);
+        idx.clear();
+        idx.reserve(v.size());
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (i == 0 || v[i].first != v[i - 1].first) {
+                if (i > 0) ptr.push_back((int)idx.size());
+                keys.push_back(v[i].first);
+            }
+            idx.push_back(v[i].second);
+        }
+        if (!v.empty()) ptr.push_back((int)idx.size());
+    };
+    to_csr(ke, k_slot, k_ptr, k_idx);
+    std::vector<long long> fk;
+    to_csr(fe, fk, f_ptr, f_idx);
+    f_node.assign(fk.begin(), fk.end());
+}
+
+void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s) {
+    if (c.n_coh_qp <= 0) return;
+    CohArgs ca;
+    ca.n_qp = c.n_coh_qp;
+    ca.coh_rec = c.coh_rec;
+    ca.cut_nodes = c.cut_nodes;
+    ca.cut_tmpl = c.cut_tmpl;
+    ca.x = c.x;
+    ca.y = c.y;
+    ca.u = U;
+    ca.isv_c = c.isv_c;
+    ca.isv_t = c.isv_t;
+    ca.coh_rows = c.coh_rows;
+    ca.coh = c.coh;
+    ca.dt = dt;
+    k_coh_points<<<(c.n_coh_qp + 127) / 128, 128, 0, s>>>(ca);
+}
+
+// one launch per size class; cut_warps x 32 threads per CTA
+void launch_cut_pairs(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
+    PairArgs pa;
+    pa.cut_nodes = c.cut_nodes;
+    pa.cut_tmpl = c.cut_tmpl;
+    pa.cut_coh_qp0 = c.cut_coh_qp0;
+    pa.cut_slot_ptr = c.cut_slot_ptr;
+    pa.rows = c.cut_rows;
+    pa.row_off = c.cut_row_off;
+    pa.coh_rows = c.coh_rows;
+    pa.u = U;
+    pa.ke = c.cut_ke;
+    pa.fe = c.cut_fe;
+    pa.want_K = want_K;
+    pa.want_f = want_f;
+    const int bs = 32 * c.tuning.cut_warps;
     for (int k = 0; k < kCutClasses; ++k) {
         const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
         if (n == 0) continue;
-        CutArgs ck = ca;
-        ck.n_cut = n;
-        ck.first = c.cut_class_off[k];
-        launch_cut_class(k, c.tuning.cut_warps, ck, s);
+        pa.n_elem = n;
+        pa.first = c.cut_class_off[k];
+        const long long threads = (long long)n * kCutClassNl[k] * kCutClassNl[k];
+        const int blocks = (int)((threads + bs - 1) / bs);
+        if (k == 0) k_cut_pairs<5><<<blocks, bs, 0, s>>>(pa);
+        else if (k == 1) k_cut_pairs<7><<<blocks, bs, 0, s>>>(pa);
+        else if (k == 2) k_cut_pairs<11><<<blocks, bs, 0, s>>>(pa);
+        else k_cut_pairs<15><<<blocks, bs, 0, s>>>(pa);
     }
 }
 
-void launch_cut_all(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, cudaStream_t s) {
+    if (want_K && c.n_fold_K > 0)
+        k_fold_K<<<(c.n_fold_K + 255) / 256, 256, 0, s>>>(c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.fold_K_idx,
+                                                         c.cut_ke, c.K);
+    if (want_f && c.n_fold_f > 0)
+        k_fold_f<<<(c.n_fold_f + 255) / 256, 256, 0, s>>>(c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.fold_f_idx,
+                                                         c.cut_fe, c.F);
+}
+
+// The cut elements' work that depends on the inputs only (quadrature rows,
+// cohesive points, pair blocks) on stream s
+void launch_cut_work(const Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
     launch_cut_points(c, s);
-    launch_cut_classes(c, ca, s);
+    launch_coh_points(c, U, dt, s);
+    launch_cut_pairs(c, U, want_f, want_K, s);
 }
 
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
-    // nothing to clear: the triangle kernel writes every value of K
+    // The triangle kernel writes every regular-element value of K (and f)
+    // once; the cut elements' rows, cohesive points and pair blocks are
+    // formed on the second stream beside it; the fold, which needs both,
+    // completes the rows cut elements touch and writes the enrichment rows
+    // and columns whole.  Nothing needs clearing first.
     const RowArgs ra = row_args(c, U, want_f, want_K);
-    // the cut elements' quadrature rows depend on the coordinates only: they
-    // are formed on the second stream beside the triangle kernel.  That one is
-    // launched first, so its CTAs are dispatched first and the row kernel's
-    // fill the SMs its last wave leaves free.
-    const bool fork = c.n_cut_pts > 0;
-    if (fork) PG_CUDA(cudaEventRecord(c.fork_ev, s));
+    const bool cut = c.n_cut > 0;
+    if (cut) PG_CUDA(cudaEventRecord(c.fork_ev, s));
     if (c.timing) cudaEventRecord(c.ea0, s);
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
-    if (fork) {
-        PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
-        launch_cut_points(c, c.aux);
-        PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
-    }
     if (c.timing) cudaEventRecord(c.ea1, s);
-    if (fork) PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
-    if (c.n_cut > 0) {
-        launch_cut_classes(c, cut_args(c, U, dt, want_f, want_K), s);
+    if (cut) {
+        PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
+        launch_cut_work(c, U, dt, want_f, want_K, c.aux);
+        PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
+        PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
+        launch_cut_fold(c, want_f, want_K, s);
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);
     return PG_OK;
 }
 
-// Times every launch shape of the two assembly kernels on this mesh (L2
-// flushed before each launch, `reps` launches each, device events) and keeps
-// the fastest of each kernel in c.tuning.  ms_tri: tile 32/64 x one CTA per
-// tile / persistent (4 values), ms_cut: 2/4/8 warps per CTA (3 values).  K is
-// left undefined (the cut kernel ran repeatedly): the next solve reassembles.
+// Times every launch shape of the two assembly stages on this mesh (L2
+// flushed before each launch, `reps` launches each, device events) and
+// keeps the fastest of each in c.tuning.  ms_tri: the row-tile kernel with
+// 32 / 64 node rows per CTA, one CTA per tile / persistent (4 values), then
+// the structured-grid kernel (the faster of 128 and 256 threads per CTA; 0
+// without a structured grid); ms_cut: the cut elements' work on one stream
+// (rows, cohesive points, pairs, fold) with 2 / 4 / 8 warps per pair CTA.
+// K is left undefined: the next solve reassembles.
 int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     cudaStream_t s = c.stream;
     reps = std::max(1, reps);
@@ -1584,18 +1757,17 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
             }
         }
     if (c.grid_emat) {
-        // the structured-grid kernel at both tile heights; ms_tri[4] reports the faster
         c.tuning.tri_grid = 1;
         float ms_grid = 0.f;
-        for (int tr : {3, 4, 7}) {
-            c.tuning.grid_rows = tr;
+        for (int bs : {128, 256}) {
+            c.tuning.grid_block = bs;
             const RowArgs ra = row_args(c, c.U, false, true);
             const float ms = timed([&] { launch_tri(c, ra, false, s); });
             if (ms_grid == 0.f || ms < ms_grid) ms_grid = ms;
             if (ms < best_tri) {
                 best_tri = ms;
                 best.tri_grid = 1;
-                best.grid_rows = tr;
+                best.grid_block = bs;
             }
         }
         if (ms_tri) ms_tri[4] = ms_grid;
@@ -1606,10 +1778,11 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     for (int k = 0; k < 3; ++k) {
         c.tuning.cut_warps = warps[k];
         float ms = 0.f;
-        if (c.n_cut > 0) {
-            const CutArgs ca = cut_args(c, c.U, 1.0, false, true);
-            ms = timed([&] { launch_cut_all(c, ca, s); });
-        }
+        if (c.n_cut > 0)
+            ms = timed([&] {
+                launch_cut_work(c, c.U, 1.0, false, true, s);
+                launch_cut_fold(c, false, true, s);
+            });
         if (ms_cut) ms_cut[k] = ms;
         if (ms < best_cut) {
             best_cut = ms;

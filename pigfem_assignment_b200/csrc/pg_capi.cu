@@ -58,7 +58,9 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
-                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
+                    c.cut_ke, c.cut_fe, c.fold_K_slot, c.fold_K_ptr, c.fold_K_idx, c.fold_f_node, c.fold_f_ptr,
+                    c.fold_f_idx, c.coh_rec, c.coh_rows, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -122,12 +124,11 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.tri_map[v], tm))) return rc;
     }
     if (hm.spec.nx > 0 && hm.spec.ny > 0 && hm.n_elem == 2 * hm.spec.nx * hm.spec.ny &&
-        hm.spec.materials.size() <= (size_t)kGridMaxMat && grid_pattern_ok(hm)) {
+        grid_pattern_ok(hm)) {
         // one structured background grid: the edge-centric sweep kernel applies
         std::vector<int> em(hm.n_elem);
         for (int e = 0; e < hm.n_elem; ++e) em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e];
         if ((rc = dev_upload(&c.grid_emat, em))) return rc;
-        grid_prepare();  // kernel attributes set here, outside any graph capture
     } else {
         c.tuning.tri_grid = 0;
     }
@@ -186,6 +187,33 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pts, pts)) ||
             (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
             return rc;
+        // deterministic assembly: pair buffers and the fold lists
+        std::vector<long long> k_slot;
+        std::vector<int> k_ptr, k_idx, f_node, f_ptr, f_idx;
+        build_fold_lists(c.n_reg, nodes, sp, sl, k_slot, k_ptr, k_idx, f_node, f_ptr, f_idx);
+        c.n_fold_K = (int)k_slot.size();
+        c.n_fold_f = (int)f_node.size();
+        if ((rc = dev_alloc(&c.cut_ke, 4 * std::max<size_t>(1, sl.size()))) ||
+            (rc = dev_alloc(&c.cut_fe, 2 * std::max<size_t>(1, sl.size()))) ||
+            (rc = dev_upload(&c.fold_K_slot, k_slot)) || (rc = dev_upload(&c.fold_K_ptr, k_ptr)) ||
+            (rc = dev_upload(&c.fold_K_idx, k_idx)) || (rc = dev_upload(&c.fold_f_node, f_node)) ||
+            (rc = dev_upload(&c.fold_f_ptr, f_ptr)) || (rc = dev_upload(&c.fold_f_idx, f_idx)))
+            return rc;
+        if (hm.n_coh_qp > 0) {
+            std::vector<int> rec(hm.n_coh_qp, -1);
+            for (int oi = 0; oi < nc; ++oi) {
+                const CutTemplate& T = cut_template(tmpl[oi]);
+                for (int ce = 0; ce < T.n_coh; ++ce)
+                    for (int q = 0; q < 2; ++q) rec[qp0[oi] + 2 * ce + q] = (oi << 8) | (ce << 1) | q;
+            }
+            for (int v : rec)
+                if (v < 0) {
+                    set_error("cohesive Gauss point not owned by any cut element");
+                    return PG_ERR_MESH;
+                }
+            if ((rc = dev_upload(&c.coh_rec, rec)) || (rc = dev_alloc(&c.coh_rows, (size_t)kCohRowDoubles * hm.n_coh_qp)))
+                return rc;
+        }
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;
@@ -396,7 +424,7 @@ int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut) {
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps) {
     PG_GUARD_CTX(c);
     if (tri_tile_nodes)
-        *tri_tile_nodes = c->c.tuning.tri_grid ? kGridTileX * c->c.tuning.grid_rows : kTriTileSizes[c->c.tuning.tri_variant];
+        *tri_tile_nodes = c->c.tuning.tri_grid ? c->c.tuning.grid_block : kTriTileSizes[c->c.tuning.tri_variant];
     if (tri_persistent) *tri_persistent = c->c.tuning.tri_persistent;
     if (cut_warps) *cut_warps = c->c.tuning.cut_warps;
     return PG_OK;
@@ -407,16 +435,15 @@ int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent,
     int v = -1;
     for (int k = 0; k < kTriTileVariants; ++k)
         if (kTriTileSizes[k] == tri_tile_nodes) v = k;
-    const bool grid = tri_tile_nodes == 3 * kGridTileX || tri_tile_nodes == 4 * kGridTileX ||
-                      tri_tile_nodes == 7 * kGridTileX;
+    const bool grid = tri_tile_nodes == 128 || tri_tile_nodes == 256;
     if ((v < 0 && !(grid && c->c.grid_emat)) || (tri_persistent != 0 && tri_persistent != 1) ||
         (cut_warps != 2 && cut_warps != 4 && cut_warps != 8)) {
-        set_error("pg_ctx_set_tuning: tile 32 or 64 (row tiles), 93, 124 or 217 (structured grid, 31 x 3, 31 x 4 "
-                  "or 31 x 7 nodes), persistent 0 or 1, warps 2, 4 or 8");
+        set_error("pg_ctx_set_tuning: tile 32 or 64 (row tiles), 128 or 256 (threads per CTA of the structured-grid "
+                  "kernel, meshes with one grid), persistent 0 or 1, warps 2, 4 or 8");
         return PG_ERR_ARG;
     }
     c->c.tuning.tri_grid = grid ? 1 : 0;
-    if (grid) c->c.tuning.grid_rows = tri_tile_nodes / kGridTileX;
+    if (grid) c->c.tuning.grid_block = tri_tile_nodes;
     if (!grid) c->c.tuning.tri_variant = v;
     c->c.tuning.tri_persistent = tri_persistent;
     c->c.tuning.cut_warps = cut_warps;

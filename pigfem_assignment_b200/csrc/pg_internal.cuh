@@ -28,6 +28,7 @@ struct DevCohLaw {
 constexpr int kCutClasses = 4;
 constexpr int kCutClassNl[kCutClasses] = {5, 7, 11, 15};
 constexpr int kCutNodeStride = 16;
+constexpr int kCohRowDoubles = 10;  // row of a cohesive Gauss point (k_coh_points)
 
 struct DevTemplate {
     int n_enr, n_child, n_coh, pad;
@@ -62,18 +63,17 @@ constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
 bool grid_pattern_ok(const HostMesh& hm);  // block rows laid out as the structured-grid kernel assumes
-void grid_prepare();  // sets the structured-grid kernel's shared-memory limit on this device
-constexpr int kGridMaxMat = 16;  // materials the structured-grid kernel stages in shared memory
-constexpr int kGridTileX = 31;    // node columns per structured-grid tile
+int grid_kpad(int nx);  // threads per (grid row, parity) segment of the structured-grid kernel
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
-// triangle tile size, persistent grid (CTAs walk the tiles) or one CTA per
-// tile, and warps (= cut elements) per CTA of the cut kernel.
+// the structured-grid kernel's CTA size, or (meshes without one grid) the
+// row-tile kernel's tile size and persistent grid (CTAs walk the tiles) or
+// one CTA per tile, and the warps per CTA of the cut elements' pair kernel.
 struct AsmTuning {
-    int tri_grid = 1;      // 1: edge-centric tiles of the structured grid (when the mesh has one)
-    int grid_rows = 3;     // node rows per structured-grid tile: 3, 4 or 7
+    int tri_grid = 1;      // 1: the structured-grid kernel (when the mesh has one grid)
+    int grid_block = 256;  // its threads per CTA: 128 or 256
     int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
-    int cut_warps = 2;     // 2, 4 or 8
+    int cut_warps = 4;     // 2, 4 or 8
 };
 
 struct Ctx {
@@ -111,6 +111,22 @@ struct Ctx {
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
+    // deterministic assembly of the cut elements: pair blocks (4 FP64) and
+    // residual terms (2 FP64) at their slot-table positions, the fold lists
+    // (K slot / node -> slot-table positions, sorted by element and pair)
+    // and the cohesive Gauss points' rows
+    double* cut_ke = nullptr;
+    double* cut_fe = nullptr;
+    long long* fold_K_slot = nullptr;  // slot << 1 | cut_only
+    int* fold_K_ptr = nullptr;
+    int* fold_K_idx = nullptr;
+    int n_fold_K = 0;
+    int* fold_f_node = nullptr;        // node << 1 | cut_only
+    int* fold_f_ptr = nullptr;
+    int* fold_f_idx = nullptr;
+    int n_fold_f = 0;
+    int* coh_rec = nullptr;            // per cohesive point: class-ordered element << 8 | sub-element << 1 | point
+    double* coh_rows = nullptr;        // per cohesive point: 10 FP64 (k_coh_points)
     MgHierarchy* mg = nullptr;         // multigrid hierarchy, built at the first multigrid solve
     // system
     double* K = nullptr;               // 4 * n_blocks
@@ -215,6 +231,11 @@ struct CutArgs {
     int which;
 };
 CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K);
+// fold lists of the cut elements' deterministic assembly (pg_capi.cu builds
+// them from the class-ordered slot tables)
+void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
+                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& k_idx,
+                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& f_idx);
 int device_point_count(int tmpl);  // quadrature points of a cut template on the device
 constexpr int kCutPointInts = 16;  // ints per point record of the cut-row kernel
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,

@@ -19,7 +19,7 @@ def gpu_K(ctx, e):
     return bsr_to_csr(e["row_ptr"], e["col"], ctx.matrix_values())
 
 
-@pytest.mark.parametrize("tile", [32, 64, 93, 124, 217])
+@pytest.mark.parametrize("tile", [32, 64, 128, 256])
 @pytest.mark.parametrize("persistent", [0, 1])
 @pytest.mark.parametrize("warps", [2, 4, 8])
 def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
@@ -35,6 +35,33 @@ def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
     ctx.close()
 
 
+@pytest.mark.parametrize("tile", [32, 64, 128, 256])
+@pytest.mark.parametrize("warps", [2, 8])
+def test_every_launch_shape_assembles_the_same_tangent_and_residual(tile, warps):
+    # the residual and tangent passes of a cohesive mesh (bilinear law, damaged
+    # state) through every launch shape: K and f_int against the oracle
+    rve = RVE(nx=20, ny=20, inclusions=[(0.45, 0.5, 0.27, 1)], cohesive=True, coh_law=1,
+              coh_params=(30.0, 0.01, 1.0e6, 1.0, 200.0), strain=0.02)
+    m = pb.Mesh(rve)
+    e = m.export()
+    ctx = pb.DeviceContext(m)
+    _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, 0, warps))
+    rng = np.random.default_rng(5)
+    U = 1e-4 * rng.standard_normal(m.info["n_dof"])
+    isv_c = np.abs(2e-5 * rng.standard_normal(m.info["n_cohesive_qp"]))
+    ctx.set_vector(0, U)
+    ctx.set_isv(isv_c, committed=True)
+    om = oracle.from_product(e, pb.template_table(), rve)
+    Ko, fo, io = om.assemble(u=U, dt=0.02, isv_c=isv_c, want_K=True, want_f=True)
+    asm = pb.Assembler(ctx)
+    asm.assemble_nonlinear(0.02, False, True)   # tangent pass
+    assert rel_fro(gpu_K(ctx, e), Ko) <= 1e-12
+    asm.assemble_nonlinear(0.02, True, False)   # residual pass
+    assert np.linalg.norm(ctx.vector(1) - fo) / np.linalg.norm(fo) <= 1e-12
+    np.testing.assert_allclose(ctx.isv(committed=False), io, rtol=1e-13, atol=0)
+    ctx.close()
+
+
 def test_autotune_times_every_shape_and_keeps_the_fastest():
     rve = config0()
     prob = pb.ProblemLinearElasticity(rve)
@@ -47,7 +74,7 @@ def test_autotune_times_every_shape_and_keeps_the_fastest():
     _lib.check(_lib.lib.pg_ctx_tuning(prob.ctx.handle, C.byref(tile), C.byref(pers), C.byref(warps)))
     best_tri = int(np.argmin(list(ms_tri)))
     if best_tri == 4:
-        assert tile.value in (93, 124, 217)  # the 31 x 3, 31 x 4 or 31 x 7 tiles of the structured grid
+        assert tile.value in (128, 256)  # threads per CTA of the structured-grid kernel
     else:
         assert (tile.value, pers.value) == ((32, 64)[best_tri // 2], best_tri % 2)
     assert warps.value == (2, 4, 8)[int(np.argmin(list(ms_cut)))]

@@ -58,19 +58,23 @@ def test_newton_budget_exhausted_reports_not_converged():
 
 
 def test_step_cuts_follow_update_time_step():
-    # three Newton iterations are enough for an elastic step (forcing terms
-    # 1e-3, then ~1e-6, then the target), not for the steps that debond the
-    # interface: those are cut by 4 until they converge
-    n_steps = 5
-    _, prob = _cohesive_problem(n_steps=n_steps, T_final=1.0, max_it=3, max_repeat=20,
-                                predictor=_lib.PG_PREDICT_ZEROTH)
-    recs = prob.solve_problem()
-    assert all(r.reason > 0 for r in recs)
-    dts = np.array([r.dt for r in recs])
-    assert abs(dts.sum() - 1.0) < 1e-12
-    assert max(r.repeats for r in recs) > 1, "no step was cut: the budget did not bind"
-    np.testing.assert_allclose(dts, expected_dt_sequence(recs, 1.0 / n_steps, 1.0), rtol=1e-12)
-    prob.ctx.close()
+    # a tight Newton budget fails the large steps that debond the interface;
+    # those are cut by 4 until they converge.  Budgets and step counts from
+    # mild to harsh: every run must follow the rule, and at least one must cut
+    cut_seen = False
+    for n_steps, max_it in ((5, 3), (2, 3), (2, 2), (1, 2)):
+        _, prob = _cohesive_problem(n_steps=n_steps, T_final=1.0, max_it=max_it, max_repeat=20,
+                                    predictor=_lib.PG_PREDICT_ZEROTH)
+        recs = prob.solve_problem()
+        prob.ctx.close()
+        assert all(r.reason > 0 for r in recs)
+        dts = np.array([r.dt for r in recs])
+        assert abs(dts.sum() - 1.0) < 1e-12
+        np.testing.assert_allclose(dts, expected_dt_sequence(recs, 1.0 / n_steps, 1.0), rtol=1e-12)
+        if max(r.repeats for r in recs) > 1:
+            cut_seen = True
+            break
+    assert cut_seen, "no step was cut: the budgets did not bind"
 
 
 def test_krylov_budget_of_five_iterations():

@@ -554,30 +554,25 @@ __device__ __forceinline__ void point_child(const DevTemplate& TG, int l, int& c
     }
 }
 
-// Quadrature rows of every cut element, one thread per point.  What a point
-// needs of the mesh is static, so the host packs it into one 64-byte record
-// (kCutPointInts ints, see build_cut_points): the thread reads its record,
-// then the coordinates it names, and writes its row.  It runs on a second
-// stream beside the structured-grid kernel.
-struct CutPointArgs {
-    int n_pts;
-    const int4* __restrict__ pts;
-    const double* __restrict__ x;
-    const double* __restrict__ y;
-    const double* __restrict__ dmat;
-    double* rows;
+// Quadrature row of one cut-element point.  What a point needs of the mesh
+// is static, so the host packs it into one 64-byte record (kCutPointInts
+// ints, see build_cut_points): the thread reads its record (cut_point_load),
+// then the coordinates it names, and writes the row {w det, d11, d12, d33,
+// (gx, gy) of each local function} contiguously (cut_point_row).
+struct CutPoint {
+    int4 r0, r1, r2, r3;
 };
 
-__global__ void __launch_bounds__(256) k_cut_points(CutPointArgs a) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n_pts) return;
-    const int4* rec = a.pts + 4 * (size_t)p;
-    const int4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3);
-    const int gn[kMaxChildNodes] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y};
-    const int mat = r2.y, lnp = r2.z, meta = r2.w;
+__device__ __forceinline__ CutPoint cut_point_load(const int4* __restrict__ rec) {
+    return CutPoint{__ldg(rec), __ldg(rec + 1), __ldg(rec + 2), __ldg(rec + 3)};
+}
+
+__device__ __forceinline__ void cut_point_row(const CutPoint& P, const double* __restrict__ x,
+                                              const double* __restrict__ y, const double* __restrict__ dmat,
+                                              double* row) {
+    const int gn[kMaxChildNodes] = {P.r0.x, P.r0.y, P.r0.z, P.r0.w, P.r1.x, P.r1.y};
+    const int mat = P.r2.y, lnp = P.r2.z, meta = P.r2.w;
     const int q = meta & 255, type = (meta >> 8) & 3, nc = (meta >> 10) & 7, nl = (meta >> 13) & 15;
-    const long long base = (long long)(unsigned)r3.x | ((long long)r3.y << 32);
-    const int nq_e = r3.z, l = r3.w;
     int ln[kMaxChildNodes];
     double cx[kMaxChildNodes], cy[kMaxChildNodes];
 #pragma unroll
@@ -585,27 +580,27 @@ __global__ void __launch_bounds__(256) k_cut_points(CutPointArgs a) {
         ln[k] = (lnp >> (4 * k)) & 15;
         cx[k] = cy[k] = 0.0;
         if (k < nc) {
-            cx[k] = __ldg(&a.x[gn[k]]);
-            cy[k] = __ldg(&a.y[gn[k]]);
+            cx[k] = __ldg(&x[gn[k]]);
+            cy[k] = __ldg(&y[gn[k]]);
         }
     }
-    const double PX[3] = {__ldg(&a.x[r1.z]), __ldg(&a.x[r1.w]), __ldg(&a.x[r2.x])};
-    const double PY[3] = {__ldg(&a.y[r1.z]), __ldg(&a.y[r1.w]), __ldg(&a.y[r2.x])};
+    const double PX[3] = {__ldg(&x[P.r1.z]), __ldg(&x[P.r1.w]), __ldg(&x[P.r2.x])};
+    const double PY[3] = {__ldg(&y[P.r1.z]), __ldg(&y[P.r1.w]), __ldg(&y[P.r2.x])};
     double pbx[3], pby[3];
     parent_gradients(PX, PY, pbx, pby);
-    const double dm[3] = {__ldg(&a.dmat[3 * mat]), __ldg(&a.dmat[3 * mat + 1]), __ldg(&a.dmat[3 * mat + 2])};
-    cut_row(a.rows + base + l, nq_e, nl, g_quad[type], q, nc, ln, cx, cy, dm, pbx, pby);
+    const double dm[3] = {__ldg(&dmat[3 * mat]), __ldg(&dmat[3 * mat + 1]), __ldg(&dmat[3 * mat + 2])};
+    cut_row(row, 1, nl, g_quad[type], q, nc, ln, cx, cy, dm, pbx, pby);
 }
 
-// Point records of k_cut_points, per point kCutPointInts ints: global nodes of
-// its child (6, unused ones repeat the first), of the parent (3), the child's
-// material, the child nodes' local numbers (4 bits each), then point q (8
-// bits), child type (2), child node count (3) and the element's local-function
-// count (4), then the element's first row offset in doubles (2 ints, low
-// first), its point count and this point's number within it.  An element's
-// rows are stored value-major (value j of point l at j nq + l), so that the
-// threads of consecutive points write consecutive doubles.  Points are in
-// class order, each element's in the order of its rows.
+// Point records of the cut-element kernel, per point kCutPointInts ints:
+// global nodes of its child (6, unused ones repeat the first), of the parent
+// (3), the child's material, the child nodes' local numbers (4 bits each),
+// then point q (8 bits), child type (2), child node count (3) and the
+// element's local-function count (4), then the offset in doubles of the
+// point's row (2 ints, low first: the element's first row + l (4 + 2 NL)),
+// the element's point count and the point's number l within it.  Points are
+// in class order, each element's in the order of its rows; one sentinel
+// record follows the last point, holding only the rows' total length.
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
                       const std::vector<long long>& roff, const int* class_off, std::vector<int>& out) {
     out.clear();
@@ -629,14 +624,21 @@ void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmp
                     r[9] = chm[(size_t)kMaxChildren * oi + ch];
                     r[10] = lnp;
                     r[11] = q | (type << 8) | (nc << 10) | ((3 + T.n_enr) << 13);
-                    r[12] = (int)(unsigned)(roff[oi] & 0xffffffffLL);
-                    r[13] = (int)(roff[oi] >> 32);
+                    const long long off = roff[oi] + (long long)l * (4 + 2 * kCutClassNl[k]);
+                    r[12] = (int)(unsigned)(off & 0xffffffffLL);
+                    r[13] = (int)(off >> 32);
                     r[14] = nq_e;
                     r[15] = l;
                     out.insert(out.end(), r, r + kCutPointInts);
                 }
             }
         }
+    // sentinel after the last point: its row offset is the rows' total length
+    int r[kCutPointInts] = {};
+    const long long total = roff.back();
+    r[12] = (int)(unsigned)(total & 0xffffffffLL);
+    r[13] = (int)(total >> 32);
+    out.insert(out.end(), r, r + kCutPointInts);
 }
 
 // ---------------------------------------------------------------------------
@@ -650,20 +652,22 @@ void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmp
 // ascending order, then enrichment columns; grid_pattern_ok checks that
 // layout on the host before this kernel is used.
 //
-// A thread owns one regular node and writes its row: in registers, it forms
-// row v of the constant-strain stiffness of every uncut triangle around the
-// node (8 for an even node, 4 for an odd one; the reference's 4-point rule
-// integrates the constant integrand exactly, its weights summing to 1/2),
-// sums them into the node's grid-neighbour blocks and stores each block
-// once with a 256-bit store.  A triangle is thus formed by each of its three
-// vertices' threads; the FP64 pipe has room for that, and nothing is staged
-// in shared memory, exchanged between threads or waited for.  The lanes of
-// a warp take nodes of one parity from one grid row (every other node
-// column), so every lane runs the same, fully unrolled triangle code.
+// A CTA stages a tile's node coordinates (and displacements) with a
+// one-node halo and the materials of its cells in shared memory -- coalesced
+// loads, all in flight at once, one barrier -- and then a thread owns one
+// regular node and writes its row: in registers, it forms row v of the
+// constant-strain stiffness of every uncut triangle around the node (8 for
+// an even node, 4 for an odd one; the reference's 4-point rule integrates
+// the constant integrand exactly, its weights summing to 1/2), sums them
+// into the node's grid-neighbour blocks and stores each block once with a
+// 256-bit store.  A triangle is thus formed by each of its three vertices'
+// threads; the FP64 pipe has room for that, and nothing but the inputs is
+// staged or exchanged.  The lanes of a warp take nodes of one parity from
+// one grid row (every other node column), so every lane runs the same,
+// fully unrolled triangle code.
 // Enrichment columns and enrichment rows are not touched: the cut-element
 // fold writes them whole.  With WF the thread also forms its two f_int
 // entries from the same row blocks.
-constexpr int kGridLanes = 32;  // lanes of a (row, parity) segment are padded to whole warps
 
 // Corner (di + 2 dj) of local vertex m of triangle t in a cell of parity cp
 // ((i + j) % 2): {n00, n10, n11}, {n00, n11, n01} for even cells,
@@ -713,7 +717,7 @@ __device__ __forceinline__ double4 load_block(const double* K, long long q) {
 
 struct GridArgs {
     int nx, ny;
-    int kpad;                           // threads per (grid row, parity) segment, a multiple of kGridLanes
+    int tiles_x;                        // tiles across the grid
     const int* __restrict__ row_ptr;
     const int* __restrict__ emat;       // per element: material, -1 for cut elements
     const double* __restrict__ x;
@@ -738,29 +742,34 @@ struct GridTri {
     __host__ __device__ static constexpr int dy(int m) { return OY + (tri_corner(cp, T, m) >> 1); }
 };
 
+// The node's cell at offset (OX - 1, OY - 1), staged: corners (c & 1, c >> 1)
+// of the cell as (x, y) pairs, and its two triangles' materials.
+struct GridCell {
+    double2 p[4];
+    int m0, m1;
+};
+
 // 2 x (signed area) of triangle T of the cell
 template <int Q, int OX, int OY, int T>
-__device__ __forceinline__ double grid_tri_J(const double (&X)[3][3], const double (&Y)[3][3]) {
+__device__ __forceinline__ double grid_tri_J(const GridCell& C) {
     using G = GridTri<Q, OX, OY, T>;
-    const double X0 = X[G::dy(0)][G::dx(0)], X1 = X[G::dy(1)][G::dx(1)], X2 = X[G::dy(2)][G::dx(2)];
-    const double Y0 = Y[G::dy(0)][G::dx(0)], Y1 = Y[G::dy(1)][G::dx(1)], Y2 = Y[G::dy(2)][G::dx(2)];
-    return (X1 - X0) * (Y2 - Y0) - (X2 - X0) * (Y1 - Y0);
+    const double2 P0 = C.p[tri_corner(G::cp, T, 0)], P1 = C.p[tri_corner(G::cp, T, 1)], P2 = C.p[tri_corner(G::cp, T, 2)];
+    return (P1.x - P0.x) * (P2.y - P0.y) - (P2.x - P0.x) * (P1.y - P0.y);
 }
 
 // Adds row v (the node's) of triangle T's stiffness, scaled by s = 1 / (2 J),
 // to the neighbour blocks acc[d] (d = 3 dy + dx; acc[4] = diagonal block as
-// k00, k01, k11) and, with WF, K_vw u_w to (fx, fy).
+// k00, k01, k11) and, with WF, K_vw u_w to (fx, fy); U: the cell's corner
+// displacements.
 template <int Q, int OX, int OY, int T, bool WK, bool WF>
-__device__ __forceinline__ void grid_tri_row(const double (&X)[3][3], const double (&Y)[3][3],
-                                             const double (&UX)[3][3], const double (&UY)[3][3], double s,
+__device__ __forceinline__ void grid_tri_row(const GridCell& C, const double2 (&U)[4], double s,
                                              const double* __restrict__ D, double (&acc)[9][4], double& fx,
                                              double& fy) {
     using G = GridTri<Q, OX, OY, T>;
     constexpr int v = G::v;
-    const double X0 = X[G::dy(0)][G::dx(0)], X1 = X[G::dy(1)][G::dx(1)], X2 = X[G::dy(2)][G::dx(2)];
-    const double Y0 = Y[G::dy(0)][G::dx(0)], Y1 = Y[G::dy(1)][G::dx(1)], Y2 = Y[G::dy(2)][G::dx(2)];
-    const double b[3] = {Y1 - Y2, Y2 - Y0, Y0 - Y1};
-    const double c[3] = {X2 - X1, X0 - X2, X1 - X0};
+    const double2 P0 = C.p[tri_corner(G::cp, T, 0)], P1 = C.p[tri_corner(G::cp, T, 1)], P2 = C.p[tri_corner(G::cp, T, 2)];
+    const double b[3] = {P1.y - P2.y, P2.y - P0.y, P0.y - P1.y};
+    const double c[3] = {P2.x - P1.x, P0.x - P2.x, P1.x - P0.x};
     const double E0 = s * __ldg(&D[0]), E1 = s * __ldg(&D[1]), E2 = s * __ldg(&D[2]);
     const double bv = b[v], cv = c[v];
     const double Xv = bv * E0, Yv = bv * E1, Zv = bv * E2, Uv = cv * E0, Vv = cv * E1, Wv = cv * E2;
@@ -784,36 +793,32 @@ __device__ __forceinline__ void grid_tri_row(const double (&X)[3][3], const doub
             }
         }
         if (WF) {
-            const double ux = UX[G::dy(w)][G::dx(w)], uy = UY[G::dy(w)][G::dx(w)];
-            fx += k0 * ux + k1 * uy;
-            fy += k2 * ux + k3 * uy;
+            const double2 uw = U[tri_corner(G::cp, T, w)];
+            fx += k0 * uw.x + k1 * uw.y;
+            fy += k2 * uw.x + k3 * uw.y;
         }
     }
 }
 
-// The uncut triangles of cell (OX, OY) around the node (cell (gi - 1 + OX,
-// gj - 1 + OY), materials m0, m1, -1 for cut or absent triangles).  When
-// both contain the node, their two scales share one division.
+// The uncut triangles of cell (OX, OY) around the node (materials -1 for
+// cut or absent triangles).  When both contain the node, their two scales
+// share one division.
 template <int Q, int OX, int OY, bool WK, bool WF>
-__device__ __forceinline__ void grid_cell(const double (&X)[3][3], const double (&Y)[3][3], const double (&UX)[3][3],
-                                          const double (&UY)[3][3], int m0, int m1,
-                                          const double* __restrict__ dmat, double (&acc)[9][4], double& fx,
-                                          double& fy) {
+__device__ __forceinline__ void grid_cell(const GridCell& C, const double2 (&U)[4], const double* __restrict__ dmat,
+                                          double (&acc)[9][4], double& fx, double& fy) {
     constexpr bool h0 = GridTri<Q, OX, OY, 0>::v >= 0, h1 = GridTri<Q, OX, OY, 1>::v >= 0;
     if constexpr (h0 && h1) {
-        if (m0 < 0 && m1 < 0) return;
-        const double J0 = grid_tri_J<Q, OX, OY, 0>(X, Y), J1 = grid_tri_J<Q, OX, OY, 1>(X, Y);
+        if (C.m0 < 0 && C.m1 < 0) return;
+        const double J0 = grid_tri_J<Q, OX, OY, 0>(C), J1 = grid_tri_J<Q, OX, OY, 1>(C);
         const double r = 0.5 / (J0 * J1);
-        if (m0 >= 0) grid_tri_row<Q, OX, OY, 0, WK, WF>(X, Y, UX, UY, r * J1, dmat + 3 * m0, acc, fx, fy);
-        if (m1 >= 0) grid_tri_row<Q, OX, OY, 1, WK, WF>(X, Y, UX, UY, r * J0, dmat + 3 * m1, acc, fx, fy);
+        if (C.m0 >= 0) grid_tri_row<Q, OX, OY, 0, WK, WF>(C, U, r * J1, dmat + 3 * C.m0, acc, fx, fy);
+        if (C.m1 >= 0) grid_tri_row<Q, OX, OY, 1, WK, WF>(C, U, r * J0, dmat + 3 * C.m1, acc, fx, fy);
     } else if constexpr (h0) {
-        if (m0 < 0) return;
-        const double s = 0.5 / grid_tri_J<Q, OX, OY, 0>(X, Y);
-        grid_tri_row<Q, OX, OY, 0, WK, WF>(X, Y, UX, UY, s, dmat + 3 * m0, acc, fx, fy);
+        if (C.m0 < 0) return;
+        grid_tri_row<Q, OX, OY, 0, WK, WF>(C, U, 0.5 / grid_tri_J<Q, OX, OY, 0>(C), dmat + 3 * C.m0, acc, fx, fy);
     } else {
-        if (m1 < 0) return;
-        const double s = 0.5 / grid_tri_J<Q, OX, OY, 1>(X, Y);
-        grid_tri_row<Q, OX, OY, 1, WK, WF>(X, Y, UX, UY, s, dmat + 3 * m1, acc, fx, fy);
+        if (C.m1 < 0) return;
+        grid_tri_row<Q, OX, OY, 1, WK, WF>(C, U, 0.5 / grid_tri_J<Q, OX, OY, 1>(C), dmat + 3 * C.m1, acc, fx, fy);
     }
 }
 
@@ -826,58 +831,61 @@ __device__ __forceinline__ void grid_store(double* K, int q0, unsigned mask, con
     }
 }
 
+// Tile of the structured-grid kernel: kGridTileC node columns (I0 even) x
+// TR node rows (2 or 4, picked by the autotuner), one thread per node; warp
+// 2 r + q takes the nodes of parity q in tile row r (every other column).
+// Staged window: the tile's nodes with a one-node halo, the cells around them.
+constexpr int kGridTileC = 64;
+constexpr int kGridWinX = kGridTileC + 2;   // staged node columns
+constexpr int kGridCellX = kGridTileC + 1;  // staged cell columns
+
+template <int OX, int OY, bool WF>
+__device__ __forceinline__ void grid_load_cell(GridCell& C, double2 (&U)[4], const double2* sXY, const double2* sU,
+                                               const int2* sM, int lx, int ly) {
+    // cell (OX, OY) of the node at window position (lx, ly): its corner (cx, cy)
+    // is window node (lx - 1 + OX + cx, ly - 1 + OY + cy)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int w = (ly - 1 + OY + (k >> 1)) * kGridWinX + lx - 1 + OX + (k & 1);
+        C.p[k] = sXY[w];
+        if (WF) U[k] = sU[w];
+    }
+    const int2 m = sM[(ly - 1 + OY) * kGridCellX + lx - 1 + OX];
+    C.m0 = m.x;
+    C.m1 = m.y;
+}
+
 template <int Q, bool WK, bool WF>
-__device__ __forceinline__ void grid_node(const GridArgs& a, int gi, int gj) {
-    const int nx = a.nx, ny = a.ny, NX1 = nx + 1;
-    const int node = gi + gj * NX1;
-    // coordinates (and displacements) of the node's 3 x 3 neighbourhood,
-    // [dy + 1][dx + 1]; entries outside the grid are never read (an odd
-    // node's triangles do not reach the diagonal ones at all)
-    double X[3][3], Y[3][3], UX[3][3], UY[3][3];
-#pragma unroll
-    for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-        for (int dx = 0; dx < 3; ++dx) {
-            const int ni = gi + dx - 1, nj = gj + dy - 1;
-            const bool in = ni >= 0 && ni <= nx && nj >= 0 && nj <= ny;
-            const int n = in ? ni + nj * NX1 : node;
-            X[dy][dx] = __ldg(&a.x[n]);
-            Y[dy][dx] = __ldg(&a.y[n]);
-            UX[dy][dx] = WF ? __ldg(&a.u[2 * n]) : 0.0;
-            UY[dy][dx] = WF ? __ldg(&a.u[2 * n + 1]) : 0.0;
-        }
-    // materials of the two triangles of the four cells around the node
-    // (cell (gi - 1 + ox, gj - 1 + oy)); -1 for a cut or absent triangle
-    int2 M[2][2];
-#pragma unroll
-    for (int oy = 0; oy < 2; ++oy)
-#pragma unroll
-        for (int ox = 0; ox < 2; ++ox) {
-            const int ci = gi - 1 + ox, cj = gj - 1 + oy;
-            const bool in = ci >= 0 && ci < nx && cj >= 0 && cj < ny;
-            M[oy][ox] = in ? __ldg(reinterpret_cast<const int2*>(a.emat) + (ci + (size_t)cj * nx)) : make_int2(-1, -1);
-        }
+__device__ __forceinline__ void grid_node(const GridArgs& a, int gi, int gj, int lx, int ly, const double2* sXY,
+                                          const double2* sU, const int2* sM) {
+    const int node = gi + gj * (a.nx + 1);
     const int q0 = WK ? __ldg(&a.row_ptr[node]) : 0;
-    const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+    const unsigned mask = grid_nbr_mask(gi, gj, a.nx, a.ny);
     double acc[9][4];
 #pragma unroll
     for (int d = 0; d < 9; ++d) acc[d][0] = acc[d][1] = acc[d][2] = acc[d][3] = 0.0;
     double fx = 0.0, fy = 0.0;
+    GridCell C;
+    double2 U[4];
     // cells in the order that completes blocks early: below (d = 0, 1, 2
     // done), above left (d = 3, 6), above right (d = 4, 5, 7, 8)
-    grid_cell<Q, 0, 0, WK, WF>(X, Y, UX, UY, M[0][0].x, M[0][0].y, a.dmat, acc, fx, fy);
-    grid_cell<Q, 1, 0, WK, WF>(X, Y, UX, UY, M[0][1].x, M[0][1].y, a.dmat, acc, fx, fy);
+    grid_load_cell<0, 0, WF>(C, U, sXY, sU, sM, lx, ly);
+    grid_cell<Q, 0, 0, WK, WF>(C, U, a.dmat, acc, fx, fy);
+    grid_load_cell<1, 0, WF>(C, U, sXY, sU, sM, lx, ly);
+    grid_cell<Q, 1, 0, WK, WF>(C, U, a.dmat, acc, fx, fy);
     if (WK) {
         if (Q == 0) grid_store<0>(a.K, q0, mask, acc);
         grid_store<1>(a.K, q0, mask, acc);
         if (Q == 0) grid_store<2>(a.K, q0, mask, acc);
     }
-    grid_cell<Q, 0, 1, WK, WF>(X, Y, UX, UY, M[1][0].x, M[1][0].y, a.dmat, acc, fx, fy);
+    grid_load_cell<0, 1, WF>(C, U, sXY, sU, sM, lx, ly);
+    grid_cell<Q, 0, 1, WK, WF>(C, U, a.dmat, acc, fx, fy);
     if (WK) {
         grid_store<3>(a.K, q0, mask, acc);
         if (Q == 0) grid_store<6>(a.K, q0, mask, acc);
     }
-    grid_cell<Q, 1, 1, WK, WF>(X, Y, UX, UY, M[1][1].x, M[1][1].y, a.dmat, acc, fx, fy);
+    grid_load_cell<1, 1, WF>(C, U, sXY, sU, sM, lx, ly);
+    grid_cell<Q, 1, 1, WK, WF>(C, U, a.dmat, acc, fx, fy);
     if (WK) {
         grid_store<4>(a.K, q0, mask, acc);
         grid_store<5>(a.K, q0, mask, acc);
@@ -890,18 +898,43 @@ __device__ __forceinline__ void grid_node(const GridArgs& a, int gi, int gj) {
     }
 }
 
-// Thread t: segment t / kpad = 2 gj + q (grid row gj, parity q), lane
-// k = t % kpad, node column gi = 2 k + ((gj + q) & 1).
-template <bool WK, bool WF>
-__global__ void __launch_bounds__(256) k_grid_rows(GridArgs a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int seg = t / a.kpad, k = t - seg * a.kpad;
-    const int gj = seg >> 1, q = seg & 1;
-    if (gj > a.ny) return;
-    const int gi = 2 * k + ((gj + q) & 1);
-    if (gi > a.nx) return;
-    if (q == 0) grid_node<0, WK, WF>(a, gi, gj);
-    else grid_node<1, WK, WF>(a, gi, gj);
+// One CTA per tile: the window's coordinates (and displacements) and cell
+// materials are staged with coalesced loads, all in flight together; then
+// every thread forms its node's row from shared memory.
+template <bool WK, bool WF, int TR>
+__global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs a) {
+    constexpr int kGridThreads = kGridTileC * TR, kGridWinY = TR + 2, kGridCellY = TR + 1;
+    __shared__ double2 sXY[kGridWinX * kGridWinY];
+    __shared__ double2 sU[WF ? kGridWinX * kGridWinY : 1];
+    __shared__ int2 sM[kGridCellX * kGridCellY];
+    const int nx = a.nx, ny = a.ny, NX1 = nx + 1;
+    const int I0 = (blockIdx.x % a.tiles_x) * kGridTileC, J0 = (blockIdx.x / a.tiles_x) * TR;
+    for (int i = threadIdx.x; i < kGridWinX * kGridWinY; i += kGridThreads) {
+        const int gi = I0 - 1 + i % kGridWinX, gj = J0 - 1 + i / kGridWinX;
+        double2 v = make_double2(0.0, 0.0), uv = make_double2(0.0, 0.0);
+        if (gi >= 0 && gi <= nx && gj >= 0 && gj <= ny) {
+            const size_t n = gi + (size_t)gj * NX1;
+            v = make_double2(__ldg(&a.x[n]), __ldg(&a.y[n]));
+            if (WF) uv = make_double2(__ldg(&a.u[2 * n]), __ldg(&a.u[2 * n + 1]));
+        }
+        sXY[i] = v;
+        if (WF) sU[i] = uv;
+    }
+    for (int i = threadIdx.x; i < kGridCellX * kGridCellY; i += kGridThreads) {
+        const int ci = I0 - 1 + i % kGridCellX, cj = J0 - 1 + i / kGridCellX;
+        sM[i] = (ci >= 0 && ci < nx && cj >= 0 && cj < ny)
+                    ? __ldg(reinterpret_cast<const int2*>(a.emat) + (ci + (size_t)cj * nx))
+                    : make_int2(-1, -1);
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = w >> 1, q = w & 1;
+    const int gj = J0 + r;
+    const int gi = I0 + 2 * lane + ((gj + q) & 1);
+    if (gj > ny || gi > nx) return;  // no barrier follows
+    const int lx = gi - I0 + 1, ly = r + 1;
+    if (q == 0) grid_node<0, WK, WF>(a, gi, gj, lx, ly, sXY, sU, sM);
+    else grid_node<1, WK, WF>(a, gi, gj, lx, ly, sXY, sU, sM);
 }
 
 // True when every regular row of the block pattern is laid out as
@@ -927,13 +960,11 @@ bool grid_pattern_ok(const HostMesh& hm) {
     return true;
 }
 
-int grid_kpad(int nx) { return ((nx + 2) / 2 + kGridLanes - 1) / kGridLanes * kGridLanes; }
-
 void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
     GridArgs ga;
     ga.nx = c.hm.spec.nx;
     ga.ny = c.hm.spec.ny;
-    ga.kpad = grid_kpad(ga.nx);
+    ga.tiles_x = (ga.nx + 1 + kGridTileC - 1) / kGridTileC;
     ga.row_ptr = c.row_ptr;
     ga.emat = c.grid_emat;
     ga.x = c.x;
@@ -942,42 +973,82 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.dmat = c.dmat;
     ga.K = c.K;
     ga.f = c.F;
-    const long long threads = 2LL * (ga.ny + 1) * ga.kpad;
-    const int bs = c.tuning.grid_block;
-    const int blocks = (int)((threads + bs - 1) / bs);
-    if (want_K && want_f) k_grid_rows<true, true><<<blocks, bs, 0, s>>>(ga);
-    else if (want_K) k_grid_rows<true, false><<<blocks, bs, 0, s>>>(ga);
-    else if (want_f) k_grid_rows<false, true><<<blocks, bs, 0, s>>>(ga);
+    const int tr = c.tuning.grid_block == 128 ? 2 : 4;  // threads per CTA = 64 x node rows per tile
+    const int blocks = ga.tiles_x * ((ga.ny + 1 + tr - 1) / tr);
+    if (tr == 2) {
+        if (want_K && want_f) k_grid_rows<true, true, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
+        else if (want_K) k_grid_rows<true, false, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
+        else if (want_f) k_grid_rows<false, true, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
+    } else {
+        if (want_K && want_f) k_grid_rows<true, true, 4><<<blocks, kGridTileC * 4, 0, s>>>(ga);
+        else if (want_K) k_grid_rows<true, false, 4><<<blocks, kGridTileC * 4, 0, s>>>(ga);
+        else if (want_f) k_grid_rows<false, true, 4><<<blocks, kGridTileC * 4, 0, s>>>(ga);
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Cut elements: per-pair integration into a compact buffer, then a fold
+// Cut elements: integration per node pair into fold order, then a fold
 // ---------------------------------------------------------------------------
 // Every cut element's (3 + n_enr)^2 node-pair blocks have a fixed place in
 // the element's slot table (cut_slot: pair (a, b) at cut_slot_ptr + a nl +
-// b, holding the block's K slot).  k_cut_pairs integrates one pair per
-// thread into the compact buffer cut_ke at the pair's slot-table position
-// (and, for residual passes, K_ab u_b into cut_fe); nothing is added into K
-// there.  k_fold_K then gives every K slot that cut elements touch its final
-// value in one thread: the regular-element value the triangle kernel wrote
-// (or zero, for blocks in enrichment rows or columns, which only cut
-// elements reach) plus its contributions in a fixed order, a list built once
-// per mesh and sorted by (element, pair).  k_fold_f does the same per node
-// for f_int.  The sums are the same on every run: no atomics.
+// b, holding the block's K slot).  k_cut_elems integrates one pair per
+// thread and stores the block at its position in fold order (kpos, built
+// once per mesh: all contributions to one K slot next to each other, by
+// element and pair), and for residual passes K_ab u_b at its position in
+// the node-sorted order (fpos); nothing is added into K there.  k_fold_K
+// then gives every K slot that cut elements touch its final value in one
+// thread: the triangle kernel's value (or zero, for blocks in enrichment
+// rows or columns, which only cut elements reach) plus its contiguous run
+// of contributions; k_fold_f does the same per node for f_int.  The sums
+// are the same on every run: no atomics.
 //
-// The quadrature rows (k_cut_points), the cohesive points (k_coh_points)
-// and the pairs depend on the coordinates, the displacements and the
-// committed cohesive state only, so they run on a second stream beside the
-// triangle kernel; only the fold waits for both.
+// Three kernels form the pairs, all on a second stream beside the triangle
+// kernel (they depend on the coordinates, the displacements and the
+// committed cohesive state only; only the fold waits for both streams):
+// k_cut_points forms every quadrature row (one thread per point, from the
+// host-packed point records), k_coh_points every cohesive Gauss point (one
+// thread each: traction-separation law, trial delta_max, row), and
+// k_cut_pairs integrates one node pair per thread from those rows.
+constexpr int kCohRow = kCohRowDoubles;  // {w dA, N0, N1, (R^T D R) 4, (R^T t) 2, pad}
 
-// Rows of the cohesive Gauss points (CohEdge2, 2 points, w = 1): one thread
-// per point evaluates the traction-separation law at its opening (writing
-// the trial delta_max) and stores {w dA, N0, N1, (R^T D R) 4, (R^T t) 2} for
-// the pair kernel.  Point qp of a cohesive sub-element ce of element ci
-// (class order) is qp = cut_coh_qp0[ci] + 2 ce + q; coh_rec[qp] packs
-// ci << 8 | ce << 1 | q.
-constexpr int kCohRow = kCohRowDoubles;
+// One thread per quadrature point: its row, point-major (the element's point
+// l at row_off[element] + l (4 + 2 NL), NL its size class's largest local
+// node count), so that a pair thread reads a point's values with four
+// 128-bit loads.  The record carries the row's offset.  A CTA's points are
+// consecutive, so their rows are one contiguous span: the threads form them
+// in shared memory and the CTA stores the span with coalesced 128-bit stores.
+constexpr int kPointThreads = 128;
+constexpr int kRowMax = 4 + 2 * kCutClassNl[kCutClasses - 1];  // widest row (34 doubles)
 
+__global__ void __launch_bounds__(kPointThreads) k_cut_points(int n_pts, const int4* __restrict__ pts,
+                                                              const double* __restrict__ x,
+                                                              const double* __restrict__ y,
+                                                              const double* __restrict__ dmat, double* rows) {
+    __shared__ __align__(16) double sRow[kPointThreads * kRowMax];
+    const int p0 = blockIdx.x * kPointThreads, p = p0 + threadIdx.x;
+    const int p1 = min(n_pts, p0 + kPointThreads);
+    // the CTA's span of rows: from its first point's row to the next CTA's
+    // (the record after the last point is a sentinel holding the rows' end)
+    const int4 rb = __ldg(pts + 4 * (size_t)p0 + 3), re = __ldg(pts + 4 * (size_t)p1 + 3);
+    const long long base = (long long)(unsigned)rb.x | ((long long)rb.y << 32);
+    const long long end = (long long)(unsigned)re.x | ((long long)re.y << 32);
+    if (p < n_pts) {
+        const CutPoint cp = cut_point_load(pts + 4 * (size_t)p);
+        const long long off = (long long)(unsigned)cp.r3.x | ((long long)cp.r3.y << 32);
+        cut_point_row(cp, x, y, dmat, sRow + (off - base));
+    }
+    __syncthreads();
+    // rows hold an even number of doubles and start at even offsets
+    const int n2 = (int)((end - base) / 2);
+    const double2* src = reinterpret_cast<const double2*>(sRow);
+    double2* dst = reinterpret_cast<double2*>(rows + base);
+    for (int i = threadIdx.x; i < n2; i += kPointThreads) dst[i] = src[i];
+}
+
+// One thread per cohesive Gauss point (CohEdge2, 2 points, w = 1): the law
+// at its opening (writing the trial delta_max) and its row.  Point qp of
+// sub-element ce of element ci (class order) is qp = cut_coh_qp0[ci] + 2 ce
+// + q; coh_rec[qp] packs ci << 8 | ce << 1 | q.
 struct CohArgs {
     int n_qp;
     const int* __restrict__ coh_rec;
@@ -1028,12 +1099,12 @@ __global__ void __launch_bounds__(128) k_coh_points(CohArgs a) {
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            double s = 0.0;
+            double sum = 0.0;
 #pragma unroll
             for (int k1 = 0; k1 < 2; ++k1)
 #pragma unroll
-                for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
-            row[3 + 2 * i + j] = s;
+                for (int k2 = 0; k2 < 2; ++k2) sum += R[k1][i] * Dc[k1][k2] * R[k2][j];
+            row[3 + 2 * i + j] = sum;
         }
     row[7] = R[0][0] * tr[0] + R[1][0] * tr[1];
     row[8] = R[0][1] * tr[0] + R[1][1] * tr[1];
@@ -1047,22 +1118,25 @@ struct PairArgs {
     const int* __restrict__ cut_tmpl;
     const int* __restrict__ cut_coh_qp0;
     const int* __restrict__ cut_slot_ptr;
+    const int* __restrict__ kpos;   // slot-table entry -> position in fold order (-1: no K slot)
+    const int* __restrict__ fpos;   // slot-table entry -> position in node order
     const double* __restrict__ rows;
     const long long* __restrict__ row_off;
     const double* __restrict__ coh_rows;
     const double* __restrict__ u;
-    double* ke;                     // 4 per slot-table entry
-    double* fe;                     // 2 per slot-table entry
+    double* ke;                     // 4 FP64 per fold position
+    double* fe;                     // 2 FP64 per node-order position
     int want_K, want_f;
 };
 
+__device__ __forceinline__ double2 ldg2(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+
 // One thread per node pair (a, b) of a cut element of size class NL (NL^2
 // threads per element; pairs beyond the element's nl^2 idle): the block
-// K_ab = sum_q w_q B_a^T D B_b over the element's quadrature rows
-// (value-major: value j of point q at j nq + q, so the threads of an element
-// read the same addresses), plus the cohesive sub-elements' N_a N_b (+-)
-// R^T D R R terms when both nodes are cohesive nodes.  Residual passes store
-// K_ab u_b, and on the diagonal pair the node's cohesive traction term.
+// K_ab = sum_q w_q B_a^T D B_b over the element's rows, plus the cohesive
+// sub-elements' N_a N_b (+-) R^T D R terms when both nodes are cohesive
+// nodes; residual passes store K_ab u_b (bulk) and, on the diagonal pair,
+// the node's cohesive traction term.
 template <int NL>
 __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
     constexpr int P = NL * NL, W = 4 + 2 * NL;
@@ -1074,15 +1148,20 @@ __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
     const int nl = 3 + T.n_enr;
     if (p >= nl * nl) return;
     const int pa = p / nl, pb = p - pa * nl;
-    const long long r0 = __ldg(&a.row_off[ci]);
-    const int nq = (int)((__ldg(&a.row_off[ci + 1]) - r0) / W);
-    const double* rw = a.rows + r0;
+    // inputs that do not depend on each other, issued together
+    const long long r0 = __ldg(&a.row_off[ci]), r1 = __ldg(&a.row_off[ci + 1]);
+    const long long sidx = __ldg(&a.cut_slot_ptr[ci]) + (long long)p;
+    const int kp = a.want_K ? __ldg(&a.kpos[sidx]) : -1;
+    const int fp = a.want_f ? __ldg(&a.fpos[sidx]) : -1;
+    const int node_b = a.want_f ? __ldg(&a.cut_nodes[(size_t)kCutNodeStride * ci + pb]) : 0;
+    const int nq = (int)((r1 - r0) / W);
     double k0 = 0.0, k1 = 0.0, k2 = 0.0, k3 = 0.0;
-    for (int q = 0; q < nq; ++q) {
-        const double wgt = __ldg(&rw[q]), d11 = __ldg(&rw[nq + q]), d12 = __ldg(&rw[2 * nq + q]),
-                     d33 = __ldg(&rw[3 * nq + q]);
-        const double ba = __ldg(&rw[(4 + 2 * pa) * nq + q]) * wgt, ca = __ldg(&rw[(5 + 2 * pa) * nq + q]) * wgt;
-        const double bb = __ldg(&rw[(4 + 2 * pb) * nq + q]), cb = __ldg(&rw[(5 + 2 * pb) * nq + q]);
+    const double* rw = a.rows + r0;
+    for (int q = 0; q < nq; ++q, rw += W) {
+        const double2 wd = ldg2(rw), dd = ldg2(rw + 2);
+        const double2 ga = ldg2(rw + 4 + 2 * pa), gb = ldg2(rw + 4 + 2 * pb);
+        const double wgt = wd.x, d11 = wd.y, d12 = dd.x, d33 = dd.y;
+        const double ba = ga.x * wgt, ca = ga.y * wgt, bb = gb.x, cb = gb.y;
         k0 += ba * d11 * bb + ca * d33 * cb;
         k1 += ba * d12 * cb + ca * d33 * bb;
         k2 += ca * d12 * bb + ba * d33 * cb;
@@ -1092,12 +1171,10 @@ __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
     // traction integral below, not the cohesive tangent times u)
     double fx = 0.0, fy = 0.0;
     if (a.want_f) {
-        const int node_b = __ldg(&a.cut_nodes[(size_t)kCutNodeStride * ci + pb]);
         const double ux = __ldg(&a.u[2 * node_b]), uy = __ldg(&a.u[2 * node_b + 1]);
         fx = k0 * ux + k1 * uy;
         fy = k2 * ux + k3 * uy;
     }
-    double tx = 0.0, ty = 0.0;  // cohesive traction of node a (diagonal pair only)
     if (T.n_coh > 0) {
         const int qp0 = __ldg(&a.cut_coh_qp0[ci]);
         for (int ce = 0; ce < T.n_coh; ++ce) {
@@ -1122,33 +1199,31 @@ __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
                 k2 += v * __ldg(&row[5]);
                 k3 += v * __ldg(&row[6]);
                 if (pa == pb) {
-                    tx += wgt * sa * Na * __ldg(&row[7]);
-                    ty += wgt * sa * Na * __ldg(&row[8]);
+                    fx += wgt * sa * Na * __ldg(&row[7]);
+                    fy += wgt * sa * Na * __ldg(&row[8]);
                 }
             }
         }
     }
-    const long long sidx = __ldg(&a.cut_slot_ptr[ci]) + (long long)p;
-    if (a.want_K) store_block(a.ke, sidx, k0, k1, k2, k3);
-    if (a.want_f) reinterpret_cast<double2*>(a.fe)[sidx] = make_double2(fx + tx, fy + ty);
+    if (kp >= 0) store_block(a.ke, kp, k0, k1, k2, k3);
+    if (fp >= 0) reinterpret_cast<double2*>(a.fe)[fp] = make_double2(fx, fy);
 }
 
 // K slots that cut elements touch, one thread each: K[slot] = (the triangle
-// kernel's value, or 0 where flagged as cut-only) + the slot's pair blocks
-// in list order.  Entry j: fold_slot[j] = slot << 1 | cut_only, pairs
-// fold_idx[fold_ptr[j] .. fold_ptr[j + 1]).
+// kernel's value, or 0 where flagged cut_only) + the slot's contiguous run
+// of pair blocks ke[ptr[j] .. ptr[j + 1]), summed in run order.
+// fold_slot[j] = slot << 1 | cut_only.
 __global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restrict__ fold_slot,
-                                                const int* __restrict__ fold_ptr, const int* __restrict__ fold_idx,
-                                                const double* __restrict__ ke, double* K) {
+                                                const int* __restrict__ fold_ptr, const double* __restrict__ ke,
+                                                double* K) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const long long sw = __ldg(&fold_slot[j]);
+    const int i0 = __ldg(&fold_ptr[j]), i1 = __ldg(&fold_ptr[j + 1]);
     const long long slot = sw >> 1;
-    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (!(sw & 1)) acc = load_block(K, slot);
-    const int i1 = __ldg(&fold_ptr[j + 1]);
-    for (int i = __ldg(&fold_ptr[j]); i < i1; ++i) {
-        const double4 v = load_block_nc(ke, __ldg(&fold_idx[i]));
+    double4 acc = (sw & 1) ? make_double4(0.0, 0.0, 0.0, 0.0) : load_block(K, slot);
+    for (int i = i0; i < i1; ++i) {
+        const double4 v = load_block_nc(ke, i);
         acc.x += v.x;
         acc.y += v.y;
         acc.z += v.z;
@@ -1158,107 +1233,86 @@ __global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restri
 }
 
 // f_int of the nodes cut elements touch, one thread each: f = (the triangle
-// kernel's value, or 0 for enrichment nodes) + the node's pair terms in
-// list order.  fold_node[j] = node << 1 | cut_only.
+// kernel's value, or 0 for enrichment nodes) + the node's contiguous run of
+// pair terms.  fold_node[j] = node << 1 | cut_only.
 __global__ void __launch_bounds__(256) k_fold_f(int n, const int* __restrict__ fold_node,
-                                                const int* __restrict__ fold_ptr, const int* __restrict__ fold_idx,
-                                                const double* __restrict__ fe, double* f) {
+                                                const int* __restrict__ fold_ptr, const double* __restrict__ fe,
+                                                double* f) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const int nw = __ldg(&fold_node[j]);
+    const int i0 = __ldg(&fold_ptr[j]), i1 = __ldg(&fold_ptr[j + 1]);
     const int node = nw >> 1;
-    double2 acc = make_double2(0.0, 0.0);
-    if (!(nw & 1)) acc = reinterpret_cast<const double2*>(f)[node];
-    const int i1 = __ldg(&fold_ptr[j + 1]);
-    for (int i = __ldg(&fold_ptr[j]); i < i1; ++i) {
-        const double2 v = __ldg(reinterpret_cast<const double2*>(fe) + __ldg(&fold_idx[i]));
+    double2 acc = (nw & 1) ? make_double2(0.0, 0.0) : reinterpret_cast<const double2*>(f)[node];
+    for (int i = i0; i < i1; ++i) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(fe) + i);
         acc.x += v.x;
         acc.y += v.y;
     }
     reinterpret_cast<double2*>(f)[node] = acc;
 }
 
-// Per-warp shared tables: one row per quadrature point of the current chunk
-// holding {wgt, d11, d12, d33, (gx, gy) of every local function}, and one
-// row per cohesive point holding {wgt, N0, N1, (R^T D R) 4, (R^T t) 2}.
+// Shape sensitivity of the cut elements' internal force (pg_sens.cu): one
+// warp per cut element.  The element's enrichment nodes on the selected
+// inclusion move by sgn * h_rel * r * (their velocity), the lanes form the
+// element's quadrature rows at the moved geometry (one point per lane) in
+// per-warp shared memory, integrate their node-pair blocks over them and
+// dot the element's internal force (bulk K_e u_e plus the cohesive
+// tractions) with wsens; lane 0 adds sgn * (that) / (2 h) to sens[inclusion].
 // NL is the size class's largest local node count; PPL = ceil(NL^2 / 32)
 // node-pair blocks per lane.
 constexpr int kQpChunk = 32;
-constexpr int kCRow = 10;
 
-template <int NL, int PPL, int W, bool SENS = false>
-__global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7 ? 16 : 8)) / W) k_assemble_cut(CutArgs a) {
-    constexpr int kCutWarps = W;
+template <int NL, int PPL, int W>
+__global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / W) k_cut_sens(CutArgs a) {
     constexpr int kQRow = 4 + 2 * NL;
-    __shared__ double sX[kCutWarps][NL], sY[kCutWarps][NL];
-    __shared__ double sU[kCutWarps][2 * NL];
-    __shared__ int sL[kCutWarps][NL];
-    __shared__ double sQ[kCutWarps][kQpChunk][kQRow];
-    __shared__ double sC[kCutWarps][2 * kMaxCoh][kCRow];
+    __shared__ double sX[W][NL], sY[W][NL];
+    __shared__ double sU[W][2 * NL];
+    __shared__ int sL[W][NL];
+    __shared__ double sQ[W][kQpChunk][kQRow];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int oi = blockIdx.x * kCutWarps + w;
+    const int oi = blockIdx.x * W + w;
     if (oi >= a.n_cut) return;
     const int ci = a.first + oi;  // class-ordered element index
-    // the node list (padded with -1), the template and the slot pointer do
-    // not depend on each other: their loads go out together
     const int node = lane < NL ? __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]) : -1;
     const int tmpl = __ldg(&a.cut_tmpl[ci]);
-    const int slot0 = __ldg(&a.cut_slot_ptr[ci]);
-    const long long roff = SENS ? 0 : __ldg(&a.row_off[ci]);
     const DevTemplate& T = c_tmpl[tmpl];
     const int nl = 3 + T.n_enr;
-    // the element's block slots are needed only at the end: issue their loads now
-    const int* slots = a.cut_slot + slot0;
-    int slot[PPL];
-#pragma unroll
-    for (int k = 0; k < PPL; ++k)
-        slot[k] = (!SENS && a.want_K && lane + 32 * k < nl * nl) ? __ldg(&slots[lane + 32 * k]) : -1;
     if (lane < nl) {
         sL[w][lane] = node;
-        if (SENS || T.n_coh > 0) {  // otherwise the quadrature rows carry all the geometry
-            sX[w][lane] = a.x[node];
-            sY[w][lane] = a.y[node];
-        }
-        if (SENS || a.want_f || T.n_coh > 0) {
-            sU[w][2 * lane] = a.u[2 * node];
-            sU[w][2 * lane + 1] = a.u[2 * node + 1];
-        }
+        sX[w][lane] = a.x[node];
+        sY[w][lane] = a.y[node];
+        sU[w][2 * lane] = a.u[2 * node];
+        sU[w][2 * lane + 1] = a.u[2 * node + 1];
     }
     __syncwarp();
-    double part = 0.0;    // SENS: this lane's share of wsens . f_e
-    int sel = -1;         // SENS: the inclusion whose radius moves
-    double hstep = 0.0;
-    if (SENS) {
-        const unsigned full = 0xffffffffu;
-        const int my_inc = (lane >= 3 && lane < nl) ? a.node_inc[sL[w][lane]] : -1;
-        // the which-th distinct inclusion among the enrichment slots, in slot order
-        int count = 0;
-        for (int l = 3; l < nl; ++l) {
-            const int v = __shfl_sync(full, my_inc, l);
-            bool seen = false;
-            for (int l2 = 3; l2 < l; ++l2) seen |= __shfl_sync(full, my_inc, l2) == v;
-            if (!seen && v >= 0) {
-                if (count == a.which) sel = v;
-                ++count;
-            }
+    const unsigned full = 0xffffffffu;
+    const int my_inc = (lane >= 3 && lane < nl) ? a.node_inc[sL[w][lane]] : -1;
+    // the which-th distinct inclusion among the enrichment slots, in slot order
+    int sel = -1, count = 0;
+    for (int l = 3; l < nl; ++l) {
+        const int v = __shfl_sync(full, my_inc, l);
+        bool seen = false;
+        for (int l2 = 3; l2 < l; ++l2) seen |= __shfl_sync(full, my_inc, l2) == v;
+        if (!seen && v >= 0) {
+            if (count == a.which) sel = v;
+            ++count;
         }
-        if (sel < 0) return;  // warp-uniform: no such inclusion in this element
-        hstep = a.h_rel * a.radius[sel];
-        if (lane < nl && my_inc == sel) {
-            const int node = sL[w][lane];
-            sX[w][lane] += a.sgn * hstep * a.vel[2 * node];
-            sY[w][lane] += a.sgn * hstep * a.vel[2 * node + 1];
-        }
-        __syncwarp();
     }
-    // parent (Tri3) gradients are constant over the element (SENS: its nodes have moved)
-    double pbx[3] = {0.0, 0.0, 0.0}, pby[3] = {0.0, 0.0, 0.0};
-    if (SENS) parent_gradients(sX[w], sY[w], pbx, pby);
-
+    if (sel < 0) return;  // warp-uniform: no such inclusion in this element
+    const double hstep = a.h_rel * a.radius[sel];
+    if (lane < nl && my_inc == sel) {
+        const int nd = sL[w][lane];
+        sX[w][lane] += a.sgn * hstep * a.vel[2 * nd];
+        sY[w][lane] += a.sgn * hstep * a.vel[2 * nd + 1];
+    }
+    __syncwarp();
+    // parent (Tri3) gradients are constant over the element (its nodes have moved)
+    double pbx[3], pby[3];
+    parent_gradients(sX[w], sY[w], pbx, pby);
     int nq_total = 0;
     for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
-
     double acc[PPL][4];
 #pragma unroll
     for (int k = 0; k < PPL; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
@@ -1270,37 +1324,25 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7
         pa[k] = p / nl;
         pb[k] = p - pa[k] * nl;
     }
-
     for (int qbase = 0; qbase < nq_total; qbase += kQpChunk) {
-        if (SENS) {
-            // geometry of one quadrature point per lane, all points in parallel
-            const int l = qbase + lane;
-            if (l < nq_total) {
-                const DevTemplate& TG = g_tmpl[tmpl];
-                int ch, q;
-                point_child(TG, l, ch, q);
-                const int nc = TG.child_n[ch];
-                const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
-                int ln[kMaxChildNodes];
-                double cx[kMaxChildNodes], cy[kMaxChildNodes];
+        // geometry of one quadrature point per lane, all points in parallel
+        const int l = qbase + lane;
+        if (l < nq_total) {
+            const DevTemplate& TG = g_tmpl[tmpl];
+            int ch, q;
+            point_child(TG, l, ch, q);
+            const int nc = TG.child_n[ch];
+            const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
+            int ln[kMaxChildNodes];
+            double cx[kMaxChildNodes], cy[kMaxChildNodes];
 #pragma unroll
-                for (int k = 0; k < kMaxChildNodes; ++k) {
-                    ln[k] = k < nc ? TG.child_nodes[ch][k] : 0;
-                    cx[k] = sX[w][ln[k]];
-                    cy[k] = sY[w][ln[k]];
-                }
-                const double dm[3] = {a.dmat[3 * mat], a.dmat[3 * mat + 1], a.dmat[3 * mat + 2]};
-                cut_row(sQ[w][lane], 1, nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm, pbx, pby);
+            for (int k = 0; k < kMaxChildNodes; ++k) {
+                ln[k] = k < nc ? TG.child_nodes[ch][k] : 0;
+                cx[k] = sX[w][ln[k]];
+                cy[k] = sY[w][ln[k]];
             }
-        } else {
-            // the chunk's rows, formed by k_cut_points (value-major: value j of
-            // point q at j nq_total + q): a coalesced read, transposed into sQ
-            const int nqc = min(kQpChunk, nq_total - qbase);
-            const double* src = a.rows + roff + qbase;
-            for (int i = lane; i < nqc * kQRow; i += 32) {
-                const int j = i / nqc, q = i - j * nqc;
-                sQ[w][q][j] = __ldg(&src[(long long)j * nq_total + q]);
-            }
+            const double dm[3] = {a.dmat[3 * mat], a.dmat[3 * mat + 1], a.dmat[3 * mat + 2]};
+            cut_row(sQ[w][lane], 1, nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dm, pbx, pby);
         }
         __syncwarp();
         // each lane integrates its node-pair blocks over the chunk's points
@@ -1322,26 +1364,19 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7
         }
         __syncwarp();
     }
-    // bulk internal force f_a = sum_b K_ab u_b
-    if (SENS || a.want_f) {
+    // this lane's share of wsens . f_e: bulk K_ab u_b ...
+    double part = 0.0;
 #pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-            if (lane + 32 * k < npairs) {
-                const int ia = pa[k], ib = pb[k];
-                const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
-                const double fx = acc[k][0] * ux + acc[k][1] * uy;
-                const double fy = acc[k][2] * ux + acc[k][3] * uy;
-                if (SENS) {
-                    part += a.wsens[2 * sL[w][ia]] * fx + a.wsens[2 * sL[w][ia] + 1] * fy;
-                } else {
-                    atomicAdd(&a.f[2 * sL[w][ia]], fx);
-                    atomicAdd(&a.f[2 * sL[w][ia] + 1], fy);
-                }
-            }
+    for (int k = 0; k < PPL; ++k) {
+        if (lane + 32 * k < npairs) {
+            const int ia = pa[k], ib = pb[k];
+            const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
+            const double fx = acc[k][0] * ux + acc[k][1] * uy;
+            const double fy = acc[k][2] * ux + acc[k][3] * uy;
+            part += a.wsens[2 * sL[w][ia]] * fx + a.wsens[2 * sL[w][ia] + 1] * fy;
         }
     }
-    if (T.n_coh == 0) goto scatter;
-    // cohesive sub-elements: two Gauss points each (CohEdge2, w = 1), one lane per point
+    // ... and the cohesive tractions: two Gauss points per sub-element, one lane each
     if (lane < 2 * T.n_coh) {
         const int ce = lane >> 1, q = lane & 1;
         const int c0 = T.coh_nodes[ce][0], c1 = T.coh_nodes[ce][1], c2 = T.coh_nodes[ce][2], c3 = T.coh_nodes[ce][3];
@@ -1358,92 +1393,26 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? (SENS ? 24 : 32) : (NL <= 7
             dg[d] = N0 * (sU[w][2 * c2 + d] - sU[w][2 * c0 + d]) + N1 * (sU[w][2 * c3 + d] - sU[w][2 * c1 + d]);
         double dl[2] = {R[0][0] * dg[0] + R[0][1] * dg[1], R[1][0] * dg[0] + R[1][1] * dg[1]};
         const int qp = a.cut_coh_qp0[ci] + lane;
-        const double dmax_c = a.isv_c[qp];
         double tr[2], Dc[2][2], dmax_t;
-        cohesive_law(a.coh, a.dt, dmax_c, dl, tr, Dc, dmax_t);
-        if (!SENS) a.isv_t[qp] = dmax_t;
-        double* row = sC[w][lane];
-        row[0] = dA * 1.0;
-        row[1] = N0;
-        row[2] = N1;
-        for (int i = 0; i < 2; ++i)
-            for (int j = 0; j < 2; ++j) {
-                double s = 0.0;
-                for (int k1 = 0; k1 < 2; ++k1)
-                    for (int k2 = 0; k2 < 2; ++k2) s += R[k1][i] * Dc[k1][k2] * R[k2][j];
-                row[3 + 2 * i + j] = s;
-            }
+        cohesive_law(a.coh, a.dt, a.isv_c[qp], dl, tr, Dc, dmax_t);
         const double tR0 = R[0][0] * tr[0] + R[1][0] * tr[1];
         const double tR1 = R[0][1] * tr[0] + R[1][1] * tr[1];
-        row[7] = tR0;
-        row[8] = tR1;
-        const double wgt = row[0];
-        if ((SENS || a.want_f) && wgt != 0.0) {
+        const double wgt = dA * 1.0;
+        if (wgt != 0.0) {
             const int cn[4] = {c0, c1, c2, c3};
             const double Nn[2] = {N0, N1};
             for (int m = 0; m < 4; ++m) {
                 const double sgn = m < 2 ? -1.0 : 1.0;
-                const int node = sL[w][cn[m]];
-                if (SENS) {
-                    part += a.wsens[2 * node] * (wgt * sgn * Nn[m & 1] * tR0) +
-                            a.wsens[2 * node + 1] * (wgt * sgn * Nn[m & 1] * tR1);
-                } else {
-                    atomicAdd(&a.f[2 * node], wgt * sgn * Nn[m & 1] * tR0);
-                    atomicAdd(&a.f[2 * node + 1], wgt * sgn * Nn[m & 1] * tR1);
-                }
+                const int nd = sL[w][cn[m]];
+                part += a.wsens[2 * nd] * (wgt * sgn * Nn[m & 1] * tR0) +
+                        a.wsens[2 * nd + 1] * (wgt * sgn * Nn[m & 1] * tR1);
             }
         }
     }
-    __syncwarp();
-    if (a.want_K) {
-        for (int ce = 0; ce < T.n_coh; ++ce) {
-            const int cn[4] = {T.coh_nodes[ce][0], T.coh_nodes[ce][1], T.coh_nodes[ce][2], T.coh_nodes[ce][3]};
+    // central difference of wsens . f_e: this pass adds sgn * (its share) / (2 h)
 #pragma unroll
-            for (int k = 0; k < PPL; ++k) {
-                if (lane + 32 * k < npairs) {
-                    int i = -1, j = -1;
-                    for (int m = 0; m < 4; ++m) {
-                        if (cn[m] == pa[k]) i = m;
-                        if (cn[m] == pb[k]) j = m;
-                    }
-                    if (i >= 0 && j >= 0) {
-                        const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
-                        for (int q = 0; q < 2; ++q) {
-                            const double* row = sC[w][2 * ce + q];
-                            const double wgt = row[0];
-                            if (wgt == 0.0) continue;
-                            const double v = wgt * sgn * row[1 + (i & 1)] * row[1 + (j & 1)];
-                            acc[k][0] += v * row[3];
-                            acc[k][1] += v * row[4];
-                            acc[k][2] += v * row[5];
-                            acc[k][3] += v * row[6];
-                        }
-                    }
-                }
-            }
-        }
-    }
-scatter:
-    if (SENS) {
-        // central difference of wsens . f_e: this pass adds sgn * (its share) / (2 h)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
-        if (lane == 0) atomicAdd(&a.sens[sel], a.sgn * part / (2.0 * hstep));
-        return;
-    }
-    if (a.want_K) {
-#pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-            const int p = lane + 32 * k;
-            if (p < npairs && slot[k] >= 0) {
-                double* d = a.K + 4 * (size_t)slot[k];
-                atomicAdd(d + 0, acc[k][0]);
-                atomicAdd(d + 1, acc[k][1]);
-                atomicAdd(d + 2, acc[k][2]);
-                atomicAdd(d + 3, acc[k][3]);
-            }
-        }
-    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(full, part, o);
+    if (lane == 0) atomicAdd(&a.sens[sel], a.sgn * part / (2.0 * hstep));
 }
 
 __global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
@@ -1488,7 +1457,7 @@ void launch_tri(const Ctx& c, const RowArgs& ra, bool want_f, cudaStream_t s) {
     }
 }
 
-// Shape-sensitivity passes of the cut-element kernel (one per size class).
+// Shape-sensitivity passes of the cut elements (one launch per size class).
 void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
     for (int k = 0; k < kCutClasses; ++k) {
         const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
@@ -1497,10 +1466,10 @@ void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
         ck.n_cut = n;
         ck.first = c.cut_class_off[k];
         const int blocks = (n + 3) / 4;
-        if (k == 0) k_assemble_cut<5, 1, 4, true><<<blocks, 128, 0, s>>>(ck);
-        else if (k == 1) k_assemble_cut<7, 2, 4, true><<<blocks, 128, 0, s>>>(ck);
-        else if (k == 2) k_assemble_cut<11, 4, 4, true><<<blocks, 128, 0, s>>>(ck);
-        else k_assemble_cut<15, 8, 4, true><<<blocks, 128, 0, s>>>(ck);
+        if (k == 0) k_cut_sens<5, 1, 4><<<blocks, 128, 0, s>>>(ck);
+        else if (k == 1) k_cut_sens<7, 2, 4><<<blocks, 128, 0, s>>>(ck);
+        else if (k == 2) k_cut_sens<11, 4, 4><<<blocks, 128, 0, s>>>(ck);
+        else k_cut_sens<15, 8, 4><<<blocks, 128, 0, s>>>(ck);
     }
 }
 
@@ -1527,61 +1496,39 @@ RowArgs row_args(const Ctx& c, const double* U, bool want_f, bool want_K) {
     return ra;
 }
 
-CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K) {
-    CutArgs ca;
+CutArgs cut_args(const Ctx& c, const double* U, double dt) {
+    CutArgs ca{};
     ca.n_cut = c.n_cut;
     ca.first = 0;
     ca.cut_nodes = c.cut_nodes;
     ca.cut_tmpl = c.cut_tmpl;
     ca.cut_child_mat = c.cut_child_mat;
     ca.cut_coh_qp0 = c.cut_coh_qp0;
-    ca.cut_slot_ptr = c.cut_slot_ptr;
-    ca.cut_slot = c.cut_slot;
     ca.x = c.x;
     ca.y = c.y;
     ca.u = U;
     ca.dmat = c.dmat;
     ca.isv_c = c.isv_c;
-    ca.isv_t = c.isv_t;
-    ca.rows = c.cut_rows;
-    ca.row_off = c.cut_row_off;
     ca.coh = c.coh;
     ca.dt = dt;
-    ca.K = c.K;
-    ca.f = c.F;
-    ca.want_K = want_K;
-    ca.want_f = want_f;
     return ca;
 }
 
-void launch_cut_points(const Ctx& c, cudaStream_t s) {
-    if (c.n_cut_pts > 0) {
-        CutPointArgs pa;
-        pa.n_pts = c.n_cut_pts;
-        pa.pts = reinterpret_cast<const int4*>(c.cut_pts);
-        pa.x = c.x;
-        pa.y = c.y;
-        pa.dmat = c.dmat;
-        pa.rows = c.cut_rows;
-        k_cut_points<<<(c.n_cut_pts + 255) / 256, 256, 0, s>>>(pa);
-    }
-}
-
-// Fold lists from the class-ordered slot tables (sp: per element its first
+// Fold order from the class-ordered slot tables (sp: per element its first
 // slot-table entry, sl: K slot of every pair, -1 none; nodes: kCutNodeStride
-// local nodes per element).  K: every touched slot with its pair entries in
-// slot-table order (element, then pair), flagged cut_only when its row or
-// column node is an enrichment node (no triangle-kernel value to add to).
-// f: every touched node with the entries of its pairs (a, *), in the same
-// order, flagged cut_only for enrichment nodes.
+// local nodes per element).  K: the pairs sorted by (slot, entry); kpos
+// gives each entry its position (-1 without a slot); every touched slot is
+// one run [k_ptr[j], k_ptr[j + 1]), flagged cut_only when its row or column
+// node is an enrichment node (no triangle-kernel value to add to).  f: the
+// pairs sorted by (node a, entry); fpos and runs likewise, cut_only for
+// enrichment nodes.
 void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
-                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& k_idx,
-                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& f_idx) {
+                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& kpos,
+                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& fpos) {
     const int nc = (int)sp.size() - 1;
     std::vector<std::pair<long long, int>> ke, fe;  // (key, slot-table entry)
     ke.reserve(sl.size());
     fe.reserve(sl.size());
-    std::vector<char> k_cut_only;
     for (int oi = 0; oi < nc; ++oi) {
         const int np = sp[oi + 1] - sp[oi];
         int nl = 0;
@@ -1594,26 +1541,31 @@ void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vecto
             fe.emplace_back(((long long)na << 1) | (na >= n_reg ? 1 : 0), idx);
         }
     }
-    auto to_csr = [](std::vector<std::pair<long long, int>>& v, auto& keys, std::vector<int>& ptr,
-                     std::vector<int>& idx) {
+    auto runs = [&](std::vector<std::pair<long long, int>>& v, std::vector<long long>& keys, std::vector<int>& ptr,
+                    std::vector<int>& pos) {
         std::sort(v.begin(), v.end());
         keys.clear();
-        ptr.assign(1, 0);
-        idx.clear();
-        idx.reserve(v.size());
+        ptr.clear();
+        pos.assign(sl.size(), -1);
         for (size_t i = 0; i < v.size(); ++i) {
             if (i == 0 || v[i].first != v[i - 1].first) {
-                if (i > 0) ptr.push_back((int)idx.size());
                 keys.push_back(v[i].first);
+                ptr.push_back((int)i);
             }
-            idx.push_back(v[i].second);
+            pos[v[i].second] = (int)i;
         }
-        if (!v.empty()) ptr.push_back((int)idx.size());
+        ptr.push_back((int)v.size());
     };
-    to_csr(ke, k_slot, k_ptr, k_idx);
+    runs(ke, k_slot, k_ptr, kpos);
     std::vector<long long> fk;
-    to_csr(fe, fk, f_ptr, f_idx);
+    runs(fe, fk, f_ptr, fpos);
     f_node.assign(fk.begin(), fk.end());
+}
+
+void launch_cut_points(const Ctx& c, cudaStream_t s) {
+    if (c.n_cut_pts > 0)
+        k_cut_points<<<(c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, 0, s>>>(
+            c.n_cut_pts, reinterpret_cast<const int4*>(c.cut_pts), c.x, c.y, c.dmat, c.cut_rows);
 }
 
 void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s) {
@@ -1641,6 +1593,8 @@ void launch_cut_pairs(const Ctx& c, const double* U, bool want_f, bool want_K, c
     pa.cut_tmpl = c.cut_tmpl;
     pa.cut_coh_qp0 = c.cut_coh_qp0;
     pa.cut_slot_ptr = c.cut_slot_ptr;
+    pa.kpos = c.cut_kpos;
+    pa.fpos = c.cut_fpos;
     pa.rows = c.cut_rows;
     pa.row_off = c.cut_row_off;
     pa.coh_rows = c.coh_rows;
@@ -1664,41 +1618,34 @@ void launch_cut_pairs(const Ctx& c, const double* U, bool want_f, bool want_K, c
     }
 }
 
-void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, cudaStream_t s) {
-    if (want_K && c.n_fold_K > 0)
-        k_fold_K<<<(c.n_fold_K + 255) / 256, 256, 0, s>>>(c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.fold_K_idx,
-                                                         c.cut_ke, c.K);
-    if (want_f && c.n_fold_f > 0)
-        k_fold_f<<<(c.n_fold_f + 255) / 256, 256, 0, s>>>(c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.fold_f_idx,
-                                                         c.cut_fe, c.F);
-}
-
-// The cut elements' work that depends on the inputs only (quadrature rows,
-// cohesive points, pair blocks) on stream s
-void launch_cut_work(const Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
+// The cut elements' quadrature rows and cohesive points (inputs only)
+void launch_cut_rows(const Ctx& c, const double* U, double dt, cudaStream_t s) {
     launch_cut_points(c, s);
     launch_coh_points(c, U, dt, s);
-    launch_cut_pairs(c, U, want_f, want_K, s);
+}
+
+void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, cudaStream_t s) {
+    if (want_K && c.n_fold_K > 0)
+        k_fold_K<<<(c.n_fold_K + 255) / 256, 256, 0, s>>>(c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.cut_ke, c.K);
+    if (want_f && c.n_fold_f > 0)
+        k_fold_f<<<(c.n_fold_f + 255) / 256, 256, 0, s>>>(c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.cut_fe, c.F);
 }
 
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
     // The triangle kernel writes every regular-element value of K (and f)
-    // once; the cut elements' rows, cohesive points and pair blocks are
-    // formed on the second stream beside it; the fold, which needs both,
-    // completes the rows cut elements touch and writes the enrichment rows
-    // and columns whole.  Nothing needs clearing first.
+    // once; then the cut elements' quadrature rows, cohesive points and pair
+    // blocks are formed, and the fold adds them to the rows they touch and
+    // writes the enrichment rows and columns whole.  Nothing needs clearing
+    // first.  All on one stream: the triangle kernel fills every SM until its
+    // last wave, so a second stream bought no overlap (measured).
     const RowArgs ra = row_args(c, U, want_f, want_K);
-    const bool cut = c.n_cut > 0;
-    if (cut) PG_CUDA(cudaEventRecord(c.fork_ev, s));
     if (c.timing) cudaEventRecord(c.ea0, s);
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
     if (c.timing) cudaEventRecord(c.ea1, s);
-    if (cut) {
-        PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
-        launch_cut_work(c, U, dt, want_f, want_K, c.aux);
-        PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
-        PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
+    if (c.n_cut > 0) {
+        launch_cut_rows(c, U, dt, s);
+        launch_cut_pairs(c, U, want_f, want_K, s);
         launch_cut_fold(c, want_f, want_K, s);
         PG_CUDA(cudaGetLastError());
     }
@@ -1712,7 +1659,8 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
 // 32 / 64 node rows per CTA, one CTA per tile / persistent (4 values), then
 // the structured-grid kernel (the faster of 128 and 256 threads per CTA; 0
 // without a structured grid); ms_cut: the cut elements' work on one stream
-// (rows, cohesive points, pairs, fold) with 2 / 4 / 8 warps per pair CTA.
+// (rows, cohesive points, pairs with their fold) with 2 / 4 / 8 warps per
+// pair CTA.
 // K is left undefined: the next solve reassembles.
 int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     cudaStream_t s = c.stream;
@@ -1780,7 +1728,8 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
         float ms = 0.f;
         if (c.n_cut > 0)
             ms = timed([&] {
-                launch_cut_work(c, c.U, 1.0, false, true, s);
+                launch_cut_rows(c, c.U, 1.0, s);
+                launch_cut_pairs(c, c.U, false, true, s);
                 launch_cut_fold(c, false, true, s);
             });
         if (ms_cut) ms_cut[k] = ms;

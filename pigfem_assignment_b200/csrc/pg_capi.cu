@@ -59,8 +59,8 @@ void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
-                    c.cut_ke, c.cut_fe, c.fold_K_slot, c.fold_K_ptr, c.fold_K_idx, c.fold_f_node, c.fold_f_ptr,
-                    c.fold_f_idx, c.coh_rec, c.coh_rows, c.K, c.Kf, c.fixed, c.ubar,
+                    c.cut_ke, c.cut_fe, c.cut_kpos, c.cut_fpos, c.fold_K_slot, c.fold_K_ptr, c.fold_f_node,
+                    c.fold_f_ptr, c.coh_rec, c.coh_rows, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
                     c.minvf, c.scal, c.iflags};
     for (void* p : ptrs)
@@ -176,29 +176,18 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
         if ((rc = dev_upload(&c.cut_coh_qp0, qp0))) return rc;
         if ((rc = dev_upload(&c.cut_slot_ptr, sp))) return rc;
         if ((rc = dev_upload(&c.cut_slot, sl))) return rc;
-        // where each cut element's quadrature rows go (4 + 2 NL doubles per point)
+        // where each cut element's quadrature rows go (4 + 2 NL doubles per point, point-major)
         std::vector<long long> roff(nc + 1, 0);
         for (int k = 0; k < kCutClasses; ++k)
             for (int oi = c.cut_class_off[k]; oi < c.cut_class_off[k + 1]; ++oi)
                 roff[oi + 1] = roff[oi] + (long long)device_point_count(tmpl[oi]) * (4 + 2 * kCutClassNl[k]);
         std::vector<int> pts;
         build_cut_points(nodes, tmpl, chm, roff, c.cut_class_off, pts);
-        c.n_cut_pts = (int)(pts.size() / kCutPointInts);
+        c.n_cut_pts = (int)(pts.size() / kCutPointInts) - 1;  // the last record is the sentinel
         if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pts, pts)) ||
             (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
             return rc;
-        // deterministic assembly: pair buffers and the fold lists
-        std::vector<long long> k_slot;
-        std::vector<int> k_ptr, k_idx, f_node, f_ptr, f_idx;
-        build_fold_lists(c.n_reg, nodes, sp, sl, k_slot, k_ptr, k_idx, f_node, f_ptr, f_idx);
-        c.n_fold_K = (int)k_slot.size();
-        c.n_fold_f = (int)f_node.size();
-        if ((rc = dev_alloc(&c.cut_ke, 4 * std::max<size_t>(1, sl.size()))) ||
-            (rc = dev_alloc(&c.cut_fe, 2 * std::max<size_t>(1, sl.size()))) ||
-            (rc = dev_upload(&c.fold_K_slot, k_slot)) || (rc = dev_upload(&c.fold_K_ptr, k_ptr)) ||
-            (rc = dev_upload(&c.fold_K_idx, k_idx)) || (rc = dev_upload(&c.fold_f_node, f_node)) ||
-            (rc = dev_upload(&c.fold_f_ptr, f_ptr)) || (rc = dev_upload(&c.fold_f_idx, f_idx)))
-            return rc;
+        // cohesive Gauss points: the owning element, sub-element and point
         if (hm.n_coh_qp > 0) {
             std::vector<int> rec(hm.n_coh_qp, -1);
             for (int oi = 0; oi < nc; ++oi) {
@@ -211,9 +200,23 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
                     set_error("cohesive Gauss point not owned by any cut element");
                     return PG_ERR_MESH;
                 }
-            if ((rc = dev_upload(&c.coh_rec, rec)) || (rc = dev_alloc(&c.coh_rows, (size_t)kCohRowDoubles * hm.n_coh_qp)))
+            if ((rc = dev_upload(&c.coh_rec, rec)) ||
+                (rc = dev_alloc(&c.coh_rows, (size_t)kCohRowDoubles * hm.n_coh_qp)))
                 return rc;
         }
+        // deterministic assembly: fold order and the pair buffers
+        std::vector<long long> k_slot;
+        std::vector<int> k_ptr, kpos, f_node, f_ptr, fpos;
+        build_fold_lists(c.n_reg, nodes, sp, sl, k_slot, k_ptr, kpos, f_node, f_ptr, fpos);
+        c.n_fold_K = (int)k_slot.size();
+        c.n_fold_f = (int)f_node.size();
+        if ((rc = dev_alloc(&c.cut_ke, 4 * std::max<size_t>(1, sl.size()))) ||
+            (rc = dev_alloc(&c.cut_fe, 2 * std::max<size_t>(1, sl.size()))) ||
+            (rc = dev_upload(&c.cut_kpos, kpos)) || (rc = dev_upload(&c.cut_fpos, fpos)) ||
+
+            (rc = dev_upload(&c.fold_K_slot, k_slot)) || (rc = dev_upload(&c.fold_K_ptr, k_ptr)) ||
+            (rc = dev_upload(&c.fold_f_node, f_node)) || (rc = dev_upload(&c.fold_f_ptr, f_ptr)))
+            return rc;
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;

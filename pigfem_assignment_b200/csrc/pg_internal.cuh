@@ -63,7 +63,6 @@ constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
 bool grid_pattern_ok(const HostMesh& hm);  // block rows laid out as the structured-grid kernel assumes
-int grid_kpad(int nx);  // threads per (grid row, parity) segment of the structured-grid kernel
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // the structured-grid kernel's CTA size, or (meshes without one grid) the
 // row-tile kernel's tile size and persistent grid (CTAs walk the tiles) or
@@ -102,31 +101,31 @@ struct Ctx {
     int* cut_child_mat = nullptr;      // kMaxChildren per element
     int* cut_coh_qp0 = nullptr;        // first cohesive quadrature point (mesh numbering)
     // quadrature rows of the cut elements ({w det, d11, d12, d33, (gx, gy) per
-    // local function} per point, 4 + 2 NL doubles for size class NL), formed by
-    // k_cut_points at every assembly and integrated by k_assemble_cut
+    // local function}, 4 + 2 NL doubles for size class NL, point-major per
+    // element), formed by k_cut_points at every assembly from one record per
+    // point (build_cut_points); per element (class order) its first row's offset
     double* cut_rows = nullptr;
-    long long* cut_row_off = nullptr;  // per element (class order): its first row's offset
-    int* cut_pts = nullptr;            // per point: its record (build_cut_points)
+    long long* cut_row_off = nullptr;
+    int* cut_pts = nullptr;
     int n_cut_pts = 0;
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
-    // deterministic assembly of the cut elements: pair blocks (4 FP64) and
-    // residual terms (2 FP64) at their slot-table positions, the fold lists
-    // (K slot / node -> slot-table positions, sorted by element and pair)
-    // and the cohesive Gauss points' rows
+    // deterministic assembly of the cut elements: pair blocks (4 FP64) in
+    // fold order and residual terms (2 FP64) in node order, each slot-table
+    // entry's positions there, and the runs the folds sum
     double* cut_ke = nullptr;
     double* cut_fe = nullptr;
+    int* cut_kpos = nullptr;
+    int* cut_fpos = nullptr;
     long long* fold_K_slot = nullptr;  // slot << 1 | cut_only
     int* fold_K_ptr = nullptr;
-    int* fold_K_idx = nullptr;
     int n_fold_K = 0;
     int* fold_f_node = nullptr;        // node << 1 | cut_only
     int* fold_f_ptr = nullptr;
-    int* fold_f_idx = nullptr;
     int n_fold_f = 0;
     int* coh_rec = nullptr;            // per cohesive point: class-ordered element << 8 | sub-element << 1 | point
-    double* coh_rows = nullptr;        // per cohesive point: 10 FP64 (k_coh_points)
+    double* coh_rows = nullptr;        // per cohesive point: kCohRowDoubles FP64 (k_coh_points)
     MgHierarchy* mg = nullptr;         // multigrid hierarchy, built at the first multigrid solve
     // system
     double* K = nullptr;               // 4 * n_blocks
@@ -196,7 +195,7 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
 int launch_to_fp32(Ctx& c, cudaStream_t s);
 int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut);
 // shape sensitivity (pg_sens.cu): per-node inclusion / velocity and the cut-kernel passes
-// Arguments of the cut-element kernel (pg_assemble.cu)
+// Arguments of the cut elements' shape-sensitivity kernel (pg_assemble.cu)
 struct CutArgs {
     int n_cut;                      // elements of this launch (one size class)
     int first;                      // its first element in the class-ordered arrays
@@ -204,24 +203,16 @@ struct CutArgs {
     const int* __restrict__ cut_tmpl;
     const int* __restrict__ cut_child_mat;
     const int* __restrict__ cut_coh_qp0;
-    const int* __restrict__ cut_slot_ptr;
-    const int* __restrict__ cut_slot;
     const double* __restrict__ x;
     const double* __restrict__ y;
     const double* __restrict__ u;
     const double* __restrict__ dmat;
     const double* __restrict__ isv_c;
-    double* isv_t;
-    const double* __restrict__ rows;          // quadrature rows from k_cut_points (not SENS)
-    const long long* __restrict__ row_off;
     DevCohLaw coh;
     double dt;
-    double* K;
-    double* f;
-    int want_K, want_f;
-    // shape sensitivity (SENS instances only): the element's enrichment nodes
-    // of its `which`-th inclusion move by sgn * h_rel * r * velocity, and the
-    // element's internal force dotted with wsens goes to sens[inclusion]
+    // the element's enrichment nodes of its `which`-th inclusion move by
+    // sgn * h_rel * r * velocity, and the element's internal force dotted
+    // with wsens goes to sens[inclusion]
     const int* node_inc;
     const double* vel;
     const double* wsens;
@@ -230,12 +221,12 @@ struct CutArgs {
     double h_rel, sgn;
     int which;
 };
-CutArgs cut_args(const Ctx& c, const double* U, double dt, bool want_f, bool want_K);
-// fold lists of the cut elements' deterministic assembly (pg_capi.cu builds
-// them from the class-ordered slot tables)
+CutArgs cut_args(const Ctx& c, const double* U, double dt);
+// fold order of the cut elements' deterministic assembly (pg_capi.cu builds
+// it from the class-ordered slot tables)
 void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
-                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& k_idx,
-                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& f_idx);
+                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& kpos,
+                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& fpos);
 int device_point_count(int tmpl);  // quadrature points of a cut template on the device
 constexpr int kCutPointInts = 16;  // ints per point record of the cut-row kernel
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,

@@ -149,7 +149,7 @@ extern "C" int pg_sensitivity_c11(pg_ctx* cx, const pg_solver_cfg* cfg, double h
     }
     k_sens_weight<<<nb(nd), kThreads, 0, s>>>(nd, c.fixed, d.L, c.dx, d.w);
     cudaMemsetAsync(d.sens, 0, std::max(1, d.n_inc) * sizeof(double), s);
-    CutArgs ca = cut_args(c, c.U, 1.0, false, false);
+    CutArgs ca = cut_args(c, c.U, 1.0);
     ca.node_inc = d.node_inc;
     ca.vel = d.vel;
     ca.wsens = d.w;

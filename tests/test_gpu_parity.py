@@ -123,8 +123,11 @@ def test_gpu_cohesive_residual_and_state_match_reference():
         asm.assemble_nonlinear(dt, True, True)
         f = ctx.vector(1)
         fref = np.concatenate([g[f"step{k}.Pint.f"], g[f"step{k}.Pint.p"]])[ref]
-        # the same function at the same U, summed in another (fixed) order
-        assert np.linalg.norm(f - fref) / np.linalg.norm(fref) <= 1e-12
+        # the same function at the same U, summed in another order: at a
+        # converged state the free entries cancel to ~1e-15 of terms as large
+        # as the stiffness of the smallest cut children times U (1e5 and
+        # more), so rounding alone leaves them at ~1e-12 of ||f||
+        assert np.linalg.norm(f - fref) / np.linalg.norm(fref) <= 1e-10
         np.testing.assert_allclose(ctx.isv(committed=False), g[f"step{k}.isv.delta_max"], rtol=1e-12, atol=0)
         # tangent against the oracle at the same state
         Ko, fo, _ = om.assemble(u=U, dt=dt, isv_c=isv_c, want_K=True, want_f=True)

@@ -590,12 +590,25 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     mine = shard_rves([2 * r.nx * r.ny for r in all_rves], world)[rank]
     rves = [all_rves[i] for i in mine]
     n_rve = len(rves)
-    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:  # mesh builds release the GIL
-        meshes = list(ex.map(pb.Mesh, rves))
+    t_gen = time.perf_counter() - t0
+    # IGFEM preprocessing and sparsity of every RVE on the GPU (pg_mesh_build_device),
+    # from a few host threads so that the builds' launches overlap
+    t1 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        meshes = list(ex.map(lambda r: pb.Mesh(r, device=local), rves))
+    t_mesh = time.perf_counter() - t1
+    t2 = time.perf_counter()
     arr = (C.c_void_p * n_rve)(*[m.handle.value for m in meshes])
     h = C.c_void_p()
     _lib.check(_lib.lib.pg_batch_create(arr, n_rve, local, C.byref(h)), "pg_batch_create")
+    t_batch = time.perf_counter() - t2
     setup_s = time.perf_counter() - t0
+    # the host builder on the same RVEs (all host threads), for comparison only
+    t3 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:  # mesh builds release the GIL
+        host_meshes = list(ex.map(pb.Mesh, rves))
+    t_host_mesh = time.perf_counter() - t3
+    del host_meshes
     ctx = _lib.lib.pg_batch_context(h)
     n_elem = sum(m.info["n_elements"] for m in meshes)
     n_dof = sum(m.info["n_dof"] for m in meshes)
@@ -615,7 +628,11 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     tot_elem = sum_over_ranks(n_elem, device=dev)
     out = {"rves": int(sum_over_ranks(n_rve, device=dev)), "elements": int(tot_elem),
            "dof": int(sum_over_ranks(n_dof, device=dev)), "ranks": world,
-           "host_setup_s": max_over_ranks(setup_s, device=dev), "assembly_ms": t_asm,
+           "host_setup_s": max_over_ranks(setup_s, device=dev),
+           "setup_split_s": {"rve_generation": t_gen, "mesh_build_gpu": t_mesh, "batch_create": t_batch,
+                             "mesh_build_host_for_comparison": t_host_mesh,
+                             "host_threads_for_comparison": min(32, os.cpu_count() or 1)},
+           "assembly_ms": t_asm,
            "elements_per_s": tot_elem / (t_asm / 1e3)}
     for name, prec in (("solve_fp64_mg", _lib.PG_PRECISION_FP64), ("solve_mixed_mg", _lib.PG_PRECISION_MIXED)):
         cfg = _lib.SolverCfg()

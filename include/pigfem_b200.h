@@ -86,6 +86,18 @@ typedef struct pg_mesh_info {
 
 /* ---- host preprocessing (Problem::init IGFEM steps + Problem::setup DOFs/sparsity) ---- */
 int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out);
+/* The same preprocessing on the GPU `device` (Mesh::analyze_nodes/detect_node,
+ * src/Mesh.cpp:2676-2714,2838-2918; Tri3::detection, src/tri3.cpp:287-541;
+ * Mesh::add_enrichments, src/Mesh.cpp:3038-3202; DofObject::distribute_dofs,
+ * src/DofObject.cpp:241-386; Solver::preallocate_matrix, src/Solver.cpp:365-441):
+ * node detection, cut templates, enrichment nodes in the reference's (edge,
+ * inclusion) set order, edge-circle roots, DOF numbering and the block-CSR
+ * pattern with its slot tables, one thread per node, element, edge or row.
+ * The resulting mesh is bit for bit the one pg_mesh_build makes (the same
+ * FP64 operations, each rounded on its own); nodes on an interface are moved
+ * by the host in node order, as the reference moves them.  A grid edge cut by
+ * two different inclusions returns PG_ERR_MESH (pg_mesh_build handles it). */
+int pg_mesh_build_device(const pg_rve_desc* rve, int32_t device, pg_mesh** out);
 int pg_mesh_info_get(const pg_mesh* m, pg_mesh_info* info);
 /* Copies out host arrays (any pointer may be NULL):
  *   xy[2*n_nodes] node coordinates (x, y interleaved; regular then enrichment nodes)

@@ -114,6 +114,7 @@ def _load() -> C.CDLL:
     v = C.c_void_p
     sig = {
         "pg_mesh_build": ([C.POINTER(RveDesc), C.POINTER(v)], C.c_int),
+        "pg_mesh_build_device": ([C.POINTER(RveDesc), C.c_int32, C.POINTER(v)], C.c_int),
         "pg_mesh_info_get": ([v, C.POINTER(MeshInfo)], C.c_int),
         "pg_mesh_export": ([v, _dp, _ip, _ip, _ip, _ip, _u8p, _dp], C.c_int),
         "pg_mesh_export_cut": ([v, _ip, _ip, _ip, _ip, _ip], C.c_int),
@@ -182,7 +183,7 @@ lib = _load()
 
 # every extern "C" symbol include/pigfem_b200.h declares
 DECLARED_SYMBOLS = (
-    "pg_mesh_build", "pg_mesh_info_get", "pg_mesh_export", "pg_mesh_export_cut", "pg_mesh_export_pattern",
+    "pg_mesh_build", "pg_mesh_build_device", "pg_mesh_info_get", "pg_mesh_export", "pg_mesh_export_cut", "pg_mesh_export_pattern",
     "pg_template_table", "pg_mesh_destroy", "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_sync",
     "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
     "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",

@@ -15,7 +15,11 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpigfem_b200.so")
 
-SOURCES = ["igfem_host.cpp", "pg_assemble.cu", "pg_solve.cu", "pg_newton.cu", "pg_mlp.cu", "pg_predict.cu", "pg_capi.cu", "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu", "pg_sens.cu"]
+SOURCES = ["igfem_host.cpp", "pg_assemble.cu", "pg_solve.cu", "pg_newton.cu", "pg_mlp.cu", "pg_predict.cu", "pg_capi.cu",
+           "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu", "pg_sens.cu", "pg_mesh_gpu.cu"]
+# per-source extra flags: the device mesh builder must round every FP64
+# operation on its own, as the host builder does (no FMA contraction)
+EXTRA_FLAGS = {"pg_mesh_gpu.cu": ["-fmad=false"]}
 HEADERS = ["igfem_host.h", "pg_internal.cuh", "pg_solve_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -47,7 +51,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     procs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc()] + ARCH + common + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc()] + ARCH + common + EXTRA_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if verbose else []
         if verbose:

@@ -259,26 +259,22 @@ using namespace pgb;
         cudaSetDevice((c)->c.device);                     \
     } while (0)
 
-extern "C" {
+namespace pgb {
 
-const char* pg_last_error(void) { return last_error_cstr(); }
-const char* pg_version(void) { return "pigfem_b200 0.1 (sm_100a)"; }
-
-int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
-    if (!rve || !out) { set_error("pg_mesh_build: null argument"); return PG_ERR_ARG; }
-    *out = nullptr;
-    RveSpec spec;
+// pg_rve_desc -> RveSpec with the argument checks both mesh builders share
+int rve_spec_from_desc(const pg_rve_desc* rve, RveSpec& spec, const char* who) {
+    const std::string w(who);
     spec.nx = rve->nx;
     spec.ny = rve->ny;
     spec.x0 = rve->x0;
     spec.x1 = rve->x1;
     spec.y0 = rve->y0;
     spec.y1 = rve->y1;
-    if (rve->n_materials <= 0 || !rve->mat_E || !rve->mat_nu) { set_error("pg_mesh_build: no materials"); return PG_ERR_ARG; }
+    if (rve->n_materials <= 0 || !rve->mat_E || !rve->mat_nu) { set_error(w + ": no materials"); return PG_ERR_ARG; }
     for (int m = 0; m < rve->n_materials; ++m) spec.materials.push_back({rve->mat_E[m], rve->mat_nu[m]});
     spec.matrix_mat = rve->matrix_mat;
     if (rve->n_inclusions < 0 || (rve->n_inclusions > 0 && (!rve->inc_cx || !rve->inc_cy || !rve->inc_r || !rve->inc_mat))) {
-        set_error("pg_mesh_build: inclusion arrays missing");
+        set_error(w + ": inclusion arrays missing");
         return PG_ERR_ARG;
     }
     for (int i = 0; i < rve->n_inclusions; ++i)
@@ -288,14 +284,30 @@ int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
     spec.coh.law = rve->coh_law;
     for (int k = 0; k < 5; ++k) spec.coh.p[k] = rve->coh_params[k];
     if (spec.cohesive && spec.coh.law == PG_COH_BILINEAR && !(spec.coh.p[4] >= 0.0)) {
-        set_error("pg_mesh_build: the bilinear law's viscosity must be >= 0");
+        set_error(w + ": the bilinear law's viscosity must be >= 0");
         return PG_ERR_ARG;
     }
     if (spec.cohesive && spec.coh.law != PG_COH_OP && spec.coh.law != PG_COH_BILINEAR) {
-        set_error("pg_mesh_build: unknown cohesive law");
+        set_error(w + ": unknown cohesive law");
         return PG_ERR_ARG;
     }
     spec.strain = rve->strain;
+    return PG_OK;
+}
+
+}  // namespace pgb
+
+extern "C" {
+
+const char* pg_last_error(void) { return last_error_cstr(); }
+const char* pg_version(void) { return "pigfem_b200 0.1 (sm_100a)"; }
+
+int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
+    if (!rve || !out) { set_error("pg_mesh_build: null argument"); return PG_ERR_ARG; }
+    *out = nullptr;
+    RveSpec spec;
+    int rc = rve_spec_from_desc(rve, spec, "pg_mesh_build");
+    if (rc != PG_OK) return rc;
     pg_mesh* m = new (std::nothrow) pg_mesh;
     if (!m) { set_error("pg_mesh_build: out of host memory"); return PG_ERR_ARG; }
     std::string err;
@@ -308,6 +320,34 @@ int pg_mesh_build(const pg_rve_desc* rve, pg_mesh** out) {
         delete m;
         set_error("pg_mesh_build: " + err);
         return PG_ERR_MESH;
+    }
+    *out = m;
+    return PG_OK;
+}
+
+int pg_mesh_build_device(const pg_rve_desc* rve, int32_t device, pg_mesh** out) {
+    if (!rve || !out) { set_error("pg_mesh_build_device: null argument"); return PG_ERR_ARG; }
+    *out = nullptr;
+    RveSpec spec;
+    int rc = rve_spec_from_desc(rve, spec, "pg_mesh_build_device");
+    if (rc != PG_OK) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("pg_mesh_build_device: no CUDA device (this library has no CPU fallback)");
+        return PG_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) { set_error("pg_mesh_build_device: invalid device"); return PG_ERR_ARG; }
+    pg_mesh* m = new (std::nothrow) pg_mesh;
+    if (!m) { set_error("pg_mesh_build_device: out of host memory"); return PG_ERR_ARG; }
+    try {
+        rc = build_mesh_device(spec, device, m->m);
+    } catch (const std::exception& ex) {
+        set_error(std::string("pg_mesh_build_device: host exception: ") + ex.what());
+        rc = PG_ERR_MESH;
+    }
+    if (rc != PG_OK) {
+        delete m;
+        return rc;
     }
     *out = m;
     return PG_OK;

@@ -184,6 +184,10 @@ struct Ctx {
 
 // error plumbing
 void set_error(const std::string& s);
+// pg_rve_desc -> RveSpec with the argument checks of the mesh builders (pg_capi.cu)
+int rve_spec_from_desc(const pg_rve_desc* rve, RveSpec& spec, const char* who);
+// IGFEM preprocessing and sparsity on the GPU, the same HostMesh as build_mesh (pg_mesh_gpu.cu)
+int build_mesh_device(const RveSpec& spec, int device, HostMesh& out);
 // device context of a host mesh (pg_capi.cu)
 int ctx_create(const HostMesh& hm, int device, Ctx& c);
 void free_ctx(Ctx& c);

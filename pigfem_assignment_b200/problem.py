@@ -28,11 +28,13 @@ from .rve import RVE
 
 
 class Mesh:
-    """Host IGFEM mesh: Mesh::generate_mesh + the IGFEM steps of
-    Problem::init (node/element detection, enrichment) + DOF numbering and
-    sparsity (Problem::setup)."""
+    """IGFEM mesh: Mesh::generate_mesh + the IGFEM steps of Problem::init
+    (node/element detection, enrichment) + DOF numbering and sparsity
+    (Problem::setup).  Built on the host (pg_mesh_build) or, with
+    device=<GPU index>, on that GPU (pg_mesh_build_device): the same mesh bit
+    for bit."""
 
-    def __init__(self, rve: RVE):
+    def __init__(self, rve: RVE, device: Optional[int] = None):
         self.rve = rve
         self._keep = []
         inc = rve.inclusions
@@ -57,7 +59,10 @@ class Mesh:
             d.coh_params[k] = v
         d.strain = rve.strain
         h = C.c_void_p()
-        check(lib.pg_mesh_build(C.byref(d), C.byref(h)), "pg_mesh_build")
+        if device is None:
+            check(lib.pg_mesh_build(C.byref(d), C.byref(h)), "pg_mesh_build")
+        else:
+            check(lib.pg_mesh_build_device(C.byref(d), int(device), C.byref(h)), "pg_mesh_build_device")
         self.handle = h
         info = _lib.MeshInfo()
         check(lib.pg_mesh_info_get(h, C.byref(info)))

@@ -603,6 +603,8 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     _lib.check(_lib.lib.pg_batch_create(arr, n_rve, local, C.byref(h)), "pg_batch_create")
     t_batch = time.perf_counter() - t2
     setup_s = time.perf_counter() - t0
+    phases = (C.c_double * 7)()
+    _lib.check(_lib.lib.pg_batch_setup_times(h, phases))
     # the host builder on the same RVEs (all host threads), for comparison only
     t3 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:  # mesh builds release the GIL
@@ -630,6 +632,9 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
            "dof": int(sum_over_ranks(n_dof, device=dev)), "ranks": world,
            "host_setup_s": max_over_ranks(setup_s, device=dev),
            "setup_split_s": {"rve_generation": t_gen, "mesh_build_gpu": t_mesh, "batch_create": t_batch,
+                             "batch_create_phases": dict(zip(("copy_meshes", "merge", "ctx_uploads", "ctx_grid_tiles",
+                                                              "ctx_cut_tables", "ctx_fold_order_gpu", "multigrid"),
+                                                             [round(v, 4) for v in phases])),
                              "mesh_build_host_for_comparison": t_host_mesh,
                              "host_threads_for_comparison": min(32, os.cpu_count() or 1)},
            "assembly_ms": t_asm,

@@ -302,6 +302,7 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
             m.y[i + j * (nx + 1)] = spec.y0 + j * hy;
         }
     m.n_elem = 2 * nx * ny;
+    m.grids.push_back({nx, ny, 0, 0, m.n_reg});
     m.conn.resize(3 * (size_t)m.n_elem);
     {
         size_t e = 0;

@@ -114,6 +114,13 @@ struct HostMesh {
     // cohesive quadrature points (2 per cohesive sub-element)
     int n_coh_qp = 0;
     std::vector<int> cut_coh_qp0;          // first cohesive qp index of each cut element
+    // the structured background grids the mesh is made of: one for a mesh
+    // built here, one per RVE in a merged batch (its regular nodes and
+    // elements from the offsets on, its enrichment nodes after them)
+    struct GridBlock {
+        int nx, ny, node_off, elem_off, n_reg;
+    };
+    std::vector<GridBlock> grids;
 
     int n_nodes() const { return n_reg + n_enr; }
     int n_dof() const { return 2 * n_nodes(); }

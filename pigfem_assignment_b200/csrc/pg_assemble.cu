@@ -716,8 +716,8 @@ __device__ __forceinline__ double4 load_block(const double* K, long long q) {
 }
 
 struct GridArgs {
-    int nx, ny;
-    int tiles_x;                        // tiles across the grid
+    const int4* __restrict__ tiles;     // per CTA: grid block, I0, J0
+    const int4* __restrict__ rves;      // per grid block: nx, ny, first node, first element
     const int* __restrict__ row_ptr;
     const int* __restrict__ emat;       // per element: material, -1 for cut elements
     const double* __restrict__ x;
@@ -835,7 +835,7 @@ __device__ __forceinline__ void grid_store(double* K, int q0, unsigned mask, con
 // TR node rows (2 or 4, picked by the autotuner), one thread per node; warp
 // 2 r + q takes the nodes of parity q in tile row r (every other column).
 // Staged window: the tile's nodes with a one-node halo, the cells around them.
-constexpr int kGridTileC = 64;
+constexpr int kGridTileC = kGridTileCols;
 constexpr int kGridWinX = kGridTileC + 2;   // staged node columns
 constexpr int kGridCellX = kGridTileC + 1;  // staged cell columns
 
@@ -856,11 +856,11 @@ __device__ __forceinline__ void grid_load_cell(GridCell& C, double2 (&U)[4], con
 }
 
 template <int Q, bool WK, bool WF>
-__device__ __forceinline__ void grid_node(const GridArgs& a, int gi, int gj, int lx, int ly, const double2* sXY,
-                                          const double2* sU, const int2* sM) {
-    const int node = gi + gj * (a.nx + 1);
+__device__ __forceinline__ void grid_node(const GridArgs& a, const int4 B, int gi, int gj, int lx, int ly,
+                                          const double2* sXY, const double2* sU, const int2* sM) {
+    const int node = B.z + gi + gj * (B.x + 1);
     const int q0 = WK ? __ldg(&a.row_ptr[node]) : 0;
-    const unsigned mask = grid_nbr_mask(gi, gj, a.nx, a.ny);
+    const unsigned mask = grid_nbr_mask(gi, gj, B.x, B.y);
     double acc[9][4];
 #pragma unroll
     for (int d = 0; d < 9; ++d) acc[d][0] = acc[d][1] = acc[d][2] = acc[d][3] = 0.0;
@@ -907,13 +907,15 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs
     __shared__ double2 sXY[kGridWinX * kGridWinY];
     __shared__ double2 sU[WF ? kGridWinX * kGridWinY : 1];
     __shared__ int2 sM[kGridCellX * kGridCellY];
-    const int nx = a.nx, ny = a.ny, NX1 = nx + 1;
-    const int I0 = (blockIdx.x % a.tiles_x) * kGridTileC, J0 = (blockIdx.x / a.tiles_x) * TR;
+    const int4 T = __ldg(&a.tiles[blockIdx.x]);
+    const int4 B = __ldg(&a.rves[T.x]);  // this tile's grid block: nx, ny, first node, first element
+    const int nx = B.x, ny = B.y, NX1 = nx + 1;
+    const int I0 = T.y, J0 = T.z;
     for (int i = threadIdx.x; i < kGridWinX * kGridWinY; i += kGridThreads) {
         const int gi = I0 - 1 + i % kGridWinX, gj = J0 - 1 + i / kGridWinX;
         double2 v = make_double2(0.0, 0.0), uv = make_double2(0.0, 0.0);
         if (gi >= 0 && gi <= nx && gj >= 0 && gj <= ny) {
-            const size_t n = gi + (size_t)gj * NX1;
+            const size_t n = (size_t)B.z + gi + (size_t)gj * NX1;
             v = make_double2(__ldg(&a.x[n]), __ldg(&a.y[n]));
             if (WF) uv = make_double2(__ldg(&a.u[2 * n]), __ldg(&a.u[2 * n + 1]));
         }
@@ -923,7 +925,7 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs
     for (int i = threadIdx.x; i < kGridCellX * kGridCellY; i += kGridThreads) {
         const int ci = I0 - 1 + i % kGridCellX, cj = J0 - 1 + i / kGridCellX;
         sM[i] = (ci >= 0 && ci < nx && cj >= 0 && cj < ny)
-                    ? __ldg(reinterpret_cast<const int2*>(a.emat) + (ci + (size_t)cj * nx))
+                    ? __ldg(reinterpret_cast<const int2*>(a.emat) + ((size_t)B.w / 2 + ci + (size_t)cj * nx))
                     : make_int2(-1, -1);
     }
     __syncthreads();
@@ -933,38 +935,45 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs
     const int gi = I0 + 2 * lane + ((gj + q) & 1);
     if (gj > ny || gi > nx) return;  // no barrier follows
     const int lx = gi - I0 + 1, ly = r + 1;
-    if (q == 0) grid_node<0, WK, WF>(a, gi, gj, lx, ly, sXY, sU, sM);
-    else grid_node<1, WK, WF>(a, gi, gj, lx, ly, sXY, sU, sM);
+    if (q == 0) grid_node<0, WK, WF>(a, B, gi, gj, lx, ly, sXY, sU, sM);
+    else grid_node<1, WK, WF>(a, B, gi, gj, lx, ly, sXY, sU, sM);
 }
 
 // True when every regular row of the block pattern is laid out as
 // k_grid_rows assumes: the node's grid neighbours (grid_nbr_mask) and
 // itself in ascending order, then only enrichment columns.
 bool grid_pattern_ok(const HostMesh& hm) {
-    const int nx = hm.spec.nx, ny = hm.spec.ny;
-    if ((long long)(nx + 1) * (ny + 1) != hm.n_reg) return false;
-    for (int gj = 0; gj <= ny; ++gj)
-        for (int gi = 0; gi <= nx; ++gi) {
-            const int i = gi + gj * (nx + 1);
-            const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
-            int q = hm.row_ptr[i];
-            for (int d = 0; d < 9; ++d) {
-                if (!(mask & (1u << d))) continue;
-                const int j = (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
-                if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
-                ++q;
+    for (const auto& gb : hm.grids) {
+        const int nx = gb.nx, ny = gb.ny, no = gb.node_off;
+        if ((long long)(nx + 1) * (ny + 1) != gb.n_reg || gb.elem_off % 2) return false;
+        for (int gj = 0; gj <= ny; ++gj)
+            for (int gi = 0; gi <= nx; ++gi) {
+                const int i = no + gi + gj * (nx + 1);
+                const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+                int q = hm.row_ptr[i];
+                for (int d = 0; d < 9; ++d) {
+                    if (!(mask & (1u << d))) continue;
+                    const int j = no + (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
+                    if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
+                    ++q;
+                }
+                // then only this block's enrichment nodes
+                for (; q < hm.row_ptr[i + 1]; ++q)
+                    if (hm.col[q] < no + gb.n_reg) return false;
             }
-            for (; q < hm.row_ptr[i + 1]; ++q)
-                if (hm.col[q] < hm.n_reg) return false;
+        // the block's elements are its grid cells in order
+        for (int e = 0; e < 2 * nx * ny; e += 2 * nx) {
+            const int ge = gb.elem_off + e;
+            const int cj = e / (2 * nx);
+            if (hm.conn[3 * (size_t)ge] != no + cj * (nx + 1)) return false;
         }
-    return true;
+    }
+    return !hm.grids.empty();
 }
 
 void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
     GridArgs ga;
-    ga.nx = c.hm.spec.nx;
-    ga.ny = c.hm.spec.ny;
-    ga.tiles_x = (ga.nx + 1 + kGridTileC - 1) / kGridTileC;
+    ga.rves = c.grid_rves;
     ga.row_ptr = c.row_ptr;
     ga.emat = c.grid_emat;
     ga.x = c.x;
@@ -974,7 +983,9 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.K = c.K;
     ga.f = c.F;
     const int tr = c.tuning.grid_block == 128 ? 2 : 4;  // threads per CTA = 64 x node rows per tile
-    const int blocks = ga.tiles_x * ((ga.ny + 1 + tr - 1) / tr);
+    ga.tiles = c.grid_tiles[tr == 2 ? 0 : 1];
+    const int blocks = c.n_grid_tiles[tr == 2 ? 0 : 1];
+    if (blocks == 0) return;
     if (tr == 2) {
         if (want_K && want_f) k_grid_rows<true, true, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
         else if (want_K) k_grid_rows<true, false, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
@@ -1514,54 +1525,6 @@ CutArgs cut_args(const Ctx& c, const double* U, double dt) {
     return ca;
 }
 
-// Fold order from the class-ordered slot tables (sp: per element its first
-// slot-table entry, sl: K slot of every pair, -1 none; nodes: kCutNodeStride
-// local nodes per element).  K: the pairs sorted by (slot, entry); kpos
-// gives each entry its position (-1 without a slot); every touched slot is
-// one run [k_ptr[j], k_ptr[j + 1]), flagged cut_only when its row or column
-// node is an enrichment node (no triangle-kernel value to add to).  f: the
-// pairs sorted by (node a, entry); fpos and runs likewise, cut_only for
-// enrichment nodes.
-void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
-                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& kpos,
-                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& fpos) {
-    const int nc = (int)sp.size() - 1;
-    std::vector<std::pair<long long, int>> ke, fe;  // (key, slot-table entry)
-    ke.reserve(sl.size());
-    fe.reserve(sl.size());
-    for (int oi = 0; oi < nc; ++oi) {
-        const int np = sp[oi + 1] - sp[oi];
-        int nl = 0;
-        while (nl * nl < np) ++nl;
-        for (int p = 0; p < np; ++p) {
-            const int idx = sp[oi] + p, a = p / nl, b = p % nl;
-            const int na = nodes[(size_t)kCutNodeStride * oi + a], nb = nodes[(size_t)kCutNodeStride * oi + b];
-            const bool cut_only = na >= n_reg || nb >= n_reg;
-            if (sl[idx] >= 0) ke.emplace_back(((long long)sl[idx] << 1) | (cut_only ? 1 : 0), idx);
-            fe.emplace_back(((long long)na << 1) | (na >= n_reg ? 1 : 0), idx);
-        }
-    }
-    auto runs = [&](std::vector<std::pair<long long, int>>& v, std::vector<long long>& keys, std::vector<int>& ptr,
-                    std::vector<int>& pos) {
-        std::sort(v.begin(), v.end());
-        keys.clear();
-        ptr.clear();
-        pos.assign(sl.size(), -1);
-        for (size_t i = 0; i < v.size(); ++i) {
-            if (i == 0 || v[i].first != v[i - 1].first) {
-                keys.push_back(v[i].first);
-                ptr.push_back((int)i);
-            }
-            pos[v[i].second] = (int)i;
-        }
-        ptr.push_back((int)v.size());
-    };
-    runs(ke, k_slot, k_ptr, kpos);
-    std::vector<long long> fk;
-    runs(fe, fk, f_ptr, fpos);
-    f_node.assign(fk.begin(), fk.end());
-}
-
 void launch_cut_points(const Ctx& c, cudaStream_t s) {
     if (c.n_cut_pts > 0)
         k_cut_points<<<(c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, 0, s>>>(
@@ -1638,6 +1601,10 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     // writes the enrichment rows and columns whole.  Nothing needs clearing
     // first.  All on one stream: the triangle kernel fills every SM until its
     // last wave, so a second stream bought no overlap (measured).
+    if (!(c.tuning.tri_grid && c.grid_emat)) {
+        const int rc = ensure_tri_map(c);
+        if (rc != PG_OK) return rc;
+    }
     const RowArgs ra = row_args(c, U, want_f, want_K);
     if (c.timing) cudaEventRecord(c.ea0, s);
     launch_tri(c, ra, want_f, s);
@@ -1689,6 +1656,8 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     AsmTuning best = c.tuning;
     float best_tri = 1e30f, best_cut = 1e30f;
     int idx = 0;
+    const int trc = ensure_tri_map(c);
+    if (trc != PG_OK) return trc;
     c.tuning.tri_grid = 0;
     for (int v = 0; v < kTriTileVariants; ++v)
         for (int p = 0; p < 2; ++p, ++idx) {

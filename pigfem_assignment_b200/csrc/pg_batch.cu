@@ -616,6 +616,9 @@ int b_upload(std::vector<void*>& owned, T** p, const std::vector<T>& v) {
 
 struct pg_batch {
     int n_rve = 0;
+    // host seconds of the set-up: mesh copies, merge, context (uploads, grid
+    // tiles, cut tables, fold order), multigrid hierarchy
+    double setup_s[7] = {0, 0, 0, 0, 0, 0, 0};
     std::vector<pgb::HostMesh> meshes;
     std::vector<int> noff;              // first node of each RVE (+ total)
     std::vector<int> eoff;              // first element of each RVE (+ total)
@@ -699,6 +702,7 @@ void merge_meshes(const std::vector<HostMesh>& ms, HostMesh& out, std::vector<in
         for (int v : m.ne_list) out.ne_list.push_back((((v >> 2) + eo) << 2) | (v & 3));
         for (int v : m.cut_slot) out.cut_slot.push_back(v >= 0 ? v + bo : -1);
         out.n_free += m.n_free;
+        for (const auto& gb : m.grids) out.grids.push_back({gb.nx, gb.ny, gb.node_off + no, gb.elem_off + eo, gb.n_reg});
     }
     out.x.resize(out.n_reg);
     out.y.resize(out.n_reg);
@@ -970,11 +974,21 @@ int pg_batch_create(const pg_mesh* const* meshes, int32_t n_rve, int32_t device,
     pg_batch* B = new (std::nothrow) pg_batch;
     if (!B) { set_error("pg_batch_create: out of host memory"); return PG_ERR_ARG; }
     B->n_rve = n_rve;
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    auto t0 = now();
     for (int r = 0; r < n_rve; ++r) B->meshes.push_back(meshes[r]->m);
+    auto t1 = now();
     HostMesh merged;
     merge_meshes(B->meshes, merged, B->noff, B->eoff);
-    int rc = ctx_create(merged, device, B->ctx.c);
+    auto t2 = now();
+    int rc = ctx_create(std::move(merged), device, B->ctx.c);
+    auto t3 = now();
     if (rc == PG_OK) rc = batch_mg_build(*B);
+    B->setup_s[0] = secs(t0, t1);
+    B->setup_s[1] = secs(t1, t2);
+    for (int k = 0; k < 4; ++k) B->setup_s[2 + k] = B->ctx.c.setup_s[k];
+    B->setup_s[6] = secs(t3, now());
     if (rc != PG_OK) {
         pg_batch_destroy(B);
         return rc;
@@ -992,6 +1006,12 @@ void pg_batch_destroy(pg_batch* B) {
 }
 
 pg_ctx* pg_batch_context(pg_batch* B) { return B ? &B->ctx : nullptr; }
+
+int pg_batch_setup_times(const pg_batch* B, double* seconds) {
+    if (!B || !seconds) { set_error("pg_batch_setup_times: null argument"); return PG_ERR_ARG; }
+    for (int k = 0; k < 7; ++k) seconds[k] = B->setup_s[k];
+    return PG_OK;
+}
 
 int pg_batch_info(const pg_batch* B, int32_t* node_offset, int32_t* element_offset, int32_t* depth) {
     if (!B) { set_error("pg_batch_info: null batch"); return PG_ERR_ARG; }

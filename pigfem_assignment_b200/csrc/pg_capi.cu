@@ -1,6 +1,7 @@
 // extern "C" entry points of libpigfem_b200 (declared in include/pigfem_b200.h).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,6 +60,7 @@ void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
+                    c.grid_rves, c.grid_tiles[0], c.grid_tiles[1],
                     c.cut_ke, c.cut_fe, c.cut_kpos, c.cut_fpos, c.fold_K_slot, c.fold_K_ptr, c.fold_f_node,
                     c.fold_f_ptr, c.coh_rec, c.coh_rows, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
@@ -77,12 +79,23 @@ void free_ctx(Ctx& c) {
 
 void set_error(const std::string& s) { g_last_error = s; }
 
+int ensure_tri_map(Ctx& c) {
+    for (int v = 0; v < kTriTileVariants; ++v) {
+        if (c.tri_map[v]) continue;
+        std::vector<int> tm;
+        build_tri_map(c.hm, kTriTileSizes[v], tm);
+        const int rc = dev_upload(&c.tri_map[v], tm);
+        if (rc) return rc;
+    }
+    return PG_OK;
+}
+
 int cuda_fail(cudaError_t e, const char* where) {
     g_last_error = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
     return PG_ERR_CUDA;
 }
 
-int ctx_create(const HostMesh& hm, int device, Ctx& c) {
+int ctx_create(HostMesh mesh, int device, Ctx& c) {
     c.device = device;
     PG_CUDA(cudaSetDevice(device));
     upload_tables();
@@ -95,7 +108,8 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     PG_CUDA(cudaEventCreate(&c.ea0));
     PG_CUDA(cudaEventCreate(&c.ea1));
     PG_CUDA(cudaEventCreate(&c.ea2));
-    c.hm = hm;
+    c.hm = std::move(mesh);
+    const HostMesh& hm = c.hm;
     c.n_nodes = hm.n_nodes();
     c.n_reg = hm.n_reg;
     c.n_elem = hm.n_elem;
@@ -106,6 +120,9 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     c.coh.law = hm.spec.coh.law;
     for (int k = 0; k < 5; ++k) c.coh.p[k] = hm.spec.coh.p[k];
 
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    auto t_phase = now();
     int rc;
     if ((rc = dev_upload(&c.x, hm.x))) return rc;
     if ((rc = dev_upload(&c.y, hm.y))) return rc;
@@ -118,20 +135,47 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
     if ((rc = dev_upload(&c.diag, hm.diag_slot))) return rc;
     if ((rc = dev_upload(&c.ne_ptr, hm.ne_ptr))) return rc;
     if ((rc = dev_upload(&c.ne_list, hm.ne_list))) return rc;
-    for (int v = 0; v < kTriTileVariants; ++v) {
-        std::vector<int> tm;
-        build_tri_map(hm, kTriTileSizes[v], tm);
-        if ((rc = dev_upload(&c.tri_map[v], tm))) return rc;
-    }
-    if (hm.spec.nx > 0 && hm.spec.ny > 0 && hm.n_elem == 2 * hm.spec.nx * hm.spec.ny &&
-        grid_pattern_ok(hm)) {
-        // one structured background grid: the edge-centric sweep kernel applies
+    c.setup_s[0] = secs(t_phase, now());
+    t_phase = now();
+    // (the row-tile kernel's block maps are built on its first use: ensure_tri_map)
+    long long grid_elems = 0;
+    for (const auto& gb : hm.grids) grid_elems += 2LL * gb.nx * gb.ny;
+    if (!hm.grids.empty() && grid_elems == hm.n_elem && grid_pattern_ok(hm)) {
+        // structured background grids (one per RVE of a batch): the grid kernel
+        // applies, through a tile table per tile height over all of them
         std::vector<int> em(hm.n_elem);
         for (int e = 0; e < hm.n_elem; ++e) em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e];
         if ((rc = dev_upload(&c.grid_emat, em))) return rc;
+        std::vector<int4> rves;
+        for (const auto& gb : hm.grids) rves.push_back(make_int4(gb.nx, gb.ny, gb.node_off, gb.elem_off));
+        if ((rc = dev_upload(&c.grid_rves, rves))) return rc;
+        for (int h = 0; h < 2; ++h) {
+            const int tr = h == 0 ? 2 : 4;
+            std::vector<int4> tiles;
+            for (int r = 0; r < (int)hm.grids.size(); ++r) {
+                const auto& gb = hm.grids[r];
+                for (int J0 = 0; J0 <= gb.ny; J0 += tr)
+                    for (int I0 = 0; I0 <= gb.nx; I0 += kGridTileCols) tiles.push_back(make_int4(r, I0, J0, 0));
+            }
+            c.n_grid_tiles[h] = (int)tiles.size();
+            if ((rc = dev_upload(&c.grid_tiles[h], tiles))) return rc;
+        }
     } else {
         c.tuning.tri_grid = 0;
     }
+    // enrichment nodes: those beyond the regular nodes of their grid block (a
+    // mesh without blocks: beyond n_reg)
+    std::vector<uint8_t> node_enr(hm.n_nodes(), 0);
+    if (hm.grids.empty()) {
+        for (int n = hm.n_reg; n < hm.n_nodes(); ++n) node_enr[n] = 1;
+    } else {
+        for (size_t r = 0; r < hm.grids.size(); ++r) {
+            const int end = r + 1 < hm.grids.size() ? hm.grids[r + 1].node_off : hm.n_nodes();
+            for (int n = hm.grids[r].node_off + hm.grids[r].n_reg; n < end; ++n) node_enr[n] = 1;
+        }
+    }
+    c.setup_s[1] = secs(t_phase, now());
+    t_phase = now();
     std::vector<double> dm(3 * hm.spec.materials.size());
     for (size_t m = 0; m < hm.spec.materials.size(); ++m) dmat_coeffs(hm.spec.materials[m], hm.spec.plane_strain, &dm[3 * m]);
     if ((rc = dev_upload(&c.dmat, dm))) return rc;
@@ -204,19 +248,14 @@ int ctx_create(const HostMesh& hm, int device, Ctx& c) {
                 (rc = dev_alloc(&c.coh_rows, (size_t)kCohRowDoubles * hm.n_coh_qp)))
                 return rc;
         }
-        // deterministic assembly: fold order and the pair buffers
-        std::vector<long long> k_slot;
-        std::vector<int> k_ptr, kpos, f_node, f_ptr, fpos;
-        build_fold_lists(c.n_reg, nodes, sp, sl, k_slot, k_ptr, kpos, f_node, f_ptr, fpos);
-        c.n_fold_K = (int)k_slot.size();
-        c.n_fold_f = (int)f_node.size();
+        c.setup_s[2] = secs(t_phase, now());
+        t_phase = now();
+        // deterministic assembly: the pair buffers and the fold order (built on the GPU)
         if ((rc = dev_alloc(&c.cut_ke, 4 * std::max<size_t>(1, sl.size()))) ||
-            (rc = dev_alloc(&c.cut_fe, 2 * std::max<size_t>(1, sl.size()))) ||
-            (rc = dev_upload(&c.cut_kpos, kpos)) || (rc = dev_upload(&c.cut_fpos, fpos)) ||
-
-            (rc = dev_upload(&c.fold_K_slot, k_slot)) || (rc = dev_upload(&c.fold_K_ptr, k_ptr)) ||
-            (rc = dev_upload(&c.fold_f_node, f_node)) || (rc = dev_upload(&c.fold_f_ptr, f_ptr)))
+            (rc = dev_alloc(&c.cut_fe, 2 * std::max<size_t>(1, sl.size()))))
             return rc;
+        if ((rc = build_fold_device(c, node_enr, (int)sl.size()))) return rc;
+        c.setup_s[3] = secs(t_phase, now());
     }
     const size_t nb = (size_t)c.n_blocks, nd = (size_t)c.n_dof, nn = (size_t)c.n_nodes;
     if ((rc = dev_alloc(&c.K, 4 * nb))) return rc;

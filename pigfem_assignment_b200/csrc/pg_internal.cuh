@@ -63,6 +63,7 @@ constexpr int kTriMapDiag = 1 << 28;
 constexpr int kTriMapSlow = 1 << 29;
 void build_tri_map(const HostMesh& hm, int tile_nodes, std::vector<int>& map);
 bool grid_pattern_ok(const HostMesh& hm);  // block rows laid out as the structured-grid kernel assumes
+constexpr int kGridTileCols = 64;          // node columns per structured-grid tile
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // the structured-grid kernel's CTA size, or (meshes without one grid) the
 // row-tile kernel's tile size and persistent grid (CTAs walk the tiles) or
@@ -94,6 +95,9 @@ struct Ctx {
     AsmTuning tuning;
     int* grid_emat = nullptr;          // structured meshes: material per element, -1 for cut elements
                                        // (set only where the structured-grid kernel applies)
+    int4* grid_rves = nullptr;         // per grid block: nx, ny, first node, first element
+    int4* grid_tiles[2] = {};          // per tile of 2 / 4 node rows: grid block, I0, J0
+    int n_grid_tiles[2] = {0, 0};
     double* dmat = nullptr;            // 3 per material: D11, D12, D33
     // cut elements, grouped by size class (kCutClassNl), in that order
     int* cut_nodes = nullptr;          // kCutNodeStride per element: 3 parent nodes, then enrichment slots, -1 unused
@@ -180,6 +184,9 @@ struct Ctx {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool timing = false;
+    // host seconds of the set-up phases of ctx_create: uploads of the mesh,
+    // grid tiles, cut-element tables and point records, fold order
+    double setup_s[4] = {0, 0, 0, 0};
 };
 
 // error plumbing
@@ -189,7 +196,8 @@ int rve_spec_from_desc(const pg_rve_desc* rve, RveSpec& spec, const char* who);
 // IGFEM preprocessing and sparsity on the GPU, the same HostMesh as build_mesh (pg_mesh_gpu.cu)
 int build_mesh_device(const RveSpec& spec, int device, HostMesh& out);
 // device context of a host mesh (pg_capi.cu)
-int ctx_create(const HostMesh& hm, int device, Ctx& c);
+int ctx_create(HostMesh hm, int device, Ctx& c);  // the context keeps the mesh (move it in)
+int ensure_tri_map(Ctx& c);  // the row-tile kernel's block maps, built on first use
 void free_ctx(Ctx& c);
 int cuda_fail(cudaError_t e, const char* where);
 
@@ -226,11 +234,9 @@ struct CutArgs {
     int which;
 };
 CutArgs cut_args(const Ctx& c, const double* U, double dt);
-// fold order of the cut elements' deterministic assembly (pg_capi.cu builds
-// it from the class-ordered slot tables)
-void build_fold_lists(int n_reg, const std::vector<int>& nodes, const std::vector<int>& sp, const std::vector<int>& sl,
-                      std::vector<long long>& k_slot, std::vector<int>& k_ptr, std::vector<int>& kpos,
-                      std::vector<int>& f_node, std::vector<int>& f_ptr, std::vector<int>& fpos);
+// fold order of the cut elements' deterministic assembly, built on the GPU
+// from the context's class-ordered cut tables (pg_mesh_gpu.cu)
+int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entries);
 int device_point_count(int tmpl);  // quadrature points of a cut template on the device
 constexpr int kCutPointInts = 16;  // ints per point record of the cut-row kernel
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,

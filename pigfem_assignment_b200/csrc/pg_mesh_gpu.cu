@@ -706,12 +706,89 @@ cudaError_t download(std::vector<T>& h, const T* d, size_t n, cudaStream_t s) {
     return cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s);
 }
 
+
+// ---------------------------------------------------------------------------
+// Fold order of the cut elements' pair blocks (pg_assemble.cu), built on the
+// GPU by a counting sort: every slot-table entry (class-ordered element oi,
+// pair p = a nl + b) counts itself into its K slot and into its row node a;
+// exclusive scans give every slot's and node's run; the entries scatter into
+// their runs; each run is then put in entry order, so the result is the
+// order (key, entry) a sort would give, the same on every run.
+// ---------------------------------------------------------------------------
+__global__ void k_fold_count(int nc, const int* __restrict__ sp, const int* __restrict__ sl,
+                             const int* __restrict__ nodes, const uint8_t* __restrict__ node_enr, int* cntK,
+                             uint8_t* cutK, int* cntF) {
+    const int oi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (oi >= nc) return;
+    const int s0 = sp[oi], np = sp[oi + 1] - s0;
+    int nl = 0;
+    while (nl * nl < np) ++nl;
+    for (int p = 0; p < np; ++p) {
+        const int a = p / nl, b = p - a * nl;
+        const int na = nodes[(size_t)kCutNodeStride * oi + a], nb = nodes[(size_t)kCutNodeStride * oi + b];
+        const int slot = sl[s0 + p];
+        if (slot >= 0) {
+            atomicAdd(&cntK[slot], 1);
+            if (node_enr[na] || node_enr[nb]) cutK[slot] = 1;
+        }
+        atomicAdd(&cntF[na], 1);
+    }
+}
+
+// runs: a key i is touched when start[i + 1] > start[i]; touched_idx holds
+// the scan of those flags (its run number)
+__global__ void k_fold_touched(long long n, const int* __restrict__ start, int* touched) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) touched[i] = start[i + 1] > start[i] ? 1 : 0;
+}
+
+template <typename KeyT>
+__global__ void k_fold_runs(long long n, const int* __restrict__ start, const int* __restrict__ run_of,
+                            const uint8_t* __restrict__ cut_only, KeyT* run_key, int* run_ptr) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || start[i + 1] == start[i]) return;
+    const int r = run_of[i];
+    run_key[r] = (KeyT)((KeyT)i << 1) | (KeyT)(cut_only[i] ? 1 : 0);
+    run_ptr[r] = start[i];
+}
+
+__global__ void k_fold_scatter(int nc, const int* __restrict__ sp, const int* __restrict__ sl,
+                               const int* __restrict__ nodes, const int* __restrict__ startK, int* fillK, int* tmpK,
+                               const int* __restrict__ startF, int* fillF, int* tmpF) {
+    const int oi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (oi >= nc) return;
+    const int s0 = sp[oi], np = sp[oi + 1] - s0;
+    int nl = 0;
+    while (nl * nl < np) ++nl;
+    for (int p = 0; p < np; ++p) {
+        const int a = p / nl;
+        const int na = nodes[(size_t)kCutNodeStride * oi + a];
+        const int slot = sl[s0 + p];
+        if (slot >= 0) tmpK[startK[slot] + atomicAdd(&fillK[slot], 1)] = s0 + p;
+        tmpF[startF[na] + atomicAdd(&fillF[na], 1)] = s0 + p;
+    }
+}
+
+// one thread per run: its entries in entry order, and each entry's position
+__global__ void k_fold_order(int nruns, const int* __restrict__ run_ptr, int* tmp, int* pos) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const int i0 = run_ptr[r], i1 = run_ptr[r + 1];
+    for (int i = i0 + 1; i < i1; ++i) {
+        const int x = tmp[i];
+        int j = i - 1;
+        while (j >= i0 && tmp[j] > x) { tmp[j + 1] = tmp[j]; --j; }
+        tmp[j + 1] = x;
+    }
+    for (int i = i0; i < i1; ++i) pos[tmp[i]] = i;
+}
+
 }  // namespace
 
 #define MESH_CUDA(call)                                                          \
     do {                                                                         \
         const cudaError_t _e = (call);                                           \
-        if (_e != cudaSuccess) return cuda_fail(_e, "pg_mesh_build_device: " #call); \
+        if (_e != cudaSuccess) return cuda_fail(_e, "device mesh set-up: " #call); \
     } while (0)
 
 int build_mesh_device(const RveSpec& spec, int device, HostMesh& m) {
@@ -754,6 +831,7 @@ int build_mesh_device(const RveSpec& spec, int device, HostMesh& m) {
     const int ninc = (int)spec.inclusions.size();
     m.n_reg = n_reg;
     m.n_elem = n_elem;
+    m.grids.push_back({nx, ny, 0, 0, n_reg});
 
     // ---- nodes and their detection ----
     std::vector<DevInclusion> hinc(ninc);
@@ -937,6 +1015,70 @@ int build_mesh_device(const RveSpec& spec, int device, HostMesh& m) {
     MESH_CUDA(download(m.cut_slot, cut_slot, (size_t)SS * n_cut, s));
     MESH_CUDA(download(m.cut_coh_qp0, coh_count, n_cut, s));
     MESH_CUDA(cudaStreamSynchronize(s));
+    return PG_OK;
+}
+
+}  // namespace pgb
+
+namespace pgb {
+
+// Device arrays of the fold order (Ctx: cut_kpos, cut_fpos, fold_K_slot /
+// fold_K_ptr, fold_f_node / fold_f_ptr) from the context's class-ordered
+// cut_nodes, cut_slot_ptr and cut_slot; node_enr flags the enrichment nodes.
+int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entries) {
+    cudaStream_t s = c.stream;
+    DevScratch S;
+    const int nc = c.n_cut;
+    const long long nbk = c.n_blocks, nn = c.n_nodes;
+    uint8_t *enr, *cutK, *cutF;
+    int *cntK, *cntF, *fillK, *fillF, *tmpK, *tmpF, *runK, *runF;
+    MESH_CUDA(S.alloc(&enr, nn));
+    MESH_CUDA(S.alloc(&cutK, nbk));
+    MESH_CUDA(S.alloc(&cutF, nn));
+    MESH_CUDA(S.alloc(&cntK, nbk + 1));
+    MESH_CUDA(S.alloc(&cntF, nn + 1));
+    MESH_CUDA(S.alloc(&fillK, nbk));
+    MESH_CUDA(S.alloc(&fillF, nn));
+    MESH_CUDA(S.alloc(&tmpK, n_entries));
+    MESH_CUDA(S.alloc(&tmpF, n_entries));
+    MESH_CUDA(S.alloc(&runK, nbk));
+    MESH_CUDA(S.alloc(&runF, nn));
+    MESH_CUDA(cudaMemcpyAsync(enr, node_enr.data(), nn, cudaMemcpyHostToDevice, s));
+    MESH_CUDA(cudaMemsetAsync(cutK, 0, nbk, s));
+    MESH_CUDA(cudaMemcpyAsync(cutF, enr, nn, cudaMemcpyDeviceToDevice, s));
+    MESH_CUDA(cudaMemsetAsync(cntK, 0, (nbk + 1) * sizeof(int), s));
+    MESH_CUDA(cudaMemsetAsync(cntF, 0, (nn + 1) * sizeof(int), s));
+    MESH_CUDA(cudaMemsetAsync(fillK, 0, nbk * sizeof(int), s));
+    MESH_CUDA(cudaMemsetAsync(fillF, 0, nn * sizeof(int), s));
+    k_fold_count<<<nb_mesh(nc), kThreadsMesh, 0, s>>>(nc, c.cut_slot_ptr, c.cut_slot, c.cut_nodes, enr, cntK, cutK,
+                                                      cntF);
+    int totK = 0, totF = 0, nrunK = 0, nrunF = 0;
+    MESH_CUDA(exclusive_scan(S, cntK, nbk + 1, totK, s));
+    MESH_CUDA(exclusive_scan(S, cntF, nn + 1, totF, s));
+    k_fold_touched<<<nb_mesh(nbk), kThreadsMesh, 0, s>>>(nbk, cntK, runK);
+    k_fold_touched<<<nb_mesh(nn), kThreadsMesh, 0, s>>>(nn, cntF, runF);
+    MESH_CUDA(exclusive_scan(S, runK, nbk, nrunK, s));
+    MESH_CUDA(exclusive_scan(S, runF, nn, nrunF, s));
+    c.n_fold_K = nrunK;
+    c.n_fold_f = nrunF;
+    MESH_CUDA(cudaMalloc((void**)&c.fold_K_slot, std::max(1, nrunK) * sizeof(long long)));
+    MESH_CUDA(cudaMalloc((void**)&c.fold_K_ptr, (nrunK + 1) * sizeof(int)));
+    MESH_CUDA(cudaMalloc((void**)&c.fold_f_node, std::max(1, nrunF) * sizeof(int)));
+    MESH_CUDA(cudaMalloc((void**)&c.fold_f_ptr, (nrunF + 1) * sizeof(int)));
+    MESH_CUDA(cudaMalloc((void**)&c.cut_kpos, std::max(1, n_entries) * sizeof(int)));
+    MESH_CUDA(cudaMalloc((void**)&c.cut_fpos, std::max(1, n_entries) * sizeof(int)));
+    MESH_CUDA(cudaMemsetAsync(c.cut_kpos, 0xff, std::max(1, n_entries) * sizeof(int), s));
+    MESH_CUDA(cudaMemsetAsync(c.cut_fpos, 0xff, std::max(1, n_entries) * sizeof(int), s));
+    k_fold_runs<long long><<<nb_mesh(nbk), kThreadsMesh, 0, s>>>(nbk, cntK, runK, cutK, c.fold_K_slot, c.fold_K_ptr);
+    k_fold_runs<int><<<nb_mesh(nn), kThreadsMesh, 0, s>>>(nn, cntF, runF, cutF, c.fold_f_node, c.fold_f_ptr);
+    MESH_CUDA(cudaMemcpyAsync(c.fold_K_ptr + nrunK, &totK, sizeof(int), cudaMemcpyHostToDevice, s));
+    MESH_CUDA(cudaMemcpyAsync(c.fold_f_ptr + nrunF, &totF, sizeof(int), cudaMemcpyHostToDevice, s));
+    k_fold_scatter<<<nb_mesh(nc), kThreadsMesh, 0, s>>>(nc, c.cut_slot_ptr, c.cut_slot, c.cut_nodes, cntK, fillK,
+                                                        tmpK, cntF, fillF, tmpF);
+    k_fold_order<<<nb_mesh(nrunK), kThreadsMesh, 0, s>>>(nrunK, c.fold_K_ptr, tmpK, c.cut_kpos);
+    k_fold_order<<<nb_mesh(nrunF), kThreadsMesh, 0, s>>>(nrunF, c.fold_f_ptr, tmpF, c.cut_fpos);
+    MESH_CUDA(cudaStreamSynchronize(s));
+    MESH_CUDA(cudaGetLastError());
     return PG_OK;
 }
 

@@ -138,6 +138,36 @@ int pg_assemble_linear_host(pg_ctx* c, const double* xy_host, double* k_host);
  * step dt, writing trial cohesive state.  The trial state restarts from the committed
  * state on every call, as InternalVars::copy_data does (Assembler.cpp:235). */
 int pg_assemble_nonlinear(pg_ctx* c, const double* U_dev, double dt, int32_t want_f, int32_t want_K, void* stream);
+/* Problem::compute_stress_strain (Problem.cpp:428-534) at every volumetric quadrature point,
+ * element by element in the reference's point order (uncut: the 4 points of the Tri3 rule;
+ * cut: each integration child's points in template order), at the displacement U_dev
+ * (device pointer; NULL: the context's solution).  Outputs (each nullable):
+ *   points_host[7*n_points]  per point: strain xx, yy, xy (engineering shear), stress xx, yy, xy
+ *                            (plane strain, D eps), J W.  A point of zero weight (a collapsed
+ *                            integration child) has NaN strain and stress, as in the reference.
+ *   n_points                 the number of volumetric points
+ *   elem_point_off[n_elem+1] first point of each element
+ *   mean[7]                  J W-weighted volume averages of strain (3) and stress (3), then the
+ *                            total J W (the homogenised response; zero-weight points skipped),
+ *                            reduced on the device in a fixed order (bit-reproducible).
+ * With points_host and mean both NULL only the counts and offsets are returned. */
+int pg_stress_strain(pg_ctx* c, const double* U_dev, double* points_host, int64_t* n_points,
+                     int32_t* elem_point_off, double* mean);
+/* Writer_ASCII_VTK::write (Writer_ASCII_VTK.cpp, Writer_VTK.cpp:164-336, 639-911): the legacy
+ * ASCII VTK file of the context's state at time t -- nodes (regular, then enrichment), cells
+ * (uncut elements; integration children in place of cut ones), displacement and external
+ * force per node (enrichment nodes: parent-edge interpolation plus their own value), and per
+ * cell the reference's material number, partition 0, the means of strain and stress over its
+ * quadrature points and the von Mises stress.  External force: zero on free DOFs, the
+ * reaction on prescribed ones -- K U, formed here, for a linear mesh (this overwrites the
+ * context's internal-force vector); for a cohesive mesh the internal force of the last
+ * residual assembly (the Newton driver leaves the accepted state of its last load step). */
+int pg_write_vtk(pg_ctx* c, const char* path, double t);
+/* WriterCohesiveOpenings::write (WriterCohesiveOpenings.cpp:39-197): one CSV line per
+ * cohesive sub-element, "inclusion,theta,delta_t/delta_c,delta_n/delta_c" at its midpoint,
+ * sorted, at precision 16 (delta_c: the Ortiz-Pandolfi law's; 2 G_c / sigma_c for the
+ * bilinear law).  PG_ERR_ARG on a mesh without a cohesive interface. */
+int pg_write_cohesive_openings(pg_ctx* c, const char* path);
 /* Assembler::assemble_new_load_step: prescribed values = t_frac * ubar. */
 int pg_new_load_step(pg_ctx* c, double t_frac);
 /* InternalVars::copy_data_in: committed cohesive state <- trial state. */

@@ -53,6 +53,8 @@
 #include "InternalVars.h"
 #include "Options.h"
 #include "Utilities.h"
+#include "Writer_ASCII_VTK.h"
+#include "WriterCohesiveOpenings.h"
 #undef private
 #undef protected
 
@@ -73,6 +75,7 @@ struct Config {
     int assemble_repeats = 0;   // >0: time assemble_linear this many times (linear only)
     int dump_K = 1;
     double snes_rtol = 0.0, snes_stol = -1.0;  // > 0 / >= 0: the shim's SNES defaults (PETSc: 1e-8, 1e-8)
+    std::string vtk_out, openings_out;  // non-empty: write the reference's VTK file / cohesive openings CSV there
 };
 
 Config read_config(const char* path) {
@@ -108,6 +111,8 @@ Config read_config(const char* path) {
         else if (k == "dump_K") ss >> c.dump_K;
         else if (k == "snes_rtol") ss >> c.snes_rtol;
         else if (k == "snes_stol") ss >> c.snes_stol;
+        else if (k == "vtk_out") ss >> c.vtk_out;
+        else if (k == "openings_out") ss >> c.openings_out;
         else { fprintf(stderr, "unknown config key %s\n", k.c_str()); exit(2); }
     }
     return c;
@@ -281,7 +286,19 @@ int main(int argc, char** argv) {
         }
         o.d1("time.assemble_repeat_total", t_asm_rep);
         o.d("time.assemble_each", each);
-        o.d1("time.init", t_init);
+        // the reference's writers on the final state (Writer_ASCII_VTK as
+    // Problem::init builds it, Problem.cpp:246-249; WriterCohesiveOpenings)
+    if (!cfg.vtk_out.empty()) {
+        Writer_ASCII_VTK w(problem);
+        w.store_mesh();
+        w.write(cfg.vtk_out, cfg.T_final);
+    }
+    if (!cfg.openings_out.empty() && cohesive) {
+        WriterCohesiveOpenings w(problem);
+        w.store_mesh();
+        w.write(cfg.openings_out, cfg.T_final);
+    }
+    o.d1("time.init", t_init);
         o.i1("time.assemble_repeats", cfg.assemble_repeats);
         o.i1("mesh.n_elem_active", (int32_t)mesh.n_local_active_elem());
         fclose(fp);
@@ -389,6 +406,27 @@ int main(int argc, char** argv) {
     dump_vec(o, "U.p", solver->_U.p);
     dump_vec(o, "F.f", solver->_F_ext.f);
     dump_vec(o, "F.p", solver->_F_ext.p);
+    if (!cohesive) {
+        // Problem::compute_stress_strain at every volumetric quadrature point
+        // (Problem.cpp:428-534), element by element, with the point's J W
+        std::vector<int32_t> qp_count;
+        std::vector<double> qp_strain, qp_stress, qp_jw;
+        for (id_type e = 0; e < mesh.n_local_elem(); ++e) {
+            Elem* el = mesh.get_elem_local(e);
+            std::vector<std::vector<double>> strain, stress;
+            problem->compute_stress_strain(strain, stress, el);
+            qp_count.push_back((int32_t)strain.size());
+            for (size_t q = 0; q < strain.size(); ++q) {
+                for (int k = 0; k < 3; ++k) qp_strain.push_back(strain[q][k]);
+                for (int k = 0; k < 3; ++k) qp_stress.push_back(stress[q][k]);
+                qp_jw.push_back(mesh.get_J(e, q) * mesh.get_W(e, q));
+            }
+        }
+        o.i("qp.count", qp_count);
+        o.d("qp.strain", qp_strain);
+        o.d("qp.stress", qp_stress);
+        o.d("qp.jw", qp_jw);
+    }
     if (cohesive) {
         SolverNonlinear* sn = dynamic_cast<SolverNonlinear*>(solver);
         dump_vec(o, "Pint.f", sn->_P_int.f);
@@ -408,6 +446,18 @@ int main(int argc, char** argv) {
         o.i("isv.qp", isv_qp);
         o.d("isv.delta_max", isv_val);
         o.i1("snes.iterations", (int32_t)(pgshim_snes_iterations() - snes0));
+    }
+    // the reference's writers on the final state (Writer_ASCII_VTK as
+    // Problem::init builds it, Problem.cpp:246-249; WriterCohesiveOpenings)
+    if (!cfg.vtk_out.empty()) {
+        Writer_ASCII_VTK w(problem);
+        w.store_mesh();
+        w.write(cfg.vtk_out, cfg.T_final);
+    }
+    if (!cfg.openings_out.empty() && cohesive) {
+        WriterCohesiveOpenings w(problem);
+        w.store_mesh();
+        w.write(cfg.openings_out, cfg.T_final);
     }
     o.d1("time.init", t_init);
     o.d1("time.assemble", problem->_assemble_time);

@@ -61,15 +61,26 @@ def run(cfg: dict, timeout: float = 600.0) -> dict:
     cfg keys: nx, ny, x0, x1, y0, y1, E_matrix, nu_matrix, plane_strain,
     strain, problem ('linear'|'cohesive'), inclusions [(cx, cy, r, E, nu)],
     coh_sigma, coh_delta, coh_beta, coh_visc, T_final, max_dt, min_dt,
-    max_iter, assemble_repeats, dump_K.
+    max_iter, assemble_repeats, dump_K, snes_rtol, snes_stol; write_vtk and
+    write_openings (True: the reference's Writer_ASCII_VTK file and
+    WriterCohesiveOpenings CSV of the final state come back as the bytes of
+    records "vtk.text" and "openings.text").
     """
     if not driver_available():
         raise FileNotFoundError(f"reference driver not built: {DRIVER}")
+    cfg = dict(cfg)
+    want_vtk = bool(cfg.pop("write_vtk", False))
+    want_open = bool(cfg.pop("write_openings", False))
     with tempfile.TemporaryDirectory() as td:
         cfg_path = os.path.join(td, "cfg.txt")
         out_path = os.path.join(td, "out.bin")
         # The reference puts its output folder under ./Output (Options.cpp:208-238).
         os.makedirs(os.path.join(td, "Output"))
+        texts = {}
+        if want_vtk:
+            texts["vtk.text"] = cfg["vtk_out"] = os.path.join(td, "final.vtk")
+        if want_open:
+            texts["openings.text"] = cfg["openings_out"] = os.path.join(td, "openings.csv")
         write_config(cfg_path, cfg)
         proc = subprocess.run([DRIVER, cfg_path, out_path, "Output/run"], cwd=td,
                               capture_output=True, text=True, timeout=timeout)
@@ -77,6 +88,9 @@ def run(cfg: dict, timeout: float = 600.0) -> dict:
             raise RuntimeError(f"reference driver failed rc={proc.returncode}\n"
                                f"{proc.stdout[-3000:]}\n{proc.stderr[-3000:]}")
         rec = read_records(out_path)
+        for key, path in texts.items():
+            with open(path, "rb") as f:
+                rec[key] = np.frombuffer(f.read(), dtype=np.uint8).copy()
         rec["_stdout"] = proc.stdout
         return rec
 

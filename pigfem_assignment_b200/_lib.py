@@ -128,6 +128,9 @@ def _load() -> C.CDLL:
         "pg_assemble_linear_host": ([v, _dp, _dp], C.c_int),
         "pg_assemble_nonlinear": ([v, _dp, C.c_double, C.c_int32, C.c_int32, v], C.c_int),
         "pg_new_load_step": ([v, C.c_double], C.c_int),
+        "pg_stress_strain": ([v, _dp, _dp, C.POINTER(C.c_int64), _ip, _dp], C.c_int),
+        "pg_write_vtk": ([v, C.c_char_p, C.c_double], C.c_int),
+        "pg_write_cohesive_openings": ([v, C.c_char_p], C.c_int),
         "pg_commit_isv": ([v], C.c_int),
         "pg_ctx_device_arrays": ([v, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp),
                                   C.POINTER(_dp)], C.c_int),
@@ -186,7 +189,7 @@ lib = _load()
 DECLARED_SYMBOLS = (
     "pg_mesh_build", "pg_mesh_build_device", "pg_mesh_info_get", "pg_mesh_export", "pg_mesh_export_cut", "pg_mesh_export_pattern",
     "pg_template_table", "pg_mesh_destroy", "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_sync",
-    "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_new_load_step",
+    "pg_assemble_linear", "pg_assemble_linear_host", "pg_assemble_nonlinear", "pg_stress_strain", "pg_write_vtk", "pg_write_cohesive_openings", "pg_new_load_step",
     "pg_commit_isv", "pg_ctx_device_arrays", "pg_solver_cfg_default", "pg_solve_linear", "pg_get_matrix",
     "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
     "pg_solve_nonlinear", "pg_mlp_create", "pg_mlp_destroy", "pg_mlp_param_count", "pg_mlp_params",

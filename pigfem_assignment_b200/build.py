@@ -16,7 +16,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpigfem_b200.so")
 
 SOURCES = ["igfem_host.cpp", "pg_assemble.cu", "pg_solve.cu", "pg_newton.cu", "pg_mlp.cu", "pg_predict.cu", "pg_capi.cu",
-           "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu", "pg_sens.cu", "pg_mesh_gpu.cu"]
+           "pg_noalloc.cu", "pg_mg.cu", "pg_batch.cu", "pg_sens.cu", "pg_mesh_gpu.cu", "pg_writer.cu"]
 # per-source extra flags: the device mesh builder must round every FP64
 # operation on its own, as the host builder does (no FMA contraction)
 EXTRA_FLAGS = {"pg_mesh_gpu.cu": ["-fmad=false"]}

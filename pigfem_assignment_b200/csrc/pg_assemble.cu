@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "pg_internal.cuh"
 
@@ -1713,6 +1714,213 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     cudaEventDestroy(e1);
     cudaFree(flush);
     PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stress and strain recovery (Problem::compute_stress_strain,
+// src/Problem.cpp:428-534) and the homogenised response
+// ---------------------------------------------------------------------------
+// At every volumetric quadrature point, element by element in the
+// reference's point order: strain = B u (Voigt, engineering shear), stress
+// = D strain, and the point's J W.  Uncut elements have the four points of
+// the Tri3 rule (their strain is constant); a cut element has its children's
+// points in template order -- a Tri3 child's four points share one strain,
+// which the device forms once from the child's quadrature row.  A point of
+// zero weight (a collapsed child) has no defined gradients: its strain and
+// stress are NaN, as the reference's inverse map leaves them.
+__constant__ double kTri3W[4] = {-0.28125, 0.260416666666666666666666666666665, 0.260416666666666666666666666666665,
+                              0.260416666666666666666666666666665};  // tri3.cpp:107-115
+
+__device__ __forceinline__ void voigt_stress(const double e[3], double d11, double d12, double d33, double s[3]) {
+    s[0] = d11 * e[0] + d12 * e[1];
+    s[1] = d12 * e[0] + d11 * e[1];
+    s[2] = d33 * e[2];
+}
+
+// out: 7 FP64 per point {strain 3, stress 3, J W}
+__global__ void k_stress_uncut(int n_elem, const int4* __restrict__ elem4, const int* __restrict__ elem_cut,
+                               const int* __restrict__ qp_off, const double* __restrict__ x,
+                               const double* __restrict__ y, const double* __restrict__ u,
+                               const double* __restrict__ dmat, double* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_elem || elem_cut[e] >= 0) return;
+    const int4 el = __ldg(&elem4[e]);
+    const int n[3] = {el.x, el.y, el.z};
+    double X[3], Y[3], ux[3], uy[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        X[v] = __ldg(&x[n[v]]);
+        Y[v] = __ldg(&y[n[v]]);
+        ux[v] = __ldg(&u[2 * n[v]]);
+        uy[v] = __ldg(&u[2 * n[v] + 1]);
+    }
+    const double J = (X[1] - X[0]) * (Y[2] - Y[0]) - (X[2] - X[0]) * (Y[1] - Y[0]);
+    const double iJ = 1.0 / J;
+    const double b[3] = {(Y[1] - Y[2]) * iJ, (Y[2] - Y[0]) * iJ, (Y[0] - Y[1]) * iJ};
+    const double c[3] = {(X[2] - X[1]) * iJ, (X[0] - X[2]) * iJ, (X[1] - X[0]) * iJ};
+    double eps[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        eps[0] += b[v] * ux[v];
+        eps[1] += c[v] * uy[v];
+        eps[2] += c[v] * ux[v] + b[v] * uy[v];
+    }
+    double sig[3];
+    voigt_stress(eps, __ldg(&dmat[3 * el.w]), __ldg(&dmat[3 * el.w + 1]), __ldg(&dmat[3 * el.w + 2]), sig);
+    double* o = out + 7 * (size_t)__ldg(&qp_off[e]);
+    for (int q = 0; q < 4; ++q, o += 7) {
+        o[0] = eps[0]; o[1] = eps[1]; o[2] = eps[2];
+        o[3] = sig[0]; o[4] = sig[1]; o[5] = sig[2];
+        o[6] = J * kTri3W[q];
+    }
+}
+
+static_assert(kCutClasses == 4, "c_class_nl lists the classes one by one");
+__constant__ int c_class_nl[kCutClasses] = {kCutClassNl[0], kCutClassNl[1], kCutClassNl[2], kCutClassNl[3]};
+
+// one thread per cut element (class order), from its quadrature rows
+// (k_cut_points, point-major); elem_of: class order -> mesh element
+__global__ void k_stress_cut(int n_cut, const int* __restrict__ class_off, const int* __restrict__ elem_of,
+                             const int* __restrict__ cut_tmpl, const int* __restrict__ cut_nodes,
+                             const long long* __restrict__ row_off, const double* __restrict__ rows,
+                             const double* __restrict__ u, const int* __restrict__ qp_off, double* out) {
+    const int oi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (oi >= n_cut) return;
+    int k = 0;
+    while (k < kCutClasses - 1 && oi >= class_off[k + 1]) ++k;
+    const int W = 4 + 2 * c_class_nl[k];
+    const DevTemplate& T = c_tmpl[cut_tmpl[oi]];
+    const int nl = 3 + T.n_enr;
+    const double* rw = rows + row_off[oi];
+    double* o = out + 7 * (size_t)qp_off[elem_of[oi]];
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int ch = 0; ch < T.n_child; ++ch) {
+        const int type = T.child_type[ch];
+        const int nq_dev = c_quad[type].nq;          // points the device forms
+        const int nq_ref = type == kChildTri3 ? 4 : nq_dev;
+        for (int q = 0; q < nq_dev; ++q, rw += W) {
+            const double wgt = rw[0];
+            double eps[3] = {0.0, 0.0, 0.0}, sig[3];
+            if (wgt != 0.0) {
+                for (int l = 0; l < nl; ++l) {
+                    const int nd = cut_nodes[(size_t)kCutNodeStride * oi + l];
+                    const double gx = rw[4 + 2 * l], gy = rw[5 + 2 * l];
+                    const double ux = u[2 * nd], uy = u[2 * nd + 1];
+                    eps[0] += gx * ux;
+                    eps[1] += gy * uy;
+                    eps[2] += gy * ux + gx * uy;
+                }
+                voigt_stress(eps, rw[1], rw[2], rw[3], sig);
+            } else {
+                eps[0] = eps[1] = eps[2] = sig[0] = sig[1] = sig[2] = nan;
+            }
+            // a Tri3 child's single device point stands for the rule's four
+            const int reps = type == kChildTri3 ? nq_ref : 1;
+            for (int r = 0; r < reps; ++r, o += 7) {
+                o[0] = eps[0]; o[1] = eps[1]; o[2] = eps[2];
+                o[3] = sig[0]; o[4] = sig[1]; o[5] = sig[2];
+                // J W of the point: the Tri3 child's row carries det x the rule's summed weight
+                o[6] = type == kChildTri3 ? wgt / c_quad[kChildTri3].w[0] * kTri3W[r] : wgt;
+            }
+        }
+    }
+}
+
+// per CTA: sums over its points of J W (strain, stress) and J W, skipping
+// points of zero weight; the CTAs' partials are added in order afterwards
+__global__ void __launch_bounds__(256) k_stress_partial(long long n_pts, const double* __restrict__ out,
+                                                        double* partial) {
+    __shared__ double sm[7][256];
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long p = blockIdx.x * 256LL + threadIdx.x; p < n_pts; p += 256LL * gridDim.x) {
+        const double* o = out + 7 * p;
+        const double w = o[6];
+        if (w == 0.0) continue;
+        for (int k = 0; k < 6; ++k) acc[k] += w * o[k];
+        acc[6] += w;
+    }
+    for (int k = 0; k < 7; ++k) sm[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int k = 0; k < 7; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x < 7) partial[7 * (size_t)blockIdx.x + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+// Point offsets and the tables the recovery needs, built on its first call.
+int stress_prepare(Ctx& c) {
+    if (c.qp_off) return PG_OK;
+    const HostMesh& hm = c.hm;
+    std::vector<int> off(hm.n_elem + 1, 0);
+    for (int e = 0; e < hm.n_elem; ++e) {
+        int n = 4;
+        const int ci = hm.elem_cut[e];
+        if (ci >= 0) {
+            const CutTemplate& T = cut_template(hm.cut_tmpl[ci]);
+            n = 0;
+            for (int ch = 0; ch < T.n_child; ++ch) {
+                const int nc = T.child_n[ch];
+                n += child_quadrature(nc == 3 ? kChildTri3 : nc == 4 ? kChildQuad4 : nc == 5 ? kChildPoly5 : kChildPoly6).nq;
+            }
+        }
+        off[e + 1] = off[e] + n;
+    }
+    // class order -> mesh element (the order ctx_create gives the cut arrays)
+    std::vector<int> elem_of;
+    for (int k = 0; k < kCutClasses; ++k) {
+        const int lo = k == 0 ? 0 : kCutClassNl[k - 1];
+        for (int ci = 0; ci < hm.n_cut; ++ci) {
+            const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
+            if (nl > lo && nl <= kCutClassNl[k]) elem_of.push_back(hm.cut_elem[ci]);
+        }
+    }
+    c.n_qp_total = off.back();
+    auto up = [&](auto** dst, const auto& v) -> int {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(*dst)>>;
+        PG_CUDA(cudaMalloc((void**)dst, std::max<size_t>(1, v.size()) * sizeof(T)));
+        if (!v.empty()) PG_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return PG_OK;
+    };
+    int rc;
+    if ((rc = up(&c.qp_off, off)) || (rc = up(&c.qp_elem_cut, hm.elem_cut)) || (rc = up(&c.qp_cut_elem, elem_of)) ||
+        (rc = up(&c.qp_class_off, std::vector<int>(c.cut_class_off, c.cut_class_off + kCutClasses + 1))))
+        return rc;
+    PG_CUDA(cudaMalloc((void**)&c.qp_out, 7 * std::max<size_t>(1, (size_t)c.n_qp_total) * sizeof(double)));
+    return PG_OK;
+}
+
+// Runs the recovery on stream s; mean7 (host, nullable): J W-weighted sums of
+// strain (3) and stress (3) divided by the total J W, then that total.
+int stress_strain(Ctx& c, const double* U, cudaStream_t s, double* mean7) {
+    int rc = stress_prepare(c);
+    if (rc != PG_OK) return rc;
+    k_stress_uncut<<<(c.n_elem + 255) / 256, 256, 0, s>>>(c.n_elem, c.elem4, c.qp_elem_cut, c.qp_off, c.x, c.y, U,
+                                                          c.dmat, c.qp_out);
+    if (c.n_cut > 0) {
+        launch_cut_points(c, s);
+        k_stress_cut<<<(c.n_cut + 127) / 128, 128, 0, s>>>(c.n_cut, c.qp_class_off, c.qp_cut_elem, c.cut_tmpl,
+                                                           c.cut_nodes, c.cut_row_off, c.cut_rows, U, c.qp_off,
+                                                           c.qp_out);
+    }
+    PG_CUDA(cudaGetLastError());
+    if (mean7) {
+        constexpr int kParts = 148 * 4;
+        double* part = nullptr;
+        PG_CUDA(cudaMallocAsync((void**)&part, 7 * kParts * sizeof(double), s));
+        k_stress_partial<<<kParts, 256, 0, s>>>(c.n_qp_total, c.qp_out, part);
+        std::vector<double> hp(7 * kParts);
+        PG_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PG_CUDA(cudaStreamSynchronize(s));
+        cudaFreeAsync(part, s);
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < kParts; ++b)
+            for (int k = 0; k < 7; ++k) acc[k] += hp[7 * b + k];
+        for (int k = 0; k < 6; ++k) mean7[k] = acc[6] != 0.0 ? acc[k] / acc[6] : 0.0;
+        mean7[6] = acc[6];
+    }
     return PG_OK;
 }
 

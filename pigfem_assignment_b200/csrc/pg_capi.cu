@@ -60,7 +60,8 @@ void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
-                    c.grid_rves, c.grid_tiles[0], c.grid_tiles[1],
+                    c.grid_rves, c.grid_tiles[0], c.grid_tiles[1], c.qp_off, c.qp_elem_cut, c.qp_cut_elem,
+                    c.qp_class_off, c.qp_out,
                     c.cut_ke, c.cut_fe, c.cut_kpos, c.cut_fpos, c.fold_K_slot, c.fold_K_ptr, c.fold_f_node,
                     c.fold_f_ptr, c.coh_rec, c.coh_rows, c.K, c.Kf, c.fixed, c.ubar,
                     c.U, c.F, c.isv_c, c.isv_t, c.r, c.z, c.p, c.q, c.dx, c.minv, c.rf, c.zf, c.pf, c.qf, c.xf,
@@ -577,6 +578,48 @@ int pg_assemble_nonlinear(pg_ctx* c, const double* U_dev, double dt, int32_t wan
     const int rc = launch_assemble(x, U, dt, want_f != 0, want_K != 0, s);
     if (rc == PG_OK && want_K) x.assembled = true;
     return rc;
+}
+
+int pg_stress_strain(pg_ctx* c, const double* U_dev, double* points_host, int64_t* n_points, int32_t* elem_point_off,
+                     double* mean) {
+    PG_GUARD_CTX(c);
+    Ctx& x = c->c;
+    int rc = stress_prepare(x);
+    if (rc != PG_OK) return rc;
+    if (n_points) *n_points = x.n_qp_total;
+    if (elem_point_off)
+        PG_CUDA(cudaMemcpy(elem_point_off, x.qp_off, ((size_t)x.n_elem + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (!points_host && !mean) return PG_OK;
+    cudaStream_t s = x.stream;
+    rc = stress_strain(x, U_dev ? U_dev : x.U, s, mean);
+    if (rc != PG_OK) return rc;
+    if (points_host)
+        PG_CUDA(cudaMemcpyAsync(points_host, x.qp_out, 7 * (size_t)x.n_qp_total * sizeof(double),
+                                cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    return PG_OK;
+}
+
+int pg_write_vtk(pg_ctx* c, const char* path, double t) {
+    PG_GUARD_CTX(c);
+    if (!path) { set_error("pg_write_vtk: null path"); return PG_ERR_ARG; }
+    try {
+        return write_vtk(c->c, path, t);
+    } catch (const std::exception& ex) {
+        set_error(std::string("pg_write_vtk: host exception: ") + ex.what());
+        return PG_ERR_ARG;
+    }
+}
+
+int pg_write_cohesive_openings(pg_ctx* c, const char* path) {
+    PG_GUARD_CTX(c);
+    if (!path) { set_error("pg_write_cohesive_openings: null path"); return PG_ERR_ARG; }
+    try {
+        return write_cohesive_openings(c->c, path);
+    } catch (const std::exception& ex) {
+        set_error(std::string("pg_write_cohesive_openings: host exception: ") + ex.what());
+        return PG_ERR_ARG;
+    }
 }
 
 int pg_new_load_step(pg_ctx* c, double t_frac) {

@@ -184,6 +184,15 @@ struct Ctx {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool timing = false;
+    // stress/strain recovery (stress_prepare, on first use): per element its
+    // first volumetric quadrature point, the cut flags, class order -> mesh
+    // element, class offsets, and 7 FP64 per point of output
+    int* qp_off = nullptr;
+    int* qp_elem_cut = nullptr;
+    int* qp_cut_elem = nullptr;
+    int* qp_class_off = nullptr;
+    double* qp_out = nullptr;
+    long long n_qp_total = 0;
     // host seconds of the set-up phases of ctx_create: uploads of the mesh,
     // grid tiles, cut-element tables and point records, fold order
     double setup_s[4] = {0, 0, 0, 0};
@@ -205,6 +214,14 @@ int cuda_fail(cudaError_t e, const char* where);
 void upload_tables();
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s);
 int launch_to_fp32(Ctx& c, cudaStream_t s);
+// Problem::compute_stress_strain at every volumetric point into c.qp_out (7 per point) and,
+// with mean7, the J W-weighted means of strain and stress and the total J W
+int stress_strain(Ctx& c, const double* U, cudaStream_t s, double* mean7);
+// point offsets per element and the recovery's tables (first call builds them)
+int stress_prepare(Ctx& c);
+// the reference's legacy ASCII VTK file and cohesive openings CSV of the context's state
+int write_vtk(Ctx& c, const std::string& path, double t);
+int write_cohesive_openings(Ctx& c, const std::string& path);
 int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut);
 // shape sensitivity (pg_sens.cu): per-node inclusion / velocity and the cut-kernel passes
 // Arguments of the cut elements' shape-sensitivity kernel (pg_assemble.cu)

@@ -151,6 +151,28 @@ class DeviceContext:
         return v[: self.info["n_cohesive_qp"]]
 
 
+def _stress_strain(ctx, U_dev: Optional[int] = None, points: bool = True):
+    """Problem::compute_stress_strain (src/Problem.cpp:428-534) over every
+    element at once, and the homogenised response.  Returns (points, offsets,
+    mean): points[n, 7] = strain xx, yy, xy (engineering), stress xx, yy, xy,
+    J W per volumetric quadrature point in the reference's order (NaN strain
+    and stress at zero-weight points of collapsed children); offsets[e] the
+    first point of element e; mean[7] = the J W-weighted averages of strain
+    and stress and the total J W."""
+    n = C.c_int64()
+    off = np.zeros(ctx.info["n_elements"] + 1, np.int32)
+    check(lib.pg_stress_strain(ctx.handle, None, None, C.byref(n), iptr(off), None), "pg_stress_strain")
+    pts = np.zeros((n.value, 7)) if points else None
+    mean = np.zeros(7)
+    ptr = C.cast(C.c_void_p(U_dev), _lib._dp) if U_dev else None
+    check(lib.pg_stress_strain(ctx.handle, ptr, dptr(pts) if points else None, None, None, dptr(mean)),
+          "pg_stress_strain")
+    return pts, off, mean
+
+
+DeviceContext.compute_stress_strain = _stress_strain
+
+
 def _set_isv(ctx, v, committed=True):
     v = np.ascontiguousarray(v, dtype=np.float64)
     check(lib.pg_set_isv(ctx.handle, 1 if committed else 0, dptr(v)))
@@ -240,6 +262,12 @@ class ProblemLinearElasticity:
     def get_solution(self) -> np.ndarray:
         return self.ctx.vector(0)
 
+    def compute_stress_strain(self, points: bool = True):
+        """Strain and stress at every volumetric quadrature point of the
+        current solution, and their volume averages (see
+        DeviceContext.compute_stress_strain)."""
+        return self.ctx.compute_stress_strain(points=points)
+
 
 class ProblemNonlinearStructural:
     """Problem::init / solve_problem for cohesive RVEs: load stepping with
@@ -289,3 +317,38 @@ class ProblemNonlinearStructural:
 
     def get_solution(self) -> np.ndarray:
         return self.ctx.vector(0)
+
+    def compute_stress_strain(self, points: bool = True):
+        """Strain and stress at every volumetric quadrature point of the
+        current solution, and their volume averages (see
+        DeviceContext.compute_stress_strain)."""
+        return self.ctx.compute_stress_strain(points=points)
+
+
+class Writer_ASCII_VTK:
+    """Writer_ASCII_VTK (src/Writer_ASCII_VTK.cpp, src/Writer_VTK.cpp): the
+    legacy ASCII VTK file of a problem's current state, in the reference's
+    layout and number format."""
+
+    def __init__(self, prob):
+        self.prob = prob
+
+    def store_mesh(self) -> None:
+        """The mesh is fixed once the context exists: nothing to store."""
+
+    def write(self, filename: str, curr_t: float) -> None:
+        check(lib.pg_write_vtk(self.prob.ctx.handle, filename.encode(), float(curr_t)), "pg_write_vtk")
+
+
+class WriterCohesiveOpenings:
+    """WriterCohesiveOpenings (src/WriterCohesiveOpenings.cpp): per cohesive
+    sub-element its inclusion, angle and normalised midpoint opening, as CSV."""
+
+    def __init__(self, prob):
+        self.prob = prob
+
+    def store_mesh(self) -> None:
+        """The mesh is fixed once the context exists: nothing to store."""
+
+    def write(self, filename: str, curr_t: float = 0.0) -> None:
+        check(lib.pg_write_cohesive_openings(self.prob.ctx.handle, filename.encode()), "pg_write_cohesive_openings")

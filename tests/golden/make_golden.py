@@ -18,7 +18,11 @@ Fixtures (numpy .npz):
                       instead of PETSc's default 1e-8, so that the trajectory
                       itself is accurate to well below the parity bounds
 Each holds the reference's enriched mesh, DOF numbering, K_ff/K_fp/K_pf/K_pp
-(linear), the solution, and (cohesive) the internal force and delta_max.
+(linear), the solution, (linear) the strain, stress and J W at every
+volumetric quadrature point (Problem::compute_stress_strain), and (cohesive)
+the internal force and delta_max; and the text of the files the reference's
+writers make of the final state: the legacy VTK file (Writer_ASCII_VTK, all
+fixtures) and the cohesive openings CSV (WriterCohesiveOpenings, cohesive).
 """
 from __future__ import annotations
 
@@ -33,7 +37,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import refio  # noqa: E402
 
-KEEP = ("mesh.", "dof.", "K.", "U.", "F.", "Pint.", "isv.", "snes.")
+KEEP = ("mesh.", "dof.", "K.", "U.", "F.", "Pint.", "isv.", "snes.", "qp.", "vtk.", "openings.")
 
 
 def save(name: str, rec: dict, extra: dict | None = None) -> None:
@@ -48,7 +52,7 @@ def save(name: str, rec: dict, extra: dict | None = None) -> None:
 def main() -> None:
     if not refio.driver_available():
         raise SystemExit("build the reference first: make -f oracle/Makefile.ref -j8")
-    lin = dict(E_matrix=3000.0, nu_matrix=0.35, strain=0.01, problem="linear")
+    lin = dict(E_matrix=3000.0, nu_matrix=0.35, strain=0.01, problem="linear", write_vtk=True)
     r = refio.run(dict(lin, nx=8, ny=8, inclusions=[(0.5, 0.5, 0.25, 70000.0, 0.2)]))
     save("linear_8x8.npz", r, {"cfg.nx": np.array([8]), "cfg.inc": np.array([[0.5, 0.5, 0.25, 70000.0, 0.2]])})
     r = refio.run(dict(lin, nx=64, ny=64, inclusions=[(0.5, 0.5, 0.25, 70000.0, 0.2)]))
@@ -65,7 +69,8 @@ def main() -> None:
     dt = 0.1
     steps = {}
     for k in range(1, 5):
-        rk = refio.run(dict(base, T_final=dt * k, max_dt=dt, strain=0.0025 * k, dump_K=0))
+        rk = refio.run(dict(base, T_final=dt * k, max_dt=dt, strain=0.0025 * k, dump_K=0,
+                            write_vtk=(k == 4), write_openings=(k == 4)))
         for key in ("U.f", "U.p", "Pint.f", "Pint.p", "isv.delta_max"):
             steps[f"step{k}.{key}"] = rk[key]
         steps[f"step{k}.snes.iterations"] = rk["snes.iterations"]

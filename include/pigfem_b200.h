@@ -322,13 +322,26 @@ int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut)
 
 /* ---- shape sensitivity ----
  * SensitivityAdjoint::solveProblem with SensitivityRightLoad (src/SensitivityAdjoint.cpp:23-63,
- * src/SensitivityRightLoad.cpp:32-125) and the shape-parameter kernels
- * (src/SensitivityShapeParameterStructural.cpp:18-230) for the radius of every circle.
- * At the context's current equilibrium U (solve first): C_11 = (sum of the right
- * edge's x reactions / height) / applied strain, and dC_11/dr_i for every
- * inclusion from one adjoint solve (cfg: CG/GMRES, any preconditioner) and a
- * central difference of each cut element's internal force under the move of its
- * enrichment nodes (h = h_rel * r_i).  dc11_dr: n_inclusions values (NULL allowed). */
+ * src/SensitivityRightLoad.cpp:32-125) and the shape parameters of
+ * Problem::addShapeSensitivityParameter (src/Problem.cpp:856-861; Circle_Inclusion's
+ * "X", "Y", "R": src/InclusionCircle.cpp:176-227; the derivative of the element
+ * force: src/SensitivityShapeParameterStructural.cpp:18-230).
+ * At the context's current equilibrium U (solve first): f = the sum of the right
+ * edge's x reactions / height (SensitivityRightLoad::evaluate), and df/dd for each
+ * parameter d = (inclusion[p], kind[p]) from one adjoint solve (cfg: CG/GMRES, any
+ * preconditioner) and the analytic shape derivative of every cut element's internal
+ * force along the parameter's velocity field.  dfdp: n_params values (NULL allowed).
+ * PG_ERR_ARG for an inclusion out of range or an unknown kind. */
+#define PG_SHAPE_X 0   /* centre x */
+#define PG_SHAPE_Y 1   /* centre y */
+#define PG_SHAPE_R 2   /* radius */
+int pg_sensitivity_shape(pg_ctx* c, const pg_solver_cfg* cfg, int32_t n_params, const int32_t* inclusion,
+                         const int32_t* kind, double* f, double* dfdp, pg_solve_stats* adjoint_stats);
+/* C_11 = f / applied strain and dC_11/dr_i for the radius of every inclusion
+ * (dc11_dr: n_inclusions values, NULL allowed).  h_rel = 0: the analytic derivative
+ * (pg_sensitivity_shape); h_rel > 0: a central difference of each cut element's
+ * internal force under moves of its enrichment nodes by +-h_rel r_i along the
+ * velocity (a cross-check of the analytic path, O(h^2) accurate). */
 int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double* c11, double* dc11_dr,
                        pg_solve_stats* adjoint_stats);
 

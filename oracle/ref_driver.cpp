@@ -53,10 +53,16 @@
 #include "InternalVars.h"
 #include "Options.h"
 #include "Utilities.h"
+#include "SensitivityRightLoad.h"
+#include "SensitivitySolver.h"
+#include "SensitivityAdjoint.h"
 #include "Writer_ASCII_VTK.h"
 #include "WriterCohesiveOpenings.h"
 #undef private
 #undef protected
+#ifdef PG_GPU_DROPIN
+#include "integration/solver_gpu.h"
+#endif
 
 namespace {
 
@@ -76,6 +82,8 @@ struct Config {
     int dump_K = 1;
     double snes_rtol = 0.0, snes_stol = -1.0;  // > 0 / >= 0: the shim's SNES defaults (PETSc: 1e-8, 1e-8)
     std::string vtk_out, openings_out;  // non-empty: write the reference's VTK file / cohesive openings CSV there
+    struct SensParam { int inc; std::string name; };
+    std::vector<SensParam> sens;        // shape parameters ("X", "Y", "R") of SensitivityRightLoad
 };
 
 Config read_config(const char* path) {
@@ -112,6 +120,7 @@ Config read_config(const char* path) {
         else if (k == "snes_rtol") ss >> c.snes_rtol;
         else if (k == "snes_stol") ss >> c.snes_stol;
         else if (k == "vtk_out") ss >> c.vtk_out;
+        else if (k == "sens") { Config::SensParam p; ss >> p.inc >> p.name; c.sens.push_back(p); }
         else if (k == "openings_out") ss >> c.openings_out;
         else { fprintf(stderr, "unknown config key %s\n", k.c_str()); exit(2); }
     }
@@ -200,8 +209,51 @@ int main(int argc, char** argv) {
         void* mem = calloc(1, sizeof(ProblemNonlinearStructural));
         problem = new (mem) ProblemNonlinearStructural;
     } else {
+#ifdef PG_GPU_DROPIN
+        // the same Problem with the B200 library's solver below it
+        // (oracle/integration/solver_gpu.h); the description is the one this
+        // driver generates the reference's mesh from
+        static std::vector<double> cx, cy, rr, mE, mnu;
+        static std::vector<int32_t> im;
+        std::map<std::pair<double, double>, int> mat_of;
+        mE.push_back(cfg.E_m);
+        mnu.push_back(cfg.nu_m);
+        for (const auto& ic : cfg.incs) {
+            auto key = std::make_pair(ic.E, ic.nu);
+            if (!mat_of.count(key)) {
+                mat_of[key] = (int)mE.size();
+                mE.push_back(ic.E);
+                mnu.push_back(ic.nu);
+            }
+            cx.push_back(ic.cx);
+            cy.push_back(ic.cy);
+            rr.push_back(ic.r);
+            im.push_back(mat_of[key]);
+        }
+        pg_rve_desc desc{};
+        desc.nx = cfg.nx;
+        desc.ny = cfg.ny;
+        desc.x0 = cfg.x0;
+        desc.x1 = cfg.x1;
+        desc.y0 = cfg.y0;
+        desc.y1 = cfg.y1;
+        desc.n_inclusions = (int32_t)cx.size();
+        desc.inc_cx = cx.data();
+        desc.inc_cy = cy.data();
+        desc.inc_r = rr.data();
+        desc.inc_mat = im.data();
+        desc.n_materials = (int32_t)mE.size();
+        desc.mat_E = mE.data();
+        desc.mat_nu = mnu.data();
+        desc.matrix_mat = 0;
+        desc.plane_strain = cfg.plane_strain;
+        desc.strain = cfg.strain;
+        void* mem = calloc(1, sizeof(ProblemLinearElasticityGPU));
+        problem = new (mem) ProblemLinearElasticityGPU(desc, 0, 1e-12);
+#else
         void* mem = calloc(1, sizeof(ProblemLinearElasticity));
         problem = new (mem) ProblemLinearElasticity;
+#endif
     }
     problem->set_parameter("plane_strain", cfg.plane_strain);
     problem->attach_mesh(&mesh);
@@ -255,6 +307,14 @@ int main(int argc, char** argv) {
     boundary->set_dirichlet_bcs_from_nodeset("left", 0, 0.0);
     for (unsigned int d = 0; d < mesh.dim(); ++d) boundary->set_dirichlet_bc(0, d, 0);
 
+    // Shape sensitivities of the right-edge load (Problem::addSensitivityFunction,
+    // Problem::addShapeSensitivityParameter, Problem.cpp:836-861); Problem::init
+    // builds the sensitivity solver (Problem.cpp:191-235)
+    if (!cfg.sens.empty()) {
+        SensitivityRightLoad fn;
+        problem->addSensitivityFunction(&fn);
+        for (const auto& p : cfg.sens) problem->addShapeSensitivityParameter((id_type)p.inc, p.name);
+    }
     const double t_init0 = now_s();
     problem->init();
     const double t_init = now_s() - t_init0;
@@ -286,19 +346,7 @@ int main(int argc, char** argv) {
         }
         o.d1("time.assemble_repeat_total", t_asm_rep);
         o.d("time.assemble_each", each);
-        // the reference's writers on the final state (Writer_ASCII_VTK as
-    // Problem::init builds it, Problem.cpp:246-249; WriterCohesiveOpenings)
-    if (!cfg.vtk_out.empty()) {
-        Writer_ASCII_VTK w(problem);
-        w.store_mesh();
-        w.write(cfg.vtk_out, cfg.T_final);
-    }
-    if (!cfg.openings_out.empty() && cohesive) {
-        WriterCohesiveOpenings w(problem);
-        w.store_mesh();
-        w.write(cfg.openings_out, cfg.T_final);
-    }
-    o.d1("time.init", t_init);
+        o.d1("time.init", t_init);
         o.i1("time.assemble_repeats", cfg.assemble_repeats);
         o.i1("mesh.n_elem_active", (int32_t)mesh.n_local_active_elem());
         fclose(fp);
@@ -311,6 +359,17 @@ int main(int argc, char** argv) {
     const double t_solve0 = now_s();
     problem->solve_problem();
     const double t_total_solve = now_s() - t_solve0;
+#ifdef PG_GPU_DROPIN
+    if (!cohesive) {
+        SolverGPULinear* gs = dynamic_cast<SolverGPULinear*>(problem->get_solver());
+        if (!gs || gs->status() != 0) {
+            fprintf(stderr, "drop-in solve failed\n");
+            return 3;
+        }
+        o.i1("gpu.iterations", gs->stats().iterations);
+        o.d1("gpu.rel_residual", gs->stats().rel_residual);
+    }
+#endif
 
     // ---- mesh -------------------------------------------------------------
     std::vector<double> xy;
@@ -446,6 +505,14 @@ int main(int argc, char** argv) {
         o.i("isv.qp", isv_qp);
         o.d("isv.delta_max", isv_val);
         o.i1("snes.iterations", (int32_t)(pgshim_snes_iterations() - snes0));
+    }
+    if (!cfg.sens.empty()) {
+        SensitivitySolver* ss = problem->_sensitivity_solver;
+        o.d1("sens.f", ss->get_function_val(0));
+        std::vector<double> g;
+        for (size_t j = 0; j < cfg.sens.size(); ++j) g.push_back(ss->get_sensitivity(0, (id_type)j));
+        o.d("sens.dfdp", g);
+        o.i1("sens.adjoint", dynamic_cast<SensitivityAdjoint*>(ss) ? 1 : 0);
     }
     // the reference's writers on the final state (Writer_ASCII_VTK as
     // Problem::init builds it, Problem.cpp:246-249; WriterCohesiveOpenings)

@@ -16,6 +16,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DRIVER = os.path.join(HERE, "_ref", "pigfem_ref_driver")
+# the same driver with the B200 library's solver below the reference's Problem
+# (integration/solver_gpu.h; `make -f oracle/Makefile.ref dropin`)
+DROPIN_DRIVER = os.path.join(HERE, "_ref", "pigfem_gpu_dropin")
 
 
 def driver_available() -> bool:
@@ -49,25 +52,30 @@ def write_config(path: str, cfg: dict) -> None:
         if k == "inclusions":
             for inc in v:
                 lines.append("inc %.17g %.17g %.17g %.17g %.17g" % tuple(inc))
+        elif k == "sens":
+            for inc, name in v:
+                lines.append(f"sens {int(inc)} {name}")
         else:
             lines.append(f"{k} {v}")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 
 
-def run(cfg: dict, timeout: float = 600.0) -> dict:
+def run(cfg: dict, timeout: float = 600.0, driver: str = None) -> dict:
     """Run the reference on ``cfg`` and return its records.
 
     cfg keys: nx, ny, x0, x1, y0, y1, E_matrix, nu_matrix, plane_strain,
     strain, problem ('linear'|'cohesive'), inclusions [(cx, cy, r, E, nu)],
     coh_sigma, coh_delta, coh_beta, coh_visc, T_final, max_dt, min_dt,
-    max_iter, assemble_repeats, dump_K, snes_rtol, snes_stol; write_vtk and
+    max_iter, assemble_repeats, dump_K, snes_rtol, snes_stol, sens [(inclusion,
+    "X"|"Y"|"R")] (shape sensitivities of the right-edge load); write_vtk and
     write_openings (True: the reference's Writer_ASCII_VTK file and
     WriterCohesiveOpenings CSV of the final state come back as the bytes of
     records "vtk.text" and "openings.text").
     """
-    if not driver_available():
-        raise FileNotFoundError(f"reference driver not built: {DRIVER}")
+    driver = driver or DRIVER
+    if not os.path.exists(driver):
+        raise FileNotFoundError(f"reference driver not built: {driver}")
     cfg = dict(cfg)
     want_vtk = bool(cfg.pop("write_vtk", False))
     want_open = bool(cfg.pop("write_openings", False))
@@ -82,7 +90,7 @@ def run(cfg: dict, timeout: float = 600.0) -> dict:
         if want_open:
             texts["openings.text"] = cfg["openings_out"] = os.path.join(td, "openings.csv")
         write_config(cfg_path, cfg)
-        proc = subprocess.run([DRIVER, cfg_path, out_path, "Output/run"], cwd=td,
+        proc = subprocess.run([driver, cfg_path, out_path, "Output/run"], cwd=td,
                               capture_output=True, text=True, timeout=timeout)
         if proc.returncode != 0 or not os.path.exists(out_path):
             raise RuntimeError(f"reference driver failed rc={proc.returncode}\n"
@@ -92,6 +100,7 @@ def run(cfg: dict, timeout: float = 600.0) -> dict:
             with open(path, "rb") as f:
                 rec[key] = np.frombuffer(f.read(), dtype=np.uint8).copy()
         rec["_stdout"] = proc.stdout
+        rec["_stderr"] = proc.stderr
         return rec
 
 

@@ -34,6 +34,9 @@ PG_RTOL_BASE_PREDICTOR = 0
 PG_RTOL_BASE_ZEROTH = 1
 PG_PRECISION_FP64 = 0
 PG_PRECISION_MIXED = 1
+PG_SHAPE_X = 0
+PG_SHAPE_Y = 1
+PG_SHAPE_R = 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -137,6 +140,8 @@ def _load() -> C.CDLL:
         "pg_solver_cfg_default": ([C.POINTER(SolverCfg)], None),
         "pg_solve_linear": ([v, C.POINTER(SolverCfg), C.POINTER(SolveStats)], C.c_int),
         "pg_sensitivity_c11": ([v, C.POINTER(SolverCfg), C.c_double, _dp, _dp, C.POINTER(SolveStats)], C.c_int),
+        "pg_sensitivity_shape": ([v, C.POINTER(SolverCfg), C.c_int32, _ip, _ip, _dp, _dp, C.POINTER(SolveStats)],
+                                 C.c_int),
         "pg_ctx_autotune": ([v, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
         "pg_ctx_tuning": ([v, _ip, _ip, _ip], C.c_int),
         "pg_ctx_set_tuning": ([v, C.c_int32, C.c_int32, C.c_int32], C.c_int),
@@ -194,7 +199,7 @@ DECLARED_SYMBOLS = (
     "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
     "pg_solve_nonlinear", "pg_mlp_create", "pg_mlp_destroy", "pg_mlp_param_count", "pg_mlp_params",
     "pg_mlp_grads", "pg_mlp_forward", "pg_mlp_gradient", "pg_mlp_adam", "pg_mlp_train", "pg_mlp_wait_selftest", "pg_predictor_features",
-    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_sensitivity_c11", "pg_ctx_autotune", "pg_ctx_tuning", "pg_ctx_set_tuning", "pg_batch_create", "pg_batch_destroy", "pg_batch_context", "pg_batch_setup_times",
+    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_sensitivity_c11", "pg_sensitivity_shape", "pg_ctx_autotune", "pg_ctx_tuning", "pg_ctx_set_tuning", "pg_batch_create", "pg_batch_destroy", "pg_batch_context", "pg_batch_setup_times",
     "pg_batch_info", "pg_batch_solve", "pg_batch_get_solution", "pg_pcg_solve_static", "pg_last_error",
     "pg_version",
 )

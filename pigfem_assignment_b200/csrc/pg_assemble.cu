@@ -1427,6 +1427,253 @@ __global__ void __launch_bounds__(32 * W, (NL <= 5 ? 24 : (NL <= 7 ? 16 : 8)) / 
     if (lane == 0) atomicAdd(&a.sens[sel], a.sgn * part / (2.0 * hstep));
 }
 
+// ---------------------------------------------------------------------------
+// Analytic shape derivative of the cut elements' internal force
+// (SensitivityShapeParameterStructural::KernelVolumetric,
+// src/SensitivityShapeParameterStructural.cpp:18-90, and the cohesive
+// traction's), by forward-mode differentiation: every coordinate carries its
+// derivative along the parameter's velocity field (nonzero at the enrichment
+// nodes of the parameter's inclusion), and the quadrature rows carry the
+// derivatives of the weight w det J and of the enrichment gradients.  The
+// derivative of sum_q w det J B^T D B u is then
+//   sum_q [ d(w det J) B^T D B u + w det J (dB^T D B u + B^T D dB u) ],
+// the reference's B^T (D dB u + sigma div v) + dB^T sigma weighted by w det J,
+// exact to rounding (no step size).
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator*(double s, Dual a) { return {s * a.v, s * a.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    const double q = a.v / b.v;
+    return {q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+    const double r = sqrt(a.v);
+    return {r, 0.5 * a.d / r};
+}
+
+// cut_row with coordinates (cx, cy) moving at (dcx, dcy): the row's values
+// and their derivatives; the parent gradients do not move (parent nodes have
+// no velocity)
+__device__ __forceinline__ void cut_row_dual(double* row, double* drow, int nl, const DevChildQuad& Q, int q, int nc,
+                                             const int* ln, const double* cx, const double* cy, const double* dcx,
+                                             const double* dcy, const double* dm, const double* pbx,
+                                             const double* pby) {
+    Dual J00{0.0, 0.0}, J01{0.0, 0.0}, J10{0.0, 0.0}, J11{0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < kMaxChildNodes; ++k) {
+        if (k < nc) {
+            const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+            const Dual X{cx[k], dcx[k]}, Y{cy[k], dcy[k]};
+            J00 = J00 + dr * X;
+            J01 = J01 + dr * Y;
+            J10 = J10 + ds * X;
+            J11 = J11 + ds * Y;
+        }
+    }
+    const Dual det = J00 * J11 - J01 * J10;
+    const Dual wgt = Q.w[q] * det;
+    const bool live = wgt.v != 0.0;
+    row[0] = live ? wgt.v : 0.0;
+    drow[0] = live ? wgt.d : 0.0;
+    for (int i = 1; i < 4; ++i) {
+        row[i] = dm[i - 1];
+        drow[i] = 0.0;
+    }
+    for (int j = 0; j < 3; ++j) {
+        row[4 + 2 * j] = pbx[j];
+        row[5 + 2 * j] = pby[j];
+        drow[4 + 2 * j] = drow[5 + 2 * j] = 0.0;
+    }
+    for (int j = 3; j < nl; ++j) row[4 + 2 * j] = row[5 + 2 * j] = drow[4 + 2 * j] = drow[5 + 2 * j] = 0.0;
+    if (live) {
+#pragma unroll
+        for (int k = 0; k < kMaxChildNodes; ++k) {
+            if (k < nc && ln[k] >= 3) {
+                const double dr = Q.dN[(q * nc + k) * 2], ds = Q.dN[(q * nc + k) * 2 + 1];
+                const Dual gx = (dr * J11 - ds * J01) / det;
+                const Dual gy = (ds * J00 - dr * J10) / det;
+                row[4 + 2 * ln[k]] = gx.v;
+                row[5 + 2 * ln[k]] = gy.v;
+                drow[4 + 2 * ln[k]] = gx.d;
+                drow[5 + 2 * ln[k]] = gy.d;
+            }
+        }
+    }
+}
+
+// One warp per cut element and pass (which-th inclusion among its enrichment
+// slots, one parameter kind): the derivative of wsens . f_e along the
+// velocity field vel, added to sens[param_of[3 inclusion + kind]].
+template <int NL, int PPL, int W>
+__global__ void __launch_bounds__(32 * W) k_cut_sens_ad(CutArgs a) {
+    constexpr int kQRow = 4 + 2 * NL;
+    __shared__ double sX[W][NL], sY[W][NL], sDX[W][NL], sDY[W][NL];
+    __shared__ double sU[W][2 * NL];
+    __shared__ int sL[W][NL];
+    __shared__ double sQ[W][kQpChunk][kQRow];
+    __shared__ double sQd[W][kQpChunk][kQRow];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int oi = blockIdx.x * W + w;
+    if (oi >= a.n_cut) return;
+    const int ci = a.first + oi;
+    const int node = lane < NL ? __ldg(&a.cut_nodes[kCutNodeStride * ci + lane]) : -1;
+    const int tmpl = __ldg(&a.cut_tmpl[ci]);
+    const DevTemplate& T = c_tmpl[tmpl];
+    const int nl = 3 + T.n_enr;
+    if (lane < nl) {
+        sL[w][lane] = node;
+        sX[w][lane] = a.x[node];
+        sY[w][lane] = a.y[node];
+        sU[w][2 * lane] = a.u[2 * node];
+        sU[w][2 * lane + 1] = a.u[2 * node + 1];
+    }
+    __syncwarp();
+    const unsigned full = 0xffffffffu;
+    const int my_inc = (lane >= 3 && lane < nl) ? a.node_inc[sL[w][lane]] : -1;
+    int sel = -1, count = 0;
+    for (int l = 3; l < nl; ++l) {
+        const int v = __shfl_sync(full, my_inc, l);
+        bool seen = false;
+        for (int l2 = 3; l2 < l; ++l2) seen |= __shfl_sync(full, my_inc, l2) == v;
+        if (!seen && v >= 0) {
+            if (count == a.which) sel = v;
+            ++count;
+        }
+    }
+    if (sel < 0) return;  // warp-uniform
+    const int param = a.param_of[3 * sel + a.kind];
+    if (param < 0) return;
+    if (lane < nl) {
+        const bool moves = my_inc == sel;
+        const int nd = sL[w][lane];
+        sDX[w][lane] = moves ? a.vel[2 * nd] : 0.0;
+        sDY[w][lane] = moves ? a.vel[2 * nd + 1] : 0.0;
+    }
+    __syncwarp();
+    double pbx[3], pby[3];
+    parent_gradients(sX[w], sY[w], pbx, pby);
+    int nq_total = 0;
+    for (int ch = 0; ch < T.n_child; ++ch) nq_total += c_quad[T.child_type[ch]].nq;
+    double acc[PPL][4];
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0;
+    const int npairs = nl * nl;
+    int pa[PPL], pb[PPL];
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+        const int p = lane + 32 * k;
+        pa[k] = p / nl;
+        pb[k] = p - pa[k] * nl;
+    }
+    for (int qbase = 0; qbase < nq_total; qbase += kQpChunk) {
+        const int l = qbase + lane;
+        if (l < nq_total) {
+            const DevTemplate& TG = g_tmpl[tmpl];
+            int ch, q;
+            point_child(TG, l, ch, q);
+            const int nc = TG.child_n[ch];
+            const int mat = a.cut_child_mat[ci * kMaxChildren + ch];
+            int ln[kMaxChildNodes];
+            double cx[kMaxChildNodes], cy[kMaxChildNodes], dcx[kMaxChildNodes], dcy[kMaxChildNodes];
+#pragma unroll
+            for (int k = 0; k < kMaxChildNodes; ++k) {
+                ln[k] = k < nc ? TG.child_nodes[ch][k] : 0;
+                cx[k] = sX[w][ln[k]];
+                cy[k] = sY[w][ln[k]];
+                dcx[k] = sDX[w][ln[k]];
+                dcy[k] = sDY[w][ln[k]];
+            }
+            const double dm[3] = {a.dmat[3 * mat], a.dmat[3 * mat + 1], a.dmat[3 * mat + 2]};
+            cut_row_dual(sQ[w][lane], sQd[w][lane], nl, g_quad[TG.child_type[ch]], q, nc, ln, cx, cy, dcx, dcy, dm,
+                         pbx, pby);
+        }
+        __syncwarp();
+        const int nqc = min(kQpChunk, nq_total - qbase);
+        for (int q = 0; q < nqc; ++q) {
+            const double* row = sQ[w][q];
+            const double* drow = sQd[w][q];
+            const double wgt = row[0], dwgt = drow[0], d11 = row[1], d12 = row[2], d33 = row[3];
+#pragma unroll
+            for (int k = 0; k < PPL; ++k) {
+                if (lane + 32 * k < npairs) {
+                    const double ba = row[4 + 2 * pa[k]], ca = row[5 + 2 * pa[k]];
+                    const double bb = row[4 + 2 * pb[k]], cb = row[5 + 2 * pb[k]];
+                    const double dba = drow[4 + 2 * pa[k]], dca = drow[5 + 2 * pa[k]];
+                    const double dbb = drow[4 + 2 * pb[k]], dcb = drow[5 + 2 * pb[k]];
+                    // d/dp of w (B_a^T D B_b), entry by entry
+                    acc[k][0] += dwgt * (ba * d11 * bb + ca * d33 * cb) +
+                                 wgt * (dba * d11 * bb + ba * d11 * dbb + dca * d33 * cb + ca * d33 * dcb);
+                    acc[k][1] += dwgt * (ba * d12 * cb + ca * d33 * bb) +
+                                 wgt * (dba * d12 * cb + ba * d12 * dcb + dca * d33 * bb + ca * d33 * dbb);
+                    acc[k][2] += dwgt * (ca * d12 * bb + ba * d33 * cb) +
+                                 wgt * (dca * d12 * bb + ca * d12 * dbb + dba * d33 * cb + ba * d33 * dcb);
+                    acc[k][3] += dwgt * (ca * d11 * cb + ba * d33 * bb) +
+                                 wgt * (dca * d11 * cb + ca * d11 * dcb + dba * d33 * bb + ba * d33 * dbb);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    double part = 0.0;
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+        if (lane + 32 * k < npairs) {
+            const int ia = pa[k], ib = pb[k];
+            const double ux = sU[w][2 * ib], uy = sU[w][2 * ib + 1];
+            const double fx = acc[k][0] * ux + acc[k][1] * uy;
+            const double fy = acc[k][2] * ux + acc[k][3] * uy;
+            part += a.wsens[2 * sL[w][ia]] * fx + a.wsens[2 * sL[w][ia] + 1] * fy;
+        }
+    }
+    // cohesive tractions at fixed U and committed state: the frame and the
+    // length move, the opening follows the frame (dt = D d(delta))
+    if (lane < 2 * T.n_coh) {
+        const int ce = lane >> 1, q = lane & 1;
+        const int c0 = T.coh_nodes[ce][0], c1 = T.coh_nodes[ce][1], c2 = T.coh_nodes[ce][2], c3 = T.coh_nodes[ce][3];
+        const Dual x0{sX[w][c0], sDX[w][c0]}, x1{sX[w][c1], sDX[w][c1]};
+        const Dual y0{sY[w][c0], sDY[w][c0]}, y1{sY[w][c1], sDY[w][c1]};
+        const Dual jx = 0.5 * (x1 - x0), jy = 0.5 * (y1 - y0);
+        const Dual mag = dsqrt(jx * jx + jy * jy);
+        const Dual nx = -jy, ny = jx;
+        const Dual dA = dsqrt(nx * nx + ny * ny);
+        const Dual R00 = jx / mag, R01 = jy / mag, R10 = nx / dA, R11 = ny / dA;
+        const double xi = q == 0 ? -0.57735026918962576450914878050196 : 0.57735026918962576450914878050196;
+        const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+        double dg[2];
+        for (int d = 0; d < 2; ++d)
+            dg[d] = N0 * (sU[w][2 * c2 + d] - sU[w][2 * c0 + d]) + N1 * (sU[w][2 * c3 + d] - sU[w][2 * c1 + d]);
+        const Dual dl0 = dg[0] * R00 + dg[1] * R01, dl1 = dg[0] * R10 + dg[1] * R11;
+        double dl[2] = {dl0.v, dl1.v};
+        const int qp = a.cut_coh_qp0[ci] + lane;
+        double tr[2], Dc[2][2], dmax_t;
+        cohesive_law(a.coh, a.dt, a.isv_c[qp], dl, tr, Dc, dmax_t);
+        const double dtr0 = Dc[0][0] * dl0.d + Dc[0][1] * dl1.d;
+        const double dtr1 = Dc[1][0] * dl0.d + Dc[1][1] * dl1.d;
+        const Dual t0{tr[0], dtr0}, t1{tr[1], dtr1};
+        const Dual tR0 = R00 * t0 + R10 * t1;
+        const Dual tR1 = R01 * t0 + R11 * t1;
+        if (dA.v != 0.0) {
+            const Dual f0 = dA * tR0, f1 = dA * tR1;
+            const int cn[4] = {c0, c1, c2, c3};
+            const double Nn[2] = {N0, N1};
+            for (int m = 0; m < 4; ++m) {
+                const double sg = m < 2 ? -1.0 : 1.0;
+                const int nd = sL[w][cn[m]];
+                part += a.wsens[2 * nd] * (sg * Nn[m & 1] * f0.d) + a.wsens[2 * nd + 1] * (sg * Nn[m & 1] * f1.d);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(full, part, o);
+    if (lane == 0) atomicAdd(&a.sens[param], part);
+}
+
 __global__ void k_to_fp32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1466,6 +1713,21 @@ void launch_tri(const Ctx& c, const RowArgs& ra, bool want_f, cudaStream_t s) {
     } else {
         if (want_f) launch_tri_tn<true, 64>(c, ra, s);
         else launch_tri_tn<false, 64>(c, ra, s);
+    }
+}
+
+// Analytic shape-sensitivity passes (one launch per size class).
+void launch_cut_sens_ad(const Ctx& c, const CutArgs& ca, cudaStream_t s) {
+    for (int k = 0; k < kCutClasses; ++k) {
+        const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
+        if (n == 0) continue;
+        CutArgs ck = ca;
+        ck.n_cut = n;
+        ck.first = c.cut_class_off[k];
+        if (k == 0) k_cut_sens_ad<5, 1, 4><<<(n + 3) / 4, 128, 0, s>>>(ck);
+        else if (k == 1) k_cut_sens_ad<7, 2, 4><<<(n + 3) / 4, 128, 0, s>>>(ck);
+        else if (k == 2) k_cut_sens_ad<11, 4, 2><<<(n + 1) / 2, 64, 0, s>>>(ck);
+        else k_cut_sens_ad<15, 8, 2><<<(n + 1) / 2, 64, 0, s>>>(ck);
     }
 }
 

@@ -249,8 +249,13 @@ struct CutArgs {
     double* sens;
     double h_rel, sgn;
     int which;
+    // analytic passes: parameter slot of (inclusion, kind) at param_of[3 inclusion + kind]
+    // (-1: not a parameter); vel is the velocity field of this pass's kind
+    const int* param_of;
+    int kind;
 };
 CutArgs cut_args(const Ctx& c, const double* U, double dt);
+void launch_cut_sens_ad(const Ctx& c, const CutArgs& ca, cudaStream_t s);
 // fold order of the cut elements' deterministic assembly, built on the GPU
 // from the context's class-ordered cut tables (pg_mesh_gpu.cu)
 int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entries);

@@ -12,6 +12,10 @@ Fixtures (numpy .npz):
   linear_3inc.npz     40x40, three circles, two inclusion materials; contains a
                       node on an interface that escapes the node-moving rule
                       (a zero-area child element)
+  sensitivity_3inc.npz   32x32, three circles: f (the right edge's mean x
+                      reaction) and df/d(x_c, y_c, r) of every inclusion from the
+                      reference's SensitivityAdjoint + SensitivityRightLoad
+  sensitivity_close.npz  40x40, two circles 0.02 apart (elements cut by both)
   cohesive_16x16.npz  Ortiz-Pandolfi cohesive interface, four load steps from
                       four prefix-consistent runs (committed state per step),
                       each Newton solve converged to SNES rtol 1e-12 (stol off)
@@ -37,7 +41,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import refio  # noqa: E402
 
-KEEP = ("mesh.", "dof.", "K.", "U.", "F.", "Pint.", "isv.", "snes.", "qp.", "vtk.", "openings.")
+KEEP = ("mesh.", "dof.", "K.", "U.", "F.", "Pint.", "isv.", "snes.", "qp.", "vtk.", "openings.", "sens.")
 
 
 def save(name: str, rec: dict, extra: dict | None = None) -> None:
@@ -60,6 +64,19 @@ def main() -> None:
     incs = [(0.3, 0.3, 0.12, 70000.0, 0.2), (0.7, 0.62, 0.2, 20000.0, 0.3), (0.3, 0.75, 0.1, 70000.0, 0.2)]
     r = refio.run(dict(lin, nx=40, ny=40, inclusions=incs))
     save("linear_3inc.npz", r, {"cfg.nx": np.array([40]), "cfg.inc": np.array(incs)})
+
+    # shape sensitivities of the right-edge load (SensitivityAdjoint with
+    # SensitivityRightLoad) for every centre coordinate and radius
+    for name, nx, sincs in (
+            ("sensitivity_3inc.npz", 32, [(0.3, 0.35, 0.16, 70000.0, 0.2), (0.7, 0.4, 0.13, 70000.0, 0.2),
+                                          (0.45, 0.75, 0.15, 20000.0, 0.3)]),
+            ("sensitivity_close.npz", 40, [(0.3, 0.5, 0.2, 70000.0, 0.2), (0.72, 0.5, 0.2, 20000.0, 0.3)])):
+        params = [(i, k) for i in range(len(sincs)) for k in ("X", "Y", "R")]
+        r = refio.run(dict(lin, nx=nx, ny=nx, inclusions=sincs, dump_K=0, write_vtk=False, sens=params))
+        assert int(r["sens.adjoint"][0]) == 1
+        save(name, r, {"cfg.nx": np.array([nx]), "cfg.inc": np.array(sincs),
+                       "cfg.sens_inc": np.array([p[0] for p in params], np.int32),
+                       "cfg.sens_kind": np.array(["XYR".index(p[1]) for p in params], np.int32)})
 
     # cohesive: step k of a run with T_final = k*dt and strain = k*0.0025 has the
     # same load history as the first k steps of any longer run of this family

@@ -8,10 +8,12 @@ with FP64 refinement), on configuration 1: a 512x512 structured TRI3 mesh
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 One step = one full assembly pass of K: the structured-grid kernel (uncut
-triangles, one thread per node row) with the cut elements' kernels beside it
-on a second stream, then the deterministic fold of the cut elements' blocks.
-Timing: CUDA events on the assembly stream around each step; the L2 (126 MB)
-is flushed by writing a 512 MB buffer between steps; max over ranks.  For N > 1
+triangles, one thread per node row), then the cut elements' kernels (rows,
+cohesive points, node pairs) and the deterministic fold of their blocks, on
+one stream.  Timing: CUDA events on the assembly stream around each step; the
+L2 (126 MB) is flushed between steps by writing a 512 MB buffer and then
+reading 256 MB of it, so that the pass starts cold and without dirty lines of
+the flush left to write back; max over ranks.  For N > 1
 every rank assembles its own replica of the RVE (replicas only: a single RVE
 does not shard without a halo exchange), so scaling is weak.
 """
@@ -77,7 +79,7 @@ def workload_config(rve, info):
         "dof": info["n_dof"],
         "free_dof": info["n_free_dof"],
         "nnz": 4 * info["n_blocks"],
-        "l2": "flushed between steps (512 MB write)",
+        "l2": "flushed between steps (512 MB written, then 256 MB read: cold, no dirty lines)",
         "parallelism": "replicas",
     }
 
@@ -275,6 +277,13 @@ def run_b200_arm(args):
     asm = pb.Assembler(ctx)
     flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 512 MB
 
+    def flush_l2(v: float):
+        # write more than the L2 holds, then read half of it back: the write
+        # evicts everything, the read leaves only clean lines behind
+        flush.fill_(v)
+        flush[: 64 * 1024 * 1024].sum()
+        torch.cuda.synchronize()
+
     def assemble_timed():
         _lib.check(_lib.lib.pg_assembly_timing(ctx.handle, 1, None, None))
         asm.assemble_linear()
@@ -298,8 +307,7 @@ def run_b200_arm(args):
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
 
     for _ in range(args.warmup):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
+        flush_l2(1.0)
         assemble_timed()
     ctx.sync()
 
@@ -310,8 +318,7 @@ def run_b200_arm(args):
     torch.cuda.synchronize()
     rows_ms, cut_ms = [], []
     for _ in range(args.steps):
-        flush.fill_(float(len(rows_ms)))
-        torch.cuda.synchronize()
+        flush_l2(float(len(rows_ms)))
         a, b = assemble_timed()
         rows_ms.append(a)
         cut_ms.append(b)
@@ -352,8 +359,7 @@ def run_b200_arm(args):
         _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, xy_p, kh_p))
     e2e_ms = []
     for _ in range(max(3, args.steps // 2)):
-        flush.fill_(2.0)
-        torch.cuda.synchronize()
+        flush_l2(2.0)
         t0 = time.perf_counter()
         _lib.check(_lib.lib.pg_assemble_linear_host(ctx.handle, xy_p, kh_p))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
@@ -585,6 +591,8 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     from pigfem_assignment_b200 import _lib
     from pigfem_assignment_b200.rve import config3_rves
 
+    # the synthetic input (the inclusion sets the reference would read from
+    # its CSV files): generated first, timed apart from the set-up
     t0 = time.perf_counter()
     all_rves = config3_rves(count=n_rve)
     mine = shard_rves([2 * r.nx * r.ny for r in all_rves], world)[rank]
@@ -592,9 +600,9 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     n_rve = len(rves)
     t_gen = time.perf_counter() - t0
     # IGFEM preprocessing and sparsity of every RVE on the GPU (pg_mesh_build_device),
-    # from a few host threads so that the builds' launches overlap
+    # from host threads so that the builds' launches overlap
     t1 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=8) as ex:
+    with ThreadPoolExecutor(max_workers=16) as ex:
         meshes = list(ex.map(lambda r: pb.Mesh(r, device=local), rves))
     t_mesh = time.perf_counter() - t1
     t2 = time.perf_counter()
@@ -602,7 +610,7 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     h = C.c_void_p()
     _lib.check(_lib.lib.pg_batch_create(arr, n_rve, local, C.byref(h)), "pg_batch_create")
     t_batch = time.perf_counter() - t2
-    setup_s = time.perf_counter() - t0
+    setup_s = time.perf_counter() - t1
     phases = (C.c_double * 7)()
     _lib.check(_lib.lib.pg_batch_setup_times(h, phases))
     # the host builder on the same RVEs (all host threads), for comparison only
@@ -619,6 +627,7 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     times = []
     for k in range(warmup + steps):
         flush.fill_(float(k))
+        flush[: 64 * 1024 * 1024].sum()
         torch.cuda.synchronize()
         _lib.check(_lib.lib.pg_assembly_timing(ctx, 1, None, None))
         _lib.check(_lib.lib.pg_assemble_linear(ctx, None))
@@ -631,8 +640,9 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     out = {"rves": int(sum_over_ranks(n_rve, device=dev)), "elements": int(tot_elem),
            "dof": int(sum_over_ranks(n_dof, device=dev)), "ranks": world,
            "host_setup_s": max_over_ranks(setup_s, device=dev),
-           "setup_split_s": {"rve_generation": t_gen, "mesh_build_gpu": t_mesh, "batch_create": t_batch,
-                             "batch_create_phases": dict(zip(("copy_meshes", "merge", "ctx_uploads", "ctx_grid_tiles",
+           "input_generation_s": t_gen,
+           "setup_split_s": {"mesh_build_gpu": t_mesh, "batch_create": t_batch,
+                             "batch_create_phases": dict(zip(("grid_records", "merge", "ctx_uploads", "ctx_grid_tiles",
                                                               "ctx_cut_tables", "ctx_fold_order_gpu", "multigrid"),
                                                              [round(v, 4) for v in phases])),
                              "mesh_build_host_for_comparison": t_host_mesh,

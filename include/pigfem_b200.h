@@ -378,9 +378,10 @@ int pg_batch_create(const pg_mesh* const* meshes, int32_t n_rve, int32_t device,
 void pg_batch_destroy(pg_batch* b);
 /* the merged system as a context: assembly, timing and host copies work on it */
 pg_ctx* pg_batch_context(pg_batch* b);
-/* host seconds of pg_batch_create's phases (7 values): copying the meshes,
- * merging them, the context's uploads, grid tiles, cut-element tables and
- * fold order (built on the GPU), and the multigrid hierarchy */
+/* host seconds of pg_batch_create's phases (7 values): recording the RVEs'
+ * grids, merging the meshes (in parallel on the host's cores, read in place),
+ * the context's uploads, grid tiles, cut-element tables and fold order (built
+ * on the GPU), and the multigrid hierarchy */
 int pg_batch_setup_times(const pg_batch* b, double* seconds);
 /* first node / element of each RVE in the merged system (n_rve + 1 entries each), multigrid depth per RVE */
 int pg_batch_info(const pg_batch* b, int32_t* node_offset, int32_t* element_offset, int32_t* depth);

@@ -1003,7 +1003,7 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
 // ---------------------------------------------------------------------------
 // Every cut element's (3 + n_enr)^2 node-pair blocks have a fixed place in
 // the element's slot table (cut_slot: pair (a, b) at cut_slot_ptr + a nl +
-// b, holding the block's K slot).  k_cut_elems integrates one pair per
+// b, holding the block's K slot).  k_cut_pairs integrates one pair per
 // thread and stores the block at its position in fold order (kpos, built
 // once per mesh: all contributions to one K slot next to each other, by
 // element and pair), and for residual passes K_ab u_b at its position in
@@ -1014,13 +1014,13 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
 // of contributions; k_fold_f does the same per node for f_int.  The sums
 // are the same on every run: no atomics.
 //
-// Three kernels form the pairs, all on a second stream beside the triangle
-// kernel (they depend on the coordinates, the displacements and the
-// committed cohesive state only; only the fold waits for both streams):
-// k_cut_points forms every quadrature row (one thread per point, from the
-// host-packed point records), k_coh_points every cohesive Gauss point (one
-// thread each: traction-separation law, trial delta_max, row), and
-// k_cut_pairs integrates one node pair per thread from those rows.
+// Three kernels form the pairs, after the triangle kernel on the same
+// stream (a second stream bought no overlap: the triangle kernel fills every
+// SM until its last wave): k_cut_points forms every quadrature row (one
+// thread per point, from the host-packed point records), k_coh_points every
+// cohesive Gauss point (one thread each: traction-separation law, trial
+// delta_max, row), and k_cut_pairs integrates one node pair per thread from
+// those rows.
 constexpr int kCohRow = kCohRowDoubles;  // {w dA, N0, N1, (R^T D R) 4, (R^T t) 2, pad}
 
 // One thread per quadrature point: its row, point-major (the element's point

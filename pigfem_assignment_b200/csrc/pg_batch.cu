@@ -21,6 +21,8 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 #include "pg_solve_kernels.cuh"
 #include "pigfem_b200.h"
@@ -619,7 +621,7 @@ struct pg_batch {
     // host seconds of the set-up: mesh copies, merge, context (uploads, grid
     // tiles, cut tables, fold order), multigrid hierarchy
     double setup_s[7] = {0, 0, 0, 0, 0, 0, 0};
-    std::vector<pgb::HostMesh> meshes;
+    std::vector<std::pair<int, int>> grid;  // background grid (nx, ny) of each RVE
     std::vector<int> noff;              // first node of each RVE (+ total)
     std::vector<int> eoff;              // first element of each RVE (+ total)
     pg_ctx ctx;                         // the merged system
@@ -651,23 +653,95 @@ struct pg_batch {
 namespace pgb {
 namespace {
 
-// Concatenates the RVE meshes into one block-diagonal mesh.
-void merge_meshes(const std::vector<HostMesh>& ms, HostMesh& out, std::vector<int>& noff, std::vector<int>& eoff) {
+// Runs fn(r) for every RVE r on the host's cores.
+template <class F>
+void for_each_rve(int R, F&& fn) {
+    const int T = (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::min(T, R); ++t)
+        pool.emplace_back([&] {
+            for (int r; (r = next.fetch_add(1)) < R;) fn(r);
+        });
+    for (auto& th : pool) th.join();
+}
+
+// Concatenates the RVE meshes into one block-diagonal mesh: every array's
+// place per RVE first (prefix sums of the sizes), then the RVEs copied and
+// renumbered in parallel, each into its own range.
+void merge_meshes(const pg_mesh* const* ms, int R, HostMesh& out, std::vector<int>& noff, std::vector<int>& eoff) {
     out = HostMesh();
-    const int R = (int)ms.size();
+    auto M = [&](int r) -> const HostMesh& { return ms[r]->m; };
     noff.assign(R + 1, 0);
     eoff.assign(R + 1, 0);
     std::vector<int> moff(R + 1, 0), coff(R + 1, 0), boff(R + 1, 0), qoff(R + 1, 0), koff(R + 1, 0);
     for (int r = 0; r < R; ++r) {
-        noff[r + 1] = noff[r] + ms[r].n_nodes();
-        eoff[r + 1] = eoff[r] + ms[r].n_elem;
-        moff[r + 1] = moff[r] + (int)ms[r].spec.materials.size();
-        coff[r + 1] = coff[r] + ms[r].n_cut;
-        boff[r + 1] = boff[r] + ms[r].n_blocks();
-        qoff[r + 1] = qoff[r] + ms[r].n_coh_qp;
-        koff[r + 1] = koff[r] + (int)ms[r].ne_list.size();
+        noff[r + 1] = noff[r] + M(r).n_nodes();
+        eoff[r + 1] = eoff[r] + M(r).n_elem;
+        moff[r + 1] = moff[r] + (int)M(r).spec.materials.size();
+        coff[r + 1] = coff[r] + M(r).n_cut;
+        boff[r + 1] = boff[r] + M(r).n_blocks();
+        qoff[r + 1] = qoff[r] + M(r).n_coh_qp;
+        koff[r + 1] = koff[r] + (int)M(r).ne_list.size();
     }
-    out.spec = ms[0].spec;
+    // the place of each RVE's part of one array, and the array sized to all
+    auto place = [&](auto field, auto& dst) {
+        std::vector<size_t> o(R + 1, 0);
+        for (int r = 0; r < R; ++r) o[r + 1] = o[r] + (M(r).*field).size();
+        dst.resize(o[R]);
+        return o;
+    };
+    const auto o_x = place(&HostMesh::x, out.x);
+    place(&HostMesh::y, out.y);
+    const auto o_conn = place(&HostMesh::conn, out.conn);
+    const auto o_emat = place(&HostMesh::elem_mat, out.elem_mat);
+    place(&HostMesh::elem_cut, out.elem_cut);
+    const auto o_cut = place(&HostMesh::cut_elem, out.cut_elem);
+    place(&HostMesh::cut_tmpl, out.cut_tmpl);
+    const auto o_cenr = place(&HostMesh::cut_enr, out.cut_enr);
+    const auto o_cchm = place(&HostMesh::cut_child_mat, out.cut_child_mat);
+    const auto o_ccoh = place(&HostMesh::cut_coh_mat, out.cut_coh_mat);
+    place(&HostMesh::cut_coh_qp0, out.cut_coh_qp0);
+    const auto o_fix = place(&HostMesh::fixed, out.fixed);
+    place(&HostMesh::ubar, out.ubar);
+    const auto o_col = place(&HostMesh::col, out.col);
+    const auto o_diag = place(&HostMesh::diag_slot, out.diag_slot);
+    const auto o_nel = place(&HostMesh::ne_list, out.ne_list);
+    const auto o_slot = place(&HostMesh::cut_slot, out.cut_slot);
+    out.row_ptr.assign((size_t)noff[R] + 1, 0);
+    out.ne_ptr.assign((size_t)noff[R] + 1, 0);
+    for_each_rve(R, [&](int r) {
+        const HostMesh& m = M(r);
+        const int no = noff[r], eo = eoff[r], mo = moff[r], co = coff[r], bo = boff[r], qo = qoff[r], ko = koff[r];
+        std::copy(m.x.begin(), m.x.end(), out.x.begin() + o_x[r]);
+        std::copy(m.y.begin(), m.y.end(), out.y.begin() + o_x[r]);
+        for (size_t i = 0; i < m.conn.size(); ++i) out.conn[o_conn[r] + i] = m.conn[i] + no;
+        for (size_t i = 0; i < m.elem_mat.size(); ++i) {
+            out.elem_mat[o_emat[r] + i] = m.elem_mat[i] + mo;
+            out.elem_cut[o_emat[r] + i] = m.elem_cut[i] >= 0 ? m.elem_cut[i] + co : -1;
+        }
+        for (size_t i = 0; i < m.cut_elem.size(); ++i) {
+            out.cut_elem[o_cut[r] + i] = m.cut_elem[i] + eo;
+            out.cut_tmpl[o_cut[r] + i] = m.cut_tmpl[i];
+            out.cut_coh_qp0[o_cut[r] + i] = m.cut_coh_qp0[i] + qo;
+        }
+        for (size_t i = 0; i < m.cut_enr.size(); ++i) out.cut_enr[o_cenr[r] + i] = m.cut_enr[i] >= 0 ? m.cut_enr[i] + no : -1;
+        for (size_t i = 0; i < m.cut_child_mat.size(); ++i)
+            out.cut_child_mat[o_cchm[r] + i] = m.cut_child_mat[i] >= 0 ? m.cut_child_mat[i] + mo : -1;
+        std::copy(m.cut_coh_mat.begin(), m.cut_coh_mat.end(), out.cut_coh_mat.begin() + o_ccoh[r]);
+        std::copy(m.fixed.begin(), m.fixed.end(), out.fixed.begin() + o_fix[r]);
+        std::copy(m.ubar.begin(), m.ubar.end(), out.ubar.begin() + o_fix[r]);
+        for (size_t i = 1; i < m.row_ptr.size(); ++i) out.row_ptr[no + i] = m.row_ptr[i] + bo;
+        for (size_t i = 0; i < m.col.size(); ++i) out.col[o_col[r] + i] = m.col[i] + no;
+        for (size_t i = 0; i < m.diag_slot.size(); ++i) out.diag_slot[o_diag[r] + i] = m.diag_slot[i] + bo;
+        for (size_t i = 1; i < m.ne_ptr.size(); ++i) out.ne_ptr[no + i] = m.ne_ptr[i] + ko;
+        for (size_t i = 0; i < m.ne_list.size(); ++i) {
+            const int v = m.ne_list[i];
+            out.ne_list[o_nel[r] + i] = (((v >> 2) + eo) << 2) | (v & 3);
+        }
+        for (size_t i = 0; i < m.cut_slot.size(); ++i) out.cut_slot[o_slot[r] + i] = m.cut_slot[i] >= 0 ? m.cut_slot[i] + bo : -1;
+    });
+    out.spec = M(0).spec;
     out.spec.materials.clear();
     out.spec.inclusions.clear();
     out.spec.nx = out.spec.ny = 0;
@@ -676,36 +750,13 @@ void merge_meshes(const std::vector<HostMesh>& ms, HostMesh& out, std::vector<in
     out.n_elem = eoff[R];
     out.n_cut = coff[R];
     out.n_coh_qp = qoff[R];
-    out.row_ptr.assign(1, 0);
-    out.ne_ptr.assign(1, 0);
     for (int r = 0; r < R; ++r) {
-        const HostMesh& m = ms[r];
-        const int no = noff[r], eo = eoff[r], mo = moff[r], co = coff[r], bo = boff[r], qo = qoff[r], ko = koff[r];
+        const HostMesh& m = M(r);
         out.spec.materials.insert(out.spec.materials.end(), m.spec.materials.begin(), m.spec.materials.end());
-        out.x.insert(out.x.end(), m.x.begin(), m.x.end());
-        out.y.insert(out.y.end(), m.y.begin(), m.y.end());
-        for (int v : m.conn) out.conn.push_back(v + no);
-        for (int v : m.elem_mat) out.elem_mat.push_back(v + mo);
-        for (int v : m.elem_cut) out.elem_cut.push_back(v >= 0 ? v + co : -1);
-        for (int v : m.cut_elem) out.cut_elem.push_back(v + eo);
-        out.cut_tmpl.insert(out.cut_tmpl.end(), m.cut_tmpl.begin(), m.cut_tmpl.end());
-        for (int v : m.cut_enr) out.cut_enr.push_back(v >= 0 ? v + no : -1);
-        for (int v : m.cut_child_mat) out.cut_child_mat.push_back(v >= 0 ? v + mo : -1);
-        out.cut_coh_mat.insert(out.cut_coh_mat.end(), m.cut_coh_mat.begin(), m.cut_coh_mat.end());
-        for (int v : m.cut_coh_qp0) out.cut_coh_qp0.push_back(v + qo);
-        out.fixed.insert(out.fixed.end(), m.fixed.begin(), m.fixed.end());
-        out.ubar.insert(out.ubar.end(), m.ubar.begin(), m.ubar.end());
-        for (size_t i = 1; i < m.row_ptr.size(); ++i) out.row_ptr.push_back(m.row_ptr[i] + bo);
-        for (int v : m.col) out.col.push_back(v + no);
-        for (int v : m.diag_slot) out.diag_slot.push_back(v + bo);
-        for (size_t i = 1; i < m.ne_ptr.size(); ++i) out.ne_ptr.push_back(m.ne_ptr[i] + ko);
-        for (int v : m.ne_list) out.ne_list.push_back((((v >> 2) + eo) << 2) | (v & 3));
-        for (int v : m.cut_slot) out.cut_slot.push_back(v >= 0 ? v + bo : -1);
         out.n_free += m.n_free;
-        for (const auto& gb : m.grids) out.grids.push_back({gb.nx, gb.ny, gb.node_off + no, gb.elem_off + eo, gb.n_reg});
+        for (const auto& gb : m.grids)
+            out.grids.push_back({gb.nx, gb.ny, gb.node_off + noff[r], gb.elem_off + eoff[r], gb.n_reg});
     }
-    out.x.resize(out.n_reg);
-    out.y.resize(out.n_reg);
 }
 
 // Builds the union hierarchy (structure once per batch).
@@ -718,7 +769,7 @@ int batch_mg_build(pg_batch& B) {
     // per-RVE grid sizes per depth
     std::vector<std::vector<std::pair<int, int>>> dims(R);
     for (int r = 0; r < R; ++r) {
-        int nx = B.meshes[r].spec.nx, ny = B.meshes[r].spec.ny;
+        int nx = B.grid[r].first, ny = B.grid[r].second;
         dims[r].push_back({nx, ny});
         while ((nx > kBCoarseCells || ny > kBCoarseCells) && (int)dims[r].size() <= kBMaxDepth) {
             nx = (nx + 1) / 2;
@@ -977,10 +1028,10 @@ int pg_batch_create(const pg_mesh* const* meshes, int32_t n_rve, int32_t device,
     auto now = [] { return std::chrono::steady_clock::now(); };
     auto secs = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
     auto t0 = now();
-    for (int r = 0; r < n_rve; ++r) B->meshes.push_back(meshes[r]->m);
+    for (int r = 0; r < n_rve; ++r) B->grid.push_back({meshes[r]->m.spec.nx, meshes[r]->m.spec.ny});
     auto t1 = now();
     HostMesh merged;
-    merge_meshes(B->meshes, merged, B->noff, B->eoff);
+    merge_meshes(meshes, n_rve, merged, B->noff, B->eoff);
     auto t2 = now();
     int rc = ctx_create(std::move(merged), device, B->ctx.c);
     auto t3 = now();

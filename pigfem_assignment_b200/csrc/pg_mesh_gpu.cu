@@ -97,15 +97,20 @@ __global__ void k_scan_add(int* v, long long n, const int* bs) {
 }
 
 // Scratch owned by one device build: freed on every exit path.
+// Scratch of one build, stream-ordered on the build's stream: many builds
+// on host threads then run side by side (a plain cudaFree would synchronise
+// the whole device at the end of each).
 struct DevScratch {
+    cudaStream_t s;
     std::vector<void*> owned;
+    explicit DevScratch(cudaStream_t st) : s(st) {}
     ~DevScratch() {
-        for (void* p : owned) cudaFree(p);
+        for (void* p : owned) cudaFreeAsync(p, s);
     }
     template <typename T>
     cudaError_t alloc(T** p, size_t n) {
         *p = nullptr;
-        const cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(1, n) * sizeof(T));
+        const cudaError_t e = cudaMallocAsync((void**)p, std::max<size_t>(1, n) * sizeof(T), s);
         if (e == cudaSuccess) owned.push_back(*p);
         return e;
     }
@@ -817,7 +822,7 @@ int build_mesh_device(const RveSpec& spec, int device, HostMesh& m) {
         cudaStream_t s;
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
-    DevScratch S;
+    DevScratch S(s);
 
     GridDesc g;
     g.nx = nx;
@@ -1027,7 +1032,7 @@ namespace pgb {
 // cut_nodes, cut_slot_ptr and cut_slot; node_enr flags the enrichment nodes.
 int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entries) {
     cudaStream_t s = c.stream;
-    DevScratch S;
+    DevScratch S(s);
     const int nc = c.n_cut;
     const long long nbk = c.n_blocks, nn = c.n_nodes;
     uint8_t *enr, *cutK, *cutF;

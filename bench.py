@@ -52,11 +52,19 @@ def parse():
     ap.add_argument("--tile", type=int, choices=[32, 64, 128, 256], default=None,
                     help="fix the triangle kernel's launch shape after any autotuning (32 / 64 node rows: "
                          "the gather kernel; 128 / 256: threads per CTA of the structured-grid kernel)")
+    ap.add_argument("--persistent", type=int, choices=[0, 1], default=None,
+                    help="with --tile: one CTA per tile (0) or the persistent kernel (1)")
     ap.add_argument("--batch-rves", type=int, default=512)
     ap.add_argument("--no-sensitivity", action="store_true")
     ap.add_argument("--profile-range", choices=["load_step"], default=None,
                     help="bracket the timed FP64 multigrid solve of the load step with cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off)")
+    ap.add_argument("--profile-case", choices=["asm512", "asm1024", "mlp", "newton"], default=None,
+                    help="run one small fixed workload for an ncu capture and exit (no JSON line)")
+    ap.add_argument("--full-configs", action="store_true",
+                    help="also run configurations 2 (50 steps) and 4 (1024^2, 20 steps) in full, every arm")
+    ap.add_argument("--train-rves", type=int, default=3,
+                    help="RVEs whose first 25 steps train the learned predictor")
     ap.add_argument("--viscosity", type=float, default=200.0,
                     help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
     return ap.parse_args()
@@ -299,9 +307,11 @@ def run_b200_arm(args):
     t_tile, t_pers, t_warps = C.c_int32(), C.c_int32(), C.c_int32()
     _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
     if args.tile is not None:
-        _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, args.tile, t_pers.value, t_warps.value))
+        pers = t_pers.value if args.persistent is None else args.persistent
+        _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, args.tile, pers, t_warps.value))
         _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
-    tri_kernel = "k_grid_rows" if t_tile.value in (128, 256) else "k_assemble_tri"
+    tri_kernel = (("k_grid_rows_pipe" if t_pers.value else "k_grid_rows") if t_tile.value in (128, 256)
+                  else "k_assemble_tri")
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
               "ms_tri_rows32_rows32p_rows64_rows64p_grid": [round(v, 4) for v in ms_tri],
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
@@ -405,10 +415,18 @@ def run_b200_arm(args):
     coh = None
     # the secondary measurements run on one GPU only (the scaling runs time the assembly alone)
     if not args.no_cohesive and not args.no_load_step and world == 1:
+        keep = [] if args.full_configs else None
         try:
-            coh = cohesive_load_steps(local, args.viscosity)
+            coh = cohesive_load_steps(local, args.viscosity, n_train=args.train_rves, keep_mlp=keep)
         except Exception as ex:  # reported, never fatal for the assembly line
             coh = {"status": f"failed: {ex}"}
+        if args.full_configs:
+            try:
+                coh["full_configs"] = full_cohesive_configs(local, args.viscosity, keep[0] if keep else None)
+            except Exception as ex:
+                coh["full_configs"] = {"status": f"failed: {ex}"}
+            for m in keep or []:
+                m.close()
 
     # ---- batched uneven RVEs (configuration 3) ----
     batch = None
@@ -472,7 +490,8 @@ def run_b200_arm(args):
 
 
 
-def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: int = 25, t_window=(0.5, 0.6)):
+def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: int = 25, t_window=(0.5, 0.6),
+                        keep_mlp=None):
     """Time per cohesive load step at 1e-8 relative Newton residual on the
     256x256 RVE (131,072 TRI3, 40 seeded circles r ~ U[0.03, 0.06], bilinear
     cohesive interfaces, 2% strain in 50 equal steps).  Every arm must reach
@@ -561,7 +580,10 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
         if pred == _lib.PG_PREDICT_LEARNED:
             _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, None))
     prob.ctx.close()
-    mlp.close()
+    if keep_mlp is not None:
+        keep_mlp.append(mlp)  # the caller closes it
+    else:
+        mlp.close()
     out["config"] = ("config2: 256x256 TRI3 (131,072 elements), 40 RSA circles r~U[0.03,0.06] gap>=0.01 seed 2, "
                      f"bilinear law sigma_c 30 MPa, G_c 0.01 N/mm, K_p 1e6 MPa/mm, viscosity {eta} MPa s/mm, "
                      f"2% strain in 50 steps, timed window of load fractions {t_window[0]}-{t_window[1]}; "
@@ -570,6 +592,77 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
                        "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
     if out["plain_fp64"]["status"] == "ok" and out["mixed_learned"]["status"] == "ok":
         out["speedup_mixed_learned"] = out["plain_fp64"]["ms_per_load_step"] / out["mixed_learned"]["ms_per_load_step"]
+    return out
+
+
+def run_cohesive_arms(rve, n_steps: int, arms, local: int, mlp=None, max_records: int = 4096):
+    """Load-steps `rve` from zero to full load once per arm (name, precision,
+    predictor) with the multigrid-preconditioned Newton at 1e-8 of the
+    zeroth-order residual, and reports each arm's totals: device-clocked
+    seconds summed over the load steps (failed attempts included), Newton and
+    Krylov iterations, step repeats, CG breakdowns answered by GMRES."""
+    import ctypes as C
+
+    import pigfem_assignment_b200.problem as pb
+    from pigfem_assignment_b200 import _lib
+
+    newton = dict(precond=_lib.PG_PREC_MG, stol=0.0, rtol_base=_lib.PG_RTOL_BASE_ZEROTH, lin_max_iter=1000)
+    out = {}
+    for name, prec, pred in arms:
+        if pred == _lib.PG_PREDICT_LEARNED and mlp is None:
+            continue
+        prob = pb.ProblemNonlinearStructural(rve, device=local)
+        prob.init()
+        prob.configure(n_steps=n_steps, T_final=1.0, t_start=0.0, t_stop=1.0, precision=prec, predictor=pred,
+                       **newton)
+        if pred == _lib.PG_PREDICT_LEARNED:
+            _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, mlp.handle))
+        recs = (_lib.StepStats * max_records)()
+        n = C.c_int32()
+        t0 = time.perf_counter()
+        rc = _lib.lib.pg_solve_nonlinear(prob.ctx.handle, C.byref(prob.cfg), recs, max_records, C.byref(n))
+        wall = time.perf_counter() - t0
+        R = recs[:min(n.value, max_records)]
+        dev_s = float(sum(r.seconds for r in R))
+        out[name] = {
+            "status": "ok" if rc == 0 else _lib.lib.pg_last_error().decode(),
+            "load_steps": len(R), "t_reached": R[-1].t_frac if R else 0.0,
+            "seconds": dev_s, "wall_seconds": wall,
+            "ms_per_load_step": 1e3 * dev_s / max(1, n_steps),
+            "newton_iterations": int(sum(r.newton_its for r in R)),
+            "krylov_iterations": int(sum(r.krylov_its for r in R)),
+            "repeated_steps": int(sum(1 for r in R if r.repeats > 1)),
+            "gmres_fallbacks": int(sum(r.gmres_fallbacks for r in R)),
+            "learned_used": int(sum(1 for r in R if r.predictor_used == _lib.PG_PREDICT_LEARNED)),
+        }
+        if pred == _lib.PG_PREDICT_LEARNED:
+            _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, None))
+        prob.ctx.close()
+    return out
+
+
+def full_cohesive_configs(local: int, eta: float, mlp=None):
+    """Configurations 2 and 4 as stated, every load step: configuration 2
+    (256^2, 40 circles, 50 steps to 2%) and configuration 4 (1024^2, 400
+    circles, 20 steps to 1%), bilinear law with viscosity `eta`; arms: the
+    reference's zeroth-order predictor in FP64, the linear extrapolation in
+    FP64 and with the FP32 V-cycle, and the learned predictor with the FP32
+    V-cycle (when a network is given)."""
+    import dataclasses
+
+    from pigfem_assignment_b200 import _lib
+    from pigfem_assignment_b200.rve import config2, config4
+
+    def with_eta(rve):
+        return dataclasses.replace(rve, coh_params=tuple(rve.coh_params[:4]) + (eta,))
+
+    arms = (("plain_fp64_zeroth", _lib.PG_PRECISION_FP64, _lib.PG_PREDICT_ZEROTH),
+            ("plain_fp64_linear", _lib.PG_PRECISION_FP64, _lib.PG_PREDICT_LINEAR),
+            ("mixed_linear", _lib.PG_PRECISION_MIXED, _lib.PG_PREDICT_LINEAR),
+            ("mixed_learned", _lib.PG_PRECISION_MIXED, _lib.PG_PREDICT_LEARNED))
+    out = {"viscosity_MPa_s_per_mm": eta}
+    out["config2_50_steps"] = run_cohesive_arms(with_eta(config2()), 50, arms, local, mlp)
+    out["config4_20_steps"] = run_cohesive_arms(with_eta(config4()), 20, arms[1:], local, mlp)
     return out
 
 
@@ -744,8 +837,66 @@ def sensitivity_cfg4(local: int, n_check: int = 8):
             "max_fd_rel_diff": max(c["rel_diff"] for c in checks)}
 
 
+def profile_case(case: str, tile=None, persistent: int = 0) -> None:
+    """Small fixed workloads for ncu captures (no JSON line; prints "ok"):
+      asm512 / asm1024: the configuration-1 circles on a 512^2 / 1024^2 grid,
+                        four linear assembly passes, L2 flushed before each
+                        (write 512 MB, read 256 MB); `tile` / `persistent`
+                        fix the launch shape (default: the context's)
+      mlp:              three forward passes of the warm-start network over
+                        2^20 node rows (16 features)
+      newton:           the first three load steps of configuration 2 (50
+                        steps to 2%, viscosity 200), FP64 multigrid Newton"""
+    import dataclasses
+
+    import torch
+
+    import pigfem_assignment_b200.problem as pb
+    from pigfem_assignment_b200 import _lib
+    from pigfem_assignment_b200.rve import config1, config2, scaled
+
+    if case in ("asm512", "asm1024"):
+        size = 512 if case == "asm512" else 1024
+        rve = config1() if size == 512 else scaled(config1(), size)
+        m = pb.Mesh(rve)
+        ctx = pb.DeviceContext(m)
+        if tile is not None:
+            _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, 4))
+        asm = pb.Assembler(ctx)
+        flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device="cuda:0")
+        for k in range(4):
+            flush.fill_(float(k))
+            flush[: 64 * 1024 * 1024].sum()
+            torch.cuda.synchronize()
+            asm.assemble_linear()
+            ctx.sync()
+        ctx.close()
+    elif case == "mlp":
+        from pigfem_assignment_b200.learned import MLP
+        mlp = MLP(device=0, seed=1)
+        X = torch.randn(1 << 20, 16, device="cuda:0", dtype=torch.float32)
+        for _ in range(3):
+            mlp.forward(X)
+        torch.cuda.synchronize()
+        mlp.close()
+    elif case == "newton":
+        rve = config2()
+        rve = dataclasses.replace(rve, coh_params=tuple(rve.coh_params[:4]) + (200.0,))
+        prob = pb.ProblemNonlinearStructural(rve)
+        prob.init()
+        prob.configure(n_steps=50, T_final=1.0, t_start=0.0, t_stop=0.06, precision=_lib.PG_PRECISION_FP64,
+                       predictor=_lib.PG_PREDICT_LINEAR, precond=_lib.PG_PREC_MG, stol=0.0,
+                       rtol_base=_lib.PG_RTOL_BASE_ZEROTH, lin_max_iter=1000)
+        prob.solve_problem()
+        prob.ctx.close()
+    print("ok", case)
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args.profile_case, args.tile, args.persistent or 0)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

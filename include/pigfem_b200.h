@@ -295,15 +295,30 @@ int pg_mlp_train(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n, i
  * the network and the device stay usable. */
 int pg_mlp_wait_selftest(pg_mlp* m, int32_t polls);
 
-/* Learned-predictor plumbing (device pointers).  s_inc = prescribed displacement
- * increment of the step, ratio = dt_{n+1}/dt_n.  Features: 16 floats per node;
- * targets and outputs: 2 floats per node (one per DOF). */
-int pg_predictor_features(pg_ctx* c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc,
-                          float* X_dev);
-int pg_predictor_targets(pg_ctx* c, const double* Un1, const double* Un, const double* Unm1, double ratio,
-                         double s_inc, float* T_dev);
-int pg_predictor_apply(pg_ctx* c, const double* Un, const double* Unm1, double ratio, double s_inc,
-                       const float* Y_dev, double* U_dev);
+/* Learned-predictor plumbing (device pointers).  The history of a step: the
+ * converged states at t_n, t_{n-1}, t_{n-2}, the steps dt_n and dt_{n-1} that
+ * led to the first two, the coming step dt, the load fraction at t_n + dt and
+ * the step's prescribed displacement increment.  The prediction is
+ *   U = U_n + (dt/dt_n) d_n + (1 + y) c,  d_n = U_n - U_{n-1},
+ *   c = dt (dt + dt_n) / (dt_n + dt_{n-1}) (d_n/dt_n - d_{n-1}/dt_{n-1})
+ * per node, y the network's output clamped to [-1, 0] (y = 0: quadratic
+ * extrapolation, y = -1: linear).  Features: 16 floats per node; targets and
+ * outputs: 2 floats per node (both y). */
+typedef struct pg_pred_history {
+    const double* U_n;
+    const double* U_nm1;
+    const double* U_nm2;
+    const double* isv_nm1;          /* committed delta_max at t_{n-1} (NULL: no damage-rate feature); the
+                                       context's committed state is taken as t_n's */
+    double dt_n, dt_nm1, dt;
+    double t_frac;
+    double s_inc;
+} pg_pred_history;
+int pg_predictor_features(pg_ctx* c, const pg_pred_history* h, float* X_dev);
+/* targets of the step that reached U_np1 (training data) */
+int pg_predictor_targets(pg_ctx* c, const pg_pred_history* h, const double* U_np1, float* T_dev);
+/* U_dev (free DOFs) = the prediction with (1 + y) scaled by `scale` (Y_dev NULL: the linear extrapolation) */
+int pg_predictor_apply(pg_ctx* c, const pg_pred_history* h, const float* Y_dev, double scale, double* U_dev);
 /* attaches a network for PG_PREDICT_LEARNED (NULL detaches; the context does not own it) */
 int pg_ctx_attach_mlp(pg_ctx* c, pg_mlp* m);
 
@@ -351,15 +366,17 @@ int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double
  * `reps` launches each) and keeps the fastest of each for later assemblies:
  * ms_tri[5] = the row-tile triangle kernel gathering over 32 / 64 consecutive
  * node rows per CTA, each with one CTA per tile / a persistent grid, then the
- * structured-grid kernel (one thread per regular node row; the faster of 128
- * and 256 threads per CTA; 0 if the mesh is not one structured grid);
+ * structured-grid kernel (one thread per regular node row; the fastest of 128
+ * and 256 threads per CTA, each with one CTA per tile or a persistent grid
+ * that stages the next tile with asynchronous copies while forming the
+ * current one; 0 if the mesh is not made of structured grids);
  * ms_cut[3] = the cut elements' work (quadrature rows, cohesive points, pair
  * blocks, fold) with 2 / 4 / 8 warps per CTA of the pair kernel (NULL
  * allowed).  K is left to be reassembled. */
 int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
 /* the launch shapes in use, and setting them by hand (tile 32 or 64 node rows per CTA of the
  * row-tile kernel, or 128 / 256 threads per CTA of the structured-grid kernel; persistent 0/1
- * for the row tiles; warps 2/4/8 per CTA of the cut elements' pair kernel) */
+ * for either; warps 2/4/8 per CTA of the cut elements' pair kernel) */
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
 int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
 

@@ -102,6 +102,15 @@ class StepStats(C.Structure):
     ]
 
 
+class PredHistory(C.Structure):
+    """pg_pred_history: device pointers of the last three converged states
+    and of the committed delta_max one step back, the step lengths, the load
+    fraction and the prescribed increment of the coming step."""
+    _fields_ = [("U_n", C.c_void_p), ("U_nm1", C.c_void_p), ("U_nm2", C.c_void_p), ("isv_nm1", C.c_void_p),
+                ("dt_n", C.c_double), ("dt_nm1", C.c_double), ("dt", C.c_double), ("t_frac", C.c_double),
+                ("s_inc", C.c_double)]
+
+
 class PgError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[pg status {code}] {msg}")
@@ -174,9 +183,9 @@ def _load() -> C.CDLL:
         "pg_mlp_adam": ([v, C.c_float], C.c_int),
         "pg_mlp_train": ([v, v, v, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_double)], C.c_int),
         "pg_mlp_wait_selftest": ([v, C.c_int32], C.c_int),
-        "pg_predictor_features": ([v, v, v, C.c_double, C.c_double, C.c_double, v], C.c_int),
-        "pg_predictor_targets": ([v, v, v, v, C.c_double, C.c_double, v], C.c_int),
-        "pg_predictor_apply": ([v, v, v, C.c_double, C.c_double, v, v], C.c_int),
+        "pg_predictor_features": ([v, C.POINTER(PredHistory), v], C.c_int),
+        "pg_predictor_targets": ([v, C.POINTER(PredHistory), v, v], C.c_int),
+        "pg_predictor_apply": ([v, C.POINTER(PredHistory), v, C.c_double, v], C.c_int),
         "pg_ctx_attach_mlp": ([v, v], C.c_int),
         "pg_last_error": ([], C.c_char_p),
         "pg_version": ([], C.c_char_p),

@@ -604,42 +604,48 @@ __device__ __forceinline__ void cut_point_row(const CutPoint& P, const double* _
 // record follows the last point, holding only the rows' total length.
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
                       const std::vector<long long>& roff, const int* class_off, std::vector<int>& out) {
-    out.clear();
+    // each element's records have a fixed place (the prefix of the points
+    // before it), so the elements fill them in parallel
+    const int nc = (int)tmpl.size();
+    std::vector<long long> rec0(nc + 1, 0);
+    std::vector<int> cls(nc, 0);
     for (int k = 0; k < kCutClasses; ++k)
-        for (int oi = class_off[k]; oi < class_off[k + 1]; ++oi) {
-            const CutTemplate& T = cut_template(tmpl[oi]);
-            const int* en = &nodes[(size_t)kCutNodeStride * oi];
-            const int nq_e = device_point_count(tmpl[oi]);
-            int l = 0;
-            for (int ch = 0; ch < T.n_child; ++ch) {
-                const int nc = T.child_n[ch];
-                const int type = nc == 3 ? kChildTri3 : nc == 4 ? kChildQuad4 : nc == 5 ? kChildPoly5 : kChildPoly6;
-                int lnp = 0;
-                for (int c = 0; c < nc; ++c) lnp |= T.child_nodes[ch][c] << (4 * c);
-                for (int q = 0; q < device_child_nq(type); ++q, ++l) {
-                    int r[kCutPointInts] = {};
-                    for (int c = 0; c < kMaxChildNodes; ++c) r[c] = en[c < nc ? T.child_nodes[ch][c] : 0];
-                    r[6] = en[0];
-                    r[7] = en[1];
-                    r[8] = en[2];
-                    r[9] = chm[(size_t)kMaxChildren * oi + ch];
-                    r[10] = lnp;
-                    r[11] = q | (type << 8) | (nc << 10) | ((3 + T.n_enr) << 13);
-                    const long long off = roff[oi] + (long long)l * (4 + 2 * kCutClassNl[k]);
-                    r[12] = (int)(unsigned)(off & 0xffffffffLL);
-                    r[13] = (int)(off >> 32);
-                    r[14] = nq_e;
-                    r[15] = l;
-                    out.insert(out.end(), r, r + kCutPointInts);
-                }
+        for (int oi = class_off[k]; oi < class_off[k + 1]; ++oi) cls[oi] = k;
+    for (int oi = 0; oi < nc; ++oi) rec0[oi + 1] = rec0[oi] + device_point_count(tmpl[oi]);
+    out.assign((size_t)(rec0[nc] + 1) * kCutPointInts, 0);
+    parallel_for(nc, 2048, [&](long long oi) {
+        const int k = cls[oi];
+        const CutTemplate& T = cut_template(tmpl[oi]);
+        const int* en = &nodes[(size_t)kCutNodeStride * oi];
+        const int nq_e = device_point_count(tmpl[oi]);
+        int* r = &out[(size_t)rec0[oi] * kCutPointInts];
+        int l = 0;
+        for (int ch = 0; ch < T.n_child; ++ch) {
+            const int nc_ = T.child_n[ch];
+            const int type = nc_ == 3 ? kChildTri3 : nc_ == 4 ? kChildQuad4 : nc_ == 5 ? kChildPoly5 : kChildPoly6;
+            int lnp = 0;
+            for (int c = 0; c < nc_; ++c) lnp |= T.child_nodes[ch][c] << (4 * c);
+            for (int q = 0; q < device_child_nq(type); ++q, ++l, r += kCutPointInts) {
+                for (int c = 0; c < kMaxChildNodes; ++c) r[c] = en[c < nc_ ? T.child_nodes[ch][c] : 0];
+                r[6] = en[0];
+                r[7] = en[1];
+                r[8] = en[2];
+                r[9] = chm[(size_t)kMaxChildren * oi + ch];
+                r[10] = lnp;
+                r[11] = q | (type << 8) | (nc_ << 10) | ((3 + T.n_enr) << 13);
+                const long long off = roff[oi] + (long long)l * (4 + 2 * kCutClassNl[k]);
+                r[12] = (int)(unsigned)(off & 0xffffffffLL);
+                r[13] = (int)(off >> 32);
+                r[14] = nq_e;
+                r[15] = l;
             }
         }
+    });
     // sentinel after the last point: its row offset is the rows' total length
-    int r[kCutPointInts] = {};
+    int* r = &out[(size_t)rec0[nc] * kCutPointInts];
     const long long total = roff.back();
     r[12] = (int)(unsigned)(total & 0xffffffffLL);
     r[13] = (int)(total >> 32);
-    out.insert(out.end(), r, r + kCutPointInts);
 }
 
 // ---------------------------------------------------------------------------
@@ -940,6 +946,95 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs
     else grid_node<1, WK, WF>(a, B, gi, gj, lx, ly, sXY, sU, sM);
 }
 
+// Asynchronous copies into shared memory (cp.async, Ampere and later): an
+// 8-byte copy, zero-filled when `valid` is false (the source address is then
+// only a placeholder and is not read: src-size 0).
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The staged window of one tile (k_grid_rows_pipe): coordinates as (x, y)
+// pairs, displacements, cell materials.
+template <int TR, bool WF>
+struct GridWin {
+    double2 xy[kGridWinX * (TR + 2)];
+    double2 u[WF ? kGridWinX * (TR + 2) : 1];
+    int2 m[kGridCellX * (TR + 1)];
+};
+
+// Issues the copies of tile t's window into W (every thread its share).
+template <int TR, bool WF>
+__device__ __forceinline__ void grid_stage_async(const GridArgs& a, int t, GridWin<TR, WF>& W) {
+    constexpr int kThreads = kGridTileC * TR, kWinY = TR + 2, kCellY = TR + 1;
+    const int4 T = __ldg(&a.tiles[t]);
+    const int4 B = __ldg(&a.rves[T.x]);
+    const int nx = B.x, ny = B.y, NX1 = nx + 1;
+    for (int i = threadIdx.x; i < kGridWinX * kWinY; i += kThreads) {
+        const int gi = T.y - 1 + i % kGridWinX, gj = T.z - 1 + i / kGridWinX;
+        const bool in = gi >= 0 && gi <= nx && gj >= 0 && gj <= ny;
+        const size_t n = in ? (size_t)B.z + gi + (size_t)gj * NX1 : 0;
+        cp_async8(&W.xy[i].x, a.x + n, in);
+        cp_async8(&W.xy[i].y, a.y + n, in);
+        if (WF) {
+            cp_async8(&W.u[i].x, a.u + 2 * n, in);
+            cp_async8(&W.u[i].y, a.u + 2 * n + 1, in);
+        }
+    }
+    for (int i = threadIdx.x; i < kGridCellX * kCellY; i += kThreads) {
+        const int ci = T.y - 1 + i % kGridCellX, cj = T.z - 1 + i / kGridCellX;
+        const bool in = ci >= 0 && ci < nx && cj >= 0 && cj < ny;
+        const size_t k = in ? (size_t)B.w / 2 + ci + (size_t)cj * nx : 0;
+        cp_async8(&W.m[i], reinterpret_cast<const int2*>(a.emat) + k, in);
+    }
+}
+
+// Persistent variant of k_grid_rows: each CTA walks the tile table with a
+// stride of the grid, and copies the next tile's window into the second of
+// two shared-memory buffers (cp.async) while its threads form the rows of
+// the current one, so that the staging latency overlaps the arithmetic
+// instead of idling the SM.  Out-of-grid window entries are zero-filled
+// (materials: out-of-grid cells read as material 0 from the fill, so they
+// are set to -1 after the copy lands).
+template <bool WK, bool WF, int TR>
+__global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows_pipe(GridArgs a, int n_tiles) {
+    __shared__ GridWin<TR, WF> W[2];
+    int t = blockIdx.x;
+    if (t >= n_tiles) return;
+    grid_stage_async<TR, WF>(a, t, W[0]);
+    cp_async_commit();
+    for (int k = 0; t < n_tiles; t += gridDim.x, ++k) {
+        GridWin<TR, WF>& cur = W[k & 1];
+        const int tn = t + gridDim.x;
+        if (tn < n_tiles) grid_stage_async<TR, WF>(a, tn, W[(k + 1) & 1]);
+        cp_async_commit();  // (an empty group when nothing was issued)
+        cp_async_wait_one();  // the current tile's copies have landed
+        const int4 T = __ldg(&a.tiles[t]);
+        const int4 B = __ldg(&a.rves[T.x]);
+        const int nx = B.x, ny = B.y;
+        // cells outside the grid are no triangles
+        for (int i = threadIdx.x; i < kGridCellX * (TR + 1); i += kGridTileC * TR) {
+            const int ci = T.y - 1 + i % kGridCellX, cj = T.z - 1 + i / kGridCellX;
+            if (!(ci >= 0 && ci < nx && cj >= 0 && cj < ny)) cur.m[i] = make_int2(-1, -1);
+        }
+        __syncthreads();
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int r = w >> 1, q = w & 1;
+        const int gj = T.z + r;
+        const int gi = T.y + 2 * lane + ((gj + q) & 1);
+        if (gj <= ny && gi <= nx) {
+            const int lx = gi - T.y + 1, ly = r + 1;
+            if (q == 0) grid_node<0, WK, WF>(a, B, gi, gj, lx, ly, cur.xy, cur.u, cur.m);
+            else grid_node<1, WK, WF>(a, B, gi, gj, lx, ly, cur.xy, cur.u, cur.m);
+        }
+        __syncthreads();  // the buffer is refilled two tiles on
+    }
+    cp_async_wait_all();
+}
+
 // True when every regular row of the block pattern is laid out as
 // k_grid_rows assumes: the node's grid neighbours (grid_nbr_mask) and
 // itself in ascending order, then only enrichment columns.
@@ -987,6 +1082,27 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
     ga.tiles = c.grid_tiles[tr == 2 ? 0 : 1];
     const int blocks = c.n_grid_tiles[tr == 2 ? 0 : 1];
     if (blocks == 0) return;
+    if (c.tuning.tri_persistent) {
+        // persistent, pipelined: as many CTAs as fit on the SMs at once
+        int dev = 0, n_sm = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        auto go = [&](auto kern) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGridTileC * tr, 0);
+            const int grid = std::min(blocks, std::max(1, per_sm) * n_sm);
+            kern<<<grid, kGridTileC * tr, 0, s>>>(ga, blocks);
+        };
+        if (tr == 2) {
+            if (want_K && want_f) go(k_grid_rows_pipe<true, true, 2>);
+            else if (want_K) go(k_grid_rows_pipe<true, false, 2>);
+            else if (want_f) go(k_grid_rows_pipe<false, true, 2>);
+        } else {
+            if (want_K && want_f) go(k_grid_rows_pipe<true, true, 4>);
+            else if (want_K) go(k_grid_rows_pipe<true, false, 4>);
+            else if (want_f) go(k_grid_rows_pipe<false, true, 4>);
+        }
+        return;
+    }
     if (tr == 2) {
         if (want_K && want_f) k_grid_rows<true, true, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
         else if (want_K) k_grid_rows<true, false, 2><<<blocks, kGridTileC * 2, 0, s>>>(ga);
@@ -1887,8 +2003,8 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
 // flushed before each launch, `reps` launches each, device events) and
 // keeps the fastest of each in c.tuning.  ms_tri: the row-tile kernel with
 // 32 / 64 node rows per CTA, one CTA per tile / persistent (4 values), then
-// the structured-grid kernel (the faster of 128 and 256 threads per CTA; 0
-// without a structured grid); ms_cut: the cut elements' work on one stream
+// the structured-grid kernel (the fastest of 128 and 256 threads per CTA,
+// one CTA per tile or persistent and pipelined; 0 without a structured grid); ms_cut: the cut elements' work on one stream
 // (rows, cohesive points, pairs with their fold) with 2 / 4 / 8 warps per
 // pair CTA.
 // K is left undefined: the next solve reassembles.
@@ -1939,17 +2055,20 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     if (c.grid_emat) {
         c.tuning.tri_grid = 1;
         float ms_grid = 0.f;
-        for (int bs : {128, 256}) {
-            c.tuning.grid_block = bs;
-            const RowArgs ra = row_args(c, c.U, false, true);
-            const float ms = timed([&] { launch_tri(c, ra, false, s); });
-            if (ms_grid == 0.f || ms < ms_grid) ms_grid = ms;
-            if (ms < best_tri) {
-                best_tri = ms;
-                best.tri_grid = 1;
-                best.grid_block = bs;
+        for (int bs : {128, 256})
+            for (int p = 0; p < 2; ++p) {
+                c.tuning.grid_block = bs;
+                c.tuning.tri_persistent = p;  // 1: the persistent, pipelined grid kernel
+                const RowArgs ra = row_args(c, c.U, false, true);
+                const float ms = timed([&] { launch_tri(c, ra, false, s); });
+                if (ms_grid == 0.f || ms < ms_grid) ms_grid = ms;
+                if (ms < best_tri) {
+                    best_tri = ms;
+                    best.tri_grid = 1;
+                    best.grid_block = bs;
+                    best.tri_persistent = p;
+                }
             }
-        }
         if (ms_tri) ms_tri[4] = ms_grid;
     } else if (ms_tri) {
         ms_tri[4] = 0.f;

@@ -20,9 +20,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <sys/mman.h>
 #include <vector>
-#include <thread>
-#include <atomic>
 
 #include "pg_solve_kernels.cuh"
 #include "pigfem_b200.h"
@@ -653,19 +652,6 @@ struct pg_batch {
 namespace pgb {
 namespace {
 
-// Runs fn(r) for every RVE r on the host's cores.
-template <class F>
-void for_each_rve(int R, F&& fn) {
-    const int T = (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
-    std::atomic<int> next{0};
-    std::vector<std::thread> pool;
-    for (int t = 0; t < std::min(T, R); ++t)
-        pool.emplace_back([&] {
-            for (int r; (r = next.fetch_add(1)) < R;) fn(r);
-        });
-    for (auto& th : pool) th.join();
-}
-
 // Concatenates the RVE meshes into one block-diagonal mesh: every array's
 // place per RVE first (prefix sums of the sizes), then the RVEs copied and
 // renumbered in parallel, each into its own range.
@@ -685,9 +671,18 @@ void merge_meshes(const pg_mesh* const* ms, int R, HostMesh& out, std::vector<in
         koff[r + 1] = koff[r] + (int)M(r).ne_list.size();
     }
     // the place of each RVE's part of one array, and the array sized to all
+    // (its pages backed by huge pages where the host allows it: sizing a
+    // multi-GB array otherwise costs a page fault per 4 KB)
     auto place = [&](auto field, auto& dst) {
         std::vector<size_t> o(R + 1, 0);
         for (int r = 0; r < R; ++r) o[r + 1] = o[r] + (M(r).*field).size();
+        dst.reserve(o[R]);
+        const size_t bytes = o[R] * sizeof(dst[0]);
+        if (bytes >= (8u << 20)) {
+            const uintptr_t a = (reinterpret_cast<uintptr_t>(dst.data()) + 4095) & ~uintptr_t(4095);
+            const uintptr_t e = reinterpret_cast<uintptr_t>(dst.data()) + bytes;
+            if (e > a) madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+        }
         dst.resize(o[R]);
         return o;
     };
@@ -710,7 +705,8 @@ void merge_meshes(const pg_mesh* const* ms, int R, HostMesh& out, std::vector<in
     const auto o_slot = place(&HostMesh::cut_slot, out.cut_slot);
     out.row_ptr.assign((size_t)noff[R] + 1, 0);
     out.ne_ptr.assign((size_t)noff[R] + 1, 0);
-    for_each_rve(R, [&](int r) {
+    parallel_for(R, 1, [&](long long rr) {
+        const int r = (int)rr;
         const HostMesh& m = M(r);
         const int no = noff[r], eo = eoff[r], mo = moff[r], co = coff[r], bo = boff[r], qo = qoff[r], ko = koff[r];
         std::copy(m.x.begin(), m.x.end(), out.x.begin() + o_x[r]);

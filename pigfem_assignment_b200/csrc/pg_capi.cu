@@ -58,7 +58,7 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 
 void free_ctx(Ctx& c) {
     mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.Uold2, c.isv_prev, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
                     c.grid_rves, c.grid_tiles[0], c.grid_tiles[1], c.qp_off, c.qp_elem_cut, c.qp_cut_elem,
                     c.qp_class_off, c.qp_out,
@@ -204,6 +204,12 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
         std::vector<int> nodes((size_t)kCutNodeStride * nc, -1), tmpl(nc), chm((size_t)kMaxChildren * nc), qp0(nc);
         std::vector<int> sp(nc + 1, 0), sl;
         for (int oi = 0; oi < nc; ++oi) {
+            const int nl = 3 + cut_template(hm.cut_tmpl[order[oi]]).n_enr;
+            sp[oi + 1] = sp[oi] + nl * nl;
+        }
+        sl.resize(sp[nc]);
+        // every element fills its own ranges: in parallel
+        parallel_for(nc, 4096, [&](long long oi) {
             const int ci = order[oi], e = hm.cut_elem[ci];
             const int nl = 3 + cut_template(hm.cut_tmpl[ci]).n_enr;
             for (int v = 0; v < 3; ++v) nodes[(size_t)kCutNodeStride * oi + v] = hm.conn[3 * e + v];
@@ -211,10 +217,10 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
             tmpl[oi] = hm.cut_tmpl[ci];
             for (int k = 0; k < kMaxChildren; ++k) chm[(size_t)kMaxChildren * oi + k] = hm.cut_child_mat[(size_t)ci * kMaxChildren + k];
             qp0[oi] = hm.cut_coh_qp0[ci];
+            int* dst = &sl[sp[oi]];
             for (int a = 0; a < nl; ++a)
-                for (int b = 0; b < nl; ++b) sl.push_back(hm.cut_slot[(size_t)ci * S * S + a * S + b]);
-            sp[oi + 1] = (int)sl.size();
-        }
+                for (int b = 0; b < nl; ++b) *dst++ = hm.cut_slot[(size_t)ci * S * S + a * S + b];
+        });
         if ((rc = dev_upload(&c.cut_nodes, nodes))) return rc;
         if ((rc = dev_upload(&c.cut_tmpl, tmpl))) return rc;
         if ((rc = dev_upload(&c.cut_child_mat, chm))) return rc;
@@ -267,7 +273,8 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
     if ((rc = dev_alloc(&c.F, nd))) return rc;
     if ((rc = dev_alloc(&c.isv_c, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
     if ((rc = dev_alloc(&c.isv_t, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
-    for (double** v : {&c.r, &c.z, &c.p, &c.q, &c.dx, &c.b, &c.res, &c.Ut, &c.Uprev, &c.Uold, &c.xi})
+    if ((rc = dev_alloc(&c.isv_prev, (size_t)std::max(1, hm.n_coh_qp)))) return rc;
+    for (double** v : {&c.r, &c.z, &c.p, &c.q, &c.dx, &c.b, &c.res, &c.Ut, &c.Uprev, &c.Uold, &c.Uold2, &c.xi})
         if ((rc = dev_alloc(v, nd))) return rc;
     if ((rc = dev_alloc(&c.minv, 4 * nn))) return rc;
     if ((rc = dev_alloc(&c.mw, 2 * nd))) return rc;

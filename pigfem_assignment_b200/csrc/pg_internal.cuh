@@ -3,8 +3,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "igfem_host.h"
@@ -15,6 +18,27 @@ struct pg_mesh {
 };
 
 namespace pgb {
+
+// Runs fn(i) for i in [0, n) on the host's cores, in chunks of `grain`
+// consecutive indices (each index exactly once; fn must not throw).
+template <class F>
+void parallel_for(long long n, long long grain, F&& fn) {
+    if (n <= 0) return;
+    const long long chunks = (n + grain - 1) / grain;
+    const int T = (int)std::min<long long>(chunks, std::max(1u, std::min(std::thread::hardware_concurrency(), 32u)));
+    if (T <= 1) {
+        for (long long i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<long long> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; ++t)
+        pool.emplace_back([&] {
+            for (long long ch; (ch = next.fetch_add(1)) < chunks;)
+                for (long long i = ch * grain, e = std::min(n, i + grain); i < e; ++i) fn(i);
+        });
+    for (auto& th : pool) th.join();
+}
 
 // Cohesive law parameters on the device.
 struct DevCohLaw {
@@ -159,6 +183,8 @@ struct Ctx {
     double* Ut = nullptr;              // Newton trial displacement
     double* Uprev = nullptr;           // last converged displacement
     double* Uold = nullptr;            // the one before (linear extrapolation predictor)
+    double* Uold2 = nullptr;           // and the one before that (learned predictor's history)
+    double* isv_prev = nullptr;        // committed delta_max one step back (learned predictor's history)
     double* V = nullptr;               // GMRES basis, (gm + 1) * n_dof, allocated on first use
     int gm = 0;
     double* hbuf = nullptr;            // GMRES multi-dot results (64)
@@ -281,11 +307,9 @@ double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s);
 void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
 
 // learned predictor (pg_predict.cu)
-int launch_features(Ctx& c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc, float* X,
-                    cudaStream_t s);
-// gate: features of the step (k_features) to apply Y only at enrichment and damaged nodes; null: everywhere
-int launch_apply(Ctx& c, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y, double* U,
-                 cudaStream_t s, const float* gate = nullptr);
+int launch_features(Ctx& c, const pg_pred_history& h, float* X, cudaStream_t s);
+// U (free DOFs) = linear extrapolation + scale * Y * curvature term (Y null: linear)
+int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s);
 double predictor_app(const Ctx& c);
 double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s);
 

@@ -29,6 +29,10 @@ namespace {
 
 inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
+// the learned start falls back to the linear one when its residual exceeds
+// the linear start's by more than this factor
+constexpr double kLearnedResidualGuard = 8.0;
+
 // res = mask(F_int) (no external force on free DOFs); returns ||res||^2
 double newton_residual(Ctx& c, const double* U, double dt, cudaStream_t s) {
     cudaMemsetAsync(c.F, 0, (size_t)c.n_dof * sizeof(double), s);
@@ -189,11 +193,14 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
     const int nd = c.n_dof;
     const double dt_nom = cfg.T_final / cfg.n_steps;
     const double t_end = cfg.t_stop * cfg.T_final;
-    double t = cfg.t_start * cfg.T_final, dt = std::min(dt_nom, t_end - t), dt_prev = dt_nom;
+    double t = cfg.t_start * cfg.T_final, dt = std::min(dt_nom, t_end - t), dt_prev = dt_nom, dt_prev2 = dt_nom;
     int nrec = 0;
-    // the previous converged state for predictors / repeats
+    // the previous converged states for predictors / repeats
     cudaMemcpyAsync(c.Uprev, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(c.Uold, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(c.Uold2, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (c.n_coh_qp > 0)
+        cudaMemcpyAsync(c.isv_prev, c.isv_c, (size_t)c.n_coh_qp * sizeof(double), cudaMemcpyDeviceToDevice, s);
     while (t < t_end - 1e-12 * cfg.T_final) {
         int repeat = 0;
         bool converged = false;
@@ -219,41 +226,43 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             }
             int used = PG_PREDICT_ZEROTH;
             double res_lin = -1.0, res_mlp = -1.0;
-            if (cfg.predictor == PG_PREDICT_LINEAR && nrec > 0) {
+            // the learned start needs two steps of history; before that it is the linear one
+            if ((cfg.predictor == PG_PREDICT_LINEAR && nrec > 0) || (cfg.predictor == PG_PREDICT_LEARNED && nrec == 1)) {
                 k_extrapolate<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.U, c.Uold, dt / dt_prev);
                 used = PG_PREDICT_LINEAR;
-            } else if (cfg.predictor == PG_PREDICT_LEARNED && nrec > 0 && c.mlp) {
-                const double ratio = dt / dt_prev;
-                const double s_inc = predictor_app(c) * dt / cfg.T_final;
+            } else if (cfg.predictor == PG_PREDICT_LEARNED && nrec > 1 && c.mlp) {
+                pg_pred_history h{};
+                h.U_n = c.Uprev;
+                h.U_nm1 = c.Uold;
+                h.U_nm2 = c.Uold2;
+                h.isv_nm1 = c.n_coh_qp > 0 ? c.isv_prev : nullptr;
+                h.dt_n = dt_prev;
+                h.dt_nm1 = dt_prev2;
+                h.dt = dt;
+                h.t_frac = tf;
+                h.s_inc = predictor_app(c) * dt / cfg.T_final;
                 // candidate 1: linear extrapolation (into Ut)
                 cudaMemcpyAsync(c.Ut, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
-                launch_apply(c, c.Uprev, c.Uold, ratio, s_inc, nullptr, c.Ut, s);
+                int rc = launch_apply(c, h, nullptr, 0.0, c.Ut, s);
+                if (rc) return rc;
                 k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.Ut);
                 res_lin = std::sqrt(predictor_residual(c, c.Ut, dt, s));
-                // candidate 2: learned correction (into U)
-                int rc = launch_features(c, c.Uprev, c.Uold, tf, ratio, s_inc, c.featX, s);
+                // candidate 2: the network's weighting of the curvature term (into U)
+                rc = launch_features(c, h, c.featX, s);
                 if (rc) return rc;
                 rc = pg_mlp_forward(c.mlp, c.featX, c.n_nodes, c.featY, s);
                 if (rc) return rc;
-                // the network's correction at full, half and quarter length:
-                // the candidate (linear included) with the smallest residual starts Newton
-                double best = res_lin, best_a = 0.0;
-                for (double a : {1.0, 0.5, 0.25}) {
-                    launch_apply(c, c.Uprev, c.Uold, ratio, a * s_inc, c.featY, c.U, s, c.featX);
-                    k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
-                    const double ra = std::sqrt(predictor_residual(c, c.U, dt, s));
-                    if (a == 1.0) res_mlp = ra;
-                    if (ra < best) {
-                        best = ra;
-                        best_a = a;
-                    }
-                }
-                if (best_a > 0.0) {
+                cudaMemcpyAsync(c.U, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
+                rc = launch_apply(c, h, c.featY, 1.0, c.U, s);
+                if (rc) return rc;
+                k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
+                res_mlp = std::sqrt(predictor_residual(c, c.U, dt, s));
+                // the learned start is taken unless its residual is far above the
+                // linear one (a start's residual is a poor judge of the Newton
+                // work it saves -- the penalty stiffness of the interfaces
+                // dominates it -- so only a gross miss falls back)
+                if (res_mlp == res_mlp && res_mlp <= kLearnedResidualGuard * res_lin) {
                     used = PG_PREDICT_LEARNED;
-                    if (best_a != 0.25) {
-                        launch_apply(c, c.Uprev, c.Uold, ratio, best_a * s_inc, c.featY, c.U, s, c.featX);
-                        k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
-                    }
                 } else {
                     cudaMemcpyAsync(c.U, c.Ut, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
                     used = PG_PREDICT_LINEAR;
@@ -275,8 +284,11 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             }
         }
         // accept: commit the cohesive state, remember the converged U
-        if (c.n_coh_qp > 0)
+        if (c.n_coh_qp > 0) {
+            cudaMemcpyAsync(c.isv_prev, c.isv_c, (size_t)c.n_coh_qp * sizeof(double), cudaMemcpyDeviceToDevice, s);
             cudaMemcpyAsync(c.isv_c, c.isv_t, (size_t)c.n_coh_qp * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        }
+        cudaMemcpyAsync(c.Uold2, c.Uold, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(c.Uold, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(c.Uprev, c.U, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
         t += dt;
@@ -288,6 +300,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
         st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_step).count();
         if (per_step && nrec < max_records) per_step[nrec] = st;
         ++nrec;
+        dt_prev2 = dt_prev;
         dt_prev = dt;
         if (repeat == 1) dt *= 1.5;
         dt = std::min(dt, dt_nom);

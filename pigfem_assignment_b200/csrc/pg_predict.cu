@@ -1,16 +1,30 @@
 // Learned Newton warm start: per-node features, training targets and the
-// application of the MLP's correction to the linear load extrapolation.
+// application of the MLP's output to the load extrapolation.
 // The reference only has the zeroth-order predictor (U_f carried over,
 // src/SolverNonlinear.cpp:254-267); this is new.
 //
-// For a step from load factor t_n to t_{n+1} with ratio = dt_{n+1} / dt_n:
-//   U_lin  = U_n + ratio (U_n - U_{n-1})                (free DOFs)
-//   U_pred = U_lin + s * MLP(features)                  s = prescribed increment of the step
-// Features of node i (16): the last increment / s (2), U_n / app (2),
-// normalised position (2), enrichment / mirror flags (2), the largest
-// committed opening over the node's cohesive points / delta_ref (1), load
-// factor (1), ratio (1), Dirichlet flags (2), |last increment| / s (1),
-// a constant 1 (1), 0 (1).  Targets: (U_{n+1} - U_lin) / s.
+// From the last three converged states (U_n, U_{n-1}, U_{n-2}, reached by
+// steps dt_n and dt_{n-1}) and the coming step dt, per node:
+//   d_n = U_n - U_{n-1},  d_{n-1} = U_{n-1} - U_{n-2}
+//   U_lin  = U_n + (dt / dt_n) d_n                      linear extrapolation
+//   c      = dt (dt + dt_n) / (dt_n + dt_{n-1}) (d_n / dt_n - d_{n-1} / dt_{n-1})
+//            (the quadratic extrapolation's term: U_quad = U_lin + c)
+//   U_pred = U_lin + g c,   g = 1 + y,  y = the network's output for the node,
+//                           clamped to [-1, 0]
+// so that each node's start lies between its linear (y = -1) and quadratic
+// (y = 0) extrapolations.  The network only weighs the curvature term of the
+// node's own history: in the elastic bulk c is tiny and any error of g costs
+// nothing; where an interface softens, y learns from the trajectories which
+// of the two extrapolations the node follows.
+//
+// Features of node i (16, scale-free, each bounded by 5): c / |d_n| (2),
+// d_n / |d_n| (2), |d_{n-1}| dt_n / (|d_n| dt_{n-1}) (1), log(1 + |d_n| /
+// s_inc) (1), enrichment / mirror flags (2), log(1 + the largest committed
+// opening over the node's cohesive points / delta_ref) (1) and the opening's
+// change over the last step / delta_ref (1), load fraction (1), dt / dt_n (1),
+// Dirichlet flags (2), a constant 1 (1), 0 (1).
+// Target: y* = (e . c) / (c . c) - 1 with e = U_{n+1} - U_lin over the
+// node's free components, clipped to [-1, 0] (both outputs).
 #include <cmath>
 
 #include "pg_internal.cuh"
@@ -20,35 +34,57 @@ namespace pgb {
 
 namespace {
 inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
+struct NodeHist {
+    double dn[2], c[2], dnorm, dprev;
+};
+
+__device__ __forceinline__ NodeHist node_hist(const pg_pred_history& h, int i) {
+    NodeHist r;
+    const double q = h.dt * (h.dt + h.dt_n) / (h.dt_n + h.dt_nm1);
+    double pn2 = 0.0;
+    for (int d = 0; d < 2; ++d) {
+        const double a = h.U_n[2 * i + d], b = h.U_nm1[2 * i + d], o = h.U_nm2[2 * i + d];
+        const double dn = a - b, dp = b - o;
+        r.dn[d] = dn;
+        r.c[d] = q * (dn / h.dt_n - dp / h.dt_nm1);
+        pn2 += dp * dp;
+    }
+    r.dnorm = sqrt(r.dn[0] * r.dn[0] + r.dn[1] * r.dn[1]);
+    r.dprev = sqrt(pn2);
+    return r;
 }
+}  // namespace
 
 __global__ void k_features(int n, int n_reg, int n_enr_initial, const uint8_t* __restrict__ fixed,
-                           const double* __restrict__ x, const double* __restrict__ y, double x0, double xs, double y0,
-                           double ys, const double* __restrict__ Un, const double* __restrict__ Unm1, double s_inc,
-                           double app, double t_frac, double ratio, const double* __restrict__ isv_c,
-                           const int* __restrict__ nq_ptr, const int* __restrict__ nq_list, double delta_ref,
-                           float* __restrict__ X) {
+                           pg_pred_history h, const double* __restrict__ isv_c, const int* __restrict__ nq_ptr,
+                           const int* __restrict__ nq_list, double delta_ref, float* __restrict__ X) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const double dux = Un[2 * i] - Unm1[2 * i], duy = Un[2 * i + 1] - Unm1[2 * i + 1];
-    double dmg = 0.0;
+    const NodeHist r = node_hist(h, i);
+    double dmg = 0.0, dmg_prev = 0.0;
     if (nq_ptr)
-        for (int k = nq_ptr[i]; k < nq_ptr[i + 1]; ++k) dmg = fmax(dmg, isv_c[nq_list[k]]);
+        for (int k = nq_ptr[i]; k < nq_ptr[i + 1]; ++k) {
+            dmg = fmax(dmg, isv_c[nq_list[k]]);
+            if (h.isv_nm1) dmg_prev = fmax(dmg_prev, h.isv_nm1[nq_list[k]]);
+        }
+    const double eps = 1e-6 * fabs(h.s_inc);
+    const double inv = 1.0 / (r.dnorm + eps);
     float f[16];
-    f[0] = (float)(dux / s_inc);
-    f[1] = (float)(duy / s_inc);
-    f[2] = (float)(Un[2 * i] / app);
-    f[3] = (float)(Un[2 * i + 1] / app);
-    f[4] = (float)((x[i] - x0) / xs);
-    f[5] = (float)((y[i] - y0) / ys);
+    f[0] = (float)fmax(-5.0, fmin(5.0, r.c[0] * inv));
+    f[1] = (float)fmax(-5.0, fmin(5.0, r.c[1] * inv));
+    f[2] = (float)(r.dn[0] * inv);
+    f[3] = (float)(r.dn[1] * inv);
+    f[4] = (float)fmin(5.0, r.dprev * h.dt_n / h.dt_nm1 * inv);
+    f[5] = (float)fmin(5.0, log1p(r.dnorm / fabs(h.s_inc)));
     f[6] = i >= n_reg ? 1.f : 0.f;
     f[7] = i >= n_reg + n_enr_initial ? 1.f : 0.f;
-    f[8] = (float)fmin(dmg / delta_ref, 50.0);
-    f[9] = (float)t_frac;
-    f[10] = (float)ratio;
-    f[11] = fixed[2 * i] ? 1.f : 0.f;
-    f[12] = fixed[2 * i + 1] ? 1.f : 0.f;
-    f[13] = (float)(sqrt(dux * dux + duy * duy) / s_inc);
+    f[8] = (float)fmin(5.0, log1p(dmg / delta_ref));
+    f[9] = h.isv_nm1 ? (float)fmax(-5.0, fmin(5.0, (dmg - dmg_prev) / delta_ref)) : 0.f;
+    f[10] = (float)h.t_frac;
+    f[11] = (float)(h.dt / h.dt_n);
+    f[12] = fixed[2 * i] ? 1.f : 0.f;
+    f[13] = fixed[2 * i + 1] ? 1.f : 0.f;
     f[14] = 1.f;
     f[15] = 0.f;
     float4* o = reinterpret_cast<float4*>(X + 16 * (size_t)i);
@@ -58,33 +94,38 @@ __global__ void k_features(int n, int n_reg, int n_enr_initial, const uint8_t* _
     o[3] = make_float4(f[12], f[13], f[14], f[15]);
 }
 
-__global__ void k_targets(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ Un1,
-                          const double* __restrict__ Un, const double* __restrict__ Unm1, double ratio, double s_inc,
-                          float* __restrict__ T) {
+__global__ void k_targets(int n, const uint8_t* __restrict__ fixed, pg_pred_history h,
+                          const double* __restrict__ Un1, float* __restrict__ T) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= nd) return;
-    const double lin = Un[i] + ratio * (Un[i] - Unm1[i]);
-    T[i] = fixed[i] ? 0.f : (float)((Un1[i] - lin) / s_inc);
-}
-
-// gate (features, may be null): the correction is applied only at nodes that
-// are enrichment nodes or carry cohesive damage (features 6 and 8); in the
-// elastic bulk the linear extrapolation is already close, and any network
-// output there only adds error.
-__global__ void k_apply(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ Un,
-                        const double* __restrict__ Unm1, double ratio, double s_inc, const float* __restrict__ Y,
-                        const float* __restrict__ gate, double* __restrict__ U) {
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= nd || fixed[i]) return;
-    bool on = Y != nullptr;
-    if (on && gate) {
-        const float* f = gate + 16 * (size_t)(i >> 1);
-        on = f[6] > 0.5f || f[8] > 0.f;
+    if (i >= n) return;
+    const NodeHist r = node_hist(h, i);
+    double ec = 0.0, cc = 0.0;
+    for (int d = 0; d < 2; ++d) {
+        if (fixed[2 * i + d]) continue;
+        const double lin = h.U_n[2 * i + d] + (h.dt / h.dt_n) * r.dn[d];
+        ec += (Un1[2 * i + d] - lin) * r.c[d];
+        cc += r.c[d] * r.c[d];
     }
-    U[i] = Un[i] + ratio * (Un[i] - Unm1[i]) + (on ? s_inc * (double)Y[i] : 0.0);
+    const double y = cc > 0.0 ? fmax(-1.0, fmin(0.0, ec / cc - 1.0)) : -1.0;
+    T[2 * i] = (float)y;
+    T[2 * i + 1] = (float)y;
 }
 
-// node -> cohesive quadrature points (for the damage feature)
+// U = U_lin + scale (1 + y) c on free DOFs (Y null: the linear extrapolation)
+__global__ void k_apply(int n, const uint8_t* __restrict__ fixed, pg_pred_history h, const float* __restrict__ Y,
+                        double scale, double* __restrict__ U) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const NodeHist r = node_hist(h, i);
+    const double y = Y ? fmax(-1.0, fmin(0.0, (double)Y[2 * i])) : 0.0;
+    const double g = Y ? scale * (1.0 + y) : 0.0;
+    for (int d = 0; d < 2; ++d) {
+        if (fixed[2 * i + d]) continue;
+        U[2 * i + d] = h.U_n[2 * i + d] + (h.dt / h.dt_n) * r.dn[d] + g * r.c[d];
+    }
+}
+
+// node -> cohesive quadrature points (for the damage features)
 int build_node_qp_map(Ctx& c) {
     if (c.nq_ptr || c.n_coh_qp == 0) return PG_OK;
     const HostMesh& m = c.hm;
@@ -121,21 +162,21 @@ double predictor_app(const Ctx& c) {
     return app != 0.0 ? app : 1.0;
 }
 
-int launch_features(Ctx& c, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc, float* X,
-                    cudaStream_t s) {
+bool history_ok(const pg_pred_history& h) {
+    return h.U_n && h.U_nm1 && h.U_nm2 && h.dt_n > 0.0 && h.dt_nm1 > 0.0 && h.dt > 0.0 && h.s_inc != 0.0;
+}
+
+int launch_features(Ctx& c, const pg_pred_history& h, float* X, cudaStream_t s) {
     int rc = build_node_qp_map(c);
     if (rc) return rc;
-    const RveSpec& sp = c.hm.spec;
-    k_features<<<nblk(c.n_nodes), kThreads, 0, s>>>(
-        c.n_nodes, c.n_reg, c.hm.n_enr_initial, c.fixed, c.x, c.y, sp.x0, sp.x1 - sp.x0, sp.y0, sp.y1 - sp.y0, Un,
-        Unm1, s_inc, predictor_app(c), t_frac, ratio, c.isv_c, c.nq_ptr, c.nq_list, predictor_delta_ref(c), X);
+    k_features<<<nblk(c.n_nodes), kThreads, 0, s>>>(c.n_nodes, c.n_reg, c.hm.n_enr_initial, c.fixed, h, c.isv_c,
+                                                    c.nq_ptr, c.nq_list, predictor_delta_ref(c), X);
     PG_CUDA(cudaGetLastError());
     return PG_OK;
 }
 
-int launch_apply(Ctx& c, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y, double* U,
-                 cudaStream_t s, const float* gate) {
-    k_apply<<<nblk(c.n_dof), kThreads, 0, s>>>(c.n_dof, c.fixed, Un, Unm1, ratio, s_inc, Y, gate, U);
+int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s) {
+    k_apply<<<nblk(c.n_nodes), kThreads, 0, s>>>(c.n_nodes, c.fixed, h, Y, scale, U);
     PG_CUDA(cudaGetLastError());
     return PG_OK;
 }
@@ -146,30 +187,30 @@ using namespace pgb;
 
 extern "C" {
 
-int pg_predictor_features(pg_ctx* cx, const double* Un, const double* Unm1, double t_frac, double ratio, double s_inc,
-                          float* X_dev) {
-    if (!cx || !Un || !Unm1 || !X_dev || s_inc == 0.0) { set_error("pg_predictor_features: bad argument"); return PG_ERR_ARG; }
+int pg_predictor_features(pg_ctx* cx, const pg_pred_history* h, float* X_dev) {
+    if (!cx || !h || !X_dev || !history_ok(*h)) { set_error("pg_predictor_features: bad argument"); return PG_ERR_ARG; }
     Ctx& c = cx->c;
     cudaSetDevice(c.device);
-    return launch_features(c, Un, Unm1, t_frac, ratio, s_inc, X_dev, c.stream);
+    return launch_features(c, *h, X_dev, c.stream);
 }
 
-int pg_predictor_targets(pg_ctx* cx, const double* Un1, const double* Un, const double* Unm1, double ratio,
-                         double s_inc, float* T_dev) {
-    if (!cx || !Un1 || !Un || !Unm1 || !T_dev || s_inc == 0.0) { set_error("pg_predictor_targets: bad argument"); return PG_ERR_ARG; }
+int pg_predictor_targets(pg_ctx* cx, const pg_pred_history* h, const double* U_np1, float* T_dev) {
+    if (!cx || !h || !U_np1 || !T_dev || !history_ok(*h)) {
+        set_error("pg_predictor_targets: bad argument");
+        return PG_ERR_ARG;
+    }
     Ctx& c = cx->c;
     cudaSetDevice(c.device);
-    k_targets<<<nblk(c.n_dof), kThreads, 0, c.stream>>>(c.n_dof, c.fixed, Un1, Un, Unm1, ratio, s_inc, T_dev);
+    k_targets<<<nblk(c.n_nodes), kThreads, 0, c.stream>>>(c.n_nodes, c.fixed, *h, U_np1, T_dev);
     PG_CUDA(cudaGetLastError());
     return PG_OK;
 }
 
-int pg_predictor_apply(pg_ctx* cx, const double* Un, const double* Unm1, double ratio, double s_inc, const float* Y_dev,
-                       double* U_dev) {
-    if (!cx || !Un || !Unm1 || !U_dev) { set_error("pg_predictor_apply: bad argument"); return PG_ERR_ARG; }
+int pg_predictor_apply(pg_ctx* cx, const pg_pred_history* h, const float* Y_dev, double scale, double* U_dev) {
+    if (!cx || !h || !U_dev || !history_ok(*h)) { set_error("pg_predictor_apply: bad argument"); return PG_ERR_ARG; }
     Ctx& c = cx->c;
     cudaSetDevice(c.device);
-    return launch_apply(c, Un, Unm1, ratio, s_inc, Y_dev, U_dev, c.stream);
+    return launch_apply(c, *h, Y_dev, scale, U_dev, c.stream);
 }
 
 int pg_ctx_attach_mlp(pg_ctx* cx, pg_mlp* m) {

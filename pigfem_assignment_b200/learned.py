@@ -65,6 +65,15 @@ class MLP:
         v = np.ascontiguousarray(v, dtype=np.float32)
         check(lib.pg_mlp_params(self.handle, v.ctypes.data_as(C.POINTER(C.c_float)), 1))
 
+    def zero_output_layer(self, bias: float = 0.0) -> None:
+        """Output weights to zero and the two used outputs' biases to `bias`:
+        the network then starts as the constant y = bias (-1: the linear
+        extrapolation of the learned predictor, 0: the quadratic one)."""
+        v = self.params()
+        v[-(16 * 64 + 16):] = 0.0
+        v[-16] = v[-15] = bias
+        self.set_params(v)
+
     def forward(self, X):
         torch = _torch()
         Y = torch.empty((X.shape[0], 2), dtype=torch.float32, device=X.device)
@@ -88,10 +97,14 @@ def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction
                        device: int = 0, rtol: float = 1e-8, newton: dict = None
                        ) -> Tuple["object", "object", List[_lib.StepStats]]:
     """Runs the first `n_train_steps` of `n_steps` equal load steps of `rve`
-    with the linear predictor and returns (features, targets) of the nodes kept
-    (every enrichment node, every node with cohesive damage, and a random
-    `keep_fraction` of the others; the Newton solver applies the network's
-    correction at the first two kinds only), plus the step records.  `newton` holds
+    with the linear predictor and returns (features, targets) of the nodes
+    kept, from the third step on (the features need three converged states),
+    plus the step records.  A free node is kept with probability
+    min(1, (|c| / c_ref)^2), c its quadratic term and c_ref the 99th
+    percentile of |c| over the step's free nodes: the plain mean square error
+    over the kept nodes then weighs every node as its error (e - g c) weighs
+    in the prediction, where y's target is noise for nodes that barely bend.
+    A random `keep_fraction` of the others is kept as well.  `newton` holds
     further pg_newton_cfg fields (e.g. the preconditioner)."""
     torch = _torch()
     prob = ProblemNonlinearStructural(rve, device=device)
@@ -100,11 +113,12 @@ def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction
     ctx = prob.ctx
     n_nodes = prob.mesh.info["n_nodes"]
     n_reg = prob.mesh.info["n_regular_nodes"]
+    n_qp = max(1, prob.mesh.info["n_cohesive_qp"])
     U_ptr = _dev_ptrs(ctx)
     nd = 2 * n_nodes
     dev = f"cuda:{device}"
-    U_n = torch.zeros(nd, dtype=torch.float64, device=dev)
-    U_nm1 = torch.zeros(nd, dtype=torch.float64, device=dev)
+    U = [torch.zeros(nd, dtype=torch.float64, device=dev) for _ in range(3)]  # U_n, U_{n-1}, U_{n-2}
+    isv_nm1 = torch.zeros(n_qp, dtype=torch.float64, device=dev)
     X = torch.empty((n_nodes, 16), dtype=torch.float32, device=dev)
     T = torch.empty((n_nodes, 2), dtype=torch.float32, device=dev)
     app = (rve.x1 - rve.x0) * rve.strain
@@ -114,33 +128,39 @@ def trajectory_samples(rve: RVE, n_steps: int, n_train_steps: int, keep_fraction
     xs, ts, recs = [], [], []
     for k in range(1, n_train_steps + 1):
         tf = k * dt
-        have_hist = k > 1
+        h = _lib.PredHistory(U[0].data_ptr(), U[1].data_ptr(), U[2].data_ptr(), isv_nm1.data_ptr(), dt, dt, dt, tf,
+                             s_inc)
+        have_hist = k > 2
         if have_hist:
-            check(lib.pg_predictor_features(ctx.handle, C.c_void_p(U_n.data_ptr()), C.c_void_p(U_nm1.data_ptr()), tf,
-                                            1.0, s_inc, C.c_void_p(X.data_ptr())))
-            check(lib.pg_predictor_apply(ctx.handle, C.c_void_p(U_n.data_ptr()), C.c_void_p(U_nm1.data_ptr()), 1.0,
-                                         s_inc, None, C.c_void_p(U_ptr)))
+            check(lib.pg_predictor_features(ctx.handle, C.byref(h), C.c_void_p(X.data_ptr())))
+        if k > 1:  # linear extrapolation as the step's start
+            check(lib.pg_predictor_apply(ctx.handle, C.byref(h), None, 0.0, C.c_void_p(U_ptr)))
+        isv_n = torch.from_numpy(np.resize(ctx.isv(committed=True), n_qp)).to(dev)
         st = prob.load_step(tf, dt)
         if st.reason <= 0:
             break
         prob.commit()
         recs.append(st)
-        U_cur = torch.empty_like(U_n)
         ctx.sync()
         torch.cuda.synchronize()
-        U_cur.copy_(torch.from_numpy(ctx.vector(0)).to(dev))
+        U_cur = torch.from_numpy(ctx.vector(0)).to(dev)
         if have_hist:
-            check(lib.pg_predictor_targets(ctx.handle, C.c_void_p(U_cur.data_ptr()), C.c_void_p(U_n.data_ptr()),
-                                           C.c_void_p(U_nm1.data_ptr()), 1.0, s_inc, C.c_void_p(T.data_ptr())))
+            check(lib.pg_predictor_targets(ctx.handle, C.byref(h), C.c_void_p(U_cur.data_ptr()),
+                                           C.c_void_p(T.data_ptr())))
             ctx.sync()
             Xh = X.cpu().numpy()
-            keep = (np.arange(n_nodes) >= n_reg) | (Xh[:, 8] > 0) | (rng.random(n_nodes) < keep_fraction)
-            free = (Xh[:, 11] == 0) | (Xh[:, 12] == 0)
+            free = (Xh[:, 12] == 0) | (Xh[:, 13] == 0)
+            w = (np.hypot(Xh[:, 0], Xh[:, 1]) * np.expm1(Xh[:, 5])) ** 2  # (|c| / s_inc)^2
+            pos = w[free & (w > 0)]
+            w_ref = np.quantile(pos, 0.99) if pos.size else 1.0
+            keep = (rng.random(n_nodes) < np.minimum(1.0, w / max(w_ref, 1e-300))) | (rng.random(n_nodes) < keep_fraction)
             sel = np.nonzero(keep & free)[0]
             xs.append(Xh[sel])
             ts.append(T.cpu().numpy()[sel])
-        U_nm1.copy_(U_n)
-        U_n.copy_(U_cur)
+        U[2].copy_(U[1])
+        U[1].copy_(U[0])
+        U[0].copy_(U_cur)
+        isv_nm1.copy_(isv_n)
     ctx.close()
     return (np.concatenate(xs) if xs else np.zeros((0, 16), np.float32),
             np.concatenate(ts) if ts else np.zeros((0, 2), np.float32), recs)

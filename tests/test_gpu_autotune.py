@@ -36,8 +36,9 @@ def test_every_launch_shape_assembles_the_same_K(tile, persistent, warps):
 
 
 @pytest.mark.parametrize("tile", [32, 64, 128, 256])
+@pytest.mark.parametrize("persistent", [0, 1])
 @pytest.mark.parametrize("warps", [2, 8])
-def test_every_launch_shape_assembles_the_same_tangent_and_residual(tile, warps):
+def test_every_launch_shape_assembles_the_same_tangent_and_residual(tile, persistent, warps):
     # the residual and tangent passes of a cohesive mesh (bilinear law, damaged
     # state) through every launch shape: K and f_int against the oracle
     rve = RVE(nx=20, ny=20, inclusions=[(0.45, 0.5, 0.27, 1)], cohesive=True, coh_law=1,
@@ -45,7 +46,7 @@ def test_every_launch_shape_assembles_the_same_tangent_and_residual(tile, warps)
     m = pb.Mesh(rve)
     e = m.export()
     ctx = pb.DeviceContext(m)
-    _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, 0, warps))
+    _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, warps))
     rng = np.random.default_rng(5)
     U = 1e-4 * rng.standard_normal(m.info["n_dof"])
     isv_c = np.abs(2e-5 * rng.standard_normal(m.info["n_cohesive_qp"]))
@@ -82,3 +83,23 @@ def test_autotune_times_every_shape_and_keeps_the_fastest():
     st = prob.solve_problem()
     assert st.status == 0
     prob.ctx.close()
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_pipelined_grid_kernel_writes_the_same_bits(tile):
+    # the persistent kernel stages the next tile asynchronously; the values it
+    # forms are the same arithmetic on the same inputs: identical K and f
+    from pigfem_assignment_b200.rve import config1, scaled
+    rve = scaled(config1(), 256)
+    m = pb.Mesh(rve)
+    ctx = pb.DeviceContext(m)
+    rng = np.random.default_rng(7)
+    ctx.set_vector(0, 1e-3 * rng.standard_normal(m.info["n_dof"]))
+    out = []
+    for persistent in (0, 1):
+        _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, 4))
+        pb.Assembler(ctx).assemble_nonlinear(1.0, True, True)
+        out.append((ctx.matrix_values(), ctx.vector(1)))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    ctx.close()

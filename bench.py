@@ -345,7 +345,7 @@ def run_b200_arm(args):
     n_blocks, n_nodes, n_cut = info["n_blocks"], info["n_nodes"], info["n_cut_elements"]
     n_uncut = n_e - n_cut
     n_reg = info["n_regular_nodes"]
-    if tri_kernel == "k_grid_rows":
+    if tri_kernel.startswith("k_grid_rows"):
         # the grid kernel writes the blocks between regular nodes; the fold writes the
         # enrichment rows and columns
         ex = mesh.export()

@@ -261,6 +261,8 @@ typedef struct pg_step_stats {
     int32_t predictor_used;         /* PG_PREDICT_* actually used for this step */
     double res_linear, res_learned; /* initial residuals of both candidates (learned predictor only) */
     double res_base;                /* the residual rtol was relative to */
+    double blend;                   /* learned predictor: the blend g of the step's learned candidate (0: linear,
+                                       1: quadratic extrapolation); -1 when no learned candidate was formed */
 } pg_step_stats;
 
 void pg_newton_cfg_default(pg_newton_cfg* cfg);
@@ -299,11 +301,12 @@ int pg_mlp_wait_selftest(pg_mlp* m, int32_t polls);
  * converged states at t_n, t_{n-1}, t_{n-2}, the steps dt_n and dt_{n-1} that
  * led to the first two, the coming step dt, the load fraction at t_n + dt and
  * the step's prescribed displacement increment.  The prediction is
- *   U = U_n + (dt/dt_n) d_n + (1 + y) c,  d_n = U_n - U_{n-1},
+ *   U = U_n + (dt/dt_n) d_n + g c,  d_n = U_n - U_{n-1},
  *   c = dt (dt + dt_n) / (dt_n + dt_{n-1}) (d_n/dt_n - d_{n-1}/dt_{n-1})
- * per node, y the network's output clamped to [-1, 0] (y = 0: quadratic
- * extrapolation, y = -1: linear).  Features: 16 floats per node; targets and
- * outputs: 2 floats per node (both y). */
+ * per node, with one blend g = sum |c_i|^2 (1 + y_i) / sum |c_i|^2 of the
+ * linear (g = 0) and quadratic (g = 1) extrapolations, y_i the network's
+ * output for node i clamped to [-1, 0].  Features: 16 floats per node;
+ * targets and outputs: 2 floats per node (both y). */
 typedef struct pg_pred_history {
     const double* U_n;
     const double* U_nm1;
@@ -317,7 +320,7 @@ typedef struct pg_pred_history {
 int pg_predictor_features(pg_ctx* c, const pg_pred_history* h, float* X_dev);
 /* targets of the step that reached U_np1 (training data) */
 int pg_predictor_targets(pg_ctx* c, const pg_pred_history* h, const double* U_np1, float* T_dev);
-/* U_dev (free DOFs) = the prediction with (1 + y) scaled by `scale` (Y_dev NULL: the linear extrapolation) */
+/* U_dev (free DOFs) = the prediction with g scaled by `scale` (Y_dev NULL: the linear extrapolation) */
 int pg_predictor_apply(pg_ctx* c, const pg_pred_history* h, const float* Y_dev, double scale, double* U_dev);
 /* attaches a network for PG_PREDICT_LEARNED (NULL detaches; the context does not own it) */
 int pg_ctx_attach_mlp(pg_ctx* c, pg_mlp* m);

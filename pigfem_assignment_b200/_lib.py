@@ -98,7 +98,7 @@ class StepStats(C.Structure):
         ("t_frac", C.c_double), ("dt", C.c_double), ("newton_its", C.c_int32), ("krylov_its", C.c_int32),
         ("gmres_fallbacks", C.c_int32), ("repeats", C.c_int32), ("res0", C.c_double), ("res", C.c_double),
         ("reason", C.c_int32), ("seconds", C.c_double), ("predictor_used", C.c_int32),
-        ("res_linear", C.c_double), ("res_learned", C.c_double), ("res_base", C.c_double),
+        ("res_linear", C.c_double), ("res_learned", C.c_double), ("res_base", C.c_double), ("blend", C.c_double),
     ]
 
 

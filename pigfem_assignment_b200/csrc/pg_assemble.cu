@@ -993,23 +993,26 @@ __device__ __forceinline__ void grid_stage_async(const GridArgs& a, int t, GridW
 }
 
 // Persistent variant of k_grid_rows: each CTA walks the tile table with a
-// stride of the grid, and copies the next tile's window into the second of
-// two shared-memory buffers (cp.async) while its threads form the rows of
+// stride of the grid, and copies the next tile's window into a free one of
+// three shared-memory buffers (cp.async) while its threads form the rows of
 // the current one, so that the staging latency overlaps the arithmetic
-// instead of idling the SM.  Out-of-grid window entries are zero-filled
-// (materials: out-of-grid cells read as material 0 from the fill, so they
-// are set to -1 after the copy lands).
+// instead of idling the SM.  With three buffers one barrier per tile
+// suffices: the buffer refilled in iteration k was last read in iteration
+// k - 2, which every thread has left once it passed iteration k - 1's
+// barrier.  Out-of-grid window entries are zero-filled (materials:
+// out-of-grid cells read as material 0 from the fill, so they are set to -1
+// after the copy lands).
 template <bool WK, bool WF, int TR>
 __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows_pipe(GridArgs a, int n_tiles) {
-    __shared__ GridWin<TR, WF> W[2];
+    __shared__ GridWin<TR, WF> W[3];
     int t = blockIdx.x;
     if (t >= n_tiles) return;
     grid_stage_async<TR, WF>(a, t, W[0]);
     cp_async_commit();
     for (int k = 0; t < n_tiles; t += gridDim.x, ++k) {
-        GridWin<TR, WF>& cur = W[k & 1];
+        GridWin<TR, WF>& cur = W[k % 3];
         const int tn = t + gridDim.x;
-        if (tn < n_tiles) grid_stage_async<TR, WF>(a, tn, W[(k + 1) & 1]);
+        if (tn < n_tiles) grid_stage_async<TR, WF>(a, tn, W[(k + 1) % 3]);
         cp_async_commit();  // (an empty group when nothing was issued)
         cp_async_wait_one();  // the current tile's copies have landed
         const int4 T = __ldg(&a.tiles[t]);
@@ -1030,7 +1033,6 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows_pipe(Gri
             if (q == 0) grid_node<0, WK, WF>(a, B, gi, gj, lx, ly, cur.xy, cur.u, cur.m);
             else grid_node<1, WK, WF>(a, B, gi, gj, lx, ly, cur.xy, cur.u, cur.m);
         }
-        __syncthreads();  // the buffer is refilled two tiles on
     }
     cp_async_wait_all();
 }

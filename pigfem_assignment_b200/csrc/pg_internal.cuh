@@ -308,8 +308,10 @@ void set_prescribed(Ctx& c, double t_frac, cudaStream_t s);
 
 // learned predictor (pg_predict.cu)
 int launch_features(Ctx& c, const pg_pred_history& h, float* X, cudaStream_t s);
-// U (free DOFs) = linear extrapolation + scale * Y * curvature term (Y null: linear)
-int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s);
+// U (free DOFs) = linear extrapolation + g * curvature term, g = scale * the curvature-weighted
+// mean of (1 + Y) (Y null: g = 0, the linear extrapolation); g_used (nullable) receives g
+int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s,
+                 double* g_used = nullptr);
 double predictor_app(const Ctx& c);
 double predictor_residual(Ctx& c, const double* U, double dt, cudaStream_t s);
 

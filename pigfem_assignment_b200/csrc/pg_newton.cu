@@ -49,6 +49,7 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
                      double r_base) {
     const int nd = c.n_dof;
     st = pg_step_stats{};
+    st.blend = -1.0;
     st.t_frac = t_frac;
     st.dt = dt;
     cudaEventRecord(c.ev0, s);
@@ -225,7 +226,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                 r_base = std::sqrt(predictor_residual(c, c.U, dt, s));
             }
             int used = PG_PREDICT_ZEROTH;
-            double res_lin = -1.0, res_mlp = -1.0;
+            double res_lin = -1.0, res_mlp = -1.0, blend = -1.0;
             // the learned start needs two steps of history; before that it is the linear one
             if ((cfg.predictor == PG_PREDICT_LINEAR && nrec > 0) || (cfg.predictor == PG_PREDICT_LEARNED && nrec == 1)) {
                 k_extrapolate<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.U, c.Uold, dt / dt_prev);
@@ -253,7 +254,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
                 rc = pg_mlp_forward(c.mlp, c.featX, c.n_nodes, c.featY, s);
                 if (rc) return rc;
                 cudaMemcpyAsync(c.U, c.Uprev, (size_t)nd * sizeof(double), cudaMemcpyDeviceToDevice, s);
-                rc = launch_apply(c, h, c.featY, 1.0, c.U, s);
+                rc = launch_apply(c, h, c.featY, 1.0, c.U, s, &blend);
                 if (rc) return rc;
                 k_apply_dirichlet<<<nblk(nd), kThreads, 0, s>>>(nd, c.fixed, c.ubar, tf, c.U);
                 res_mlp = std::sqrt(predictor_residual(c, c.U, dt, s));
@@ -272,6 +273,7 @@ int pg_solve_nonlinear(pg_ctx* cx, const pg_newton_cfg* cfg_in, pg_step_stats* p
             st.predictor_used = used;
             st.res_linear = res_lin;
             st.res_learned = res_mlp;
+            st.blend = blend;
             if (rc != PG_OK) return rc;
             converged = st.reason > 0;
             acc_newton += st.newton_its;

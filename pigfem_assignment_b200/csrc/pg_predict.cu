@@ -9,13 +9,15 @@
 //   U_lin  = U_n + (dt / dt_n) d_n                      linear extrapolation
 //   c      = dt (dt + dt_n) / (dt_n + dt_{n-1}) (d_n / dt_n - d_{n-1} / dt_{n-1})
 //            (the quadratic extrapolation's term: U_quad = U_lin + c)
-//   U_pred = U_lin + g c,   g = 1 + y,  y = the network's output for the node,
-//                           clamped to [-1, 0]
-// so that each node's start lies between its linear (y = -1) and quadratic
-// (y = 0) extrapolations.  The network only weighs the curvature term of the
-// node's own history: in the elastic bulk c is tiny and any error of g costs
-// nothing; where an interface softens, y learns from the trajectories which
-// of the two extrapolations the node follows.
+//   U_pred = U_lin + g c,   g = sum_i w_i (1 + y_i) / sum_i w_i,  w_i = |c_i|^2,
+// y_i = the network's output for node i clamped to [-1, 0] (-1: the node
+// follows its linear extrapolation, 0: its quadratic one).  Each node's
+// network output, from its own history and damage state, votes with the
+// weight its curvature term has in the prediction, and one blend g of the
+// linear and quadratic extrapolations is applied to all nodes: a blend that
+// varied from node to node would add a rough field, which the stiffness
+// turns into a large residual (measured: ~60x the linear start's), while a
+// uniform blend keeps the extrapolation smooth.
 //
 // Features of node i (16, scale-free, each bounded by 5): c / |d_n| (2),
 // d_n / |d_n| (2), |d_{n-1}| dt_n / (|d_n| dt_{n-1}) (1), log(1 + |d_n| /
@@ -111,14 +113,45 @@ __global__ void k_targets(int n, const uint8_t* __restrict__ fixed, pg_pred_hist
     T[2 * i + 1] = (float)y;
 }
 
-// U = U_lin + scale (1 + y) c on free DOFs (Y null: the linear extrapolation)
-__global__ void k_apply(int n, const uint8_t* __restrict__ fixed, pg_pred_history h, const float* __restrict__ Y,
-                        double scale, double* __restrict__ U) {
+// per CTA: sum of w_i and of w_i (1 + y_i) over its nodes (free components
+// of c only); the CTAs' partials are added in order on the host
+constexpr int kBlendThreads = 256;
+__global__ void __launch_bounds__(kBlendThreads) k_blend_partial(int n, const uint8_t* __restrict__ fixed,
+                                                                 pg_pred_history h, const float* __restrict__ Y,
+                                                                 double* __restrict__ part) {
+    __shared__ double sw[kBlendThreads], swy[kBlendThreads];
+    double w = 0.0, wy = 0.0;
+    for (int i = blockIdx.x * kBlendThreads + threadIdx.x; i < n; i += kBlendThreads * gridDim.x) {
+        const NodeHist r = node_hist(h, i);
+        double cc = 0.0;
+        for (int d = 0; d < 2; ++d)
+            if (!fixed[2 * i + d]) cc += r.c[d] * r.c[d];
+        const double y = fmax(-1.0, fmin(0.0, (double)Y[2 * i]));
+        w += cc;
+        wy += cc * (1.0 + y);
+    }
+    sw[threadIdx.x] = w;
+    swy[threadIdx.x] = wy;
+    __syncthreads();
+    for (int st = kBlendThreads / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) {
+            sw[threadIdx.x] += sw[threadIdx.x + st];
+            swy[threadIdx.x] += swy[threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sw[0];
+        part[2 * blockIdx.x + 1] = swy[0];
+    }
+}
+
+// U = U_lin + g c on free DOFs
+__global__ void k_apply(int n, const uint8_t* __restrict__ fixed, pg_pred_history h, double g,
+                        double* __restrict__ U) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
     const NodeHist r = node_hist(h, i);
-    const double y = Y ? fmax(-1.0, fmin(0.0, (double)Y[2 * i])) : 0.0;
-    const double g = Y ? scale * (1.0 + y) : 0.0;
     for (int d = 0; d < 2; ++d) {
         if (fixed[2 * i + d]) continue;
         U[2 * i + d] = h.U_n[2 * i + d] + (h.dt / h.dt_n) * r.dn[d] + g * r.c[d];
@@ -175,8 +208,34 @@ int launch_features(Ctx& c, const pg_pred_history& h, float* X, cudaStream_t s) 
     return PG_OK;
 }
 
-int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s) {
-    k_apply<<<nblk(c.n_nodes), kThreads, 0, s>>>(c.n_nodes, c.fixed, h, Y, scale, U);
+int predictor_blend(Ctx& c, const pg_pred_history& h, const float* Y, double& g, cudaStream_t s) {
+    constexpr int kParts = 148 * 2;
+    double* part = nullptr;
+    PG_CUDA(cudaMallocAsync((void**)&part, 2 * kParts * sizeof(double), s));
+    k_blend_partial<<<kParts, kBlendThreads, 0, s>>>(c.n_nodes, c.fixed, h, Y, part);
+    std::vector<double> hp(2 * kParts);
+    PG_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    cudaFreeAsync(part, s);
+    double w = 0.0, wy = 0.0;
+    for (int b = 0; b < kParts; ++b) {
+        w += hp[2 * b];
+        wy += hp[2 * b + 1];
+    }
+    g = w > 0.0 ? std::max(0.0, std::min(1.0, wy / w)) : 0.0;
+    return PG_OK;
+}
+
+int launch_apply(Ctx& c, const pg_pred_history& h, const float* Y, double scale, double* U, cudaStream_t s,
+                 double* g_used) {
+    double g = 0.0;
+    if (Y) {
+        const int rc = predictor_blend(c, h, Y, g, s);
+        if (rc) return rc;
+        g *= scale;
+    }
+    if (g_used) *g_used = g;
+    k_apply<<<nblk(c.n_nodes), kThreads, 0, s>>>(c.n_nodes, c.fixed, h, g, U);
     PG_CUDA(cudaGetLastError());
     return PG_OK;
 }
@@ -210,7 +269,7 @@ int pg_predictor_apply(pg_ctx* cx, const pg_pred_history* h, const float* Y_dev,
     if (!cx || !h || !U_dev || !history_ok(*h)) { set_error("pg_predictor_apply: bad argument"); return PG_ERR_ARG; }
     Ctx& c = cx->c;
     cudaSetDevice(c.device);
-    return launch_apply(c, *h, Y_dev, scale, U_dev, c.stream);
+    return launch_apply(c, *h, Y_dev, scale, U_dev, c.stream, nullptr);
 }
 
 int pg_ctx_attach_mlp(pg_ctx* cx, pg_mlp* m) {

@@ -332,10 +332,13 @@ int pg_set_vector(pg_ctx* c, int32_t which, const double* in);
 int pg_get_isv(pg_ctx* c, int32_t committed, double* out);/* n_cohesive_qp delta_max values */
 int pg_set_isv(pg_ctx* c, int32_t committed, const double* in);
 /* Device time of the last assembly, from CUDA events recorded on the assembly stream
- * while timing is enabled: ms_rows = the triangle kernel, ms_cut = from its end to the end
- * of the pass (the cut elements' work on the second stream, as far as it outlasts the
- * triangle kernel, and the fold).  Their sum is the pass.  Pass NULLs to only switch
- * timing on/off. */
+ * while timing is enabled.  enable = 1 (split): ms_rows = the triangle kernel, ms_cut =
+ * from its end to the end of the pass (the cut elements' kernels and the fold); the event
+ * between them keeps the cut kernels from starting in the triangle kernel's last wave.
+ * enable = 2 (whole pass): ms_rows = the pass, ms_cut = 0, with the cut kernels launched
+ * as programmatic dependents of the triangle kernel as in untimed passes.  0: off.  The
+ * values returned are those of the mode in force during the last assembly; pass NULLs
+ * to only switch modes. */
 int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut);
 
 /* ---- shape sensitivity ----

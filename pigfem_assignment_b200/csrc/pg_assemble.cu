@@ -695,6 +695,14 @@ __host__ __device__ inline unsigned grid_nbr_mask(int gi, int gj, int nx, int ny
            (e ? 32u : 0u) | (n && even && w ? 64u : 0u) | (n ? 128u : 0u) | (n && even && e ? 256u : 0u);
 }
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched with
+// launch_pdl may start while the kernel before it on the stream is still
+// running, once every CTA of that one has called pdl_trigger (or exited);
+// pdl_wait blocks until the kernel before has completed and its writes are
+// visible.  Both are no-ops for a kernel launched the ordinary way.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // One 2x2 block as a single 256-bit store (K is a cudaMalloc allocation, so
 // every block is 32-byte aligned).
 __device__ __forceinline__ void store_block(double* K, long long q, double k0, double k1, double k2, double k3) {
@@ -910,6 +918,7 @@ __device__ __forceinline__ void grid_node(const GridArgs& a, const int4 B, int g
 // every thread forms its node's row from shared memory.
 template <bool WK, bool WF, int TR>
 __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows(GridArgs a) {
+    pdl_trigger();  // the cut elements' row kernels may fill the SMs this grid frees
     constexpr int kGridThreads = kGridTileC * TR, kGridWinY = TR + 2, kGridCellY = TR + 1;
     __shared__ double2 sXY[kGridWinX * kGridWinY];
     __shared__ double2 sU[WF ? kGridWinX * kGridWinY : 1];
@@ -1004,6 +1013,7 @@ __device__ __forceinline__ void grid_stage_async(const GridArgs& a, int t, GridW
 // after the copy lands).
 template <bool WK, bool WF, int TR>
 __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows_pipe(GridArgs a, int n_tiles) {
+    pdl_trigger();
     __shared__ GridWin<TR, WF> W[3];
     int t = blockIdx.x;
     if (t >= n_tiles) return;
@@ -1155,6 +1165,7 @@ __global__ void __launch_bounds__(kPointThreads) k_cut_points(int n_pts, const i
                                                               const double* __restrict__ y,
                                                               const double* __restrict__ dmat, double* rows) {
     __shared__ __align__(16) double sRow[kPointThreads * kRowMax];
+    pdl_trigger();  // reads only the mesh: runs beside the triangle kernel's last CTAs
     const int p0 = blockIdx.x * kPointThreads, p = p0 + threadIdx.x;
     const int p1 = min(n_pts, p0 + kPointThreads);
     // the CTA's span of rows: from its first point's row to the next CTA's
@@ -1173,6 +1184,7 @@ __global__ void __launch_bounds__(kPointThreads) k_cut_points(int n_pts, const i
     const double2* src = reinterpret_cast<const double2*>(sRow);
     double2* dst = reinterpret_cast<double2*>(rows + base);
     for (int i = threadIdx.x; i < n2; i += kPointThreads) dst[i] = src[i];
+    pdl_wait();  // completes only after the kernel before it: the chain stays ordered
 }
 
 // One thread per cohesive Gauss point (CohEdge2, 2 points, w = 1): the law
@@ -1195,8 +1207,12 @@ struct CohArgs {
 };
 
 __global__ void __launch_bounds__(128) k_coh_points(CohArgs a) {
+    pdl_trigger();
     const int qp = blockIdx.x * blockDim.x + threadIdx.x;
-    if (qp >= a.n_qp) return;
+    if (qp >= a.n_qp) {
+        pdl_wait();
+        return;
+    }
     const int rec = __ldg(&a.coh_rec[qp]);
     const int ci = rec >> 8, ce = (rec >> 1) & 127, q = rec & 1;
     const DevTemplate& T = g_tmpl[__ldg(&a.cut_tmpl[ci])];
@@ -1239,6 +1255,7 @@ __global__ void __launch_bounds__(128) k_coh_points(CohArgs a) {
     row[7] = R[0][0] * tr[0] + R[1][0] * tr[1];
     row[8] = R[0][1] * tr[0] + R[1][1] * tr[1];
     row[9] = 0.0;
+    pdl_wait();
 }
 
 struct PairArgs {
@@ -1269,6 +1286,8 @@ __device__ __forceinline__ double2 ldg2(const double* p) { return __ldg(reinterp
 // the node's cohesive traction term.
 template <int NL>
 __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
+    pdl_wait();  // the rows of k_cut_points / k_coh_points
+    pdl_trigger();
     constexpr int P = NL * NL, W = 4 + 2 * NL;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int oi = (int)(t / P), p = (int)(t - (long long)oi * P);
@@ -1346,6 +1365,8 @@ __global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
 __global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restrict__ fold_slot,
                                                 const int* __restrict__ fold_ptr, const double* __restrict__ ke,
                                                 double* K) {
+    pdl_wait();  // the pair blocks, and (through the chain) the triangle kernel's K
+    pdl_trigger();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const long long sw = __ldg(&fold_slot[j]);
@@ -1368,6 +1389,8 @@ __global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restri
 __global__ void __launch_bounds__(256) k_fold_f(int n, const int* __restrict__ fold_node,
                                                 const int* __restrict__ fold_ptr, const double* __restrict__ fe,
                                                 double* f) {
+    pdl_wait();
+    pdl_trigger();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const int nw = __ldg(&fold_node[j]);
@@ -1906,10 +1929,27 @@ CutArgs cut_args(const Ctx& c, const double* U, double dt) {
     return ca;
 }
 
+// Launches kern with the programmatic-stream-serialization attribute (see
+// pdl_trigger / pdl_wait).
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 void launch_cut_points(const Ctx& c, cudaStream_t s) {
     if (c.n_cut_pts > 0)
-        k_cut_points<<<(c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, 0, s>>>(
-            c.n_cut_pts, reinterpret_cast<const int4*>(c.cut_pts), c.x, c.y, c.dmat, c.cut_rows);
+        launch_pdl(k_cut_points, (c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, s, c.n_cut_pts,
+                   reinterpret_cast<const int4*>(c.cut_pts), c.x, c.y, c.dmat, c.cut_rows);
 }
 
 void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s) {
@@ -1927,7 +1967,7 @@ void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s)
     ca.coh_rows = c.coh_rows;
     ca.coh = c.coh;
     ca.dt = dt;
-    k_coh_points<<<(c.n_coh_qp + 127) / 128, 128, 0, s>>>(ca);
+    launch_pdl(k_coh_points, (c.n_coh_qp + 127) / 128, 128, s, ca);
 }
 
 // one launch per size class; cut_warps x 32 threads per CTA
@@ -1955,10 +1995,10 @@ void launch_cut_pairs(const Ctx& c, const double* U, bool want_f, bool want_K, c
         pa.first = c.cut_class_off[k];
         const long long threads = (long long)n * kCutClassNl[k] * kCutClassNl[k];
         const int blocks = (int)((threads + bs - 1) / bs);
-        if (k == 0) k_cut_pairs<5><<<blocks, bs, 0, s>>>(pa);
-        else if (k == 1) k_cut_pairs<7><<<blocks, bs, 0, s>>>(pa);
-        else if (k == 2) k_cut_pairs<11><<<blocks, bs, 0, s>>>(pa);
-        else k_cut_pairs<15><<<blocks, bs, 0, s>>>(pa);
+        if (k == 0) launch_pdl(k_cut_pairs<5>, blocks, bs, s, pa);
+        else if (k == 1) launch_pdl(k_cut_pairs<7>, blocks, bs, s, pa);
+        else if (k == 2) launch_pdl(k_cut_pairs<11>, blocks, bs, s, pa);
+        else launch_pdl(k_cut_pairs<15>, blocks, bs, s, pa);
     }
 }
 
@@ -1970,9 +2010,9 @@ void launch_cut_rows(const Ctx& c, const double* U, double dt, cudaStream_t s) {
 
 void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, cudaStream_t s) {
     if (want_K && c.n_fold_K > 0)
-        k_fold_K<<<(c.n_fold_K + 255) / 256, 256, 0, s>>>(c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.cut_ke, c.K);
+        launch_pdl(k_fold_K, (c.n_fold_K + 255) / 256, 256, s, c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.cut_ke, c.K);
     if (want_f && c.n_fold_f > 0)
-        k_fold_f<<<(c.n_fold_f + 255) / 256, 256, 0, s>>>(c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.cut_fe, c.F);
+        launch_pdl(k_fold_f, (c.n_fold_f + 255) / 256, 256, s, c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.cut_fe, c.F);
 }
 
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
@@ -1990,7 +2030,7 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     if (c.timing) cudaEventRecord(c.ea0, s);
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
-    if (c.timing) cudaEventRecord(c.ea1, s);
+    if (c.timing && c.timing_split) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {
         launch_cut_rows(c, U, dt, s);
         launch_cut_pairs(c, U, want_f, want_K, s);

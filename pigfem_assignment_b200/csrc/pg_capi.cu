@@ -743,12 +743,18 @@ int pg_assembly_timing(pg_ctx* c, int32_t enable, float* ms_rows, float* ms_cut)
         if (!x.timing) { set_error("pg_assembly_timing: timing was not enabled"); return PG_ERR_STATE; }
         PG_CUDA(cudaEventSynchronize(x.ea2));
         float a = 0.f, b = 0.f;
-        PG_CUDA(cudaEventElapsedTime(&a, x.ea0, x.ea1));
-        PG_CUDA(cudaEventElapsedTime(&b, x.ea1, x.ea2));
+        if (x.timing_split) {
+            PG_CUDA(cudaEventElapsedTime(&a, x.ea0, x.ea1));
+            PG_CUDA(cudaEventElapsedTime(&b, x.ea1, x.ea2));
+        } else {
+            PG_CUDA(cudaEventElapsedTime(&a, x.ea0, x.ea2));
+        }
         if (ms_rows) *ms_rows = a;
         if (ms_cut) *ms_cut = b;
     }
+    if (enable < 0 || enable > 2) { set_error("pg_assembly_timing: enable is 0, 1 or 2"); return PG_ERR_ARG; }
     x.timing = enable != 0;
+    x.timing_split = enable == 1;
     return PG_OK;
 }
 

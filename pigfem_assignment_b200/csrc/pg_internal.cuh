@@ -210,6 +210,7 @@ struct Ctx {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool timing = false;
+    bool timing_split = false;         // an event between the triangle kernel and the cut kernels too
     // stress/strain recovery (stress_prepare, on first use): per element its
     // first volumetric quadrature point, the cut flags, class order -> mesh
     // element, class offsets, and 7 FP64 per point of output

@@ -63,7 +63,7 @@ def parse():
                     help="run one small fixed workload for an ncu capture and exit (no JSON line)")
     ap.add_argument("--full-configs", action="store_true",
                     help="also run configurations 2 (50 steps) and 4 (1024^2, 20 steps) in full, every arm")
-    ap.add_argument("--train-rves", type=int, default=3,
+    ap.add_argument("--train-rves", type=int, default=8,
                     help="RVEs whose first 25 steps train the learned predictor")
     ap.add_argument("--viscosity", type=float, default=200.0,
                     help="bilinear-law viscosity of the cohesive comparison (MPa s/mm)")
@@ -498,7 +498,7 @@ def run_b200_arm(args):
 
 
 
-def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: int = 25, t_window=(0.5, 0.6),
+def cohesive_load_steps(local: int, eta: float, n_train: int = 8, train_steps: int = 25, t_window=(0.5, 0.6),
                         keep_mlp=None):
     """Time per cohesive load step at 1e-8 relative Newton residual on the
     256x256 RVE (131,072 TRI3, 40 seeded circles r ~ U[0.03, 0.06], bilinear
@@ -533,7 +533,7 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
     # training trajectories use the reference's SNES tests (rtol of the predictor, stol)
     xs, ts = [], []
     for k in range(n_train):
-        x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.0, seed=k,
+        x, t, _ = trajectory_samples(with_eta(config2(seed=100 + k)), 50, train_steps, keep_fraction=0.02, seed=k,
                                      device=local, newton=dict(precond=_lib.PG_PREC_MG, lin_max_iter=1000))
         xs.append(x)
         ts.append(t)
@@ -542,8 +542,9 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
     perm = np.random.default_rng(0).permutation(len(X))
     dev = f"cuda:{local}"
     mlp = MLP(device=local, seed=1)
-    hist = mlp.train(torch.from_numpy(X[perm]).to(dev), torch.from_numpy(T[perm]).to(dev), epochs=40, batch=8192,
-                     lr=2e-3)
+    mlp.zero_output_layer(-1.0)  # starts as the linear extrapolation
+    hist = mlp.train(torch.from_numpy(X[perm]).to(dev), torch.from_numpy(T[perm]).to(dev), epochs=60, batch=8192,
+                     lr=5e-4)
     train_s = time.perf_counter() - t0
 
     rve = with_eta(config2())
@@ -584,6 +585,8 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 3, train_steps: i
                 float(np.median([r.res_learned / r.res_linear for r in R if r.res_linear > 0 and r.res_learned > 0]))
                 if any(r.res_linear > 0 and r.res_learned > 0 for r in R) else None),
             "max_final_res_over_base": float(max((r.res / r.res_base) for r in R if r.res_base > 0)) if R else None,
+            "learned_blend_median": (float(np.median([r.blend for r in R if r.blend >= 0]))
+                                     if any(r.blend >= 0 for r in R) else None),
         }
         if pred == _lib.PG_PREDICT_LEARNED:
             _lib.check(_lib.lib.pg_ctx_attach_mlp(prob.ctx.handle, None))

@@ -58,7 +58,7 @@ cudaStream_t pick(Ctx& c, void* s) { return s ? (cudaStream_t)s : c.stream; }
 
 void free_ctx(Ctx& c) {
     mg_free(c);
-    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.Uold2, c.isv_prev, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
+    void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.Uold2, c.isv_prev, c.red_ws, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
                     c.grid_rves, c.grid_tiles[0], c.grid_tiles[1], c.qp_off, c.qp_elem_cut, c.qp_cut_elem,
                     c.qp_class_off, c.qp_out,
@@ -283,6 +283,15 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
     if ((rc = dev_alloc(&c.minvf, 4 * nn))) return rc;
     if ((rc = dev_alloc(&c.hbuf, 128))) return rc;
     if ((rc = dev_alloc(&c.scal, 64))) return rc;
+    {
+        // the largest grid of a reduction: a thread per DOF, or kRowLanes per node row
+        const int cap = (int)std::max<long long>({((long long)nd + kThreads - 1) / kThreads,
+                                                  ((long long)kRowLanes * (long long)nn + kThreads - 1) / kThreads,
+                                                  1184LL}) + 1;
+        if ((rc = dev_alloc(&c.red_ws, red_ws_doubles(cap)))) return rc;
+        const double capd = (double)cap;
+        PG_CUDA(cudaMemcpy(c.red_ws, &capd, sizeof(double), cudaMemcpyHostToDevice));
+    }
     if ((rc = dev_alloc(&c.iflags, 64))) return rc;
     PG_CUDA(cudaMallocHost((void**)&c.h_scal, 64 * sizeof(double)));
     PG_CUDA(cudaMallocHost((void**)&c.h_iflags, 64 * sizeof(int)));

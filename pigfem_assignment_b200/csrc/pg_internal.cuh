@@ -197,6 +197,7 @@ struct Ctx {
     float* featX = nullptr;            // 16 features per node
     float* featY = nullptr;            // 2 outputs per node
     double* scal = nullptr;            // device scalars
+    double* red_ws = nullptr;          // deterministic grid-sum workspace (grid_add)
     int* iflags = nullptr;             // device flags
     double* h_scal = nullptr;          // pinned host mirror
     int* h_iflags = nullptr;

@@ -629,7 +629,8 @@ __global__ void k_mgcg_s1(double* sc, const int* fl) {
 __global__ void __launch_bounds__(kThreads) k_mgcg_spmv(int n, const int* __restrict__ row_ptr,
                                                         const int* __restrict__ col, const double* __restrict__ K,
                                                         const double* __restrict__ p, const uint8_t* __restrict__ fixed,
-                                                        double* __restrict__ q, double* sc, const int* fl) {
+                                                        double* __restrict__ q, double* sc, const int* fl,
+                                                        double* ws) {
     if (fl[0]) return;
     // kRowLanes lanes per block row (bsr_row_group); lane 0 of each group finishes the row
     const int t = blockIdx.x * kThreads + threadIdx.x;
@@ -645,12 +646,12 @@ __global__ void __launch_bounds__(kThreads) k_mgcg_spmv(int n, const int* __rest
         part = p[2 * i] * y0 + p[2 * i + 1] * y1;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&sc[0], s);
+    grid_add(ws, 0, s, &sc[0]);
 }
 
 __global__ void __launch_bounds__(kThreads) k_mgcg_update(int nd, double* __restrict__ x, double* __restrict__ r,
                                                           const double* __restrict__ p, const double* __restrict__ q,
-                                                          double* sc, int* fl) {
+                                                          double* sc, int* fl, double* ws) {
     if (fl[0]) return;
     const double pq = sc[0];
     if (!(pq > 0.0)) {
@@ -670,7 +671,7 @@ __global__ void __launch_bounds__(kThreads) k_mgcg_update(int nd, double* __rest
         part = ri * ri;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&sc[3], s);
+    grid_add(ws, 1, s, &sc[3]);
 }
 
 __global__ void k_mgcg_s2(double* sc, int* fl) {
@@ -681,12 +682,12 @@ __global__ void k_mgcg_s2(double* sc, int* fl) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_mgcg_dot(int nd, const double* __restrict__ a, const double* __restrict__ b,
-                                                       double* out, const int* fl) {
+                                                       double* out, const int* fl, double* ws) {
     if (fl[0]) return;
     const int i = blockIdx.x * kThreads + threadIdx.x;
     const double v = i < nd ? a[i] * b[i] : 0.0;
     const double s = block_sum(v);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+    grid_add(ws, 2, s, out);
 }
 
 __global__ void __launch_bounds__(kThreads) k_mgcg_pupdate(int nd, const double* __restrict__ z, double* __restrict__ p,
@@ -699,7 +700,7 @@ __global__ void __launch_bounds__(kThreads) k_mgcg_pupdate(int nd, const double*
 
 __global__ void __launch_bounds__(kThreads) k_mgcg_start(int nd, const uint8_t* __restrict__ fixed,
                                                          const double* __restrict__ b, double* __restrict__ r,
-                                                         double* __restrict__ x, double* sc) {
+                                                         double* __restrict__ x, double* sc, double* ws) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     double part = 0.0;
     if (i < nd) {
@@ -709,7 +710,7 @@ __global__ void __launch_bounds__(kThreads) k_mgcg_start(int nd, const uint8_t* 
         part = v * v;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&sc[3], s);
+    grid_add(ws, 1, s, &sc[3]);
 }
 
 __global__ void k_mgcg_tol(double* sc, double rtol2) { sc[4] = rtol2 * sc[3]; }
@@ -1259,12 +1260,12 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
     if ((rc = mg_numeric(c, f32, s))) return rc;
     const int n = c.n_nodes, nd = c.n_dof;
     cudaMemsetAsync(m.sc, 0, 8 * sizeof(double), s);
-    k_mgcg_start<<<nb(nd), kThreads, 0, s>>>(nd, c.fixed, c.b, c.r, c.dx, m.sc);
+    k_mgcg_start<<<nb(nd), kThreads, 0, s>>>(nd, c.fixed, c.b, c.r, c.dx, m.sc, c.red_ws);
     k_mgcg_tol<<<1, 1, 0, s>>>(m.sc, cfg.rtol * cfg.rtol);
     // z = V(r), p = z, sc[2] = r.z
     mg_apply(c, m, f32, s, c.r, c.z, nullptr);
     k_copy<double><<<nb(nd), kThreads, 0, s>>>(nd, c.z, c.p);
-    k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl);
+    k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_ws);
     int hf[8] = {};
     double hs[8] = {};
     cudaMemcpyAsync(hs, m.sc, sizeof hs, cudaMemcpyDeviceToHost, s);
@@ -1284,11 +1285,12 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
         PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int it = 0; it < kChunk; ++it) {
             k_mgcg_s1<<<1, 1, 0, s>>>(m.sc, m.fl);
-            k_mgcg_spmv<<<nb(kRowLanes * n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.p, c.fixed, c.q, m.sc, m.fl);
-            k_mgcg_update<<<nb(nd), kThreads, 0, s>>>(nd, c.dx, c.r, c.p, c.q, m.sc, m.fl);
+            k_mgcg_spmv<<<nb(kRowLanes * n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.p, c.fixed, c.q, m.sc, m.fl,
+                                                                 c.red_ws);
+            k_mgcg_update<<<nb(nd), kThreads, 0, s>>>(nd, c.dx, c.r, c.p, c.q, m.sc, m.fl, c.red_ws);
             k_mgcg_s2<<<1, 1, 0, s>>>(m.sc, m.fl);
             mg_apply(c, m, f32, s, c.r, c.z, m.fl);
-            k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl);
+            k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_ws);
             k_mgcg_pupdate<<<nb(nd), kThreads, 0, s>>>(nd, c.z, c.p, m.sc, m.fl);
         }
         PG_CUDA(cudaStreamEndCapture(s, &graph));

@@ -51,7 +51,10 @@ constexpr size_t kOffQ = kOffP + 2 * (size_t)kStaticMaxNodes;
 constexpr size_t kOffMinv = kOffQ + 2 * (size_t)kStaticMaxNodes;
 constexpr size_t kOffScal = kOffMinv + 4 * (size_t)kStaticMaxNodes;
 constexpr size_t kOffFlags = kOffScal + S_NSCAL;
-constexpr size_t kScratchDoubles = kOffFlags + F_NFLAGS;
+// the deterministic grid sums' workspace (grid_add): one partial per block of the largest grid
+constexpr int kStaticRedCap = (kStaticMaxNodes + kThreads - 1) / kThreads + 1;
+constexpr size_t kOffRed = kOffFlags + F_NFLAGS;
+constexpr size_t kScratchDoubles = kOffRed + (size_t)kRedHeader + (size_t)kRedSlots * kStaticRedCap;
 
 // In host code this name is only a handle for cudaGetSymbolAddress, not a
 // device address.
@@ -59,6 +62,12 @@ static __device__ __align__(256) double g_pcg_scratch[kScratchDoubles];
 
 std::mutex g_setup_mutex;
 double* g_scratch_dev[64] = {};
+
+// the workspace's capacity and cleared tickets
+__global__ void k_static_red_init(double* ws) {
+    if (threadIdx.x == 0) ws[0] = (double)kStaticRedCap;
+    if (threadIdx.x > 0 && threadIdx.x < kRedHeader) ws[threadIdx.x] = 0.0;
+}
 
 // Block-Jacobi inverse of each node's masked 2x2 diagonal block, found by
 // scanning the row for the diagonal column (the caller's pattern carries
@@ -112,7 +121,7 @@ __global__ void __launch_bounds__(kThreads) k_static_resid(int n, const int* __r
                                                            const int* __restrict__ col, const double* __restrict__ K,
                                                            const double* __restrict__ x,
                                                            const uint8_t* __restrict__ fixed,
-                                                           const double* __restrict__ b, double* out) {
+                                                           const double* __restrict__ b, double* out, double* ws) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     double rr = 0.0, bb = 0.0;
     if (i < n) {
@@ -125,10 +134,8 @@ __global__ void __launch_bounds__(kThreads) k_static_resid(int n, const int* __r
     }
     const double a = block_sum(rr);
     const double c = block_sum(bb);
-    if (threadIdx.x == 0) {
-        atomicAdd(&out[0], a);
-        atomicAdd(&out[1], c);
-    }
+    grid_add(ws, 1, a, &out[0]);
+    grid_add(ws, 2, c, &out[1]);
 }
 
 // Device address of the scratch array on the current device (looked up once).
@@ -185,13 +192,15 @@ int pcg_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, cons
     double* minv = base + kOffMinv;
     double* scal = base + kOffScal;
     int* flags = reinterpret_cast<int*>(base + kOffFlags);
+    double* ws = base + kOffRed;
     const int gb = (n + kThreads - 1) / kThreads, gd = (nd + kThreads - 1) / kThreads;
 
     cudaError_t e = cudaMemsetAsync(scal, 0, (S_NSCAL + F_NFLAGS) * sizeof(double), s);
     if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: clearing the scalars and flags");
+    k_static_red_init<<<1, kRedHeader, 0, s>>>(ws);
     k_static_start<<<gd, kThreads, 0, s>>>(nd, fixed, b, r, x);
     k_static_prec<<<gb, kThreads, 0, s>>>(n, row_ptr, col, K, fixed, minv, flags);
-    k_cg_init<double, double><<<gb, kThreads, 0, s>>>(n, r, z, p, minv, scal);
+    k_cg_init<double, double><<<gb, kThreads, 0, s>>>(n, r, z, p, minv, scal, ws);
     k_static_tol<<<1, 1, 0, s>>>(scal, rtol * rtol);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: launch");
@@ -217,8 +226,8 @@ int pcg_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, cons
         const int m = max_iter - launched < kStaticChunk ? max_iter - launched : kStaticChunk;
         for (int it = 0; it < m; ++it) {
             const int P = (launched + it) & 1;
-            k_spmv_cg<double, double><<<gb, kThreads, 0, s>>>(n, P, row_ptr, col, K, p, fixed, q, scal, flags);
-            k_cg_update<double, double><<<gb, kThreads, 0, s>>>(n, P, x, r, z, p, q, minv, scal, flags);
+            k_spmv_cg<double, double><<<gb, kThreads, 0, s>>>(n, P, row_ptr, col, K, p, fixed, q, scal, flags, ws);
+            k_cg_update<double, double><<<gb, kThreads, 0, s>>>(n, P, x, r, z, p, q, minv, scal, flags, ws);
             k_cg_pupdate<double><<<gb, kThreads, 0, s>>>(n, P, z, p, scal, flags);
         }
         launched += m;
@@ -231,7 +240,7 @@ int pcg_static(int32_t n_nodes, const int32_t* row_ptr, const int32_t* col, cons
     // true residual of the returned x (the q slot of the scratch is free now)
     e = cudaMemsetAsync(q, 0, 2 * sizeof(double), s);
     if (e != cudaSuccess) return cuda_fail(e, "pg_pcg_solve_static: clearing the residual accumulator");
-    k_static_resid<<<gb, kThreads, 0, s>>>(n, row_ptr, col, K, x, fixed, b, q);
+    k_static_resid<<<gb, kThreads, 0, s>>>(n, row_ptr, col, K, x, fixed, b, q, ws);
     double res[2] = {0.0, 0.0};
     e = cudaMemcpyAsync(res, q, sizeof res, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -18,6 +18,15 @@ enum : int {
 };
 enum : int { F_DONE = 0, F_BREAKDOWN = 1, F_ITERS = 2, F_NFLAGS = 8 };
 
+// Deterministic grid sums.  A reduction workspace holds its slot capacity
+// (ws[0], in blocks), kRedSlots arrival tickets (from ws[1], two per double)
+// and kRedSlots x capacity block partials (from ws[kRedHeader]).  Slots:
+// 0-3 for the scalar sums of one kernel, 4 + j for the j-th product of the
+// GMRES multi-dot.  Sequential kernels on one stream may reuse a slot.
+constexpr int kRedSlots = 72;
+constexpr int kRedHeader = 40;
+inline size_t red_ws_doubles(int cap) { return (size_t)kRedHeader + (size_t)kRedSlots * (size_t)cap; }
+
 __device__ __forceinline__ double block_sum(double d) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
@@ -33,6 +42,41 @@ __device__ __forceinline__ double block_sum(double d) {
         for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
     }
     return d;  // valid in thread 0
+}
+
+// Adds the sum over the grid's blocks of s (each block's s valid in its
+// thread 0) to *out in a fixed order: every block stores its s in the slot's
+// partials, and the last block to take a ticket adds them in block order
+// (a fixed tree over fixed strided sums) -- the same bits on every run,
+// where atomically added block sums vary with the blocks' arrival.  Every
+// thread of the block must call it.  A grid larger than the workspace's
+// capacity falls back to the atomic sum.
+__device__ __forceinline__ void grid_add(double* ws, int slot, double s, double* out) {
+    __shared__ int s_last;
+    const int cap = (int)ws[0];
+    if ((int)gridDim.x > cap) {
+        if (threadIdx.x == 0) atomicAdd(out, s);
+        return;
+    }
+    unsigned* tickets = reinterpret_cast<unsigned*>(ws + 1);
+    double* part = ws + kRedHeader + (size_t)slot * cap;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        __threadfence();
+        const unsigned t = atomicAdd(&tickets[slot], 1u);
+        s_last = (t == gridDim.x - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc += __ldcg(&part[b]);
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) {
+            *out += acc;
+            tickets[slot] = 0u;
+        }
+    }
 }
 
 // y_i = sum_j K_ij x_j over 2x2 blocks (FP64 accumulation), masked rows zeroed
@@ -127,7 +171,7 @@ template <typename MT, typename VT>
 __global__ void __launch_bounds__(kThreads) k_spmv_cg(int n, int P, const int* __restrict__ row_ptr, const int* __restrict__ col,
                                                        const MT* __restrict__ K, const VT* __restrict__ p,
                                                        const uint8_t* __restrict__ fixed, VT* __restrict__ q, double* scal,
-                                                       const int* flags) {
+                                                       const int* flags, double* ws) {
     if (flags[F_DONE]) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         scal[S_RZ0 + P] = 0.0;
@@ -145,7 +189,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_cg(int n, int P, const int* _
         part = (double)p[2 * i] * (double)q0 + (double)p[2 * i + 1] * (double)q1;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&scal[S_PQ0 + P], s);
+    grid_add(ws, 0, s, &scal[S_PQ0 + P]);
 }
 
 template <typename VT>
@@ -163,7 +207,7 @@ __device__ __forceinline__ void apply_prec(const PT* __restrict__ minv, int node
 
 template <typename VT, typename PT>
 __global__ void __launch_bounds__(kThreads) k_cg_init(int n, const VT* __restrict__ r, VT* __restrict__ z, VT* __restrict__ p,
-                                                       const PT* __restrict__ minv, double* scal) {
+                                                       const PT* __restrict__ minv, double* scal, double* ws) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     double prz = 0.0, prr = 0.0;
     if (i < n) {
@@ -179,16 +223,15 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int n, const VT* __restric
     }
     const double a = block_sum(prz);
     const double b = block_sum(prr);
-    if (threadIdx.x == 0) {
-        atomicAdd(&scal[S_RZ0 + 1], a);
-        atomicAdd(&scal[S_RR0 + 1], b);
-    }
+    grid_add(ws, 1, a, &scal[S_RZ0 + 1]);
+    grid_add(ws, 2, b, &scal[S_RR0 + 1]);
 }
 
 template <typename VT, typename PT>
 __global__ void __launch_bounds__(kThreads) k_cg_update(int n, int P, VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ z,
                                                          const VT* __restrict__ p, const VT* __restrict__ q,
-                                                         const PT* __restrict__ minv, double* scal, int* flags) {
+                                                         const PT* __restrict__ minv, double* scal, int* flags,
+                                                         double* ws) {
     if (flags[F_DONE]) return;
     const int Q = 1 - P;
     const double pq = scal[S_PQ0 + P];
@@ -218,13 +261,11 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(int n, int P, VT* __rest
     }
     const double a = block_sum(prz);
     const double b = block_sum(prr);
-    if (threadIdx.x == 0) {
-        atomicAdd(&scal[S_RZ0 + P], a);
-        atomicAdd(&scal[S_RR0 + P], b);
-        if (blockIdx.x == 0) {
-            scal[S_PQ0 + Q] = 0.0;
-            flags[F_ITERS] += 1;
-        }
+    grid_add(ws, 1, a, &scal[S_RZ0 + P]);
+    grid_add(ws, 2, b, &scal[S_RR0 + P]);
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        scal[S_PQ0 + Q] = 0.0;
+        flags[F_ITERS] += 1;
     }
 }
 
@@ -293,11 +334,11 @@ __global__ inline void k_to_float_scaled(int nd, const double* __restrict__ a, f
     if (i < nd) b[i] = (float)(a[i] * s);
 }
 
-__global__ inline void k_dot_self(int nd, const double* __restrict__ a, double* out) {
+__global__ inline void k_dot_self(int nd, const double* __restrict__ a, double* out, double* ws) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     const double v = (i < nd) ? a[i] * a[i] : 0.0;
     const double s = block_sum(v);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+    grid_add(ws, 3, s, out);
 }
 
 __global__ inline void k_apply_dirichlet(int nd, const uint8_t* __restrict__ fixed, const double* __restrict__ ubar,
@@ -341,13 +382,13 @@ __global__ inline void k_apply_prec_vec(int n, const double* __restrict__ minv, 
 
 // out[j] += V_j . w for j < k (V: k vectors of length nd, contiguous)
 __global__ inline void k_multidot(int nd, int k, const double* __restrict__ V, const double* __restrict__ w,
-                                  double* out) {
+                                  double* out, double* ws) {
     for (int j = 0; j < k; ++j) {
         const double* vj = V + (size_t)j * nd;
         double part = 0.0;
         for (int i = blockIdx.x * kThreads + threadIdx.x; i < nd; i += gridDim.x * kThreads) part += vj[i] * w[i];
         const double s = block_sum(part);
-        if (threadIdx.x == 0) atomicAdd(&out[j], s);
+        grid_add(ws, 4 + j, s, &out[j]);
     }
 }
 
@@ -391,7 +432,8 @@ template <typename MT>
 __global__ void __launch_bounds__(kThreads) k_mr_av(int n, const int* __restrict__ row_ptr, const int* __restrict__ col,
                                                     const MT* __restrict__ K, const double* __restrict__ v,
                                                     const uint8_t* __restrict__ fixed, const double* __restrict__ r1,
-                                                    double* __restrict__ y, double* scal, const int* flags) {
+                                                    double* __restrict__ y, double* scal, const int* flags,
+                                                    double* ws) {
     if (flags[F_DONE]) return;
     const double c = scal[M_OLDB] > 0.0 ? scal[M_BETA] / scal[M_OLDB] : 0.0;
     const int i = blockIdx.x * kThreads + threadIdx.x;
@@ -406,13 +448,14 @@ __global__ void __launch_bounds__(kThreads) k_mr_av(int n, const int* __restrict
         part = v[2 * i] * y0 + v[2 * i + 1] * y1;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&scal[M_ALFA], s);
+    grid_add(ws, 0, s, &scal[M_ALFA]);
 }
 
 // y -= (alfa/beta) r2; r2new = y (written over r1); z = M^-1 r2new (into y); bb += r2new.z
 __global__ inline void __launch_bounds__(kThreads) k_mr_2(int n, double* __restrict__ y, const double* __restrict__ r2,
                                                            double* __restrict__ r1_to_r2new,
-                                                           const double* __restrict__ minv, double* scal, const int* flags) {
+                                                           const double* __restrict__ minv, double* scal, const int* flags,
+                                                           double* ws) {
     if (flags[F_DONE]) return;
     const double c = scal[M_ALFA] / scal[M_BETA];
     const int i = blockIdx.x * kThreads + threadIdx.x;
@@ -428,7 +471,7 @@ __global__ inline void __launch_bounds__(kThreads) k_mr_2(int n, double* __restr
         part = a0 * z0 + a1 * z1;
     }
     const double s = block_sum(part);
-    if (threadIdx.x == 0) atomicAdd(&scal[M_BB], s);
+    grid_add(ws, 1, s, &scal[M_BB]);
 }
 
 // Lanczos / Givens scalar recurrences of MINRES (Paige & Saunders 1975)
@@ -489,11 +532,12 @@ __global__ inline void k_prec_absjacobi(int n, const int* __restrict__ diag, con
     m[3] = fixed[2 * i + 1] ? 0.0 : 1.0 / fabs(b[3]);
 }
 
-__global__ inline void k_dot2(int nd, const double* __restrict__ a, const double* __restrict__ b, double* out) {
+__global__ inline void k_dot2(int nd, const double* __restrict__ a, const double* __restrict__ b, double* out,
+                              double* ws) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     const double v = (i < nd) ? a[i] * b[i] : 0.0;
     const double s = block_sum(v);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+    grid_add(ws, 3, s, out);
 }
 
 // out = mask(a)

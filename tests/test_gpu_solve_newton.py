@@ -81,3 +81,28 @@ def test_gpu_solve_nonlinear_driver_records_steps():
     assert all(r.reason > 0 for r in recs)
     assert abs(sum(r.dt for r in recs) - 1.0) < 1e-12
     prob.ctx.close()
+
+
+@pytest.mark.parametrize("precision", [_lib.PG_PRECISION_FP64, _lib.PG_PRECISION_MIXED])
+def test_cohesive_load_stepping_is_bit_reproducible(precision):
+    """The Krylov dot products add their block sums in a fixed order, so a
+    softening load path -- where rounding differences grow into different
+    Newton and Krylov iteration counts -- is the same on every run, bit for
+    bit."""
+    from pigfem_assignment_b200.rve import config2
+    rve = config2(nx=64, n_inc=8)
+    rve.coh_params = tuple(rve.coh_params[:4]) + (200.0,)
+    runs = []
+    for _ in range(2):
+        prob = pb.ProblemNonlinearStructural(rve)
+        prob.init()
+        prob.configure(n_steps=50, T_final=1.0, t_start=0.0, t_stop=0.4, precision=precision,
+                       predictor=_lib.PG_PREDICT_LINEAR, precond=_lib.PG_PREC_MG, stol=0.0,
+                       rtol_base=_lib.PG_RTOL_BASE_ZEROTH, lin_max_iter=1000)
+        recs = prob.solve_problem()
+        runs.append((prob.get_solution(), prob.ctx.isv(committed=True),
+                     [(r.newton_its, r.krylov_its, r.repeats) for r in recs]))
+        prob.ctx.close()
+    assert runs[0][2] == runs[1][2]
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])

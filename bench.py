@@ -315,7 +315,10 @@ def run_b200_arm(args):
         _lib.check(_lib.lib.pg_ctx_tuning(ctx.handle, C.byref(t_tile), C.byref(t_pers), C.byref(t_warps)))
     tri_kernel = (("k_grid_rows_pipe" if t_pers.value else "k_grid_rows") if t_tile.value in (128, 256)
                   else "k_assemble_tri")
+    ov = C.c_int32()
+    _lib.check(_lib.lib.pg_ctx_cut_overlap(ctx.handle, -1, C.byref(ov)))
     tuning = {"tri_tile_nodes": t_tile.value, "tri_persistent": t_pers.value, "cut_warps_per_cta": t_warps.value,
+              "cut_overlap_cta_slots": ov.value,
               "ms_tri_rows32_rows32p_rows64_rows64p_grid": [round(v, 4) for v in ms_tri],
               "ms_cut_w2_w4_w8": [round(v, 4) for v in ms_cut]}
 

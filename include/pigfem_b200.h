@@ -385,6 +385,11 @@ int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
  * for either; warps 2/4/8 per CTA of the cut elements' pair kernel) */
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
 int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
+/* With the persistent structured-grid kernel: the CTA slots per SM it leaves to the cut
+ * elements' row and pair kernels, which then run beside it on a second stream (0: after it
+ * on the same stream; the autotuner times 0, 1 and 2 on whole passes).  set < 0 only reads;
+ * get may be NULL. */
+int pg_ctx_cut_overlap(pg_ctx* c, int32_t set, int32_t* get);
 
 /* ---- batches of independent linear-elastic RVEs ----
  * No counterpart in the reference, which solves one RVE per run

@@ -154,6 +154,7 @@ def _load() -> C.CDLL:
         "pg_ctx_autotune": ([v, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
         "pg_ctx_tuning": ([v, _ip, _ip, _ip], C.c_int),
         "pg_ctx_set_tuning": ([v, C.c_int32, C.c_int32, C.c_int32], C.c_int),
+        "pg_ctx_cut_overlap": ([v, C.c_int32, _ip], C.c_int),
         "pg_batch_create": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
         "pg_batch_destroy": ([v], None),
         "pg_batch_context": ([v], C.c_void_p),
@@ -208,7 +209,7 @@ DECLARED_SYMBOLS = (
     "pg_get_vector", "pg_set_vector", "pg_get_isv", "pg_set_isv", "pg_assembly_timing", "pg_newton_cfg_default", "pg_newton_load_step",
     "pg_solve_nonlinear", "pg_mlp_create", "pg_mlp_destroy", "pg_mlp_param_count", "pg_mlp_params",
     "pg_mlp_grads", "pg_mlp_forward", "pg_mlp_gradient", "pg_mlp_adam", "pg_mlp_train", "pg_mlp_wait_selftest", "pg_predictor_features",
-    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_sensitivity_c11", "pg_sensitivity_shape", "pg_ctx_autotune", "pg_ctx_tuning", "pg_ctx_set_tuning", "pg_batch_create", "pg_batch_destroy", "pg_batch_context", "pg_batch_setup_times",
+    "pg_predictor_targets", "pg_predictor_apply", "pg_ctx_attach_mlp", "pg_sensitivity_c11", "pg_sensitivity_shape", "pg_ctx_autotune", "pg_ctx_tuning", "pg_ctx_set_tuning", "pg_ctx_cut_overlap", "pg_batch_create", "pg_batch_destroy", "pg_batch_context", "pg_batch_setup_times",
     "pg_batch_info", "pg_batch_solve", "pg_batch_get_solution", "pg_pcg_solve_static", "pg_last_error",
     "pg_version",
 )

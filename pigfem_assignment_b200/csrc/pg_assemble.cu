@@ -1101,6 +1101,7 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         auto go = [&](auto kern) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGridTileC * tr, 0);
+            if (c.tuning.cut_overlap > 0 && c.n_cut > 0) per_sm -= c.tuning.cut_overlap;  // room for the cut kernels
             const int grid = std::min(blocks, std::max(1, per_sm) * n_sm);
             kern<<<grid, kGridTileC * tr, 0, s>>>(ga, blocks);
         };
@@ -2028,6 +2029,23 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     }
     const RowArgs ra = row_args(c, U, want_f, want_K);
     if (c.timing) cudaEventRecord(c.ea0, s);
+    const bool overlap = c.n_cut > 0 && c.tuning.cut_overlap > 0 && c.tuning.tri_persistent && c.tuning.tri_grid &&
+                         c.grid_emat && !(c.timing && c.timing_split);
+    if (overlap) {
+        // the cut elements' rows and pairs on the second stream, beside the
+        // persistent grid kernel (which leaves them CTA slots); the fold joins
+        PG_CUDA(cudaEventRecord(c.fork_ev, s));
+        PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
+        launch_cut_rows(c, U, dt, c.aux);
+        launch_cut_pairs(c, U, want_f, want_K, c.aux);
+        PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
+        launch_tri(c, ra, want_f, s);
+        PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
+        launch_cut_fold(c, want_f, want_K, s);
+        PG_CUDA(cudaGetLastError());
+        if (c.timing) cudaEventRecord(c.ea2, s);
+        return PG_OK;
+    }
     launch_tri(c, ra, want_f, s);
     PG_CUDA(cudaGetLastError());
     if (c.timing && c.timing_split) cudaEventRecord(c.ea1, s);
@@ -2129,6 +2147,21 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
         if (ms < best_cut) {
             best_cut = ms;
             best.cut_warps = warps[k];
+        }
+    }
+    // with the persistent grid kernel: the whole pass with the cut kernels
+    // after it, or beside it with 1 or 2 CTA slots per SM left to them
+    best.cut_overlap = 0;
+    if (c.n_cut > 0 && best.tri_grid && best.tri_persistent && c.grid_emat) {
+        c.tuning = best;
+        float best_pass = 1e30f;
+        for (int ov = 0; ov <= 2; ++ov) {
+            c.tuning.cut_overlap = ov;
+            const float ms = timed([&] { launch_assemble(c, c.U, 1.0, false, true, s); });
+            if (ms < best_pass) {
+                best_pass = ms;
+                best.cut_overlap = ov;
+            }
         }
     }
     c.tuning = best;

@@ -549,6 +549,16 @@ int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent,
     return PG_OK;
 }
 
+int pg_ctx_cut_overlap(pg_ctx* c, int32_t set, int32_t* get) {
+    PG_GUARD_CTX(c);
+    if (set >= 0) {
+        if (set > 2) { set_error("pg_ctx_cut_overlap: 0, 1 or 2 CTA slots per SM"); return PG_ERR_ARG; }
+        c->c.tuning.cut_overlap = set;
+    }
+    if (get) *get = c->c.tuning.cut_overlap;
+    return PG_OK;
+}
+
 int pg_ctx_sync(pg_ctx* c) {
     PG_GUARD_CTX(c);
     PG_CUDA(cudaStreamSynchronize(c->c.stream));

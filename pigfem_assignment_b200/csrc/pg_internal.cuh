@@ -98,6 +98,10 @@ struct AsmTuning {
     int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
     int cut_warps = 4;     // 2, 4 or 8
+    // with the persistent structured-grid kernel: CTA slots per SM it leaves to
+    // the cut elements' row and pair kernels, which then run beside it on a
+    // second stream (0: after it, on the same stream)
+    int cut_overlap = 0;
 };
 
 struct Ctx {

@@ -87,8 +87,9 @@ def test_autotune_times_every_shape_and_keeps_the_fastest():
 
 @pytest.mark.parametrize("tile", [128, 256])
 def test_pipelined_grid_kernel_writes_the_same_bits(tile):
-    # the persistent kernel stages the next tile asynchronously; the values it
-    # forms are the same arithmetic on the same inputs: identical K and f
+    # the persistent kernel stages the next tile asynchronously, and the cut
+    # kernels may run beside it on a second stream; the values are the same
+    # arithmetic on the same inputs: identical K and f
     from pigfem_assignment_b200.rve import config1, scaled
     rve = scaled(config1(), 256)
     m = pb.Mesh(rve)
@@ -96,10 +97,12 @@ def test_pipelined_grid_kernel_writes_the_same_bits(tile):
     rng = np.random.default_rng(7)
     ctx.set_vector(0, 1e-3 * rng.standard_normal(m.info["n_dof"]))
     out = []
-    for persistent in (0, 1):
+    for persistent, overlap in ((0, 0), (1, 0), (1, 1), (1, 2)):
         _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, 4))
+        _lib.check(_lib.lib.pg_ctx_cut_overlap(ctx.handle, overlap, None))
         pb.Assembler(ctx).assemble_nonlinear(1.0, True, True)
         out.append((ctx.matrix_values(), ctx.vector(1)))
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    for k in range(1, len(out)):
+        assert np.array_equal(out[0][0], out[k][0])
+        assert np.array_equal(out[0][1], out[k][1])
     ctx.close()

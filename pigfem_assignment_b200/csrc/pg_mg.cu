@@ -479,8 +479,8 @@ __global__ void k_mg_prolong(int nxf, int nyf, int nxc, const T* __restrict__ xc
 // back up.  Their operators, diagonal inverses and vectors are first copied
 // into shared memory (one coalesced pass), so no phase waits on L2; the
 // result of level `first` goes back to its x for the caller's prolongation.
-constexpr int kMgBottomNodes = 300;        // levels at most this size may run in k_mg_bottom
-constexpr int kMgBottomSmem = 200 * 1024;  // and their shared-memory copy at most this many bytes
+constexpr int kMgBottomNodes = 1200;       // levels at most this size may run in k_mg_bottom
+constexpr int kMgBottomSmem = 220 * 1024;  // and their shared-memory copy at most this many bytes
 constexpr int kMgBottomThreads = 512;
 constexpr int kMgBottomLevels = 8;
 
@@ -493,17 +493,23 @@ struct MgBottomArgs {
     const T* A[kMgBottomLevels];
     const T* Dinv[kMgBottomLevels];
     const uint8_t* fixed[kMgBottomLevels];
+    int staged[kMgBottomLevels];            // 1: A and D^-1 copied into shared memory; 0: read from global (L2)
     T* x0;                                  // level `first`'s x (global): the result
     const double* XT;                       // coarsest: transposed masked inverse
     int nc;
     T omega;
 };
 
-// shared-memory bytes of k_mg_bottom for levels of n nodes: A (36 n), D^-1 (4 n),
-// b, x, x2, r (2 n each), fixed (2 n bytes, rounded to 8)
+// shared-memory bytes of k_mg_bottom for a level of n nodes: b, x, x2, r (2 n
+// each) and fixed (2 n bytes, rounded to 8), and with its operator staged A
+// (36 n) and D^-1 (4 n) too
 template <typename T>
-size_t mg_bottom_level_bytes(int n) {
-    return (size_t)(36 + 4 + 8) * n * sizeof(T) + (((size_t)2 * n + 7) & ~(size_t)7);
+size_t mg_bottom_vec_bytes(int n) {
+    return (size_t)8 * n * sizeof(T) + (((size_t)2 * n + 7) & ~(size_t)7);
+}
+template <typename T>
+size_t mg_bottom_op_bytes(int n) {
+    return (size_t)(36 + 4) * n * sizeof(T);
 }
 
 template <typename T>
@@ -523,15 +529,23 @@ __global__ void __launch_bounds__(kMgBottomThreads) k_mg_bottom(MgBottomArgs<T> 
     unsigned char* p = g_bottom_smem;
     for (int k = 0; k < a.nlev; ++k) {
         const int n = (a.nx[k] + 1) * (a.ny[k] + 1);
-        sA[k] = reinterpret_cast<T*>(p);
-        sD[k] = sA[k] + 36 * n;
-        sb[k] = sD[k] + 4 * n;
+        T* q0 = reinterpret_cast<T*>(p);
+        if (a.staged[k]) {
+            sA[k] = q0;
+            sD[k] = sA[k] + 36 * n;
+            q0 = sD[k] + 4 * n;
+        } else {
+            // a larger level: its operator stays in global memory (L2), only its vectors here
+            sA[k] = const_cast<T*>(a.A[k]);
+            sD[k] = const_cast<T*>(a.Dinv[k]);
+        }
+        sb[k] = q0;
         sx[k] = sb[k] + 2 * n;
         sx2[k] = sx[k] + 2 * n;
         sr[k] = sx2[k] + 2 * n;
         sf[k] = reinterpret_cast<uint8_t*>(sr[k] + 2 * n);
         p = reinterpret_cast<unsigned char*>(sf[k]) + ((2 * n + 7) & ~7);
-        if (k < a.nlev - 1) {
+        if (k < a.nlev - 1 && a.staged[k]) {
             for (int q = tid; q < 36 * n; q += kMgBottomThreads) sA[k][q] = a.A[k][q];
             for (int q = tid; q < 4 * n; q += kMgBottomThreads) sD[k][q] = a.Dinv[k][q];
         }
@@ -1019,18 +1033,31 @@ int mg_numeric(Ctx& c, bool f32, cudaStream_t s) {
 template <typename T>
 const T* vcycle(Ctx& c, MgHierarchy& m, cudaStream_t s, const T* b0, const int* done);
 
-// First level of the fused bottom (k_mg_bottom): going up from the coarsest,
-// levels of at most kMgBottomNodes nodes while their shared-memory copy stays
-// within kMgBottomSmem bytes (and at most kMgBottomLevels levels).
+// First level of the fused bottom (k_mg_bottom) and which of its levels have
+// their operator staged in shared memory: going up from the coarsest, the
+// levels of at most kMgBottomNodes nodes (at most kMgBottomLevels) whose
+// vectors fit in kMgBottomSmem bytes together; then, coarsest first, each
+// level's operator is staged while it still fits (the coarsest level, solved
+// by its explicit inverse, needs none); the others read theirs from L2.
 template <typename T>
-int mg_bottom_first(const MgHierarchy& m, size_t* smem) {
+int mg_bottom_first(const MgHierarchy& m, size_t* smem, int* staged) {
     int kb = m.nlev;
-    size_t bytes = mg_bottom_level_bytes<T>(m.L[m.nlev].n);
+    size_t bytes = mg_bottom_vec_bytes<T>(m.L[m.nlev].n);
     for (int k = m.nlev - 1; k >= 1 && m.nlev - k + 1 <= kMgBottomLevels; --k) {
-        const size_t add = mg_bottom_level_bytes<T>(m.L[k].n);
+        const size_t add = mg_bottom_vec_bytes<T>(m.L[k].n);
         if (m.L[k].n > kMgBottomNodes || bytes + add > (size_t)kMgBottomSmem) break;
         bytes += add;
         kb = k;
+    }
+    for (int k = m.nlev; k >= kb; --k) {
+        int& st = staged[k - kb];
+        st = 0;
+        if (k == m.nlev) continue;
+        const size_t add = mg_bottom_op_bytes<T>(m.L[k].n);
+        if (bytes + add <= (size_t)kMgBottomSmem) {
+            bytes += add;
+            st = 1;
+        }
     }
     *smem = bytes;
     return kb;
@@ -1038,8 +1065,8 @@ int mg_bottom_first(const MgHierarchy& m, size_t* smem) {
 
 // Levels kb .. nlev in one launch; level kb's result ends in its x (xf).
 template <typename T>
-void launch_bottom(MgHierarchy& m, int kb, size_t smem, int nxf, int nyf, const T* rf, cudaStream_t s,
-                   const int* done) {
+void launch_bottom(MgHierarchy& m, int kb, size_t smem, const int* staged, int nxf, int nyf, const T* rf,
+                   cudaStream_t s, const int* done) {
     MgBottomArgs<T> a;
     a.nlev = m.nlev - kb + 1;
     a.nxf = nxf;
@@ -1051,6 +1078,7 @@ void launch_bottom(MgHierarchy& m, int kb, size_t smem, int nxf, int nyf, const 
         a.nx[j] = L.nx;
         a.ny[j] = L.ny;
         a.fixed[j] = L.fixed;
+        a.staged[j] = staged[j];
         if constexpr (std::is_same<T, float>::value) {
             a.A[j] = L.Af;
             a.Dinv[j] = L.Dinvf;
@@ -1088,11 +1116,12 @@ const double* vcycle<double>(Ctx& c, MgHierarchy& m, cudaStream_t s, const doubl
     double* xs[kMgMaxLevels + 1];
     xs[0] = cur;
     size_t bsm = 0;
-    const int kb = mg_bottom_first<double>(m, &bsm);
+    int staged[kMgBottomLevels];
+    const int kb = mg_bottom_first<double>(m, &bsm, staged);
     for (int k = 1; k <= m.nlev; ++k) {
         MgLevel& L = m.L[k];
         if (k == kb) {  // this level and all coarser ones: one launch
-            launch_bottom<double>(m, kb, bsm, nxf, nyf, rf, s, done);
+            launch_bottom<double>(m, kb, bsm, staged, nxf, nyf, rf, s, done);
             xs[k] = L.x;
             break;
         }
@@ -1155,11 +1184,12 @@ const float* vcycle<float>(Ctx& c, MgHierarchy& m, cudaStream_t s, const float* 
     float* xs[kMgMaxLevels + 1];
     xs[0] = cur;
     size_t bsm = 0;
-    const int kb = mg_bottom_first<float>(m, &bsm);
+    int staged[kMgBottomLevels];
+    const int kb = mg_bottom_first<float>(m, &bsm, staged);
     for (int k = 1; k <= m.nlev; ++k) {
         MgLevel& L = m.L[k];
         if (k == kb) {  // this level and all coarser ones: one launch
-            launch_bottom<float>(m, kb, bsm, nxf, nyf, rf, s, done);
+            launch_bottom<float>(m, kb, bsm, staged, nxf, nyf, rf, s, done);
             xs[k] = L.xf;
             break;
         }

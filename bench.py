@@ -390,12 +390,17 @@ def run_b200_arm(args):
     load = None
     if not args.no_load_step and world == 1:
         load = {}
-        variants = (("plain_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_MG),
-                    ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED, _lib.PG_PREC_MG),
-                    ("block_jacobi_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_BLOCK_JACOBI))
-        for name, prec, pc in variants:
+        # the *_atomic_sums arms add the Krylov block sums atomically (deterministic = 0):
+        # the cost of the fixed-order sums is the difference to the arm without the suffix
+        variants = (("plain_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_MG, True),
+                    ("mixed_fp32_fp64", _lib.PG_PRECISION_MIXED, _lib.PG_PREC_MG, True),
+                    ("block_jacobi_fp64", _lib.PG_PRECISION_FP64, _lib.PG_PREC_BLOCK_JACOBI, True),
+                    ("plain_fp64_atomic_sums", _lib.PG_PRECISION_FP64, _lib.PG_PREC_MG, False),
+                    ("block_jacobi_fp64_atomic_sums", _lib.PG_PRECISION_FP64, _lib.PG_PREC_BLOCK_JACOBI, False))
+        for name, prec, pc, det in variants:
             solver = pb.Solver(ctx)
-            solver.configure(precision=prec, precond=pc, rtol=1e-8, inner_rtol=1e-3, check_every=64)
+            solver.configure(precision=prec, precond=pc, rtol=1e-8, inner_rtol=1e-3, check_every=64,
+                             deterministic=det)
             # one untimed warm-up step per arm: its first solve also builds the multigrid
             # hierarchy (a one-time cost per mesh, reported as first_solve_ms)
             first_ms = None

@@ -204,6 +204,10 @@ typedef struct pg_solver_cfg {
     int32_t check_every;            /* host residual check cadence (iterations per captured graph) */
     int32_t inclusion_modes;        /* PG_PREC_MG on cohesive meshes: 1 adds the inclusions' rigid motions
                                        (3 per inclusion) as a coarse space (default 0) */
+    int32_t deterministic;          /* 1 (default): every Krylov dot product is summed in a fixed order (block
+                                       partials added in block order by the grid's last block), so a solve is
+                                       bit-reproducible run to run; 0: block partials are added with atomics,
+                                       order-dependent in the last bits, a few microseconds less per reduction */
 } pg_solver_cfg;
 
 typedef struct pg_solve_stats {
@@ -243,6 +247,7 @@ typedef struct pg_newton_cfg {
     int32_t inclusion_modes;        /* as in pg_solver_cfg (default 0) */
     double t_start, t_stop;         /* pg_solve_nonlinear steps the load fraction from t_start (the current U and
                                        committed state are converged there) to t_stop; defaults 0 and 1 */
+    int32_t deterministic;          /* as in pg_solver_cfg (default 1): with 1 a load path is bit-reproducible */
 } pg_newton_cfg;
 /* rtol relative to the residual of the step's own predictor (SNES, the reference) */
 #define PG_RTOL_BASE_PREDICTOR 0

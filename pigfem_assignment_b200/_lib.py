@@ -66,7 +66,7 @@ class SolverCfg(C.Structure):
         ("krylov", C.c_int32), ("precond", C.c_int32), ("precision", C.c_int32),
         ("rtol", C.c_double), ("max_iter", C.c_int32), ("inner_rtol", C.c_double),
         ("max_refine", C.c_int32), ("gmres_restart", C.c_int32), ("check_every", C.c_int32),
-        ("inclusion_modes", C.c_int32),
+        ("inclusion_modes", C.c_int32), ("deterministic", C.c_int32),
     ]
 
 
@@ -90,6 +90,7 @@ class NewtonCfg(C.Structure):
         ("lin_rtol", C.c_double), ("inner_rtol", C.c_double), ("lin_max_iter", C.c_int32),
         ("max_repeat", C.c_int32), ("predictor", C.c_int32), ("rtol_base", C.c_int32),
         ("inclusion_modes", C.c_int32), ("t_start", C.c_double), ("t_stop", C.c_double),
+        ("deterministic", C.c_int32),
     ]
 
 

@@ -291,6 +291,7 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
         if ((rc = dev_alloc(&c.red_ws, red_ws_doubles(cap)))) return rc;
         const double capd = (double)cap;
         PG_CUDA(cudaMemcpy(c.red_ws, &capd, sizeof(double), cudaMemcpyHostToDevice));
+        c.red_active = c.red_ws;
     }
     if ((rc = dev_alloc(&c.iflags, 64))) return rc;
     PG_CUDA(cudaMallocHost((void**)&c.h_scal, 64 * sizeof(double)));
@@ -687,6 +688,7 @@ void pg_solver_cfg_default(pg_solver_cfg* cfg) {
     cfg->gmres_restart = 60;
     cfg->check_every = 64;
     cfg->inclusion_modes = 0;
+    cfg->deterministic = 1;
 }
 
 int pg_solve_linear(pg_ctx* c, const pg_solver_cfg* cfg_in, pg_solve_stats* stats) {

@@ -202,6 +202,7 @@ struct Ctx {
     float* featY = nullptr;            // 2 outputs per node
     double* scal = nullptr;            // device scalars
     double* red_ws = nullptr;          // deterministic grid-sum workspace (grid_add)
+    double* red_active = nullptr;      // red_ws, or null while a solve sums with atomics (cfg.deterministic 0)
     int* iflags = nullptr;             // device flags
     double* h_scal = nullptr;          // pinned host mirror
     int* h_iflags = nullptr;

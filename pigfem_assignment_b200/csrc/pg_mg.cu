@@ -1290,12 +1290,12 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
     if ((rc = mg_numeric(c, f32, s))) return rc;
     const int n = c.n_nodes, nd = c.n_dof;
     cudaMemsetAsync(m.sc, 0, 8 * sizeof(double), s);
-    k_mgcg_start<<<nb(nd), kThreads, 0, s>>>(nd, c.fixed, c.b, c.r, c.dx, m.sc, c.red_ws);
+    k_mgcg_start<<<nb(nd), kThreads, 0, s>>>(nd, c.fixed, c.b, c.r, c.dx, m.sc, c.red_active);
     k_mgcg_tol<<<1, 1, 0, s>>>(m.sc, cfg.rtol * cfg.rtol);
     // z = V(r), p = z, sc[2] = r.z
     mg_apply(c, m, f32, s, c.r, c.z, nullptr);
     k_copy<double><<<nb(nd), kThreads, 0, s>>>(nd, c.z, c.p);
-    k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_ws);
+    k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_active);
     int hf[8] = {};
     double hs[8] = {};
     cudaMemcpyAsync(hs, m.sc, sizeof hs, cudaMemcpyDeviceToHost, s);
@@ -1316,11 +1316,11 @@ int mg_pcg_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
         for (int it = 0; it < kChunk; ++it) {
             k_mgcg_s1<<<1, 1, 0, s>>>(m.sc, m.fl);
             k_mgcg_spmv<<<nb(kRowLanes * n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, c.p, c.fixed, c.q, m.sc, m.fl,
-                                                                 c.red_ws);
-            k_mgcg_update<<<nb(nd), kThreads, 0, s>>>(nd, c.dx, c.r, c.p, c.q, m.sc, m.fl, c.red_ws);
+                                                                 c.red_active);
+            k_mgcg_update<<<nb(nd), kThreads, 0, s>>>(nd, c.dx, c.r, c.p, c.q, m.sc, m.fl, c.red_active);
             k_mgcg_s2<<<1, 1, 0, s>>>(m.sc, m.fl);
             mg_apply(c, m, f32, s, c.r, c.z, m.fl);
-            k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_ws);
+            k_mgcg_dot<<<nb(nd), kThreads, 0, s>>>(nd, c.r, c.z, m.sc + 2, m.fl, c.red_active);
             k_mgcg_pupdate<<<nb(nd), kThreads, 0, s>>>(nd, c.z, c.p, m.sc, m.fl);
         }
         PG_CUDA(cudaStreamEndCapture(s, &graph));

@@ -71,6 +71,7 @@ int newton_load_step(Ctx& c, double t_frac, double dt, const pg_newton_cfg& cfg,
     lin.precision = cfg.precision;
     lin.precond = cfg.precond;
     lin.inclusion_modes = cfg.inclusion_modes;
+    lin.deterministic = cfg.deterministic;
     lin.krylov = PG_KRYLOV_CG;
     lin.max_iter = cfg.lin_max_iter;
     lin.inner_rtol = cfg.inner_rtol;
@@ -159,6 +160,7 @@ void pg_newton_cfg_default(pg_newton_cfg* cfg) {
     cfg->inclusion_modes = 0;
     cfg->t_start = 0.0;
     cfg->t_stop = 1.0;
+    cfg->deterministic = 1;
 }
 
 int pg_newton_load_step(pg_ctx* cx, double t_frac, double dt, const pg_newton_cfg* cfg_in, pg_step_stats* stats) {

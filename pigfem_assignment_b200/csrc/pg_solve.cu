@@ -42,7 +42,7 @@ int pcg_run(Ctx& c, cudaStream_t s, const MT* K, VT* x, VT* r, VT* z, VT* p, VT*
     cudaMemsetAsync(c.scal, 0, S_NSCAL * sizeof(double), s);
     cudaMemsetAsync(c.iflags, 0, F_NFLAGS * sizeof(int), s);
     cudaMemcpyAsync(c.scal + S_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, s);
-    k_cg_init<VT, PT><<<nblk(n), kThreads, 0, s>>>(n, r, z, p, minv, c.scal, c.red_ws);
+    k_cg_init<VT, PT><<<nblk(n), kThreads, 0, s>>>(n, r, z, p, minv, c.scal, c.red_active);
     cudaMemcpyAsync(c.h_scal, c.scal, S_NSCAL * sizeof(double), cudaMemcpyDeviceToHost, s);
     PG_CUDA(cudaStreamSynchronize(s));
     rr_final = c.h_scal[S_RR0 + 1];
@@ -55,8 +55,8 @@ int pcg_run(Ctx& c, cudaStream_t s, const MT* K, VT* x, VT* r, VT* z, VT* p, VT*
     for (int it = 0; it < chunk; ++it) {
         const int P = it & 1;
         k_spmv_cg<MT, VT><<<nblk(n), kThreads, 0, s>>>(n, P, c.row_ptr, c.col, K, p, c.fixed, q, c.scal, c.iflags,
-                                                          c.red_ws);
-        k_cg_update<VT, PT><<<nblk(n), kThreads, 0, s>>>(n, P, x, r, z, p, q, minv, c.scal, c.iflags, c.red_ws);
+                                                          c.red_active);
+        k_cg_update<VT, PT><<<nblk(n), kThreads, 0, s>>>(n, P, x, r, z, p, q, minv, c.scal, c.iflags, c.red_active);
         k_cg_pupdate<VT><<<nblk(n), kThreads, 0, s>>>(n, P, z, p, c.scal, c.iflags);
     }
     PG_CUDA(cudaStreamEndCapture(s, &graph));
@@ -128,7 +128,7 @@ int gmres_solve(Ctx& c, const pg_solver_cfg& cfg, double rtol, int max_iter, pg_
             std::fill(hcol.begin(), hcol.end(), 0.0);
             for (int pass = 0; pass < 2; ++pass) {
                 cudaMemsetAsync(c.hbuf, 0, (j + 1) * sizeof(double), s);
-                k_multidot<<<std::min(nblk(nd), 1184), kThreads, 0, s>>>(nd, j + 1, c.V, w, c.hbuf, c.red_ws);
+                k_multidot<<<std::min(nblk(nd), 1184), kThreads, 0, s>>>(nd, j + 1, c.V, w, c.hbuf, c.red_active);
                 k_multi_axpy<<<nblk(nd), kThreads, 0, s>>>(nd, j + 1, c.V, c.hbuf, w);
                 std::vector<double> hh(j + 1);
                 cudaMemcpyAsync(hh.data(), c.hbuf, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -198,7 +198,7 @@ int minres_solve(Ctx& c, double rtol, int max_iter, int chunk, pg_solve_stats& s
     cudaMemsetAsync(c.mw, 0, 2 * (size_t)nd * sizeof(double), s);
     // beta1^2 = b . M^-1 b
     cudaMemsetAsync(c.scal + S_AUX, 0, sizeof(double), s);
-    k_dot2<<<nblk(nd), kThreads, 0, s>>>(nd, c.b, y, c.scal + S_AUX, c.red_ws);
+    k_dot2<<<nblk(nd), kThreads, 0, s>>>(nd, c.b, y, c.scal + S_AUX, c.red_active);
     cudaMemcpyAsync(c.h_scal + S_AUX, c.scal + S_AUX, sizeof(double), cudaMemcpyDeviceToHost, s);
     PG_CUDA(cudaStreamSynchronize(s));
     const double beta1 = std::sqrt(std::max(c.h_scal[S_AUX], 0.0));
@@ -220,8 +220,8 @@ int minres_solve(Ctx& c, double rtol, int max_iter, int chunk, pg_solve_stats& s
         const int P = k & 1, Q = 1 - P;
         k_mr_v<<<nblk(nd), kThreads, 0, s>>>(nd, y, v, c.scal, c.iflags);
         k_mr_av<double><<<nblk(n), kThreads, 0, s>>>(n, c.row_ptr, c.col, c.K, v, c.fixed, buf[P], y, c.scal, c.iflags,
-                                                       c.red_ws);
-        k_mr_2<<<nblk(n), kThreads, 0, s>>>(n, y, buf[Q], buf[P], c.minv, c.scal, c.iflags, c.red_ws);
+                                                       c.red_active);
+        k_mr_2<<<nblk(n), kThreads, 0, s>>>(n, y, buf[Q], buf[P], c.minv, c.scal, c.iflags, c.red_active);
         k_mr_scalars<<<1, 1, 0, s>>>(c.scal, c.iflags);
         k_mr_w<<<nblk(nd), kThreads, 0, s>>>(nd, v, W[P], W[Q], c.dx, c.scal, c.iflags);
         k_mr_seal<<<1, 1, 0, s>>>(c.iflags);
@@ -258,7 +258,7 @@ double residual_into(Ctx& c, cudaStream_t s, const double* x, const double* b, d
 
 double dev_norm2(Ctx& c, const double* v, int n, cudaStream_t s) {
     cudaMemsetAsync(c.scal + S_AUX, 0, sizeof(double), s);
-    k_dot_self<<<nblk(n), kThreads, 0, s>>>(n, v, c.scal + S_AUX, c.red_ws);
+    k_dot_self<<<nblk(n), kThreads, 0, s>>>(n, v, c.scal + S_AUX, c.red_active);
     cudaMemcpyAsync(c.h_scal + S_AUX, c.scal + S_AUX, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     return c.h_scal[S_AUX];
@@ -275,6 +275,7 @@ int krylov_solve(Ctx& c, const pg_solver_cfg& cfg, pg_solve_stats& st, cudaStrea
     st.refinements = 0;
     st.status = PG_OK;
     st.rel_residual = 0.0;
+    c.red_active = cfg.deterministic ? c.red_ws : nullptr;
     const int block = cfg.precond == PG_PREC_BLOCK_JACOBI ? 1 : 0;
     const int ident = cfg.precond == PG_PREC_NONE ? 1 : 0;
     const int chunk = cfg.check_every > 1 ? ((cfg.check_every + 1) & ~1) : 32;

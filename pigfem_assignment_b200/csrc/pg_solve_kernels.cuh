@@ -49,15 +49,16 @@ __device__ __forceinline__ double block_sum(double d) {
 // partials, and the last block to take a ticket adds them in block order
 // (a fixed tree over fixed strided sums) -- the same bits on every run,
 // where atomically added block sums vary with the blocks' arrival.  Every
-// thread of the block must call it.  A grid larger than the workspace's
-// capacity falls back to the atomic sum.
+// thread of the block must call it.  A null workspace (a solve that asked
+// for no fixed order) or a grid larger than the workspace's capacity falls
+// back to the atomic sum.
 __device__ __forceinline__ void grid_add(double* ws, int slot, double s, double* out) {
     __shared__ int s_last;
-    const int cap = (int)ws[0];
-    if ((int)gridDim.x > cap) {
+    if (ws == nullptr || (int)gridDim.x > (int)ws[0]) {
         if (threadIdx.x == 0) atomicAdd(out, s);
         return;
     }
+    const int cap = (int)ws[0];
     unsigned* tickets = reinterpret_cast<unsigned*>(ws + 1);
     double* part = ws + kRedHeader + (size_t)slot * cap;
     if (threadIdx.x == 0) {

@@ -221,13 +221,14 @@ class Solver:
 
     def configure(self, precision: int = _lib.PG_PRECISION_FP64, precond: int = _lib.PG_PREC_BLOCK_JACOBI,
                   rtol: float = 1e-8, inner_rtol: float = 1e-4, max_iter: int = 200000,
-                  check_every: int = 64) -> None:
+                  check_every: int = 64, deterministic: bool = True) -> None:
         self.cfg.precision = precision
         self.cfg.precond = precond
         self.cfg.rtol = rtol
         self.cfg.inner_rtol = inner_rtol
         self.cfg.max_iter = max_iter
         self.cfg.check_every = check_every
+        self.cfg.deterministic = int(deterministic)
 
     def solve_linear(self) -> _lib.SolveStats:
         check(lib.pg_solve_linear(self.ctx.handle, C.byref(self.cfg), C.byref(self.stats)), "pg_solve_linear")

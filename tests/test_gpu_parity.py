@@ -212,3 +212,25 @@ def test_gpu_assembly_is_bit_reproducible():
         assert np.array_equal(fs[0], fs[k])
     ctx.close()
 
+
+
+@pytest.mark.parametrize("precond", [_lib.PG_PREC_BLOCK_JACOBI, _lib.PG_PREC_MG])
+def test_linear_solve_reduction_order(precond):
+    """deterministic = 1 (the default) sums every Krylov dot product in block
+    order: two solves give the same bits and iteration counts.  deterministic
+    = 0 adds the block sums atomically; it reaches the same tolerance and
+    agrees with the fixed-order solution within it."""
+    import dataclasses
+    rve = dataclasses.replace(config1(), nx=256, ny=256)
+    prob = pb.ProblemLinearElasticity(rve)
+    prob.init()
+    prob.assembler.assemble_linear()
+    sols = []
+    for det in (True, True, False):
+        prob.solver.configure(precond=precond, rtol=1e-10, deterministic=det)
+        st = prob.solver.solve_linear()
+        assert st.status == _lib.PG_OK and st.rel_residual <= 1e-10
+        sols.append((prob.get_solution().copy(), st.iterations))
+    assert np.array_equal(sols[0][0], sols[1][0]) and sols[0][1] == sols[1][1]
+    assert np.linalg.norm(sols[2][0] - sols[0][0]) <= 1e-8 * np.linalg.norm(sols[0][0])
+    prob.ctx.close()

@@ -2021,8 +2021,10 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     // once; then the cut elements' quadrature rows, cohesive points and pair
     // blocks are formed, and the fold adds them to the rows they touch and
     // writes the enrichment rows and columns whole.  Nothing needs clearing
-    // first.  All on one stream: the triangle kernel fills every SM until its
-    // last wave, so a second stream bought no overlap (measured).
+    // first.  One stream, the kernels chained by programmatic dependent
+    // launch, unless the tuning leaves the persistent grid kernel's SMs some
+    // CTA slots (cut_overlap): then the rows and pairs run on the second
+    // stream beside it and the fold waits for both.
     if (!(c.tuning.tri_grid && c.grid_emat)) {
         const int rc = ensure_tri_map(c);
         if (rc != PG_OK) return rc;

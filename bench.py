@@ -170,9 +170,9 @@ def profiled_traffic(kernel: str):
 
 
 def launches_per_pass(mesh) -> int:
-    """Kernels one linear assembly launches: the uncut-triangle kernel, the
-    cut elements' quadrature-row kernel, one pair kernel per non-empty size
-    class (local node count <= 5, 7, 11, 15) and the fold of K."""
+    """Kernels one linear assembly launches: the uncut-triangle kernel, one
+    cut-element kernel per non-empty size class (local node count <= 5, 7,
+    11, 15) and the fold of the K slots that two or more cut blocks share."""
     import numpy as np
 
     import pigfem_assignment_b200.problem as pb
@@ -180,7 +180,7 @@ def launches_per_pass(mesh) -> int:
     n_enr = tmpl[np.asarray(mesh.export()["cut_tmpl"], dtype=np.int64), 1] if mesh.info["n_cut_elements"] else []
     nl = 3 + np.asarray(n_enr)
     classes = {int(np.searchsorted([5, 7, 11, 15], v)) for v in nl}
-    return 1 + (2 if classes else 0) + len(classes)
+    return 1 + (1 if classes else 0) + len(classes)
 
 
 def measured_peak_hbm():

@@ -603,7 +603,8 @@ __device__ __forceinline__ void cut_point_row(const CutPoint& P, const double* _
 // in class order, each element's in the order of its rows; one sentinel
 // record follows the last point, holding only the rows' total length.
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
-                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out) {
+                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out,
+                      std::vector<int>& pt_off) {
     // each element's records have a fixed place (the prefix of the points
     // before it), so the elements fill them in parallel
     const int nc = (int)tmpl.size();
@@ -612,6 +613,7 @@ void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmp
     for (int k = 0; k < kCutClasses; ++k)
         for (int oi = class_off[k]; oi < class_off[k + 1]; ++oi) cls[oi] = k;
     for (int oi = 0; oi < nc; ++oi) rec0[oi + 1] = rec0[oi] + device_point_count(tmpl[oi]);
+    pt_off.assign(rec0.begin(), rec0.end());
     out.assign((size_t)(rec0[nc] + 1) * kCutPointInts, 0);
     parallel_for(nc, 2048, [&](long long oi) {
         const int k = cls[oi];
@@ -646,6 +648,19 @@ void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmp
     const long long total = roff.back();
     r[12] = (int)(unsigned)(total & 0xffffffffLL);
     r[13] = (int)(total >> 32);
+}
+
+void cut_row_spans(const std::vector<long long>& roff, const int* class_off, int span[4][3]) {
+    for (int k = 0; k < kCutClasses; ++k)
+        for (int w = 0; w < 3; ++w) {
+            const int epc = cut_elems_per_cta(32 * kCutCtaWarps[w], kCutClassNl[k]);
+            long long widest = 0;
+            for (int e0 = class_off[k]; e0 < class_off[k + 1]; e0 += epc) {
+                const int e1 = std::min(class_off[k + 1], e0 + epc);
+                widest = std::max(widest, roff[e1] - roff[e0]);
+            }
+            span[k][w] = (int)std::min<long long>(widest, 1LL << 30);
+        }
 }
 
 // ---------------------------------------------------------------------------
@@ -1128,28 +1143,32 @@ void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaSt
 }
 
 // ---------------------------------------------------------------------------
-// Cut elements: integration per node pair into fold order, then a fold
+// Cut elements: integration per element row, then a fold of shared slots
 // ---------------------------------------------------------------------------
 // Every cut element's (3 + n_enr)^2 node-pair blocks have a fixed place in
 // the element's slot table (cut_slot: pair (a, b) at cut_slot_ptr + a nl +
-// b, holding the block's K slot).  k_cut_pairs integrates one pair per
-// thread and stores the block at its position in fold order (kpos, built
-// once per mesh: all contributions to one K slot next to each other, by
-// element and pair), and for residual passes K_ab u_b at its position in
-// the node-sorted order (fpos); nothing is added into K there.  k_fold_K
-// then gives every K slot that cut elements touch its final value in one
-// thread: the triangle kernel's value (or zero, for blocks in enrichment
-// rows or columns, which only cut elements reach) plus its contiguous run
-// of contributions; k_fold_f does the same per node for f_int.  The sums
-// are the same on every run: no atomics.
+// b, holding the block's K slot).  k_cut_elems forms the element's
+// quadrature rows in shared memory and integrates one row of blocks (a, *)
+// per thread.  A block whose K slot takes no other contribution (half of
+// them) goes into K there: stored where only cut elements reach the slot
+// (enrichment rows and columns), else added to the triangle kernel's value
+// by a reduction that waits for nothing -- with a single addend its result
+// is the same in any order.  The others are stored at their position in
+// fold order (kpos, built once per mesh: all contributions to one K slot
+// next to each other, by element and pair), and for residual passes K_ab
+// u_b at its position in the node-sorted order (fpos).  k_fold_K then gives
+// every K slot of two or more contributions its final value in one thread:
+// the triangle kernel's value (or zero, for blocks in enrichment rows or
+// columns, which only cut elements reach) plus its contiguous run of
+// contributions; k_fold_f does the same per node for f_int.  The sums are
+// the same on every run.
 //
-// Three kernels form the pairs, after the triangle kernel on the same
-// stream (a second stream bought no overlap: the triangle kernel fills every
-// SM until its last wave): k_cut_points forms every quadrature row (one
-// thread per point, from the host-packed point records), k_coh_points every
-// cohesive Gauss point (one thread each: traction-separation law, trial
-// delta_max, row), and k_cut_pairs integrates one node pair per thread from
-// those rows.
+// After the triangle kernel on the same stream, chained by programmatic
+// dependent launch: k_coh_points forms every cohesive Gauss point (one
+// thread each: traction-separation law, trial delta_max, row), k_cut_elems
+// (one launch per size class) the quadrature rows and the blocks, then the
+// folds.  k_cut_points forms the same quadrature rows in global memory for
+// the stress recovery.
 constexpr int kCohRow = kCohRowDoubles;  // {w dA, N0, N1, (R^T D R) 4, (R^T t) 2, pad}
 
 // One thread per quadrature point: its row, point-major (the element's point
@@ -1259,7 +1278,7 @@ __global__ void __launch_bounds__(128) k_coh_points(CohArgs a) {
     pdl_wait();
 }
 
-struct PairArgs {
+struct ElemArgs {
     int n_elem;                     // elements of this size class
     int first;                      // its first element in class order
     const int* __restrict__ cut_nodes;
@@ -1267,121 +1286,225 @@ struct PairArgs {
     const int* __restrict__ cut_coh_qp0;
     const int* __restrict__ cut_slot_ptr;
     const int* __restrict__ kpos;   // slot-table entry -> position in fold order (-1: no K slot)
+    const long long* __restrict__ kdir;  // slot-table entry -> slot << 1 | cut_only of a one-entry run, else -1
     const int* __restrict__ fpos;   // slot-table entry -> position in node order
-    const double* __restrict__ rows;
+    const int4* __restrict__ pts;   // point records (build_cut_points)
+    const int* __restrict__ pt_off; // per element its first point record
     const long long* __restrict__ row_off;
+    const double* __restrict__ x;
+    const double* __restrict__ y;
+    const double* __restrict__ dmat;
     const double* __restrict__ coh_rows;
     const double* __restrict__ u;
     double* ke;                     // 4 FP64 per fold position
     double* fe;                     // 2 FP64 per node-order position
+    double* K;
     int want_K, want_f;
+    int direct;                     // 1: one-entry runs go straight into K (the triangle kernel has finished)
 };
 
-__device__ __forceinline__ double2 ldg2(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
 
-// One thread per node pair (a, b) of a cut element of size class NL (NL^2
-// threads per element; pairs beyond the element's nl^2 idle): the block
-// K_ab = sum_q w_q B_a^T D B_b over the element's rows, plus the cohesive
-// sub-elements' N_a N_b (+-) R^T D R terms when both nodes are cohesive
-// nodes; residual passes store K_ab u_b (bulk) and, on the diagonal pair,
-// the node's cohesive traction term.
+// One CTA per cut_elems_per_cta(blockDim.x, NL) consecutive elements of size
+// class NL.  The CTA first forms its elements' quadrature rows in shared
+// memory (one thread per point, from the point records; the mesh is all it
+// reads, so this part runs beside the kernel before it), then one thread per
+// local function a of an element integrates the element's row a of blocks:
+// K_ab = sum_q w_q B_a^T D B_b over the rows for every b, plus the cohesive
+// sub-elements' N_a N_b (+-) R^T D R terms where both nodes are cohesive
+// nodes.  Residual passes store K_ab u_b (bulk) for every b and, on the
+// diagonal block, add the node's cohesive traction term.  A block whose K
+// slot no other contribution reaches goes straight into K (direct); the
+// others go to their place in fold order.
 template <int NL>
-__global__ void __launch_bounds__(256) k_cut_pairs(PairArgs a) {
-    pdl_wait();  // the rows of k_cut_points / k_coh_points
+__global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_elems(ElemArgs a) {
+    extern __shared__ __align__(16) double sRow[];
     pdl_trigger();
-    constexpr int P = NL * NL, W = 4 + 2 * NL;
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int oi = (int)(t / P), p = (int)(t - (long long)oi * P);
-    if (oi >= a.n_elem) return;
-    const int ci = a.first + oi;
-    const DevTemplate& T = g_tmpl[__ldg(&a.cut_tmpl[ci])];
-    const int nl = 3 + T.n_enr;
-    if (p >= nl * nl) return;
-    const int pa = p / nl, pb = p - pa * nl;
-    // inputs that do not depend on each other, issued together
+    constexpr int W = 4 + 2 * NL;
+    const int epc = cut_elems_per_cta(blockDim.x, NL);
+    const int e0 = blockIdx.x * epc, e1 = min(a.n_elem, e0 + epc);
+    const int c0 = a.first + e0;
+    const long long base = __ldg(&a.row_off[c0]);
+    // this thread's element and local function; its static tables are
+    // loaded while the rows are formed
+    const int le = threadIdx.x / NL, pa = threadIdx.x - le * NL;
+    const bool act = le < epc && e0 + le < a.n_elem;
+    const int ci = c0 + (act ? le : 0);
+    const int tm = __ldg(&a.cut_tmpl[ci]);
     const long long r0 = __ldg(&a.row_off[ci]), r1 = __ldg(&a.row_off[ci + 1]);
-    const long long sidx = __ldg(&a.cut_slot_ptr[ci]) + (long long)p;
-    const int kp = a.want_K ? __ldg(&a.kpos[sidx]) : -1;
-    const int fp = a.want_f ? __ldg(&a.fpos[sidx]) : -1;
-    const int node_b = a.want_f ? __ldg(&a.cut_nodes[(size_t)kCutNodeStride * ci + pb]) : 0;
-    const int nq = (int)((r1 - r0) / W);
-    double k0 = 0.0, k1 = 0.0, k2 = 0.0, k3 = 0.0;
-    const double* rw = a.rows + r0;
-    for (int q = 0; q < nq; ++q, rw += W) {
-        const double2 wd = ldg2(rw), dd = ldg2(rw + 2);
-        const double2 ga = ldg2(rw + 4 + 2 * pa), gb = ldg2(rw + 4 + 2 * pb);
-        const double wgt = wd.x, d11 = wd.y, d12 = dd.x, d33 = dd.y;
-        const double ba = ga.x * wgt, ca = ga.y * wgt, bb = gb.x, cb = gb.y;
-        k0 += ba * d11 * bb + ca * d33 * cb;
-        k1 += ba * d12 * cb + ca * d33 * bb;
-        k2 += ca * d12 * bb + ba * d33 * cb;
-        k3 += ca * d11 * cb + ba * d33 * bb;
+    const int sp_e = __ldg(&a.cut_slot_ptr[ci]);
+    {
+        const int p0 = __ldg(&a.pt_off[c0]), p1 = __ldg(&a.pt_off[a.first + e1]);
+        for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) {
+            const CutPoint cp = cut_point_load(a.pts + 4 * (size_t)p);
+            const long long off = (long long)(unsigned)cp.r3.x | ((long long)cp.r3.y << 32);
+            cut_point_row(cp, a.x, a.y, a.dmat, sRow + (off - base));
+        }
     }
-    // bulk internal force term K_ab u_b (the cohesive part of f_int is the
-    // traction integral below, not the cohesive tangent times u)
+    __syncthreads();
+    if (!act) return;
+    const DevTemplate& T = g_tmpl[tm];
+    const int nl = 3 + T.n_enr;
+    if (pa >= nl) return;
+    const int nq = (int)((r1 - r0) / W);
+    const long long sp0 = sp_e + (long long)pa * nl;
+    const int* en = a.cut_nodes + (size_t)kCutNodeStride * ci;
+    // where the row's blocks go (static tables), in flight during the
+    // integration: kdir in direct mode, else the fold position
+    long long kd[NL];
+#pragma unroll
+    for (int b = 0; b < NL; ++b) {
+        kd[b] = -1;
+        if (a.want_K && b < nl) kd[b] = a.direct ? __ldg(&a.kdir[sp0 + b]) : -2 - (long long)__ldg(&a.kpos[sp0 + b]);
+    }
+    pdl_wait();  // the kernel before has finished: K's triangle values, the cohesive rows
+    double k[NL][4];
+#pragma unroll
+    for (int b = 0; b < NL; ++b) k[b][0] = k[b][1] = k[b][2] = k[b][3] = 0.0;
+    const double* rw = sRow + (r0 - base);
+    for (int q = 0; q < nq; ++q, rw += W) {
+        const double2 wd = lds2(rw), dd = lds2(rw + 2), ga = lds2(rw + 4 + 2 * pa);
+        const double wgt = wd.x, d11 = wd.y, d12 = dd.x, d33 = dd.y;
+        const double ba = ga.x * wgt, ca = ga.y * wgt;
+#pragma unroll
+        for (int b = 0; b < NL; ++b) {
+            if (b < nl) {
+                const double2 gb = lds2(rw + 4 + 2 * b);
+                const double bb = gb.x, cb = gb.y;
+                k[b][0] += ba * d11 * bb + ca * d33 * cb;
+                k[b][1] += ba * d12 * cb + ca * d33 * bb;
+                k[b][2] += ca * d12 * bb + ba * d33 * cb;
+                k[b][3] += ca * d11 * cb + ba * d33 * bb;
+            }
+        }
+    }
+    // bulk internal force terms K_ab u_b (the cohesive part of f_int is the
+    // traction integral below, not the cohesive tangent times u); every
+    // block but the diagonal one is final here
     double fx = 0.0, fy = 0.0;
     if (a.want_f) {
-        const double ux = __ldg(&a.u[2 * node_b]), uy = __ldg(&a.u[2 * node_b + 1]);
-        fx = k0 * ux + k1 * uy;
-        fy = k2 * ux + k3 * uy;
+#pragma unroll
+        for (int b = 0; b < NL; ++b) {
+            if (b < nl) {
+                const int nb = __ldg(&en[b]);
+                const double ux = __ldg(&a.u[2 * nb]), uy = __ldg(&a.u[2 * nb + 1]);
+                const double gx = k[b][0] * ux + k[b][1] * uy, gy = k[b][2] * ux + k[b][3] * uy;
+                if (b == pa) {
+                    fx = gx;
+                    fy = gy;
+                } else {
+                    const int fp = __ldg(&a.fpos[sp0 + b]);
+                    if (fp >= 0) reinterpret_cast<double2*>(a.fe)[fp] = make_double2(gx, gy);
+                }
+            }
+        }
     }
     if (T.n_coh > 0) {
         const int qp0 = __ldg(&a.cut_coh_qp0[ci]);
         for (int ce = 0; ce < T.n_coh; ++ce) {
-            int i = -1, j = -1;
+            int i = -1;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
+            for (int m = 0; m < 4; ++m)
                 if (T.coh_nodes[ce][m] == pa) i = m;
-                if (T.coh_nodes[ce][m] == pb) j = m;
-            }
-            if (i < 0 || j < 0) continue;
-            const double sgn = ((i < 2) == (j < 2)) ? 1.0 : -1.0;
+            if (i < 0) continue;
             const double sa = i < 2 ? -1.0 : 1.0;
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const double* row = a.coh_rows + (size_t)kCohRow * (qp0 + 2 * ce + q);
                 const double wgt = __ldg(&row[0]);
                 if (wgt == 0.0) continue;
-                const double Na = __ldg(&row[1 + (i & 1)]), Nb = __ldg(&row[1 + (j & 1)]);
-                const double v = wgt * sgn * Na * Nb;
-                k0 += v * __ldg(&row[3]);
-                k1 += v * __ldg(&row[4]);
-                k2 += v * __ldg(&row[5]);
-                k3 += v * __ldg(&row[6]);
-                if (pa == pb) {
-                    fx += wgt * sa * Na * __ldg(&row[7]);
-                    fy += wgt * sa * Na * __ldg(&row[8]);
+                const double Na = __ldg(&row[1 + (i & 1)]);
+                const double D0 = __ldg(&row[3]), D1 = __ldg(&row[4]), D2 = __ldg(&row[5]), D3 = __ldg(&row[6]);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int b = T.coh_nodes[ce][m];
+                    const double sgn = ((i < 2) == (m < 2)) ? 1.0 : -1.0;
+                    const double v = wgt * sgn * Na * __ldg(&row[1 + (m & 1)]);
+#pragma unroll
+                    for (int bb = 0; bb < NL; ++bb)
+                        if (bb == b) {
+                            k[bb][0] += v * D0;
+                            k[bb][1] += v * D1;
+                            k[bb][2] += v * D2;
+                            k[bb][3] += v * D3;
+                        }
+                }
+                fx += wgt * sa * Na * __ldg(&row[7]);
+                fy += wgt * sa * Na * __ldg(&row[8]);
+            }
+        }
+    }
+    if (a.want_f) {
+        const int fp = __ldg(&a.fpos[sp0 + pa]);
+        if (fp >= 0) reinterpret_cast<double2*>(a.fe)[fp] = make_double2(fx, fy);
+    }
+    // kd >= 0: the slot's only contribution (slot << 1 | cut_only): stored
+    // (a block only cut elements reach) or added to the triangle kernel's
+    // value -- one addend, so the reduction is exact in any order and waits
+    // for nothing; kd <= -2: the fold position -2 - kd
+    if (a.want_K) {
+#pragma unroll
+        for (int b = 0; b < NL; ++b) {
+            if (b < nl) {
+                const long long v = kd[b];
+                if (v >= 0) {
+                    double* dst = a.K + 4 * (v >> 1);
+                    if (v & 1) {
+                        store_block(a.K, v >> 1, k[b][0], k[b][1], k[b][2], k[b][3]);
+                    } else {
+                        atomicAdd(dst, k[b][0]);
+                        atomicAdd(dst + 1, k[b][1]);
+                        atomicAdd(dst + 2, k[b][2]);
+                        atomicAdd(dst + 3, k[b][3]);
+                    }
+                } else if (v <= -2) {
+                    store_block(a.ke, -2 - v, k[b][0], k[b][1], k[b][2], k[b][3]);
                 }
             }
         }
     }
-    if (kp >= 0) store_block(a.ke, kp, k0, k1, k2, k3);
-    if (fp >= 0) reinterpret_cast<double2*>(a.fe)[fp] = make_double2(fx, fy);
 }
 
-// K slots that cut elements touch, one thread each: K[slot] = (the triangle
-// kernel's value, or 0 where flagged cut_only) + the slot's contiguous run
-// of pair blocks ke[ptr[j] .. ptr[j + 1]), summed in run order.
-// fold_slot[j] = slot << 1 | cut_only.
+// K slots that cut elements touch, one thread per run: K[slot] = (the
+// triangle kernel's value, or 0 where flagged cut_only) + the slot's
+// contiguous run of blocks ke[i0 .. i1), summed in run order.  fold_slot[j]
+// = slot << 1 | cut_only; the run's range is rng[j] when given (the runs of
+// two or more blocks, when k_cut_elems stored the others in K itself), else
+// ptr[j] .. ptr[j + 1] (every run).
 __global__ void __launch_bounds__(256) k_fold_K(int n, const long long* __restrict__ fold_slot,
-                                                const int* __restrict__ fold_ptr, const double* __restrict__ ke,
-                                                double* K) {
-    pdl_wait();  // the pair blocks, and (through the chain) the triangle kernel's K
+                                                const int* __restrict__ fold_ptr, const int2* __restrict__ rng,
+                                                const double* __restrict__ ke, double* K) {
+    pdl_wait();  // the blocks, and (through the chain) the triangle kernel's K
     pdl_trigger();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const long long sw = __ldg(&fold_slot[j]);
-    const int i0 = __ldg(&fold_ptr[j]), i1 = __ldg(&fold_ptr[j + 1]);
-    const long long slot = sw >> 1;
-    double4 acc = (sw & 1) ? make_double4(0.0, 0.0, 0.0, 0.0) : load_block(K, slot);
-    for (int i = i0; i < i1; ++i) {
-        const double4 v = load_block_nc(ke, i);
-        acc.x += v.x;
-        acc.y += v.y;
-        acc.z += v.z;
-        acc.w += v.w;
+    int i0, i1;
+    if (rng) {
+        const int2 r = __ldg(&rng[j]);
+        i0 = r.x;
+        i1 = r.y;
+    } else {
+        i0 = __ldg(&fold_ptr[j]);
+        i1 = __ldg(&fold_ptr[j + 1]);
     }
-    store_block(K, slot, acc.x, acc.y, acc.z, acc.w);
+    const long long slot = sw >> 1;
+    // plain loads, so that the run's loads are all in flight at once
+    double2 a01 = make_double2(0.0, 0.0), a23 = make_double2(0.0, 0.0);
+    if (!(sw & 1)) {
+        const double2* kb = reinterpret_cast<const double2*>(K + 4 * slot);
+        a01 = kb[0];
+        a23 = kb[1];
+    }
+    const double2* kv = reinterpret_cast<const double2*>(ke);
+    for (int i = i0; i < i1; ++i) {
+        const double2 v01 = __ldg(kv + 2 * (size_t)i), v23 = __ldg(kv + 2 * (size_t)i + 1);
+        a01.x += v01.x;
+        a01.y += v01.y;
+        a23.x += v23.x;
+        a23.y += v23.y;
+    }
+    store_block(K, slot, a01.x, a01.y, a23.x, a23.y);
 }
 
 // f_int of the nodes cut elements touch, one thread each: f = (the triangle
@@ -1933,11 +2056,11 @@ CutArgs cut_args(const Ctx& c, const double* U, double dt) {
 // Launches kern with the programmatic-stream-serialization attribute (see
 // pdl_trigger / pdl_wait).
 template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Args... args) {
+void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1949,7 +2072,7 @@ void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Arg
 
 void launch_cut_points(const Ctx& c, cudaStream_t s) {
     if (c.n_cut_pts > 0)
-        launch_pdl(k_cut_points, (c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, s, c.n_cut_pts,
+        launch_pdl(k_cut_points, (c.n_cut_pts + kPointThreads - 1) / kPointThreads, kPointThreads, 0, s, c.n_cut_pts,
                    reinterpret_cast<const int4*>(c.cut_pts), c.x, c.y, c.dmat, c.cut_rows);
 }
 
@@ -1968,63 +2091,101 @@ void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s)
     ca.coh_rows = c.coh_rows;
     ca.coh = c.coh;
     ca.dt = dt;
-    launch_pdl(k_coh_points, (c.n_coh_qp + 127) / 128, 128, s, ca);
+    launch_pdl(k_coh_points, (c.n_coh_qp + 127) / 128, 128, 0, s, ca);
 }
 
-// one launch per size class; cut_warps x 32 threads per CTA
-void launch_cut_pairs(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {
-    PairArgs pa;
-    pa.cut_nodes = c.cut_nodes;
-    pa.cut_tmpl = c.cut_tmpl;
-    pa.cut_coh_qp0 = c.cut_coh_qp0;
-    pa.cut_slot_ptr = c.cut_slot_ptr;
-    pa.kpos = c.cut_kpos;
-    pa.fpos = c.cut_fpos;
-    pa.rows = c.cut_rows;
-    pa.row_off = c.cut_row_off;
-    pa.coh_rows = c.coh_rows;
-    pa.u = U;
-    pa.ke = c.cut_ke;
-    pa.fe = c.cut_fe;
-    pa.want_K = want_K;
-    pa.want_f = want_f;
-    const int bs = 32 * c.tuning.cut_warps;
+template <int NL>
+int launch_elems_nl(const ElemArgs& ea, int blocks, int bs, size_t smem, cudaStream_t s) {
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k_cut_elems<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "k_cut_elems shared memory");
+    }
+    launch_pdl(k_cut_elems<NL>, blocks, bs, smem, s, ea);
+    return PG_OK;
+}
+
+// one launch per size class; cut_warps x 32 threads per CTA.  direct: the
+// blocks of one-contribution slots go into K (the triangle kernel runs
+// before on the same stream); otherwise every block goes to fold order.
+int launch_cut_elems(const Ctx& c, const double* U, bool want_f, bool want_K, bool direct, cudaStream_t s) {
+    ElemArgs ea;
+    ea.cut_nodes = c.cut_nodes;
+    ea.cut_tmpl = c.cut_tmpl;
+    ea.cut_coh_qp0 = c.cut_coh_qp0;
+    ea.cut_slot_ptr = c.cut_slot_ptr;
+    ea.kpos = c.cut_kpos;
+    ea.kdir = c.cut_kdir;
+    ea.fpos = c.cut_fpos;
+    ea.pts = reinterpret_cast<const int4*>(c.cut_pts);
+    ea.pt_off = c.cut_pt_off;
+    ea.row_off = c.cut_row_off;
+    ea.x = c.x;
+    ea.y = c.y;
+    ea.dmat = c.dmat;
+    ea.coh_rows = c.coh_rows;
+    ea.u = U;
+    ea.ke = c.cut_ke;
+    ea.fe = c.cut_fe;
+    ea.K = c.K;
+    ea.want_K = want_K;
+    ea.want_f = want_f;
+    ea.direct = direct ? 1 : 0;
+    const int w = c.tuning.cut_warps == 2 ? 0 : c.tuning.cut_warps == 8 ? 2 : 1;
+    const int bs = 32 * kCutCtaWarps[w];
     for (int k = 0; k < kCutClasses; ++k) {
         const int n = c.cut_class_off[k + 1] - c.cut_class_off[k];
         if (n == 0) continue;
-        pa.n_elem = n;
-        pa.first = c.cut_class_off[k];
-        const long long threads = (long long)n * kCutClassNl[k] * kCutClassNl[k];
-        const int blocks = (int)((threads + bs - 1) / bs);
-        if (k == 0) launch_pdl(k_cut_pairs<5>, blocks, bs, s, pa);
-        else if (k == 1) launch_pdl(k_cut_pairs<7>, blocks, bs, s, pa);
-        else if (k == 2) launch_pdl(k_cut_pairs<11>, blocks, bs, s, pa);
-        else launch_pdl(k_cut_pairs<15>, blocks, bs, s, pa);
+        ea.n_elem = n;
+        ea.first = c.cut_class_off[k];
+        const int epc = cut_elems_per_cta(bs, kCutClassNl[k]);
+        const int blocks = (n + epc - 1) / epc;
+        const size_t smem = sizeof(double) * (size_t)std::max(2, c.cut_span[k][w]);
+        if (smem > 227 * 1024) {
+            set_error("cut elements: a CTA's quadrature rows exceed the shared memory (use fewer warps per CTA)");
+            return PG_ERR_LIMIT;
+        }
+        int rc;
+        if (k == 0) rc = launch_elems_nl<5>(ea, blocks, bs, smem, s);
+        else if (k == 1) rc = launch_elems_nl<7>(ea, blocks, bs, smem, s);
+        else if (k == 2) rc = launch_elems_nl<11>(ea, blocks, bs, smem, s);
+        else rc = launch_elems_nl<15>(ea, blocks, bs, smem, s);
+        if (rc != PG_OK) return rc;
     }
+    return PG_OK;
 }
 
-// The cut elements' quadrature rows and cohesive points (inputs only)
-void launch_cut_rows(const Ctx& c, const double* U, double dt, cudaStream_t s) {
-    launch_cut_points(c, s);
-    launch_coh_points(c, U, dt, s);
-}
-
-void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, cudaStream_t s) {
-    if (want_K && c.n_fold_K > 0)
-        launch_pdl(k_fold_K, (c.n_fold_K + 255) / 256, 256, s, c.n_fold_K, c.fold_K_slot, c.fold_K_ptr, c.cut_ke, c.K);
+// direct: fold only the runs of two or more blocks (launch_cut_elems stored the others)
+void launch_cut_fold(const Ctx& c, bool want_f, bool want_K, bool direct, cudaStream_t s) {
+    const int nK = direct ? c.n_fold_Km : c.n_fold_K;
+    if (want_K && nK > 0)
+        launch_pdl(k_fold_K, (nK + 255) / 256, 256, 0, s, nK, direct ? c.fold_Km_slot : c.fold_K_slot, c.fold_K_ptr,
+                   direct ? c.fold_Km_rng : nullptr, c.cut_ke, c.K);
     if (want_f && c.n_fold_f > 0)
-        launch_pdl(k_fold_f, (c.n_fold_f + 255) / 256, 256, s, c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.cut_fe, c.F);
+        launch_pdl(k_fold_f, (c.n_fold_f + 255) / 256, 256, 0, s, c.n_fold_f, c.fold_f_node, c.fold_f_ptr, c.cut_fe,
+                   c.F);
+}
+
+// the cut elements' whole pass after the triangle kernel on stream s
+int launch_cut_all(const Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
+    launch_coh_points(c, U, dt, s);
+    const int rc = launch_cut_elems(c, U, want_f, want_K, true, s);
+    if (rc != PG_OK) return rc;
+    launch_cut_fold(c, want_f, want_K, true, s);
+    return PG_OK;
 }
 
 int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K, cudaStream_t s) {
     // The triangle kernel writes every regular-element value of K (and f)
-    // once; then the cut elements' quadrature rows, cohesive points and pair
-    // blocks are formed, and the fold adds them to the rows they touch and
-    // writes the enrichment rows and columns whole.  Nothing needs clearing
-    // first.  One stream, the kernels chained by programmatic dependent
-    // launch, unless the tuning leaves the persistent grid kernel's SMs some
-    // CTA slots (cut_overlap): then the rows and pairs run on the second
-    // stream beside it and the fold waits for both.
+    // once; then the cut elements' cohesive points, quadrature rows and
+    // blocks are formed, the blocks of slots no other contribution reaches
+    // go into K, and the fold adds the rest to the rows they touch and writes
+    // the remaining enrichment rows and columns whole.  Nothing needs
+    // clearing first.  One stream, the kernels chained by programmatic
+    // dependent launch, unless the tuning leaves the persistent grid kernel's
+    // SMs some CTA slots (cut_overlap): then the cut elements' kernels run on
+    // the second stream beside it, every block goes to fold order, and the
+    // fold waits for both.
     if (!(c.tuning.tri_grid && c.grid_emat)) {
         const int rc = ensure_tri_map(c);
         if (rc != PG_OK) return rc;
@@ -2038,12 +2199,13 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
         // persistent grid kernel (which leaves them CTA slots); the fold joins
         PG_CUDA(cudaEventRecord(c.fork_ev, s));
         PG_CUDA(cudaStreamWaitEvent(c.aux, c.fork_ev, 0));
-        launch_cut_rows(c, U, dt, c.aux);
-        launch_cut_pairs(c, U, want_f, want_K, c.aux);
+        launch_coh_points(c, U, dt, c.aux);
+        const int rc = launch_cut_elems(c, U, want_f, want_K, false, c.aux);
+        if (rc != PG_OK) return rc;
         PG_CUDA(cudaEventRecord(c.join_ev, c.aux));
         launch_tri(c, ra, want_f, s);
         PG_CUDA(cudaStreamWaitEvent(s, c.join_ev, 0));
-        launch_cut_fold(c, want_f, want_K, s);
+        launch_cut_fold(c, want_f, want_K, false, s);
         PG_CUDA(cudaGetLastError());
         if (c.timing) cudaEventRecord(c.ea2, s);
         return PG_OK;
@@ -2052,9 +2214,8 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     PG_CUDA(cudaGetLastError());
     if (c.timing && c.timing_split) cudaEventRecord(c.ea1, s);
     if (c.n_cut > 0) {
-        launch_cut_rows(c, U, dt, s);
-        launch_cut_pairs(c, U, want_f, want_K, s);
-        launch_cut_fold(c, want_f, want_K, s);
+        const int rc = launch_cut_all(c, U, dt, want_f, want_K, s);
+        if (rc != PG_OK) return rc;
         PG_CUDA(cudaGetLastError());
     }
     if (c.timing) cudaEventRecord(c.ea2, s);
@@ -2067,8 +2228,8 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
 // 32 / 64 node rows per CTA, one CTA per tile / persistent (4 values), then
 // the structured-grid kernel (the fastest of 128 and 256 threads per CTA,
 // one CTA per tile or persistent and pipelined; 0 without a structured grid); ms_cut: the cut elements' work on one stream
-// (rows, cohesive points, pairs with their fold) with 2 / 4 / 8 warps per
-// pair CTA.
+// (cohesive points, rows and blocks, the fold) with 2 / 4 / 8 warps per
+// k_cut_elems CTA.
 // K is left undefined: the next solve reassembles.
 int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     cudaStream_t s = c.stream;
@@ -2139,12 +2300,12 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
     for (int k = 0; k < 3; ++k) {
         c.tuning.cut_warps = warps[k];
         float ms = 0.f;
-        if (c.n_cut > 0)
-            ms = timed([&] {
-                launch_cut_rows(c, c.U, 1.0, s);
-                launch_cut_pairs(c, c.U, false, true, s);
-                launch_cut_fold(c, false, true, s);
-            });
+        int rc = PG_OK;
+        if (c.n_cut > 0) ms = timed([&] { rc = launch_cut_all(c, c.U, 1.0, false, true, s); });
+        if (rc != PG_OK) {
+            cudaFree(flush);
+            return rc;
+        }
         if (ms_cut) ms_cut[k] = ms;
         if (ms < best_cut) {
             best_cut = ms;
@@ -2339,7 +2500,7 @@ int stress_prepare(Ctx& c) {
     auto up = [&](auto** dst, const auto& v) -> int {
         using T = std::remove_pointer_t<std::remove_reference_t<decltype(*dst)>>;
         PG_CUDA(cudaMalloc((void**)dst, std::max<size_t>(1, v.size()) * sizeof(T)));
-        if (!v.empty()) PG_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        if (!v.empty()) PG_CUDA(h2d_sync(*dst, v.data(), v.size() * sizeof(T)));
         return PG_OK;
     };
     int rc;

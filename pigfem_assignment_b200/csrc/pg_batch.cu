@@ -599,7 +599,7 @@ template <typename T>
 int b_alloc(std::vector<void*>& owned, T** p, size_t n) {
     *p = nullptr;
     PG_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
-    PG_CUDA(cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+    PG_CUDA(fill_sync(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
     owned.push_back((void*)*p);
     return PG_OK;
 }
@@ -608,7 +608,7 @@ template <typename T>
 int b_upload(std::vector<void*>& owned, T** p, const std::vector<T>& v) {
     int rc = b_alloc(owned, p, v.size());
     if (rc) return rc;
-    if (!v.empty()) PG_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (!v.empty()) PG_CUDA(h2d_sync(*p, v.data(), v.size() * sizeof(T)));
     return PG_OK;
 }
 

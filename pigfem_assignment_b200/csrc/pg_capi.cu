@@ -22,7 +22,7 @@ int dev_upload(T** dst, const std::vector<T>& src) {
     *dst = nullptr;
     if (src.empty()) return PG_OK;
     PG_CUDA(cudaMalloc((void**)dst, src.size() * sizeof(T)));
-    PG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(*dst, src.data(), src.size() * sizeof(T)));
     return PG_OK;
 }
 
@@ -31,7 +31,7 @@ int dev_alloc(T** dst, size_t n) {
     *dst = nullptr;
     if (n == 0) n = 1;
     PG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
-    PG_CUDA(cudaMemset(*dst, 0, n * sizeof(T)));
+    PG_CUDA(fill_sync(*dst, 0, n * sizeof(T)));
     return PG_OK;
 }
 
@@ -60,6 +60,7 @@ void free_ctx(Ctx& c) {
     mg_free(c);
     void* ptrs[] = {c.xi, c.mw, c.nq_ptr, c.nq_list, c.featX, c.featY, c.b, c.res, c.Ut, c.Uprev, c.Uold, c.Uold2, c.isv_prev, c.red_ws, c.V, c.hbuf, c.x, c.y, c.elem4, c.row_ptr, c.col, c.diag, c.ne_ptr, c.ne_list, c.tri_map[0], c.tri_map[1], c.grid_emat, c.dmat, c.cut_nodes, c.cut_tmpl,
                     c.cut_child_mat, c.cut_coh_qp0, c.cut_slot_ptr, c.cut_slot, c.cut_rows, c.cut_row_off, c.cut_pts,
+                    c.cut_pt_off, c.cut_kdir, c.fold_Km_slot, c.fold_Km_rng,
                     c.grid_rves, c.grid_tiles[0], c.grid_tiles[1], c.qp_off, c.qp_elem_cut, c.qp_cut_elem,
                     c.qp_class_off, c.qp_out,
                     c.cut_ke, c.cut_fe, c.cut_kpos, c.cut_fpos, c.fold_K_slot, c.fold_K_ptr, c.fold_f_node,
@@ -232,10 +233,12 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
         for (int k = 0; k < kCutClasses; ++k)
             for (int oi = c.cut_class_off[k]; oi < c.cut_class_off[k + 1]; ++oi)
                 roff[oi + 1] = roff[oi] + (long long)device_point_count(tmpl[oi]) * (4 + 2 * kCutClassNl[k]);
-        std::vector<int> pts;
-        build_cut_points(nodes, tmpl, chm, roff, c.cut_class_off, pts);
+        std::vector<int> pts, pt_off;
+        build_cut_points(nodes, tmpl, chm, roff, c.cut_class_off, pts, pt_off);
         c.n_cut_pts = (int)(pts.size() / kCutPointInts) - 1;  // the last record is the sentinel
+        cut_row_spans(roff, c.cut_class_off, c.cut_span);
         if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pts, pts)) ||
+            (rc = dev_upload(&c.cut_pt_off, pt_off)) ||
             (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
             return rc;
         // cohesive Gauss points: the owning element, sub-element and point
@@ -290,7 +293,7 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
                                                   1184LL}) + 1;
         if ((rc = dev_alloc(&c.red_ws, red_ws_doubles(cap)))) return rc;
         const double capd = (double)cap;
-        PG_CUDA(cudaMemcpy(c.red_ws, &capd, sizeof(double), cudaMemcpyHostToDevice));
+        PG_CUDA(h2d_sync(c.red_ws, &capd, sizeof(double)));
         c.red_active = c.red_ws;
     }
     if ((rc = dev_alloc(&c.iflags, 64))) return rc;
@@ -743,7 +746,7 @@ int pg_set_vector(pg_ctx* c, int32_t which, const double* in) {
     double* dst = which == 0 ? x.U : which == 1 ? x.F : nullptr;
     if (!dst) { set_error("pg_set_vector: unknown vector"); return PG_ERR_ARG; }
     PG_CUDA(cudaStreamSynchronize(x.stream));
-    PG_CUDA(cudaMemcpy(dst, in, (size_t)x.n_dof * sizeof(double), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(dst, in, (size_t)x.n_dof * sizeof(double)));
     return PG_OK;
 }
 
@@ -785,7 +788,7 @@ int pg_set_isv(pg_ctx* c, int32_t committed, const double* in) {
     if (!in) { set_error("pg_set_isv: null input"); return PG_ERR_ARG; }
     if (x.n_coh_qp == 0) return PG_OK;
     PG_CUDA(cudaStreamSynchronize(x.stream));
-    PG_CUDA(cudaMemcpy(committed ? x.isv_c : x.isv_t, in, (size_t)x.n_coh_qp * sizeof(double), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(committed ? x.isv_c : x.isv_t, in, (size_t)x.n_coh_qp * sizeof(double)));
     return PG_OK;
 }
 

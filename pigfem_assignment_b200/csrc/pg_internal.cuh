@@ -19,6 +19,23 @@ struct pg_mesh {
 
 namespace pgb {
 
+// cudaMemcpy from pageable host memory and cudaMemset run on the legacy
+// default stream, which the library's non-blocking streams do not wait for,
+// and may return before the data is in place (a pageable copy returns once
+// the data is staged).  Set-up code copies and fills through these two, which
+// wait until the data is written, so that a kernel launched next on any
+// stream reads it.
+inline cudaError_t h2d_sync(void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+inline cudaError_t fill_sync(void* dst, int value, size_t bytes) {
+    cudaError_t e = cudaMemset(dst, value, bytes);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+
 // Runs fn(i) for i in [0, n) on the host's cores, in chunks of `grain`
 // consecutive indices (each index exactly once; fn must not throw).
 template <class F>
@@ -140,6 +157,10 @@ struct Ctx {
     long long* cut_row_off = nullptr;
     int* cut_pts = nullptr;
     int n_cut_pts = 0;
+    int* cut_pt_off = nullptr;         // per element (class order) its first point record, then the total
+    // the widest span of rows (doubles) that one CTA of k_cut_elems forms in
+    // shared memory, per size class and CTA size (2, 4, 8 warps)
+    int cut_span[4][3] = {};
     int* cut_slot_ptr = nullptr;
     int* cut_slot = nullptr;           // (3 + n_enr)^2 block slots per element
     int cut_class_off[5] = {0, 0, 0, 0, 0};
@@ -153,6 +174,14 @@ struct Ctx {
     long long* fold_K_slot = nullptr;  // slot << 1 | cut_only
     int* fold_K_ptr = nullptr;
     int n_fold_K = 0;
+    // slots with one cut contribution take it straight from k_cut_elems: per
+    // slot-table entry slot << 1 | cut_only for those, -2 - (fold position)
+    // for the others, -1 without a K slot; the runs of two or more (their key
+    // and their range of ke) are left to k_fold_K
+    long long* cut_kdir = nullptr;
+    long long* fold_Km_slot = nullptr;
+    int2* fold_Km_rng = nullptr;
+    int n_fold_Km = 0;
     int* fold_f_node = nullptr;        // node << 1 | cut_only
     int* fold_f_ptr = nullptr;
     int n_fold_f = 0;
@@ -295,7 +324,14 @@ int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entrie
 int device_point_count(int tmpl);  // quadrature points of a cut template on the device
 constexpr int kCutPointInts = 16;  // ints per point record of the cut-row kernel
 void build_cut_points(const std::vector<int>& nodes, const std::vector<int>& tmpl, const std::vector<int>& chm,
-                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out);
+                      const std::vector<long long>& roff, const int* class_off, std::vector<int>& out,
+                      std::vector<int>& pt_off);
+// per size class and CTA size (2, 4, 8 warps): the widest span of rows
+// (doubles) of the elements one CTA of k_cut_elems takes
+void cut_row_spans(const std::vector<long long>& roff, const int* class_off, int span[4][3]);
+constexpr int kCutCtaWarps[3] = {2, 4, 8};
+// elements of size class NL per CTA of k_cut_elems: one thread per local function
+__host__ __device__ constexpr int cut_elems_per_cta(int threads, int nl) { return threads / nl; }
 void launch_cut_sens(const Ctx& c, const CutArgs& ca, cudaStream_t s);
 
 // solver entry points (pg_solve.cu)

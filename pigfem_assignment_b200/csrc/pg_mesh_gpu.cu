@@ -774,6 +774,33 @@ __global__ void k_fold_scatter(int nc, const int* __restrict__ sp, const int* __
     }
 }
 
+// one thread per K run: a run of one entry gives that entry its slot (the
+// cut-element kernel adds it to K itself); the others are flagged for the fold
+__global__ void k_fold_single(int nruns, const int* __restrict__ run_ptr, const int* __restrict__ tmp,
+                              const long long* __restrict__ run_key, long long* kdir, int* multi) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const int i0 = run_ptr[r];
+    const bool single = run_ptr[r + 1] - i0 == 1;
+    if (single) kdir[tmp[i0]] = run_key[r];
+    multi[r] = single ? 0 : 1;
+}
+
+// entries of the longer runs: kdir = -2 - (their fold position)
+__global__ void k_fold_kdir_multi(int n, const int* __restrict__ kpos, long long* kdir) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n && kdir[e] == -1 && kpos[e] >= 0) kdir[e] = -2 - (long long)kpos[e];
+}
+
+__global__ void k_fold_multi(int nruns, const int* __restrict__ flag, const int* __restrict__ idx,
+                             const long long* __restrict__ run_key, const int* __restrict__ run_ptr,
+                             long long* m_key, int2* m_rng) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns || !flag[r]) return;
+    m_key[idx[r]] = run_key[r];
+    m_rng[idx[r]] = make_int2(run_ptr[r], run_ptr[r + 1]);
+}
+
 // one thread per run: its entries in entry order, and each entry's position
 __global__ void k_fold_order(int nruns, const int* __restrict__ run_ptr, int* tmp, int* pos) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1082,6 +1109,23 @@ int build_fold_device(Ctx& c, const std::vector<uint8_t>& node_enr, int n_entrie
                                                         tmpK, cntF, fillF, tmpF);
     k_fold_order<<<nb_mesh(nrunK), kThreadsMesh, 0, s>>>(nrunK, c.fold_K_ptr, tmpK, c.cut_kpos);
     k_fold_order<<<nb_mesh(nrunF), kThreadsMesh, 0, s>>>(nrunF, c.fold_f_ptr, tmpF, c.cut_fpos);
+    // the runs of one contribution go straight into K; the rest stay with the fold
+    int *multi, *midx;
+    MESH_CUDA(S.alloc(&multi, std::max(1, nrunK)));
+    MESH_CUDA(S.alloc(&midx, std::max(1, nrunK)));
+    MESH_CUDA(cudaMalloc((void**)&c.cut_kdir, std::max(1, n_entries) * sizeof(long long)));
+    MESH_CUDA(cudaMemsetAsync(c.cut_kdir, 0xff, std::max(1, n_entries) * sizeof(long long), s));
+    k_fold_single<<<nb_mesh(nrunK), kThreadsMesh, 0, s>>>(nrunK, c.fold_K_ptr, tmpK, c.fold_K_slot, c.cut_kdir,
+                                                          multi);
+    k_fold_kdir_multi<<<nb_mesh(n_entries), kThreadsMesh, 0, s>>>(n_entries, c.cut_kpos, c.cut_kdir);
+    int n_multi = 0;
+    MESH_CUDA(cudaMemcpyAsync(midx, multi, std::max(1, nrunK) * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    MESH_CUDA(exclusive_scan(S, midx, nrunK, n_multi, s));
+    c.n_fold_Km = n_multi;
+    MESH_CUDA(cudaMalloc((void**)&c.fold_Km_slot, std::max(1, n_multi) * sizeof(long long)));
+    MESH_CUDA(cudaMalloc((void**)&c.fold_Km_rng, std::max(1, n_multi) * sizeof(int2)));
+    k_fold_multi<<<nb_mesh(nrunK), kThreadsMesh, 0, s>>>(nrunK, multi, midx, c.fold_K_slot, c.fold_K_ptr,
+                                                         c.fold_Km_slot, c.fold_Km_rng);
     MESH_CUDA(cudaStreamSynchronize(s));
     MESH_CUDA(cudaGetLastError());
     return PG_OK;

@@ -843,7 +843,7 @@ template <typename T>
 int mg_alloc(MgHierarchy& m, T** p, size_t n) {
     *p = nullptr;
     PG_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
-    PG_CUDA(cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+    PG_CUDA(fill_sync(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
     m.owned.push_back((void*)*p);
     return PG_OK;
 }
@@ -904,8 +904,8 @@ int modes_build(Ctx& c, MgHierarchy& m) {
         (rc = mg_alloc(m, &m.E, 9 * (size_t)ni)) || (rc = mg_alloc(m, &m.Einv, 9 * (size_t)ni)) ||
         (rc = mg_alloc(m, &m.w, 3 * (size_t)ni)))
         return rc;
-    PG_CUDA(cudaMemcpy(m.z_inc, zinc.data(), zinc.size() * sizeof(int), cudaMemcpyHostToDevice));
-    PG_CUDA(cudaMemcpy(m.zval, zval.data(), zval.size() * sizeof(double), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(m.z_inc, zinc.data(), zinc.size() * sizeof(int)));
+    PG_CUDA(h2d_sync(m.zval, zval.data(), zval.size() * sizeof(double)));
     m.n_inc = ni;
     return PG_OK;
 }

@@ -427,12 +427,12 @@ int pg_mlp_create(int32_t device, uint64_t seed, pg_mlp** out) {
     m->grads = m->params + kNParams;
     m->m = m->grads + kNParams;
     m->v = m->m + kNParams;
-    PG_CUDA(cudaMemset(m->params, 0, 4 * kNParams * sizeof(float)));
+    PG_CUDA(fill_sync(m->params, 0, 4 * kNParams * sizeof(float)));
     PG_CUDA(cudaMalloc((void**)&m->loss, sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&m->err, sizeof(int)));
-    PG_CUDA(cudaMemset(m->err, 0, sizeof(int)));
+    PG_CUDA(fill_sync(m->err, 0, sizeof(int)));
     PG_CUDA(cudaMalloc((void**)&m->probe, TILE * (IN + 2) * sizeof(float)));
-    PG_CUDA(cudaMemset(m->probe, 0, TILE * (IN + 2) * sizeof(float)));
+    PG_CUDA(fill_sync(m->probe, 0, TILE * (IN + 2) * sizeof(float)));
     cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, device);
     PG_CUDA(cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
     PG_CUDA(cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
@@ -445,7 +445,7 @@ int pg_mlp_create(int32_t device, uint64_t seed, pg_mlp** out) {
     for (int i = 0; i < kW2; ++i) hp.W2[i] = nd(rng) * std::sqrt(2.f / HID);
     for (int o = 0; o < USED; ++o)
         for (int j = 0; j < HID; ++j) hp.W3[o * HID + j] = 0.1f * nd(rng) * std::sqrt(1.f / HID);
-    PG_CUDA(cudaMemcpy(m->params, h.data(), kNParams * sizeof(float), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(m->params, h.data(), kNParams * sizeof(float)));
     *out = m;
     return PG_OK;
 }
@@ -468,8 +468,8 @@ int pg_mlp_params(pg_mlp* m, float* host, int32_t set) {
     cudaSetDevice(m->device);
     PG_CUDA(cudaStreamSynchronize(m->stream));
     if (set) {
-        PG_CUDA(cudaMemcpy(m->params, host, kNParams * sizeof(float), cudaMemcpyHostToDevice));
-        PG_CUDA(cudaMemset(m->m, 0, 2 * kNParams * sizeof(float)));
+        PG_CUDA(h2d_sync(m->params, host, kNParams * sizeof(float)));
+        PG_CUDA(fill_sync(m->m, 0, 2 * kNParams * sizeof(float)));
         m->step = 0;
     } else {
         PG_CUDA(cudaMemcpy(host, m->params, kNParams * sizeof(float), cudaMemcpyDeviceToHost));

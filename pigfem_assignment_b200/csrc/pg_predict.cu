@@ -178,9 +178,9 @@ int build_node_qp_map(Ctx& c) {
         ptr[i + 1] = (int)list.size();
     }
     PG_CUDA(cudaMalloc((void**)&c.nq_ptr, ptr.size() * sizeof(int)));
-    PG_CUDA(cudaMemcpy(c.nq_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(c.nq_ptr, ptr.data(), ptr.size() * sizeof(int)));
     PG_CUDA(cudaMalloc((void**)&c.nq_list, std::max<size_t>(1, list.size()) * sizeof(int)));
-    if (!list.empty()) PG_CUDA(cudaMemcpy(c.nq_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!list.empty()) PG_CUDA(h2d_sync(c.nq_list, list.data(), list.size() * sizeof(int)));
     return PG_OK;
 }
 

@@ -89,16 +89,16 @@ int sens_setup(Ctx& c, SensData& d, int n_slots) {
     PG_CUDA(cudaMalloc((void**)&d.node_inc, nn * sizeof(int)));
     for (int kind = 0; kind < 3; ++kind) {
         PG_CUDA(cudaMalloc((void**)&d.vel[kind], vel[kind].size() * sizeof(double)));
-        PG_CUDA(cudaMemcpy(d.vel[kind], vel[kind].data(), vel[kind].size() * sizeof(double), cudaMemcpyHostToDevice));
+        PG_CUDA(h2d_sync(d.vel[kind], vel[kind].data(), vel[kind].size() * sizeof(double)));
     }
     PG_CUDA(cudaMalloc((void**)&d.radius, rad.size() * sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&d.L, d.hL.size() * sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&d.w, d.hL.size() * sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&d.sens, std::max(1, n_slots) * sizeof(double)));
     PG_CUDA(cudaMalloc((void**)&d.param_of, 3 * (size_t)std::max(1, d.n_inc) * sizeof(int)));
-    PG_CUDA(cudaMemcpy(d.node_inc, inc.data(), nn * sizeof(int), cudaMemcpyHostToDevice));
-    PG_CUDA(cudaMemcpy(d.radius, rad.data(), rad.size() * sizeof(double), cudaMemcpyHostToDevice));
-    PG_CUDA(cudaMemcpy(d.L, d.hL.data(), d.hL.size() * sizeof(double), cudaMemcpyHostToDevice));
+    PG_CUDA(h2d_sync(d.node_inc, inc.data(), nn * sizeof(int)));
+    PG_CUDA(h2d_sync(d.radius, rad.data(), rad.size() * sizeof(double)));
+    PG_CUDA(h2d_sync(d.L, d.hL.data(), d.hL.size() * sizeof(double)));
     return PG_OK;
 }
 

@@ -381,19 +381,21 @@ int pg_sensitivity_c11(pg_ctx* c, const pg_solver_cfg* cfg, double h_rel, double
  * and 256 threads per CTA, each with one CTA per tile or a persistent grid
  * that stages the next tile with asynchronous copies while forming the
  * current one; 0 if the mesh is not made of structured grids);
- * ms_cut[3] = the cut elements' work (quadrature rows, cohesive points, pair
- * blocks, fold) with 2 / 4 / 8 warps per CTA of the pair kernel (NULL
- * allowed).  K is left to be reassembled. */
+ * ms_cut[3] = the cut elements' work (cohesive points, quadrature rows and
+ * blocks, fold) with 2 / 4 / 8 warps per CTA of the cut-element kernel (NULL
+ * allowed); then, with the structured-grid kernel, whole passes of both its
+ * variants with the cut elements' kernels after it or beside it
+ * (pg_ctx_cut_overlap).  K is left to be reassembled. */
 int pg_ctx_autotune(pg_ctx* c, int32_t reps, float* ms_tri, float* ms_cut);
 /* the launch shapes in use, and setting them by hand (tile 32 or 64 node rows per CTA of the
  * row-tile kernel, or 128 / 256 threads per CTA of the structured-grid kernel; persistent 0/1
- * for either; warps 2/4/8 per CTA of the cut elements' pair kernel) */
+ * for either; warps 2/4/8 per CTA of the cut elements' kernel) */
 int pg_ctx_tuning(pg_ctx* c, int32_t* tri_tile_nodes, int32_t* tri_persistent, int32_t* cut_warps);
 int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent, int32_t cut_warps);
-/* With the persistent structured-grid kernel: the CTA slots per SM it leaves to the cut
- * elements' row and pair kernels, which then run beside it on a second stream (0: after it
- * on the same stream; the autotuner times 0, 1 and 2 on whole passes).  set < 0 only reads;
- * get may be NULL. */
+/* With the structured-grid kernel: 0 runs the cut elements' kernels after it on the same
+ * stream; 1 or 2 runs them beside it on a second stream, the persistent grid kernel leaving
+ * them that many CTA slots per SM.  The autotuner times every combination with both grid
+ * variants on whole passes.  set < 0 only reads; get may be NULL. */
 int pg_ctx_cut_overlap(pg_ctx* c, int32_t set, int32_t* get);
 
 /* ---- batches of independent linear-elastic RVEs ----

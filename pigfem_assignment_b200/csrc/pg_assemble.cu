@@ -2182,18 +2182,18 @@ int launch_assemble(Ctx& c, const double* U, double dt, bool want_f, bool want_K
     // go into K, and the fold adds the rest to the rows they touch and writes
     // the remaining enrichment rows and columns whole.  Nothing needs
     // clearing first.  One stream, the kernels chained by programmatic
-    // dependent launch, unless the tuning leaves the persistent grid kernel's
-    // SMs some CTA slots (cut_overlap): then the cut elements' kernels run on
-    // the second stream beside it, every block goes to fold order, and the
-    // fold waits for both.
+    // dependent launch, unless the tuning sets cut_overlap with the grid
+    // kernel (the persistent one then leaves that many CTA slots per SM):
+    // then the cut elements' kernels run on the second stream beside it,
+    // every block goes to fold order, and the fold waits for both.
     if (!(c.tuning.tri_grid && c.grid_emat)) {
         const int rc = ensure_tri_map(c);
         if (rc != PG_OK) return rc;
     }
     const RowArgs ra = row_args(c, U, want_f, want_K);
     if (c.timing) cudaEventRecord(c.ea0, s);
-    const bool overlap = c.n_cut > 0 && c.tuning.cut_overlap > 0 && c.tuning.tri_persistent && c.tuning.tri_grid &&
-                         c.grid_emat && !(c.timing && c.timing_split);
+    const bool overlap = c.n_cut > 0 && c.tuning.cut_overlap > 0 && c.tuning.tri_grid && c.grid_emat &&
+                         !(c.timing && c.timing_split);
     if (overlap) {
         // the cut elements' rows and pairs on the second stream, beside the
         // persistent grid kernel (which leaves them CTA slots); the fold joins
@@ -2275,6 +2275,9 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
                 best.tri_grid = 0;
             }
         }
+    // the fastest CTA size of the grid kernel per variant (one CTA per tile, persistent)
+    float grid_ms_of[2] = {1e30f, 1e30f};
+    int grid_bs_of[2] = {256, 256};
     if (c.grid_emat) {
         c.tuning.tri_grid = 1;
         float ms_grid = 0.f;
@@ -2284,6 +2287,10 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
                 c.tuning.tri_persistent = p;  // 1: the persistent, pipelined grid kernel
                 const RowArgs ra = row_args(c, c.U, false, true);
                 const float ms = timed([&] { launch_tri(c, ra, false, s); });
+                if (ms < grid_ms_of[p]) {
+                    grid_ms_of[p] = ms;
+                    grid_bs_of[p] = bs;
+                }
                 if (ms_grid == 0.f || ms < ms_grid) ms_grid = ms;
                 if (ms < best_tri) {
                     best_tri = ms;
@@ -2312,20 +2319,27 @@ int autotune_assembly(Ctx& c, int reps, float* ms_tri, float* ms_cut) {
             best.cut_warps = warps[k];
         }
     }
-    // with the persistent grid kernel: the whole pass with the cut kernels
-    // after it, or beside it with 1 or 2 CTA slots per SM left to them
+    // with the grid kernel, whole passes decide: each variant of it (its
+    // fastest CTA size) with the cut elements' kernels after it on the same
+    // stream, or beside it on the second stream -- the persistent one leaving
+    // them 1 or 2 CTA slots per SM
     best.cut_overlap = 0;
-    if (c.n_cut > 0 && best.tri_grid && best.tri_persistent && c.grid_emat) {
-        c.tuning = best;
+    if (c.n_cut > 0 && best.tri_grid && c.grid_emat) {
         float best_pass = 1e30f;
-        for (int ov = 0; ov <= 2; ++ov) {
-            c.tuning.cut_overlap = ov;
-            const float ms = timed([&] { launch_assemble(c, c.U, 1.0, false, true, s); });
-            if (ms < best_pass) {
-                best_pass = ms;
-                best.cut_overlap = ov;
+        AsmTuning pick = best;
+        for (int p = 0; p < 2; ++p)
+            for (int ov = 0; ov <= (p ? 2 : 1); ++ov) {
+                c.tuning = best;
+                c.tuning.tri_persistent = p;
+                c.tuning.grid_block = grid_bs_of[p];
+                c.tuning.cut_overlap = ov;
+                const float ms = timed([&] { launch_assemble(c, c.U, 1.0, false, true, s); });
+                if (ms < best_pass) {
+                    best_pass = ms;
+                    pick = c.tuning;
+                }
             }
-        }
+        best = pick;
     }
     c.tuning = best;
     c.assembled = false;

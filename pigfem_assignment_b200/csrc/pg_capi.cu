@@ -556,7 +556,7 @@ int pg_ctx_set_tuning(pg_ctx* c, int32_t tri_tile_nodes, int32_t tri_persistent,
 int pg_ctx_cut_overlap(pg_ctx* c, int32_t set, int32_t* get) {
     PG_GUARD_CTX(c);
     if (set >= 0) {
-        if (set > 2) { set_error("pg_ctx_cut_overlap: 0, 1 or 2 CTA slots per SM"); return PG_ERR_ARG; }
+        if (set > 2) { set_error("pg_ctx_cut_overlap: 0 (after the grid kernel), 1 or 2 (beside it)"); return PG_ERR_ARG; }
         c->c.tuning.cut_overlap = set;
     }
     if (get) *get = c->c.tuning.cut_overlap;

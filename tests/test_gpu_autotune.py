@@ -97,7 +97,7 @@ def test_pipelined_grid_kernel_writes_the_same_bits(tile):
     rng = np.random.default_rng(7)
     ctx.set_vector(0, 1e-3 * rng.standard_normal(m.info["n_dof"]))
     out = []
-    for persistent, overlap in ((0, 0), (1, 0), (1, 1), (1, 2)):
+    for persistent, overlap in ((0, 0), (0, 1), (1, 0), (1, 1), (1, 2)):
         _lib.check(_lib.lib.pg_ctx_set_tuning(ctx.handle, tile, persistent, 4))
         _lib.check(_lib.lib.pg_ctx_cut_overlap(ctx.handle, overlap, None))
         pb.Assembler(ctx).assemble_nonlinear(1.0, True, True)

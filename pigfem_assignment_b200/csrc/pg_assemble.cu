@@ -1316,7 +1316,7 @@ __device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_c
 // diagonal block, add the node's cohesive traction term.  A block whose K
 // slot no other contribution reaches goes straight into K (direct); the
 // others go to their place in fold order.
-template <int NL>
+template <int NL, bool WF, bool COH>
 __global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_elems(ElemArgs a) {
     extern __shared__ __align__(16) double sRow[];
     pdl_trigger();
@@ -1382,7 +1382,7 @@ __global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_el
     // traction integral below, not the cohesive tangent times u); every
     // block but the diagonal one is final here
     double fx = 0.0, fy = 0.0;
-    if (a.want_f) {
+    if (WF) {
 #pragma unroll
         for (int b = 0; b < NL; ++b) {
             if (b < nl) {
@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_el
             }
         }
     }
-    if (T.n_coh > 0) {
+    if (COH && T.n_coh > 0) {
         const int qp0 = __ldg(&a.cut_coh_qp0[ci]);
         for (int ce = 0; ce < T.n_coh; ++ce) {
             int i = -1;
@@ -1434,7 +1434,7 @@ __global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_el
             }
         }
     }
-    if (a.want_f) {
+    if (WF) {
         const int fp = __ldg(&a.fpos[sp0 + pa]);
         if (fp >= 0) reinterpret_cast<double2*>(a.fe)[fp] = make_double2(fx, fy);
     }
@@ -2094,15 +2094,27 @@ void launch_coh_points(const Ctx& c, const double* U, double dt, cudaStream_t s)
     launch_pdl(k_coh_points, (c.n_coh_qp + 127) / 128, 128, 0, s, ca);
 }
 
-template <int NL>
-int launch_elems_nl(const ElemArgs& ea, int blocks, int bs, size_t smem, cudaStream_t s) {
+template <int NL, bool WF, bool COH>
+int launch_elems_inst(const ElemArgs& ea, int blocks, int bs, size_t smem, cudaStream_t s) {
     if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(k_cut_elems<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(k_cut_elems<NL, WF, COH>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "k_cut_elems shared memory");
     }
-    launch_pdl(k_cut_elems<NL>, blocks, bs, smem, s, ea);
+    launch_pdl(k_cut_elems<NL, WF, COH>, blocks, bs, smem, s, ea);
     return PG_OK;
+}
+
+// residual passes (WF) and cohesive meshes (COH) take their own instances, so
+// that the stiffness-only pass of a linear mesh carries neither in registers
+template <int NL>
+int launch_elems_nl(const ElemArgs& ea, bool coh, int blocks, int bs, size_t smem, cudaStream_t s) {
+    if (ea.want_f) {
+        return coh ? launch_elems_inst<NL, true, true>(ea, blocks, bs, smem, s)
+                   : launch_elems_inst<NL, true, false>(ea, blocks, bs, smem, s);
+    }
+    return coh ? launch_elems_inst<NL, false, true>(ea, blocks, bs, smem, s)
+               : launch_elems_inst<NL, false, false>(ea, blocks, bs, smem, s);
 }
 
 // one launch per size class; cut_warps x 32 threads per CTA.  direct: the
@@ -2146,10 +2158,11 @@ int launch_cut_elems(const Ctx& c, const double* U, bool want_f, bool want_K, bo
             return PG_ERR_LIMIT;
         }
         int rc;
-        if (k == 0) rc = launch_elems_nl<5>(ea, blocks, bs, smem, s);
-        else if (k == 1) rc = launch_elems_nl<7>(ea, blocks, bs, smem, s);
-        else if (k == 2) rc = launch_elems_nl<11>(ea, blocks, bs, smem, s);
-        else rc = launch_elems_nl<15>(ea, blocks, bs, smem, s);
+        const bool coh = c.n_coh_qp > 0;
+        if (k == 0) rc = launch_elems_nl<5>(ea, coh, blocks, bs, smem, s);
+        else if (k == 1) rc = launch_elems_nl<7>(ea, coh, blocks, bs, smem, s);
+        else if (k == 2) rc = launch_elems_nl<11>(ea, coh, blocks, bs, smem, s);
+        else rc = launch_elems_nl<15>(ea, coh, blocks, bs, smem, s);
         if (rc != PG_OK) return rc;
     }
     return PG_OK;

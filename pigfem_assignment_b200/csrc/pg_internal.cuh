@@ -108,16 +108,16 @@ constexpr int kGridTileCols = 64;          // node columns per structured-grid t
 // Autotuned launch shapes of the assembly kernels (pg_ctx_autotune):
 // the structured-grid kernel's CTA size, or (meshes without one grid) the
 // row-tile kernel's tile size and persistent grid (CTAs walk the tiles) or
-// one CTA per tile, and the warps per CTA of the cut elements' pair kernel.
+// one CTA per tile, and the warps per CTA of the cut-element kernel.
 struct AsmTuning {
     int tri_grid = 1;      // 1: the structured-grid kernel (when the mesh has one grid)
     int grid_block = 256;  // its threads per CTA: 128 or 256
     int tri_variant = 1;   // otherwise: index into kTriTileSizes
     int tri_persistent = 0;
     int cut_warps = 4;     // 2, 4 or 8
-    // with the persistent structured-grid kernel: CTA slots per SM it leaves to
-    // the cut elements' row and pair kernels, which then run beside it on a
-    // second stream (0: after it, on the same stream)
+    // with the structured-grid kernel: 0 runs the cut elements' kernels after
+    // it on the same stream; 1 or 2 runs them beside it on a second stream (the
+    // persistent grid kernel leaving them that many CTA slots per SM)
     int cut_overlap = 0;
 };
 

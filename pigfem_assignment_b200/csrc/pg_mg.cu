@@ -479,7 +479,9 @@ __global__ void k_mg_prolong(int nxf, int nyf, int nxc, const T* __restrict__ xc
 // back up.  Their operators, diagonal inverses and vectors are first copied
 // into shared memory (one coalesced pass), so no phase waits on L2; the
 // result of level `first` goes back to its x for the caller's prolongation.
-constexpr int kMgBottomNodes = 1200;       // levels at most this size may run in k_mg_bottom
+// (taking the 33x33 level as well, its operators read from L2, made the bottom
+// 151 us instead of 34 us per cycle: slower than that level's seven launches)
+constexpr int kMgBottomNodes = 300;        // levels at most this size may run in k_mg_bottom
 constexpr int kMgBottomSmem = 220 * 1024;  // and their shared-memory copy at most this many bytes
 constexpr int kMgBottomThreads = 512;
 constexpr int kMgBottomLevels = 8;

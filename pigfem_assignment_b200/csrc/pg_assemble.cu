@@ -2535,6 +2535,8 @@ int stress_prepare(Ctx& c) {
         (rc = up(&c.qp_class_off, std::vector<int>(c.cut_class_off, c.cut_class_off + kCutClasses + 1))))
         return rc;
     PG_CUDA(cudaMalloc((void**)&c.qp_out, 7 * std::max<size_t>(1, (size_t)c.n_qp_total) * sizeof(double)));
+    if (c.n_cut > 0 && !c.cut_rows)
+        PG_CUDA(cudaMalloc((void**)&c.cut_rows, std::max<size_t>(1, (size_t)c.cut_rows_len) * sizeof(double)));
     return PG_OK;
 }
 

@@ -238,9 +238,9 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
         c.n_cut_pts = (int)(pts.size() / kCutPointInts) - 1;  // the last record is the sentinel
         cut_row_spans(roff, c.cut_class_off, c.cut_span);
         if ((rc = dev_upload(&c.cut_row_off, roff)) || (rc = dev_upload(&c.cut_pts, pts)) ||
-            (rc = dev_upload(&c.cut_pt_off, pt_off)) ||
-            (rc = dev_alloc(&c.cut_rows, (size_t)std::max(1LL, roff[nc]))))
+            (rc = dev_upload(&c.cut_pt_off, pt_off)))
             return rc;
+        c.cut_rows_len = roff[nc];  // allocated by the stress recovery, the only user of rows in global memory
         // cohesive Gauss points: the owning element, sub-element and point
         if (hm.n_coh_qp > 0) {
             std::vector<int> rec(hm.n_coh_qp, -1);

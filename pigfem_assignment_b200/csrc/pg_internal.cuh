@@ -151,9 +151,12 @@ struct Ctx {
     int* cut_coh_qp0 = nullptr;        // first cohesive quadrature point (mesh numbering)
     // quadrature rows of the cut elements ({w det, d11, d12, d33, (gx, gy) per
     // local function}, 4 + 2 NL doubles for size class NL, point-major per
-    // element), formed by k_cut_points at every assembly from one record per
-    // point (build_cut_points); per element (class order) its first row's offset
-    double* cut_rows = nullptr;
+    // element), formed from one record per point (build_cut_points): in
+    // shared memory by k_cut_elems at every assembly, and in global memory by
+    // k_cut_points for the stress recovery; per element (class order) its
+    // first row's offset
+    double* cut_rows = nullptr;        // (stress recovery only, allocated on its first use)
+    long long cut_rows_len = 0;
     long long* cut_row_off = nullptr;
     int* cut_pts = nullptr;
     int n_cut_pts = 0;

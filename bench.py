@@ -588,6 +588,7 @@ def cohesive_load_steps(local: int, eta: float, n_train: int = 8, train_steps: i
             "newton_iterations": int(sum(r.newton_its for r in R)),
             "krylov_iterations": int(sum(r.krylov_its for r in R)),
             "repeated_steps": int(sum(1 for r in R if r.repeats > 1)),
+            "gmres_fallbacks": int(sum(r.gmres_fallbacks for r in R)),
             "learned_used": int(sum(1 for r in R if r.predictor_used == _lib.PG_PREDICT_LEARNED)),
             "learned_over_linear_start_residual": (
                 float(np.median([r.res_learned / r.res_linear for r in R if r.res_linear > 0 and r.res_learned > 0]))

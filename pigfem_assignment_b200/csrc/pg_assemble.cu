@@ -1286,7 +1286,8 @@ struct ElemArgs {
     const int* __restrict__ cut_coh_qp0;
     const int* __restrict__ cut_slot_ptr;
     const int* __restrict__ kpos;   // slot-table entry -> position in fold order (-1: no K slot)
-    const long long* __restrict__ kdir;  // slot-table entry -> slot << 1 | cut_only of a one-entry run, else -1
+    const long long* __restrict__ kdir;  // slot-table entry -> slot << 1 | cut_only of a one-entry run,
+                                         // else -2 - (fold position), -1 without a K slot (direct passes)
     const int* __restrict__ fpos;   // slot-table entry -> position in node order
     const int4* __restrict__ pts;   // point records (build_cut_points)
     const int* __restrict__ pt_off; // per element its first point record
@@ -1313,9 +1314,10 @@ __device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_c
 // K_ab = sum_q w_q B_a^T D B_b over the rows for every b, plus the cohesive
 // sub-elements' N_a N_b (+-) R^T D R terms where both nodes are cohesive
 // nodes.  Residual passes store K_ab u_b (bulk) for every b and, on the
-// diagonal block, add the node's cohesive traction term.  A block whose K
-// slot no other contribution reaches goes straight into K (direct); the
-// others go to their place in fold order.
+// diagonal block, add the node's cohesive traction term.  In direct passes
+// a block whose K slot no other contribution reaches goes straight into K
+// (stored, or added to the triangle kernel's value by a single-addend
+// reduction); every other block goes to its place in fold order.
 template <int NL, bool WF, bool COH>
 __global__ void __launch_bounds__(256, NL <= 5 ? 3 : (NL <= 7 ? 2 : 1)) k_cut_elems(ElemArgs a) {
     extern __shared__ __align__(16) double sRow[];

@@ -1064,34 +1064,43 @@ __global__ void __launch_bounds__(kGridTileC * TR, 12 / TR) k_grid_rows_pipe(Gri
 
 // True when every regular row of the block pattern is laid out as
 // k_grid_rows assumes: the node's grid neighbours (grid_nbr_mask) and
-// itself in ascending order, then only enrichment columns.
-bool grid_pattern_ok(const HostMesh& hm) {
-    for (const auto& gb : hm.grids) {
-        const int nx = gb.nx, ny = gb.ny, no = gb.node_off;
-        if ((long long)(nx + 1) * (ny + 1) != gb.n_reg || gb.elem_off % 2) return false;
-        for (int gj = 0; gj <= ny; ++gj)
-            for (int gi = 0; gi <= nx; ++gi) {
-                const int i = no + gi + gj * (nx + 1);
-                const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
-                int q = hm.row_ptr[i];
-                for (int d = 0; d < 9; ++d) {
-                    if (!(mask & (1u << d))) continue;
-                    const int j = no + (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
-                    if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
-                    ++q;
-                }
-                // then only this block's enrichment nodes
-                for (; q < hm.row_ptr[i + 1]; ++q)
-                    if (hm.col[q] < no + gb.n_reg) return false;
+// itself in ascending order, then only enrichment columns; checked per grid
+// block (one per RVE of a batch).
+static bool grid_block_pattern_ok(const HostMesh& hm, const HostMesh::GridBlock& gb) {
+    const int nx = gb.nx, ny = gb.ny, no = gb.node_off;
+    if ((long long)(nx + 1) * (ny + 1) != gb.n_reg || gb.elem_off % 2) return false;
+    for (int gj = 0; gj <= ny; ++gj)
+        for (int gi = 0; gi <= nx; ++gi) {
+            const int i = no + gi + gj * (nx + 1);
+            const unsigned mask = grid_nbr_mask(gi, gj, nx, ny);
+            int q = hm.row_ptr[i];
+            for (int d = 0; d < 9; ++d) {
+                if (!(mask & (1u << d))) continue;
+                const int j = no + (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
+                if (q >= hm.row_ptr[i + 1] || hm.col[q] != j) return false;
+                ++q;
             }
-        // the block's elements are its grid cells in order
-        for (int e = 0; e < 2 * nx * ny; e += 2 * nx) {
-            const int ge = gb.elem_off + e;
-            const int cj = e / (2 * nx);
-            if (hm.conn[3 * (size_t)ge] != no + cj * (nx + 1)) return false;
+            // then only this block's enrichment nodes
+            for (; q < hm.row_ptr[i + 1]; ++q)
+                if (hm.col[q] < no + gb.n_reg) return false;
         }
+    // the block's elements are its grid cells in order
+    for (int e = 0; e < 2 * nx * ny; e += 2 * nx) {
+        const int ge = gb.elem_off + e;
+        const int cj = e / (2 * nx);
+        if (hm.conn[3 * (size_t)ge] != no + cj * (nx + 1)) return false;
     }
-    return !hm.grids.empty();
+    return true;
+}
+
+bool grid_pattern_ok(const HostMesh& hm) {
+    if (hm.grids.empty()) return false;
+    // every grid block, in parallel
+    std::atomic<bool> ok{true};
+    parallel_for((long long)hm.grids.size(), 1, [&](long long g) {
+        if (ok.load(std::memory_order_relaxed) && !grid_block_pattern_ok(hm, hm.grids[g])) ok.store(false);
+    });
+    return ok.load();
 }
 
 void launch_grid(const Ctx& c, const double* U, bool want_f, bool want_K, cudaStream_t s) {

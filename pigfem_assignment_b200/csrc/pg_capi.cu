@@ -129,8 +129,9 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
     if ((rc = dev_upload(&c.x, hm.x))) return rc;
     if ((rc = dev_upload(&c.y, hm.y))) return rc;
     std::vector<int4> e4(hm.n_elem);
-    for (int e = 0; e < hm.n_elem; ++e)
+    parallel_for(hm.n_elem, 1 << 16, [&](long long e) {
         e4[e] = make_int4(hm.conn[3 * e], hm.conn[3 * e + 1], hm.conn[3 * e + 2], hm.elem_mat[e]);
+    });
     if ((rc = dev_upload(&c.elem4, e4))) return rc;
     if ((rc = dev_upload(&c.row_ptr, hm.row_ptr))) return rc;
     if ((rc = dev_upload(&c.col, hm.col))) return rc;
@@ -146,7 +147,7 @@ int ctx_create(HostMesh mesh, int device, Ctx& c) {
         // structured background grids (one per RVE of a batch): the grid kernel
         // applies, through a tile table per tile height over all of them
         std::vector<int> em(hm.n_elem);
-        for (int e = 0; e < hm.n_elem; ++e) em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e];
+        parallel_for(hm.n_elem, 1 << 16, [&](long long e) { em[e] = hm.elem_cut[e] >= 0 ? -1 : hm.elem_mat[e]; });
         if ((rc = dev_upload(&c.grid_emat, em))) return rc;
         std::vector<int4> rves;
         for (const auto& gb : hm.grids) rves.push_back(make_int4(gb.nx, gb.ny, gb.node_off, gb.elem_off));

@@ -48,9 +48,11 @@ class MLP:
         self.handle = h
         self.device = device
 
+    _destroy = lib.pg_mlp_destroy  # held by the class: usable while the interpreter shuts down
+
     def close(self):
         if getattr(self, "handle", None):
-            lib.pg_mlp_destroy(self.handle)
+            self._destroy(self.handle)
             self.handle = None
 
     def __del__(self):

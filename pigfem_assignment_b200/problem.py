@@ -68,10 +68,14 @@ class Mesh:
         check(lib.pg_mesh_info_get(h, C.byref(info)))
         self.info = {f: getattr(info, f) for f, _ in _lib.MeshInfo._fields_}
 
+    # held by the class, so that a mesh collected while the interpreter shuts
+    # down (module globals already cleared) is still released
+    _destroy = lib.pg_mesh_destroy
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib.pg_mesh_destroy(h)
+            self._destroy(h)
             self.handle = None
 
     def export(self) -> Dict[str, np.ndarray]:
@@ -120,9 +124,11 @@ class DeviceContext:
         self.handle = h
         self.info = mesh.info
 
+    _destroy = lib.pg_ctx_destroy  # (as Mesh._destroy)
+
     def close(self):
         if getattr(self, "handle", None):
-            lib.pg_ctx_destroy(self.handle)
+            self._destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -725,26 +725,6 @@ __device__ __forceinline__ void store_block(double* K, long long q, double k0, d
     asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "d"(k0), "d"(k1), "d"(k2), "d"(k3) : "memory");
 }
 
-// One 2x2 block as a single 256-bit load through the read-only path (data
-// the launch does not write).
-__device__ __forceinline__ double4 load_block_nc(const double* K, long long q) {
-    double4 v;
-    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
-                 : "l"(K + 4 * q));
-    return v;
-}
-
-// The same from memory the launch also writes (plain load).
-__device__ __forceinline__ double4 load_block(const double* K, long long q) {
-    double4 v;
-    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
-                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
-                 : "l"(K + 4 * q)
-                 : "memory");
-    return v;
-}
-
 struct GridArgs {
     const int4* __restrict__ tiles;     // per CTA: grid block, I0, J0
     const int4* __restrict__ rves;      // per grid block: nx, ny, first node, first element

@@ -37,7 +37,7 @@ namespace {
 
 constexpr int kStaticMaxNodes = PG_STATIC_MAX_NODES;
 constexpr int kStaticChunk = 32;   // iterations launched between two host reads of the status flags
-// set-up verdicts in the breakdown flag (CG itself writes 1 there)
+// set-up outcomes in the breakdown flag (CG itself writes 1 there)
 constexpr int kStaticNoDiag = 2;    // a free DOF whose row has no diagonal block
 constexpr int kStaticSingular = 3;  // a free DOF's diagonal block (or pivot) is zero or not finite
 

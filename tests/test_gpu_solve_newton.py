@@ -17,7 +17,7 @@ def test_gpu_newton_follows_reference_trajectory(precision):
     """Four load steps (dt = 0.1, 0.25% strain each) from zero state: the
     converged displacements and delta_max after every step match the
     reference's (its SNES Newton, run to rtol 1e-12 for the fixture) within
-    the north star's displacement bound 1e-8, delta_max within 1e-10."""
+    the displacement bound 1e-8, delta_max within 1e-10."""
     g = golden("cohesive_16x16.npz")
     rve = rve_from_golden(g, cohesive=True)
     nsteps = int(g["cfg.nsteps"][0])

@@ -5,7 +5,7 @@ of a few seeded cohesive RVEs, then load-steps a held-out RVE with the
 zeroth-order (the reference's), linear and learned predictors.  The learned
 start -- one blend of each node's linear and quadratic extrapolation, voted
 by the network over the nodes -- must be formed and taken at most steps, the
-run must converge to the same load path (the Newton residual is the judge),
+run must converge to the same load path (the Newton residual decides),
 and it may cost at most 10% more Newton iterations than the linear start.
 What it gains on the benchmark configuration is measured in bench.py
 (cohesive_load_step); on these smooth paths (G_c 1 N/mm) every start needs

@@ -20,7 +20,7 @@ def test_oracle_K_matches_reference(name):
     om = oracle.from_reference(g)
     K, _, _ = om.assemble()
     err = rel_fro(permute_to_ref(K, om.ref_dof), ref_full_K(g))
-    # FP64 path tolerance of the north star: relative Frobenius error <= 1e-12
+    # FP64 path tolerance: relative Frobenius error <= 1e-12
     assert err <= 1e-12, err
 
 

@@ -18,7 +18,8 @@
 // Weight gradients: dW2 and dW1 come out of one M=128 GEMM whose A stacks
 // dZ2^T over dZ1^T and whose B stacks H1^T over X^T (the off-diagonal blocks
 // are not read); dW3 uses A = [dY^T; 0].  They accumulate in tensor memory
-// over all tiles a CTA processes and are flushed with FP32 atomics once.
+// over all tiles a CTA processes; each CTA then writes its part of the
+// gradient to its own slot and k_grad_sum adds the parts in CTA order.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -63,6 +64,28 @@ constexpr uint32_t SMEM_ALLOC = O_B3 + 32768 + 1024;
 struct Params {
     float* W1; float* b1; float* W2; float* b2; float* W3; float* b3;
 };
+
+constexpr int kW1 = HID * IN, kB1 = HID, kW2 = HID * HID, kB2 = HID, kW3 = OUT * HID, kB3 = OUT;
+constexpr int kNParams = kW1 + kB1 + kW2 + kB2 + kW3 + kB3;
+
+__host__ __device__ inline Params carve(float* base) {
+    Params q;
+    q.W1 = base;
+    q.b1 = q.W1 + kW1;
+    q.W2 = q.b1 + kB1;
+    q.b2 = q.W2 + kW2;
+    q.W3 = q.b2 + kB2;
+    q.b3 = q.W3 + kW3;
+    return q;
+}
+
+// Sum over a warp's lanes by a fixed butterfly: every lane gets the same
+// value, in the same order on every run.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
 // byte offset of element (row, k) in a canonical K-major tile with K columns
 __device__ __forceinline__ uint32_t kmaj(int row, int k, int K) {
@@ -184,18 +207,25 @@ __device__ __forceinline__ bool gemm(uint32_t sbase, uint32_t a_off, uint32_t b_
     return ok;
 }
 
-// Training (want_grad) or inference pass over n rows.
+// Training (kTrain) or inference pass over n rows.  Training writes this
+// CTA's gradient (kNParams floats, summed over its tiles) to gpart + CTA *
+// kNParams and its share of the loss to lpart[CTA]; k_grad_sum adds the CTAs'
+// parts in CTA order.  Every sum inside a CTA has a fixed order too (warp
+// butterflies, then the four warps in order, then the tiles in order), so a
+// gradient is the same bits on every run.
 template <bool kTrain>
 __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, const float* __restrict__ T, int n,
-                                               Params p, Params g, float* Y_out, double* loss, int* err,
+                                               Params p, float* gpart, float* Y_out, double* lpart, int* err,
                                                WaitCfg wc) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
     __shared__ __align__(8) uint64_t mbar_storage;
     __shared__ uint32_t tmem_slot;
-    __shared__ float sgb[HID + HID + OUT];
+    constexpr int NB = HID + HID + OUT;  // bias gradients: b1, b2, b3
+    __shared__ float sgb[NB];
     __shared__ float sloss;
+    __shared__ float swarp[NT / 32][NB + 1];  // per warp: this tile's bias-gradient and loss sums
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&mbar_storage);
 
@@ -216,7 +246,8 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
     }
     if (kTrain) {
         for (int i = tid; i < 32768 / 16; i += NT) reinterpret_cast<uint4*>(sm + O_A3)[i] = make_uint4(0, 0, 0, 0);
-        for (int i = tid; i < HID + HID + OUT; i += NT) sgb[i] = 0.f;
+        for (int i = tid; i < NB; i += NT) sgb[i] = 0.f;
+        for (int i = tid; i < (NT / 32) * (NB + 1); i += NT) (&swarp[0][0])[i] = 0.f;
         if (tid == 0) sloss = 0.f;
     }
     if (tid == 0) {
@@ -300,17 +331,26 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
                 dy[o] = 2.f * e / (float)n;
                 lrow += e * e;
             }
-        atomicAdd(&sloss, lrow);
-        for (int o = 0; o < USED; ++o) atomicAdd(&sgb[2 * HID + o], dy[o]);
+        const int lane = tid & 31;
+        {
+            const float ls = warp_sum(lrow);
+            if (lane == 0) swarp[warp][NB] = ls;
+        }
+        for (int o = 0; o < USED; ++o) {
+            const float v = warp_sum(dy[o]);
+            if (lane == 0) swarp[warp][2 * HID + o] = v;
+        }
         st_row(sm + O_DY, tid, dy, OUT);
         for (int o = 0; o < USED; ++o) st_bf16(sm, O_A3 + kmaj(o, tid, TILE), dy[o]);
         ok = gemm(sbase, O_DY, O_W3T, OUT, HID, tmem + C_Z1, false, mbar, phase, wc, gi, inflight);  // dH2
         if (!ok) break;
         float d2[HID];
         for (int c = 0; c < HID; c += 16) tmem_ld16(tmem + lane_base + C_Z1 + c, d2 + c);
+#pragma unroll
         for (int j = 0; j < HID; ++j) {
             d2[j] = ((m2 >> j) & 1ull) ? d2[j] : 0.f;
-            atomicAdd(&sgb[HID + j], d2[j]);
+            const float v = warp_sum(d2[j]);
+            if (lane == 0) swarp[warp][HID + j] = v;
         }
         st_row(sm + O_DZ2, tid, d2, HID);
         for (int j = 0; j < HID; ++j) st_bf16(sm, O_AT + kmaj(j, tid, TILE), d2[j]);
@@ -318,10 +358,20 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
         if (!ok) break;
         float d1[HID];
         for (int c = 0; c < HID; c += 16) tmem_ld16(tmem + lane_base + C_Z2 + c, d1 + c);
+#pragma unroll
         for (int j = 0; j < HID; ++j) {
             d1[j] = ((m1 >> j) & 1ull) ? d1[j] : 0.f;
-            atomicAdd(&sgb[j], d1[j]);
+            const float v = warp_sum(d1[j]);
+            if (lane == 0) swarp[warp][j] = v;
             st_bf16(sm, O_AT + kmaj(HID + j, tid, TILE), d1[j]);
+        }
+        // this tile's sums, the warps added in order (the tile's other smem
+        // writes are fenced by the barrier inside the next GEMM)
+        __syncthreads();
+        for (int i = tid; i <= NB; i += NT) {
+            const float v = ((swarp[0][i] + swarp[1][i]) + swarp[2][i]) + swarp[3][i];
+            if (i < NB) sgb[i] += v;
+            else sloss += v;
         }
         // weight gradients, accumulated in tensor memory over this CTA's tiles
         ok = gemm(sbase, O_AT, O_BT, TILE, HID + IN, tmem + C_DW12, !first, mbar, phase, wc, gi, inflight);
@@ -334,37 +384,55 @@ __global__ void __launch_bounds__(NT, 1) k_mlp(const float* __restrict__ X, cons
     // MMAs still pending after a timed-out wait write tensor memory: wait for
     // them (bounded again) before that memory is freed below
     if (!ok && inflight) mbar_wait(mbar, phase, kPollLimit);
-    if (kTrain && ok && !first) {
-        // D12 rows 0..63: dW2 (cols 0..63); rows 64..127: dW1 (cols 64..79); D3 rows 0..15: dW3
+    if (kTrain) {
+        // this CTA's part: D12 rows 0..63: dW2 (cols 0..63); rows 64..127:
+        // dW1 (cols 64..79); D3 rows 0..15: dW3 (the rows of unused outputs
+        // zero); every entry written, zero when the CTA stopped early
+        Params g = carve(gpart + (size_t)blockIdx.x * kNParams);
+        const bool have = ok && !first;
         const int m = tid;
         float v[16];
         if (m < HID) {
             for (int c = 0; c < HID; c += 16) {
-                tmem_ld16(tmem + lane_base + C_DW12 + c, v);
-                for (int i = 0; i < 16; ++i) atomicAdd(&g.W2[m * HID + c + i], v[i]);
+                if (have) tmem_ld16(tmem + lane_base + C_DW12 + c, v);
+                for (int i = 0; i < 16; ++i) g.W2[m * HID + c + i] = have ? v[i] : 0.f;
             }
         } else {
-            tmem_ld16(tmem + lane_base + C_DW12 + HID, v);
-            for (int i = 0; i < IN; ++i) atomicAdd(&g.W1[(m - HID) * IN + i], v[i]);
+            if (have) tmem_ld16(tmem + lane_base + C_DW12 + HID, v);
+            for (int i = 0; i < IN; ++i) g.W1[(m - HID) * IN + i] = have ? v[i] : 0.f;
         }
         for (int c = 0; c < HID; c += 16) {
-            tmem_ld16(tmem + lane_base + C_DW3 + c, v);
-            if (m < USED)
-                for (int i = 0; i < 16; ++i) atomicAdd(&g.W3[m * HID + c + i], v[i]);
+            if (have) tmem_ld16(tmem + lane_base + C_DW3 + c, v);
+            if (m < OUT)
+                for (int i = 0; i < 16; ++i) g.W3[m * HID + c + i] = (have && m < USED) ? v[i] : 0.f;
         }
-    }
-    if (kTrain) {
         __syncthreads();
         for (int i = tid; i < HID; i += NT) {
-            atomicAdd(&g.b1[i], sgb[i]);
-            atomicAdd(&g.b2[i], sgb[HID + i]);
+            g.b1[i] = have ? sgb[i] : 0.f;
+            g.b2[i] = have ? sgb[HID + i] : 0.f;
         }
-        if (tid < OUT) atomicAdd(&g.b3[tid], sgb[2 * HID + tid]);
-        if (tid == 0) atomicAdd(loss, (double)sloss / (double)n);
+        if (tid < OUT) g.b3[tid] = have ? sgb[2 * HID + tid] : 0.f;
+        if (tid == 0) lpart[blockIdx.x] = have ? (double)sloss / (double)n : 0.0;
     }
     fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+// g[i] = the CTAs' parts of parameter i added in CTA order; *loss likewise
+__global__ void k_grad_sum(const float* __restrict__ part, int nparts, float* g, const double* __restrict__ lpart,
+                           double* loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kNParams) {
+        float acc = 0.f;
+        for (int b = 0; b < nparts; ++b) acc += part[(size_t)b * kNParams + i];
+        g[i] = acc;
+    }
+    if (i == 0) {
+        double l = 0.0;
+        for (int b = 0; b < nparts; ++b) l += lpart[b];
+        *loss = l;
+    }
 }
 
 __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
@@ -379,19 +447,6 @@ __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, floa
     p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-constexpr int kW1 = HID * IN, kB1 = HID, kW2 = HID * HID, kB2 = HID, kW3 = OUT * HID, kB3 = OUT;
-constexpr int kNParams = kW1 + kB1 + kW2 + kB2 + kW3 + kB3;
-
-Params carve(float* base) {
-    Params q;
-    q.W1 = base;
-    q.b1 = q.W1 + kW1;
-    q.W2 = q.b1 + kB1;
-    q.b2 = q.W2 + kW2;
-    q.W3 = q.b2 + kB2;
-    q.b3 = q.W3 + kW3;
-    return q;
-}
 
 }  // namespace mlp
 }  // namespace pgb
@@ -404,6 +459,8 @@ struct pg_mlp {
     float* m = nullptr;
     float* v = nullptr;
     double* loss = nullptr;
+    float* gpart = nullptr;    // per CTA of a gradient launch: its part of the gradient (kNParams)
+    double* lpart = nullptr;   // and of the loss
     int* err = nullptr;
     float* probe = nullptr;    // one tile of inputs and outputs for pg_mlp_wait_selftest
     int step = 0;
@@ -434,6 +491,8 @@ int pg_mlp_create(int32_t device, uint64_t seed, pg_mlp** out) {
     PG_CUDA(cudaMalloc((void**)&m->probe, TILE * (IN + 2) * sizeof(float)));
     PG_CUDA(fill_sync(m->probe, 0, TILE * (IN + 2) * sizeof(float)));
     cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, device);
+    PG_CUDA(cudaMalloc((void**)&m->gpart, (size_t)m->n_sms * kNParams * sizeof(float)));
+    PG_CUDA(cudaMalloc((void**)&m->lpart, (size_t)m->n_sms * sizeof(double)));
     PG_CUDA(cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
     PG_CUDA(cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
     // He initialisation (host, seeded), last layer scaled to start near zero output
@@ -455,6 +514,8 @@ void pg_mlp_destroy(pg_mlp* m) {
     cudaSetDevice(m->device);
     if (m->params) cudaFree(m->params);
     if (m->loss) cudaFree(m->loss);
+    if (m->gpart) cudaFree(m->gpart);
+    if (m->lpart) cudaFree(m->lpart);
     if (m->err) cudaFree(m->err);
     if (m->probe) cudaFree(m->probe);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -505,8 +566,9 @@ int pg_mlp_forward(pg_mlp* m, const float* X_dev, int32_t n, float* Y_dev, void*
     cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
     const int tiles = (n + TILE - 1) / TILE;
     const int grid = tiles < m->n_sms ? tiles : m->n_sms;
-    Params p = carve(m->params), g = carve(m->grads);
-    k_mlp<false><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, nullptr, n, p, g, Y_dev, m->loss, m->err, WaitCfg{kPollLimit, -1});
+    Params p = carve(m->params);
+    k_mlp<false><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, nullptr, n, p, nullptr, Y_dev, nullptr, m->err,
+                                              WaitCfg{kPollLimit, -1});
     PG_CUDA(cudaGetLastError());
     if (s == m->stream) return mlp_check_err(m);
     return PG_OK;
@@ -520,8 +582,8 @@ int pg_mlp_forward(pg_mlp* m, const float* X_dev, int32_t n, float* Y_dev, void*
 int pg_mlp_wait_selftest(pg_mlp* m, int32_t polls) {
     if (!m || polls < 1) { set_error("pg_mlp_wait_selftest: bad argument"); return PG_ERR_ARG; }
     cudaSetDevice(m->device);
-    Params p = carve(m->params), g = carve(m->grads);
-    k_mlp<false><<<1, NT, SMEM_ALLOC, m->stream>>>(m->probe, nullptr, TILE, p, g, m->probe + TILE * IN, m->loss, m->err,
+    Params p = carve(m->params);
+    k_mlp<false><<<1, NT, SMEM_ALLOC, m->stream>>>(m->probe, nullptr, TILE, p, nullptr, m->probe + TILE * IN, nullptr, m->err,
                                                    WaitCfg{polls, 0});
     PG_CUDA(cudaGetLastError());
     return mlp_check_err(m);
@@ -532,12 +594,13 @@ int pg_mlp_gradient(pg_mlp* m, const float* X_dev, const float* T_dev, int32_t n
     if (!m || !X_dev || !T_dev || n <= 0) { set_error("pg_mlp_gradient: bad argument"); return PG_ERR_ARG; }
     cudaSetDevice(m->device);
     cudaStream_t s = m->stream;
-    PG_CUDA(cudaMemsetAsync(m->grads, 0, kNParams * sizeof(float), s));
-    PG_CUDA(cudaMemsetAsync(m->loss, 0, sizeof(double), s));
     const int tiles = (n + TILE - 1) / TILE;
     const int grid = tiles < m->n_sms ? tiles : m->n_sms;
-    Params p = carve(m->params), g = carve(m->grads);
-    k_mlp<true><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, T_dev, n, p, g, nullptr, m->loss, m->err, WaitCfg{kPollLimit, -1});
+    Params p = carve(m->params);
+    k_mlp<true><<<grid, NT, SMEM_ALLOC, s>>>(X_dev, T_dev, n, p, m->gpart, nullptr, m->lpart, m->err,
+                                             WaitCfg{kPollLimit, -1});
+    PG_CUDA(cudaGetLastError());
+    k_grad_sum<<<(kNParams + 255) / 256, 256, 0, s>>>(m->gpart, grid, m->grads, m->lpart, m->loss);
     PG_CUDA(cudaGetLastError());
     int rc = mlp_check_err(m);
     if (rc) return rc;

@@ -1,6 +1,7 @@
 """The tcgen05 BF16 MLP kernels of the learned warm start against the CPU
 oracle (oracle/mlp_oracle.py): forward values, loss and every parameter
-gradient, and that Adam training on the GPU reduces the loss."""
+gradient, that a gradient is the same bits on every run, and that Adam
+training on the GPU reduces the loss."""
 import ctypes as C
 
 import numpy as np
@@ -91,6 +92,34 @@ def test_gradients_match_oracle(mlp, n):
         ref = go[k][:2]
         assert np.linalg.norm(gg[k][:2] - ref) <= 3e-2 * np.linalg.norm(ref) + 1e-7, k
         assert np.abs(gg[k][2:]).max() == 0.0
+
+
+def test_gradient_is_bit_reproducible(mlp):
+    """Each CTA's part of the gradient is summed in a fixed order and the
+    parts are added in CTA order: two gradients of the same rows agree bit
+    for bit, and so do two trainings from the same start."""
+    rng = np.random.default_rng(3)
+    n = 50000  # more tiles than CTAs: every CTA sums several tiles
+    X = torch.from_numpy(rng.standard_normal((n, 16)).astype(np.float32)).cuda()
+    T = torch.from_numpy(rng.standard_normal((n, 2)).astype(np.float32)).cuda()
+    out = []
+    for _ in range(2):
+        set_params(mlp, mo.init_params(4))
+        loss = C.c_double()
+        _lib.check(_lib.lib.pg_mlp_gradient(mlp, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), n,
+                                            C.byref(loss)))
+        g = np.zeros(_lib.lib.pg_mlp_param_count(), np.float32)
+        _lib.check(_lib.lib.pg_mlp_grads(mlp, g.ctypes.data_as(C.POINTER(C.c_float))))
+        hist = np.zeros(3)
+        _lib.check(_lib.lib.pg_mlp_train(mlp, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), n, 3, 4096,
+                                         C.c_float(1e-3), hist.ctypes.data_as(C.POINTER(C.c_double))))
+        w = np.zeros(_lib.lib.pg_mlp_param_count(), np.float32)
+        _lib.check(_lib.lib.pg_mlp_params(mlp, w.ctypes.data_as(C.POINTER(C.c_float)), 0))
+        out.append((loss.value, g, hist, w))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][3], out[1][3])
 
 
 def test_training_reduces_loss(mlp):

@@ -333,12 +333,40 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
     }
 
     // ---- node detection with the node-moving rule (Mesh.cpp:2838-2918) ----
+    // A node is tested against the inclusions in descending order, and only
+    // those whose bounding box holds it get past the first test.  So the
+    // inclusions are binned by bounding box on a uniform grid of cells about
+    // one diameter wide, and a node walks its cell's list (ascending, read
+    // backwards): the same inclusions in the same order as a scan over all.
     const int ninc = (int)spec.inclusions.size();
+    double dmax = 0.0;
+    for (const auto& inc : spec.inclusions) dmax = std::max(dmax, 2.0 * inc.r);
+    const double W = spec.x1 - spec.x0, H = spec.y1 - spec.y0;
+    const int nbx = dmax > 0.0 ? std::max(1, std::min(256, (int)(W / dmax))) : 1;
+    const int nby = dmax > 0.0 ? std::max(1, std::min(256, (int)(H / dmax))) : 1;
+    const double bsx = W / nbx, bsy = H / nby;
+    // floor((v - v0) / bs) clamped to the grid: monotonic in v, so a point
+    // inside a bounding box lands in one of the box's cells
+    auto bin_of = [](double v, double v0, double bs, int nb) {
+        const double f = std::floor((v - v0) / bs);
+        return f < 0.0 ? 0 : (f >= nb ? nb - 1 : (int)f);
+    };
+    std::vector<std::vector<int>> bins((size_t)nbx * nby);
+    for (int j = 0; j < ninc; ++j) {
+        const Inclusion& inc = spec.inclusions[j];
+        const int i0 = bin_of(inc.cx - inc.r, spec.x0, bsx, nbx), i1 = bin_of(inc.cx + inc.r, spec.x0, bsx, nbx);
+        const int j0 = bin_of(inc.cy - inc.r, spec.y0, bsy, nby), j1 = bin_of(inc.cy + inc.r, spec.y0, bsy, nby);
+        for (int bj = j0; bj <= j1; ++bj)
+            for (int bi = i0; bi <= i1; ++bi) bins[(size_t)bj * nbx + bi].push_back(j);
+    }
     m.node_detect.assign(m.n_reg, -1);
     for (int n = 0; n < m.n_reg; ++n) {
         int moved = 0;
         int result = -1;
-        for (int j = ninc - 1; j >= 0; --j) {
+        const std::vector<int>* list =
+            &bins[(size_t)bin_of(m.y[n], spec.y0, bsy, nby) * nbx + bin_of(m.x[n], spec.x0, bsx, nbx)];
+        for (int li = (int)list->size() - 1; li >= 0; --li) {
+            const int j = (*list)[li];
             const Inclusion& inc = spec.inclusions[j];
             const double px = m.x[n], py = m.y[n];
             if (!(inc.cx - inc.r <= px && inc.cy - inc.r <= py && px <= inc.cx + inc.r && py <= inc.cy + inc.r)) continue;
@@ -360,7 +388,9 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
             m.y[n] = py + dist * nyn;
             ++moved;
             ++m.n_moved;
-            j = ninc;  // restart the scan over the inclusions
+            // restart the scan over the inclusions, from the moved node's cell
+            list = &bins[(size_t)bin_of(m.y[n], spec.y0, bsy, nby) * nbx + bin_of(m.x[n], spec.x0, bsx, nbx)];
+            li = (int)list->size();
         }
         m.node_detect[n] = result;
     }
@@ -486,38 +516,58 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
     }
 
     // ---- 2x2-block sparsity over nodes ----
-    std::vector<std::vector<int>> adj(nn);
-    for (int e = 0; e < m.n_elem; ++e) {
-        if (m.elem_cut[e] >= 0) continue;
-        const int* c = &m.conn[3 * e];
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) adj[c[a]].push_back(c[b]);
-    }
+    // every element a node belongs to lists its nodes in the node's row (with
+    // repeats), plus the node itself; each row is then sorted and made
+    // unique in place, and the rows are packed into col
+    std::vector<int> cand_ptr(nn + 1, 0);
+    std::vector<int> cut_L((size_t)m.n_cut * kMaxElemNodes), cut_nl(m.n_cut);
     for (int c = 0; c < m.n_cut; ++c) {
         const int e = m.cut_elem[c];
         const CutTemplate& T = templates()[m.cut_tmpl[c]];
-        int L[kMaxElemNodes];
-        const int nl = 3 + T.n_enr;
+        int* L = &cut_L[(size_t)c * kMaxElemNodes];
+        cut_nl[c] = 3 + T.n_enr;
         for (int v = 0; v < 3; ++v) L[v] = m.conn[3 * e + v];
         for (int s = 0; s < T.n_enr; ++s) L[3 + s] = m.cut_enr[(size_t)c * kMaxEnr + s];
-        for (int a = 0; a < nl; ++a)
-            for (int b = 0; b < nl; ++b) adj[L[a]].push_back(L[b]);
+    }
+    for (int e = 0; e < m.n_elem; ++e)
+        if (m.elem_cut[e] < 0)
+            for (int a = 0; a < 3; ++a) cand_ptr[m.conn[3 * e + a] + 1] += 3;
+    for (int c = 0; c < m.n_cut; ++c)
+        for (int a = 0; a < cut_nl[c]; ++a) cand_ptr[cut_L[(size_t)c * kMaxElemNodes + a] + 1] += cut_nl[c];
+    for (int n = 0; n < nn; ++n) cand_ptr[n + 1] += cand_ptr[n] + 1;  // + the node itself
+    std::vector<int> cand(cand_ptr.back());
+    {
+        std::vector<int> fill(cand_ptr.begin(), cand_ptr.end() - 1);
+        for (int n = 0; n < nn; ++n) cand[fill[n]++] = n;
+        for (int e = 0; e < m.n_elem; ++e) {
+            if (m.elem_cut[e] >= 0) continue;
+            const int* cn = &m.conn[3 * e];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) cand[fill[cn[a]]++] = cn[b];
+        }
+        for (int c = 0; c < m.n_cut; ++c) {
+            const int* L = &cut_L[(size_t)c * kMaxElemNodes];
+            for (int a = 0; a < cut_nl[c]; ++a)
+                for (int b = 0; b < cut_nl[c]; ++b) cand[fill[L[a]]++] = L[b];
+        }
     }
     m.row_ptr.assign(nn + 1, 0);
+    std::vector<int> row_len(nn);
     for (int n = 0; n < nn; ++n) {
-        auto& v = adj[n];
-        v.push_back(n);
-        std::sort(v.begin(), v.end());
-        v.erase(std::unique(v.begin(), v.end()), v.end());
-        m.row_ptr[n + 1] = m.row_ptr[n] + (int)v.size();
+        int* b = cand.data() + cand_ptr[n];
+        int* e = cand.data() + cand_ptr[n + 1];
+        std::sort(b, e);
+        row_len[n] = (int)(std::unique(b, e) - b);
+        m.row_ptr[n + 1] = m.row_ptr[n] + row_len[n];
     }
     m.col.resize(m.row_ptr.back());
     m.diag_slot.resize(nn);
     for (int n = 0; n < nn; ++n) {
-        std::copy(adj[n].begin(), adj[n].end(), m.col.begin() + m.row_ptr[n]);
-        m.diag_slot[n] = (int)(std::lower_bound(adj[n].begin(), adj[n].end(), n) - adj[n].begin()) + m.row_ptr[n];
-        std::vector<int>().swap(adj[n]);
+        const int* b = cand.data() + cand_ptr[n];
+        std::copy(b, b + row_len[n], m.col.begin() + m.row_ptr[n]);
+        m.diag_slot[n] = (int)(std::lower_bound(b, b + row_len[n], n) - b) + m.row_ptr[n];
     }
+    std::vector<int>().swap(cand);
     auto slot_of = [&](int r, int c) -> int {
         const int* b = m.col.data() + m.row_ptr[r];
         const int* e = m.col.data() + m.row_ptr[r + 1];

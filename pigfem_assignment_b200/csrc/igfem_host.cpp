@@ -320,17 +320,23 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
     }
     m.elem_mat.assign(m.n_elem, spec.matrix_mat);
 
-    // node -> element lists in element order (Mesh::generate_node_elem, serial)
-    std::vector<int> nel_ptr(m.n_reg + 1, 0), nel;
-    for (int e = 0; e < m.n_elem; ++e)
-        for (int v = 0; v < 3; ++v) nel_ptr[m.conn[3 * e + v] + 1]++;
-    for (int n = 0; n < m.n_reg; ++n) nel_ptr[n + 1] += nel_ptr[n];
-    nel.resize(nel_ptr.back());
-    {
-        std::vector<int> fill(nel_ptr.begin(), nel_ptr.end() - 1);
-        for (int e = 0; e < m.n_elem; ++e)
-            for (int v = 0; v < 3; ++v) nel[fill[m.conn[3 * e + v]]++] = e;
-    }
+    // the first element (in element order) a node belongs to: the node-moving
+    // rule takes its edge length from it (Mesh::generate_node_elem lists a
+    // node's elements in element order).  A node's cells in increasing index
+    // order, each cell's two triangles in order.
+    auto first_elem = [&](int n) {
+        const int gi = n % (nx + 1), gj = n / (nx + 1);
+        const int cells[4][2] = {{gi - 1, gj - 1}, {gi, gj - 1}, {gi - 1, gj}, {gi, gj}};
+        for (const auto& cl : cells) {
+            if (cl[0] < 0 || cl[0] >= nx || cl[1] < 0 || cl[1] >= ny) continue;
+            for (int t = 0; t < 2; ++t) {
+                const int e = 2 * (cl[0] + cl[1] * nx) + t;
+                for (int v = 0; v < 3; ++v)
+                    if (m.conn[3 * (size_t)e + v] == n) return e;
+            }
+        }
+        return -1;
+    };
 
     // ---- node detection with the node-moving rule (Mesh.cpp:2838-2918) ----
     // A node is tested against the inclusions in descending order, and only
@@ -379,7 +385,7 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
             if (moved >= 5) { err << "unable to move node " << n << " off an inclusion surface"; return err.str(); }
             const double nrm = std::sqrt(dx * dx + dy * dy);
             const double nxn = dx / nrm, nyn = dy / nrm;
-            const int e0 = nel[nel_ptr[n]];
+            const int e0 = first_elem(n);
             int other = m.conn[3 * e0 + 0];
             if (other == n) other = m.conn[3 * e0 + 1];
             const double ox = m.x[other], oy = m.y[other];
@@ -423,9 +429,11 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
     }
 
     // ---- enrichment nodes (Mesh.cpp:3064-3202, 3600-3660) ----
-    // unique (edge, inclusion) pairs in std::set order
+    // unique (edge, inclusion) pairs in the reference's std::set order: the
+    // keys sorted lexicographically and made unique
+    using EdgeKey = std::pair<std::pair<int, int>, int>;
     std::vector<int> slot_inc(m.n_cut * 6, -1);
-    std::set<std::pair<std::pair<int, int>, int>> cut_edges;
+    std::vector<EdgeKey> cut_edges;
     for (int c = 0; c < m.n_cut; ++c) {
         const int e = m.cut_elem[c];
         const CutTemplate& T = templates()[m.cut_tmpl[c]];
@@ -436,12 +444,13 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
             slot_inc[c * 6 + s] = inc;
             int a = m.conn[3 * e + kEdgeNodes[T.cut_edge[s]][0]], b = m.conn[3 * e + kEdgeNodes[T.cut_edge[s]][1]];
             if (a > b) std::swap(a, b);
-            cut_edges.insert({{a, b}, inc});
+            cut_edges.push_back({{a, b}, inc});
         }
     }
+    std::sort(cut_edges.begin(), cut_edges.end());
+    cut_edges.erase(std::unique(cut_edges.begin(), cut_edges.end()), cut_edges.end());
     m.n_enr_initial = (int)cut_edges.size();
     m.n_enr = spec.cohesive ? 2 * m.n_enr_initial : m.n_enr_initial;
-    std::map<std::pair<std::pair<int, int>, int>, int> enr_index;
     m.x.resize(m.n_reg + m.n_enr);
     m.y.resize(m.n_reg + m.n_enr);
     m.enr_edge.resize(2 * m.n_enr);
@@ -474,7 +483,6 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
                 m.enr_edge[2 * idx + 1] = b;
                 m.enr_inc[idx] = inc;
             }
-            enr_index[ce] = k;
             ++k;
         }
     }
@@ -485,7 +493,8 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
         for (int s = 0; s < T.n_cut_edges; ++s) {
             int a = m.conn[3 * e + kEdgeNodes[T.cut_edge[s]][0]], b = m.conn[3 * e + kEdgeNodes[T.cut_edge[s]][1]];
             if (a > b) std::swap(a, b);
-            const int k = enr_index.at({{a, b}, slot_inc[c * 6 + s]});
+            const EdgeKey key{{a, b}, slot_inc[c * 6 + s]};
+            const int k = (int)(std::lower_bound(cut_edges.begin(), cut_edges.end(), key) - cut_edges.begin());
             m.cut_enr[(size_t)c * kMaxEnr + s] = m.n_reg + k;
             if (spec.cohesive) m.cut_enr[(size_t)c * kMaxEnr + s + T.n_cut_edges] = m.n_reg + k + m.n_enr_initial;
         }
@@ -516,10 +525,13 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
     }
 
     // ---- 2x2-block sparsity over nodes ----
-    // every element a node belongs to lists its nodes in the node's row (with
-    // repeats), plus the node itself; each row is then sorted and made
-    // unique in place, and the rows are packed into col
-    std::vector<int> cand_ptr(nn + 1, 0);
+    // The pattern is the union of every element's node pairs.  On the
+    // structured background grid a regular node's row holds its grid
+    // neighbours -- the four axis neighbours inside the grid, and the four
+    // diagonal ones for even nodes ((i + j) % 2 == 0), the only nodes a cell
+    // diagonal passes through -- in index order, then the enrichment nodes of
+    // the cut elements it belongs to; an enrichment node's row holds the
+    // local nodes of its cut elements.  Only those lists need sorting.
     std::vector<int> cut_L((size_t)m.n_cut * kMaxElemNodes), cut_nl(m.n_cut);
     for (int c = 0; c < m.n_cut; ++c) {
         const int e = m.cut_elem[c];
@@ -529,45 +541,57 @@ std::string build_mesh(const RveSpec& spec, HostMesh& m) {
         for (int v = 0; v < 3; ++v) L[v] = m.conn[3 * e + v];
         for (int s = 0; s < T.n_enr; ++s) L[3 + s] = m.cut_enr[(size_t)c * kMaxEnr + s];
     }
-    for (int e = 0; e < m.n_elem; ++e)
-        if (m.elem_cut[e] < 0)
-            for (int a = 0; a < 3; ++a) cand_ptr[m.conn[3 * e + a] + 1] += 3;
+    std::vector<int> xptr(nn + 1, 0);
     for (int c = 0; c < m.n_cut; ++c)
-        for (int a = 0; a < cut_nl[c]; ++a) cand_ptr[cut_L[(size_t)c * kMaxElemNodes + a] + 1] += cut_nl[c];
-    for (int n = 0; n < nn; ++n) cand_ptr[n + 1] += cand_ptr[n] + 1;  // + the node itself
-    std::vector<int> cand(cand_ptr.back());
-    {
-        std::vector<int> fill(cand_ptr.begin(), cand_ptr.end() - 1);
-        for (int n = 0; n < nn; ++n) cand[fill[n]++] = n;
-        for (int e = 0; e < m.n_elem; ++e) {
-            if (m.elem_cut[e] >= 0) continue;
-            const int* cn = &m.conn[3 * e];
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) cand[fill[cn[a]]++] = cn[b];
+        for (int a = 0; a < cut_nl[c]; ++a) {
+            const int na = cut_L[(size_t)c * kMaxElemNodes + a];
+            xptr[na + 1] += na < m.n_reg ? cut_nl[c] - 3 : cut_nl[c];
         }
+    for (int n = 0; n < nn; ++n) xptr[n + 1] += xptr[n];
+    std::vector<int> xcol(xptr.back());
+    {
+        std::vector<int> fill(xptr.begin(), xptr.end() - 1);
         for (int c = 0; c < m.n_cut; ++c) {
             const int* L = &cut_L[(size_t)c * kMaxElemNodes];
             for (int a = 0; a < cut_nl[c]; ++a)
-                for (int b = 0; b < cut_nl[c]; ++b) cand[fill[L[a]]++] = L[b];
+                for (int b = L[a] < m.n_reg ? 3 : 0; b < cut_nl[c]; ++b) xcol[fill[L[a]]++] = L[b];
         }
     }
-    m.row_ptr.assign(nn + 1, 0);
-    std::vector<int> row_len(nn);
+    std::vector<int> xlen(nn, 0);
     for (int n = 0; n < nn; ++n) {
-        int* b = cand.data() + cand_ptr[n];
-        int* e = cand.data() + cand_ptr[n + 1];
+        int* b = xcol.data() + xptr[n];
+        int* e = xcol.data() + xptr[n + 1];
+        if (b == e) continue;
         std::sort(b, e);
-        row_len[n] = (int)(std::unique(b, e) - b);
-        m.row_ptr[n + 1] = m.row_ptr[n] + row_len[n];
+        xlen[n] = (int)(std::unique(b, e) - b);
+    }
+    // grid neighbours of node (gi, gj) as bits d = 3 (dy + 1) + (dx + 1)
+    auto nbr_mask = [nx, ny](int gi, int gj) {
+        const bool even = ((gi + gj) & 1) == 0;
+        const bool w = gi > 0, ea = gi < nx, so = gj > 0, no = gj < ny;
+        return (so && even && w ? 1u : 0u) | (so ? 2u : 0u) | (so && even && ea ? 4u : 0u) | (w ? 8u : 0u) | 16u |
+               (ea ? 32u : 0u) | (no && even && w ? 64u : 0u) | (no ? 128u : 0u) | (no && even && ea ? 256u : 0u);
+    };
+    m.row_ptr.assign(nn + 1, 0);
+    for (int n = 0; n < nn; ++n) {
+        const int reg = n < m.n_reg ? __builtin_popcount(nbr_mask(n % (nx + 1), n / (nx + 1))) : 0;
+        m.row_ptr[n + 1] = m.row_ptr[n] + reg + xlen[n];
     }
     m.col.resize(m.row_ptr.back());
     m.diag_slot.resize(nn);
     for (int n = 0; n < nn; ++n) {
-        const int* b = cand.data() + cand_ptr[n];
-        std::copy(b, b + row_len[n], m.col.begin() + m.row_ptr[n]);
-        m.diag_slot[n] = (int)(std::lower_bound(b, b + row_len[n], n) - b) + m.row_ptr[n];
+        int q = m.row_ptr[n];
+        if (n < m.n_reg) {
+            const int gi = n % (nx + 1), gj = n / (nx + 1);
+            const unsigned mask = nbr_mask(gi, gj);
+            for (int d = 0; d < 9; ++d)
+                if (mask & (1u << d)) m.col[q++] = (gi + d % 3 - 1) + (gj + d / 3 - 1) * (nx + 1);
+        }
+        std::copy(xcol.data() + xptr[n], xcol.data() + xptr[n] + xlen[n], m.col.begin() + q);
+        const int* b = m.col.data() + m.row_ptr[n];
+        const int* e = m.col.data() + m.row_ptr[n + 1];
+        m.diag_slot[n] = (int)(std::lower_bound(b, e, n) - m.col.data());
     }
-    std::vector<int>().swap(cand);
     auto slot_of = [&](int r, int c) -> int {
         const int* b = m.col.data() + m.row_ptr[r];
         const int* e = m.col.data() + m.row_ptr[r + 1];

@@ -103,3 +103,37 @@ def test_mesh_errors_are_status_codes():
         pb.Mesh(RVE(nx=0, ny=4))
     with pytest.raises(PgError):
         pb.Mesh(RVE(nx=4, ny=4, inclusions=[(0.5, 0.5, -1.0, 1)]))
+
+
+@pytest.mark.parametrize("case", ["bonded", "cohesive", "many"])
+def test_block_pattern_is_the_union_of_element_node_pairs(case):
+    """The host builder writes a regular node's row from its grid neighbours
+    and the cut elements' node lists; the pattern must be exactly the sorted
+    union of every element's node pairs (uncut triangles: their 3 nodes; cut
+    elements: their parents and enrichment nodes)."""
+    from pigfem_assignment_b200.rve import RVE
+    if case == "bonded":
+        rve = RVE(nx=24, ny=20, inclusions=[(0.5, 0.5, 0.25, 1), (0.1, 0.1, 0.05, 1)], strain=0.01)
+    elif case == "cohesive":
+        rve = RVE(nx=32, ny=32, inclusions=[(0.3, 0.5, 0.2, 1), (0.72, 0.5, 0.2, 1)], cohesive=True, coh_law=1,
+                  coh_params=(30.0, 0.01, 1.0e6, 1.0, 200.0), strain=0.01)
+    else:
+        circ = rsa_circles(7, 30, 0.03, 0.08, 0.01)
+        rve = RVE(nx=64, ny=64, inclusions=[(x, y, r, 1) for x, y, r in circ], strain=0.01)
+    m = pb.Mesh(rve)
+    e = m.export()
+    nn = m.info["n_nodes"]
+    rows = [set([n]) for n in range(nn)]
+    for t, el in enumerate(e["conn"]):
+        if e["elem_cut"][t] >= 0:
+            continue
+        for a in el:
+            rows[a].update(int(b) for b in el)
+    for c in range(len(e["cut_elem"])):
+        nodes = [int(v) for v in e["conn"][e["cut_elem"][c]]] + [int(v) for v in e["cut_enr"][c] if v >= 0]
+        for a in nodes:
+            rows[a].update(nodes)
+    row_ptr, col = e["row_ptr"], e["col"]
+    assert row_ptr[-1] == sum(len(r) for r in rows)
+    for n in range(nn):
+        assert list(col[row_ptr[n]:row_ptr[n + 1]]) == sorted(rows[n]), n

@@ -752,6 +752,13 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
     dev = f"cuda:{local}"
     t_asm = max_over_ranks(statistics.median(times), device=dev)
     tot_elem = sum_over_ranks(n_elem, device=dev)
+    # algorithmic bytes of the batch pass, as for the single RVE: every K block, the uncut
+    # elements' and the nodes' inputs, the cut elements' point records
+    n_blocks = sum(m.info["n_blocks"] for m in meshes)
+    n_nodes_b = sum(m.info["n_nodes"] for m in meshes)
+    n_cut_b = sum(m.info["n_cut_elements"] for m in meshes)
+    tot_bytes = sum_over_ranks(32 * n_blocks + 13 * (n_elem - n_cut_b) + 16 * n_nodes_b + 64 * n_cut_b, device=dev)
+    peak, peak_kind = measured_peak_hbm()
     out = {"rves": int(sum_over_ranks(n_rve, device=dev)), "elements": int(tot_elem),
            "dof": int(sum_over_ranks(n_dof, device=dev)), "ranks": world,
            "host_setup_s": max_over_ranks(setup_s, device=dev),
@@ -763,7 +770,10 @@ def batched_rves(local: int, n_rve: int, steps: int, warmup: int, rank: int = 0,
                                                               "ctx_cut_tables", "ctx_fold_order_gpu", "multigrid"),
                                                              [round(v, 4) for v in phases]))},
            "assembly_ms": t_asm,
-           "elements_per_s": tot_elem / (t_asm / 1e3)}
+           "elements_per_s": tot_elem / (t_asm / 1e3),
+           "roofline": {"bound": "hbm", "pass_bytes": tot_bytes, "achieved": tot_bytes / (t_asm / 1e3) / 1e9,
+                        "peak": peak, "unit": "GB/s", "frac": tot_bytes / (t_asm / 1e3) / 1e9 / peak,
+                        "peak_kind": peak_kind}}
     for name, prec in (("solve_fp64_mg", _lib.PG_PRECISION_FP64), ("solve_mixed_mg", _lib.PG_PRECISION_MIXED)):
         cfg = _lib.SolverCfg()
         _lib.lib.pg_solver_cfg_default(C.byref(cfg))
